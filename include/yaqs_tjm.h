@@ -1,0 +1,194 @@
+/*
+ * yaqs_tjm.h — C-ABI of the B200 tensor-jump-method (TJM) trajectory engine.
+ *
+ * This is the drop-in boundary for the analog TJM path of Yaqs.jl
+ * (MaxFroehlich1410/yaqs-julia).  A Julia caller passes its own arrays
+ * (Array{ComplexF64,3} MPS tensors, Array{ComplexF64,4} MPO tensors) by
+ * pointer: ComplexF64 is interleaved (re, im) double pairs and Julia arrays
+ * are column-major, so no repacking is needed on the host.  All sites are
+ * 0-based here (Julia's are 1-based; the shim subtracts one).
+ *
+ * Every entry point returns a status code (YAQS_OK == 0).  On failure
+ * yaqs_last_error(ctx) returns a message; the caller turns it into error().
+ * The library copies inputs to the device and never keeps host pointers
+ * after a call returns.  Distinct contexts may be used from distinct host
+ * threads; one context must not be used by two threads at once.
+ */
+#ifndef YAQS_TJM_H
+#define YAQS_TJM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (errors of Simulator.jl:136,139, MPS.jl:357-360) ---- */
+enum {
+  YAQS_OK = 0,
+  YAQS_E_ARG = 1,         /* malformed descriptor, size or pointer             */
+  YAQS_E_OOM = 2,         /* device memory admission failed                     */
+  YAQS_E_NONFINITE = 3,   /* NaN/Inf met where the reference raises an error    */
+  YAQS_E_NOCONV = 4,      /* an iterative solver hit its iteration limit        */
+  YAQS_E_TIMEOUT = 5,     /* a bounded device wait gave up                      */
+  YAQS_E_CUDA = 6,        /* CUDA runtime error                                 */
+  YAQS_E_RNG = 7,         /* injected uniform stream exhausted                  */
+  YAQS_E_UNSUPPORTED = 8  /* valid for the reference, not served by this engine */
+};
+
+typedef struct yaqs_ctx yaqs_ctx;
+
+/*
+ * Matrix product state (MPS.jl:33-43).  chi has L+1 entries, chi[0] ==
+ * chi[L] == 1.  tensors[i] holds chi[i]*2*chi[i+1] complex values laid out
+ * column-major as (left, phys, right) — the Julia layout (MPS.jl:22).
+ * Physical dimension is 2 (qubits).
+ */
+typedef struct {
+  int32_t L;
+  const int32_t* chi;
+  const double* const* tensors;
+} yaqs_mps_desc;
+
+/*
+ * Matrix product operator (MPO.jl:32-41).  w has L+1 entries, w[0] ==
+ * w[L] == 1.  tensors[i] is (w[i], 2, 2, w[i+1]) column-major complex,
+ * index order (left, phys_out, phys_in, right) (MPO.jl:19-24).  The
+ * operator must be Hermitian: the engine runs Lanczos, which is what the
+ * reference's :auto Krylov mode selects for a Hermitian H_eff
+ * (Algorithms.jl:120-176).
+ */
+typedef struct {
+  int32_t L;
+  const int32_t* w;
+  const double* const* tensors;
+} yaqs_mpo_desc;
+
+/*
+ * One LocalNoiseProcess (Noise.jl:15-20): a 1-site process or a 2-site
+ * process on adjacent sites (site[1] == site[0] + 1).  matrix is the jump
+ * operator (2x2 or 4x4, column-major, interleaved complex; the 4x4 basis
+ * index is p1 + 2*p2, first site fastest, Dissipation.jl:105).  The two
+ * classification flags are computed by the caller exactly as the reference
+ * does, because the reference uses two different rules:
+ *   pauli_name — Dissipation.is_pauli: name in the Pauli/crosstalk list
+ *                (Dissipation.jl:14-21) → dissipation is a scalar decay;
+ *   pauli_proc — StochasticProcess.is_pauli(op) for 1-site processes
+ *                (StochasticProcess.jl:336-341) and is_pauli_proc(proc) for
+ *                2-site ones (:343-357) → jump weight uses the local norm.
+ */
+typedef struct {
+  int32_t nsites;
+  int32_t site[2];
+  double strength;
+  double matrix[32];
+  int32_t pauli_name;
+  int32_t pauli_proc;
+} yaqs_noise_proc;
+
+/* NoiseModel (Noise.jl:35-37).  present == 0 means `nothing`. */
+typedef struct {
+  int32_t present;
+  int32_t n;
+  const yaqs_noise_proc* procs;
+} yaqs_noise_desc;
+
+/*
+ * Observable (SimulationConfigs.jl:23-56).  LOCAL1: 2x2 operator on
+ * site[0] (MPS.jl:608-624).  LOCAL2: 4x4 operator on site[0], site[0]+1
+ * (MPS.jl:626-651).  ENTROPY: von Neumann entropy -sum s^2 ln s^2 of the
+ * Schmidt values across the bond between site[0] and site[0]+1 (an
+ * addition; the reference has no entropy observable).
+ */
+enum { YAQS_OBS_LOCAL1 = 1, YAQS_OBS_LOCAL2 = 2, YAQS_OBS_ENTROPY = 3 };
+typedef struct {
+  int32_t kind;
+  int32_t site[2];
+  double matrix[32];
+} yaqs_obs_desc;
+
+/*
+ * Uniform draws of stochastic_process! (StochasticProcess.jl:221-244).
+ * PHILOX:   Philox-4x32-10 keyed by seed, one stream per trajectory (the
+ *           stream id is cfg->traj_offset + trajectory index), one draw per
+ *           counter value, 53-bit doubles in [0,1).
+ * INJECTED: trajectory t consumes uniforms[t*stride + k] for k = 0,1,2,...
+ *           in the reference's order (u1 per stochastic step, u2 only when a
+ *           jump happens).  Running out returns YAQS_E_RNG.
+ */
+enum { YAQS_RNG_PHILOX = 0, YAQS_RNG_INJECTED = 1 };
+typedef struct {
+  int32_t mode;
+  uint64_t seed;
+  const double* uniforms;
+  int64_t stride;
+} yaqs_rng_desc;
+
+enum { YAQS_PREC_FP64 = 0, YAQS_PREC_MIXED = 1 };
+
+/*
+ * TimeEvolutionConfig (SimulationConfigs.jl:68-92).  n_times is
+ * length(0:dt:T).  krylov_dim / krylov_tol are the reference's krylovdim=25
+ * and tol=1e-10 (Algorithms.jl:185).  krylov_exit_tol > 0 lets a Lanczos
+ * solve stop before krylov_dim once the a-priori bound
+ * prod_i(beta_i*|dt|)/k! falls below it (relative to |v|); 0 runs every
+ * solve to krylov_dim or breakdown, like the reference.
+ */
+typedef struct {
+  double dt;
+  int32_t n_times;
+  int32_t num_traj;
+  int32_t max_bond_dim;
+  double truncation_threshold;
+  int32_t order;
+  int32_t sample_timesteps;
+  int32_t krylov_dim;
+  double krylov_tol;
+  double krylov_exit_tol;
+  int32_t precision;
+  int32_t traj_offset;
+} yaqs_tev_config;
+
+/* Counters of one run (summed over trajectories). */
+typedef struct {
+  int64_t matvecs;         /* effective-Hamiltonian products               */
+  int64_t krylov_solves;   /* expm_krylov calls                            */
+  int64_t svds;            /* two-site splits                              */
+  int64_t jumps;           /* applied quantum jumps                        */
+  int64_t nonfinite_fixes; /* NaN/Inf replaced before an SVD (Algorithms.jl:414-417) */
+  double flops;            /* algorithmic flops of the H_eff products       */
+  double device_ms;        /* device time of the run (CUDA events)          */
+} yaqs_run_stats;
+
+/* ---- context ---- */
+int yaqs_ctx_create(int32_t device, yaqs_ctx** out);
+int yaqs_ctx_destroy(yaqs_ctx* ctx);
+const char* yaqs_last_error(const yaqs_ctx* ctx);
+const char* yaqs_version(void);
+
+/*
+ * Analog TJM run: replaces the trajectory loop of Simulator._run_analog
+ * (Simulator.jl:22-69) with every trajectory of the run advancing together
+ * on one GPU; each trajectory follows analog_tjm_2 (AnalogTJM.jl:104-137)
+ * when cfg->order == 2, else analog_tjm_1 (AnalogTJM.jl:144-176).
+ * psi0 is normalised first, as Simulator.run does (Simulator.jl:128).
+ * Outputs (any may be NULL):
+ *   traj_out   [num_traj][n_obs][n_out]  real(expect) per trajectory
+ *   mean_out   [n_obs][n_out]            mean over trajectories
+ *              (aggregate_trajectories!, SimulationConfigs.jl:168-181)
+ *   maxchi_out [num_traj][n_out]         max bond dimension at each sample
+ * with n_out = n_times if sample_timesteps else 1.  The caller applies the
+ * reference's num_traj = 1 rule for noiseless runs (Simulator.jl:27-29).
+ */
+int yaqs_analog_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0,
+                    const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                    const yaqs_obs_desc* obs, int32_t n_obs,
+                    const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                    double* traj_out, double* mean_out, int32_t* maxchi_out,
+                    yaqs_run_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YAQS_TJM_H */

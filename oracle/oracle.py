@@ -1,0 +1,142 @@
+"""ctypes front of the C++ FP64 oracle (oracle/tjm_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py as the checker.  It takes the same C-ABI
+descriptors as the product library (include/yaqs_tjm.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from yaqs_julia_b200 import _abi as A
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle_tjm.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++ only)."""
+    if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(
+            os.path.join(_HERE, "tjm_oracle.cpp")):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        P = C.POINTER
+        L.orc_analog_run.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.NoiseDesc), P(A.ObsDesc), C.c_int32,
+                                     P(A.TevConfig), P(A.RngDesc), C.c_int32, C.c_int32, C.c_int32,
+                                     A.DPTR, P(C.c_int32), P(A.RunStats)]
+        L.orc_tdvp_evolve.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.ObsDesc), C.c_int32, P(A.TevConfig),
+                                      C.c_int32, A.DPTR]
+        L.orc_svd.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR, A.DPTR]
+        L.orc_qr.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR]
+        L.orc_truncation_rank.argtypes = [C.c_int32, A.DPTR, C.c_double, C.c_int32, C.c_int32]
+        L.orc_truncation_rank.restype = C.c_int32
+        L.orc_expm_site.argtypes = [C.c_int32] * 5 + [A.DPTR] * 4 + [C.c_double, C.c_int32, C.c_double,
+                                                                    C.c_double, A.DPTR, P(C.c_int32)]
+        L.orc_project_site.argtypes = [C.c_int32] * 5 + [A.DPTR] * 5
+        L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
+        L.orc_philox_uniform.restype = C.c_double
+        L.orc_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(st):
+    if st != A.YAQS_OK:
+        raise RuntimeError(f"oracle: {A.STATUS_NAMES.get(st, st)}: {lib().orc_last_error().decode()}")
+
+
+def analog_run(desc, t_begin=0, t_end=None, nthreads=None):
+    """Run trajectories [t_begin, t_end) of a packed problem (api.Descriptors).
+    Returns (traj [num_traj, n_obs, n_out], maxchi [num_traj, n_out], stats)."""
+    L = lib()
+    nt = desc.num_traj
+    t_end = nt if t_end is None else t_end
+    traj = np.zeros((nt, max(desc.n_obs, 1), desc.n_out))
+    chi = np.zeros((nt, desc.n_out), dtype=np.int32)
+    st = A.RunStats()
+    nth = nthreads or os.cpu_count() or 1
+    _check(L.orc_analog_run(C.byref(desc.mps), C.byref(desc.mpo), C.byref(desc.noise), desc.obs, desc.n_obs,
+                            C.byref(desc.cfg), C.byref(desc.rng), t_begin, t_end, nth, A.dptr(traj),
+                            chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st)))
+    return traj[:, :desc.n_obs, :], chi, st.as_dict()
+
+
+def tdvp_evolve(desc, n_steps):
+    out = np.zeros((n_steps + 1, max(desc.n_obs, 1)))
+    _check(lib().orc_tdvp_evolve(C.byref(desc.mps), C.byref(desc.mpo), desc.obs, desc.n_obs, C.byref(desc.cfg),
+                                 n_steps, A.dptr(out)))
+    return out[:, :desc.n_obs]
+
+
+def svd(M):
+    M = np.asfortranarray(M, dtype=np.complex128)
+    m, n = M.shape
+    k = min(m, n)
+    U = np.zeros((m, k), dtype=np.complex128, order="F")
+    Vt = np.zeros((k, n), dtype=np.complex128, order="F")
+    S = np.zeros(k)
+    _check(lib().orc_svd(m, n, A.dptr(M.reshape(-1, order="F").view(np.float64)),
+                         A.dptr(U.reshape(-1, order="F").view(np.float64)), A.dptr(S),
+                         A.dptr(Vt.reshape(-1, order="F").view(np.float64))))
+    return U, S, Vt
+
+
+def qr(M):
+    M = np.asfortranarray(M, dtype=np.complex128)
+    m, n = M.shape
+    k = min(m, n)
+    Q = np.zeros((m, k), dtype=np.complex128, order="F")
+    R = np.zeros((k, n), dtype=np.complex128, order="F")
+    _check(lib().orc_qr(m, n, A.dptr(M.reshape(-1, order="F").view(np.float64)),
+                        A.dptr(Q.reshape(-1, order="F").view(np.float64)),
+                        A.dptr(R.reshape(-1, order="F").view(np.float64))))
+    return Q, R
+
+
+def truncation_rank(S, thr, max_bond, rule):
+    S = np.ascontiguousarray(S, dtype=np.float64)
+    return lib().orc_truncation_rank(S.size, A.dptr(S), thr, max_bond, rule)
+
+
+def _fbuf(a):
+    return np.asfortranarray(a, dtype=np.complex128).reshape(-1, order="F").view(np.float64)
+
+
+def project_site(Lenv, Renv, W, x):
+    chil, wl, _ = Lenv.shape
+    chir, wr, _ = Renv.shape
+    D = W.shape[1]
+    out = np.zeros((chil, D, chir), dtype=np.complex128, order="F")
+    bl, br, bw, bx = _fbuf(Lenv), _fbuf(Renv), _fbuf(W), _fbuf(x)
+    _check(lib().orc_project_site(chil, D, chir, wl, wr, A.dptr(bl), A.dptr(br), A.dptr(bw), A.dptr(bx),
+                                  A.dptr(out.reshape(-1, order="F").view(np.float64))))
+    return out
+
+
+def expm_site(Lenv, Renv, W, x, dt, kdim=25, tol=1e-10, exit_tol=0.0):
+    chil, wl, _ = Lenv.shape
+    chir, wr, _ = Renv.shape
+    D = W.shape[1]
+    out = np.zeros((chil, D, chir), dtype=np.complex128, order="F")
+    mv = C.c_int32(0)
+    bl, br, bw, bx = _fbuf(Lenv), _fbuf(Renv), _fbuf(W), _fbuf(x)
+    _check(lib().orc_expm_site(chil, D, chir, wl, wr, A.dptr(bl), A.dptr(br), A.dptr(bw), A.dptr(bx), dt, kdim,
+                               tol, exit_tol, A.dptr(out.reshape(-1, order="F").view(np.float64)), C.byref(mv)))
+    return out, mv.value
+
+
+def philox_uniform(seed, stream, draw):
+    return lib().orc_philox_uniform(seed, stream, draw)

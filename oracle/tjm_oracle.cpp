@@ -1,0 +1,1492 @@
+// tjm_oracle.cpp — TEST INFRASTRUCTURE ONLY.
+//
+// CPU FP64 restatement of the analog tensor-jump-method path of Yaqs.jl
+// (MaxFroehlich1410/yaqs-julia).  It is the checker for the CUDA engine and
+// the timed CPU baseline; nothing in the product links or calls it.  Only
+// tests/, __graft_entry__.smoke() and bench.py's CPU legs load it.
+//
+// Each routine names the reference file:line it restates.  Three pieces of
+// arithmetic live in third-party Julia packages that are not in the
+// reference tree and are restated from their published methods:
+//   * KrylovKit 0.10.2 `exponentiate` (Algorithms.jl:185): Lanczos with
+//     full (classical Gram-Schmidt, two pass) re-orthogonalisation, then the
+//     exact exponential of the small tridiagonal matrix through its
+//     eigendecomposition (Hochbruck-Lubich Krylov exponential).
+//   * LAPACK QR/LQ (Decompositions.jl:18-73, MPS.jl:182-311): Householder
+//     reflections in the zlarfg convention (real R diagonal, beta =
+//     -sign(Re alpha)*|x|).
+//   * LAPACK SVD (Algorithms.jl:420): one-sided (Hestenes) Jacobi.
+// QR and SVD factors are unique only up to phases and, for zero singular
+// values, up to the choice of null vectors.  The restatement fixes that
+// choice deterministically (see null_tol below) so the CUDA engine can
+// reproduce it bit-for-bit up to rounding.
+//
+// Layouts follow the reference (column-major): MPS tensor (l, p, r)
+// (MPS.jl:22), MPO tensor (wl, p_out, p_in, wr) (MPO.jl:19-24), environment
+// (bra, mpo, ket) (Algorithms.jl:191-211).  Sites are 0-based.
+
+#include "../include/yaqs_tjm.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using cd = std::complex<double>;
+using std::vector;
+
+// Relative thresholds that make null directions deterministic.
+constexpr double kQrNullTol = 1e-14;    // trailing column treated as exactly zero
+constexpr double kSvdNullTol = 1e-14;   // singular value treated as exactly zero
+constexpr int kJacobiMaxSweeps = 60;
+
+inline double nrm2(const cd* x, long n) {
+  double s = 0;
+  for (long i = 0; i < n; ++i) s += std::norm(x[i]);
+  return std::sqrt(s);
+}
+
+// ---------------------------------------------------------------------------
+// Tensors
+// ---------------------------------------------------------------------------
+struct Ten {  // MPS-like rank-3 tensor (l, d, r), column-major
+  int l = 1, d = 2, r = 1;
+  vector<cd> v;
+  Ten() {}
+  Ten(int l_, int d_, int r_) : l(l_), d(d_), r(r_), v((size_t)l_ * d_ * r_) {}
+  cd& at(int a, int p, int b) { return v[a + (size_t)l * (p + (size_t)d * b)]; }
+  cd at(int a, int p, int b) const { return v[a + (size_t)l * (p + (size_t)d * b)]; }
+};
+
+struct Wt {  // MPO tensor (wl, d, d, wr)
+  int wl = 1, d = 2, wr = 1;
+  vector<cd> v;
+  Wt() {}
+  Wt(int wl_, int d_, int wr_) : wl(wl_), d(d_), wr(wr_), v((size_t)wl_ * d_ * d_ * wr_) {}
+  cd at(int m, int po, int pi, int mr) const {
+    return v[m + (size_t)wl * (po + (size_t)d * (pi + (size_t)d * mr))];
+  }
+  cd& at(int m, int po, int pi, int mr) {
+    return v[m + (size_t)wl * (po + (size_t)d * (pi + (size_t)d * mr))];
+  }
+};
+
+struct Env {  // (bra, w, ket)
+  int b = 1, w = 1, k = 1;
+  vector<cd> v;
+  Env() {}
+  Env(int b_, int w_, int k_) : b(b_), w(w_), k(k_), v((size_t)b_ * w_ * k_) {}
+  cd at(int x, int m, int y) const { return v[x + (size_t)b * (m + (size_t)w * y)]; }
+  cd& at(int x, int m, int y) { return v[x + (size_t)b * (m + (size_t)w * y)]; }
+};
+
+struct State {
+  int L = 0;
+  vector<Ten> t;
+  int oc = 0;  // orth_center (0-based)
+};
+
+// C(m x n) = A(m x k) * B(k x n), column-major with leading dims = rows.
+void matmul(int m, int n, int k, const cd* A, const cd* B, cd* C) {
+  for (long i = 0; i < (long)m * n; ++i) C[i] = 0;
+  for (int j = 0; j < n; ++j)
+    for (int p = 0; p < k; ++p) {
+      cd b = B[p + (size_t)k * j];
+      if (b == cd(0)) continue;
+      const cd* a = A + (size_t)m * p;
+      cd* c = C + (size_t)m * j;
+      for (int i = 0; i < m; ++i) c[i] += a[i] * b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Householder QR / LQ (restates LAPACK geqrf/orgqr as used by
+// Decompositions.jl:18-73 and MPS.jl:182-311).
+// ---------------------------------------------------------------------------
+// Thin QR of M (m x n): Q (m x kq), R (kq x n), kq = min(m, n).
+void house_qr(int m, int n, const cd* M, vector<cd>& Q, vector<cd>& R) {
+  const int kq = std::min(m, n);
+  vector<cd> A(M, M + (size_t)m * n);
+  vector<cd> tau(kq, 0.0);
+  const double fro = nrm2(M, (long)m * n);
+  const double null_abs = kQrNullTol * fro;
+  for (int j = 0; j < kq; ++j) {
+    cd* col = &A[(size_t)m * j];
+    cd alpha = col[j];
+    double xn2 = 0;
+    for (int i = j + 1; i < m; ++i) xn2 += std::norm(col[i]);
+    double full = std::sqrt(std::norm(alpha) + xn2);
+    if (full <= null_abs || (xn2 == 0.0 && alpha.imag() == 0.0)) {
+      tau[j] = 0.0;
+      for (int i = j + 1; i < m; ++i) col[i] = 0.0;
+      continue;
+    }
+    double beta = (alpha.real() >= 0.0) ? -full : full;
+    tau[j] = (cd(beta) - alpha) / beta;
+    cd scale = 1.0 / (alpha - beta);
+    for (int i = j + 1; i < m; ++i) col[i] *= scale;
+    col[j] = beta;
+    cd ct = std::conj(tau[j]);
+    for (int c = j + 1; c < n; ++c) {
+      cd* x = &A[(size_t)m * c];
+      cd s = x[j];
+      for (int i = j + 1; i < m; ++i) s += std::conj(col[i]) * x[i];
+      s *= ct;
+      x[j] -= s;
+      for (int i = j + 1; i < m; ++i) x[i] -= s * col[i];
+    }
+  }
+  R.assign((size_t)kq * n, 0.0);
+  for (int c = 0; c < n; ++c)
+    for (int i = 0; i <= std::min(c, kq - 1); ++i) R[i + (size_t)kq * c] = A[i + (size_t)m * c];
+  Q.assign((size_t)m * kq, 0.0);
+  for (int c = 0; c < kq; ++c) Q[c + (size_t)m * c] = 1.0;
+  for (int j = kq - 1; j >= 0; --j) {
+    if (tau[j] == cd(0)) continue;
+    const cd* v = &A[(size_t)m * j];
+    for (int c = j; c < kq; ++c) {
+      cd* q = &Q[(size_t)m * c];
+      cd s = q[j];
+      for (int i = j + 1; i < m; ++i) s += std::conj(v[i]) * q[i];
+      s *= tau[j];
+      q[j] -= s;
+      for (int i = j + 1; i < m; ++i) q[i] -= s * v[i];
+    }
+  }
+}
+
+// Thin LQ of M (m x n) = Lm (m x k) * Qm (k x n), via QR of M^H.
+void house_lq(int m, int n, const cd* M, vector<cd>& Lm, vector<cd>& Qm) {
+  vector<cd> MH((size_t)n * m);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < n; ++j) MH[j + (size_t)n * i] = std::conj(M[i + (size_t)m * j]);
+  vector<cd> Q, R;
+  house_qr(n, m, MH.data(), Q, R);  // Q (n x k), R (k x m)
+  const int k = std::min(m, n);
+  Lm.assign((size_t)m * k, 0.0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < k; ++j) Lm[i + (size_t)m * j] = std::conj(R[j + (size_t)k * i]);
+  Qm.assign((size_t)k * n, 0.0);
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j < n; ++j) Qm[i + (size_t)k * j] = std::conj(Q[j + (size_t)n * i]);
+}
+
+// ---------------------------------------------------------------------------
+// One-sided Jacobi SVD (restates the `svd` of Algorithms.jl:420,
+// Decompositions.jl:105, Dissipation.jl:281, StochasticProcess.jl:280).
+// M (m x n) = U (m x k) diag(S) Vt (k x n), k = min(m,n), S descending.
+// ---------------------------------------------------------------------------
+// Orthonormal completion: fills column `slot` of X (rows x cols) with the
+// first unit vector e_c whose component orthogonal to columns `have` exceeds
+// 1/2 in norm (two Gram-Schmidt passes), normalised.
+void complete_column(int rows, vector<cd>& X, const vector<int>& have, int slot) {
+  vector<cd> y(rows);
+  for (int c = 0; c < rows; ++c) {
+    std::fill(y.begin(), y.end(), cd(0));
+    y[c] = 1.0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int h : have) {
+        const cd* x = &X[(size_t)rows * h];
+        cd s = 0;
+        for (int i = 0; i < rows; ++i) s += std::conj(x[i]) * y[i];
+        for (int i = 0; i < rows; ++i) y[i] -= s * x[i];
+      }
+    double nr = nrm2(y.data(), rows);
+    if (nr > 0.5) {
+      for (int i = 0; i < rows; ++i) X[(size_t)rows * slot + i] = y[i] / nr;
+      return;
+    }
+  }
+}
+
+void jacobi_svd(int m, int n, const cd* M, vector<cd>& U, vector<double>& S, vector<cd>& Vt) {
+  const bool tr = m < n;
+  const int q = tr ? n : m;  // rows of B
+  const int p = tr ? m : n;  // columns of B (the shorter side)
+  vector<cd> B((size_t)q * p);
+  if (!tr) {
+    std::copy(M, M + (size_t)m * n, B.begin());
+  } else {
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < n; ++j) B[j + (size_t)q * i] = std::conj(M[i + (size_t)m * j]);
+  }
+  vector<cd> X((size_t)p * p, 0.0);
+  for (int i = 0; i < p; ++i) X[i + (size_t)p * i] = 1.0;
+  const double tol = 2.220446049250313e-16 * q;
+  // Round-robin (tournament) ordering: p' = p rounded up to even, p'-1 rounds
+  // of p'/2 disjoint pairs.  The same order is used on the GPU.
+  const int pe = p + (p & 1);
+  vector<int> slots(pe);
+  for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
+    int rotations = 0;
+    for (int i = 0; i < pe; ++i) slots[i] = i;
+    for (int round = 0; round < pe - 1; ++round) {
+      for (int pr = 0; pr < pe / 2; ++pr) {
+        int a = slots[pr], b = slots[pe - 1 - pr];
+        int i = std::min(a, b), j = std::max(a, b);
+        if (j >= p) continue;
+        cd* bi = &B[(size_t)q * i];
+        cd* bj = &B[(size_t)q * j];
+        double al = 0, be = 0;
+        cd g = 0;
+        for (int r = 0; r < q; ++r) {
+          al += std::norm(bi[r]);
+          be += std::norm(bj[r]);
+          g += std::conj(bi[r]) * bj[r];
+        }
+        double ag = std::abs(g);
+        if (!(ag > tol * std::sqrt(al * be))) continue;
+        ++rotations;
+        double zeta = (be - al) / (2.0 * ag);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        double c = 1.0 / std::sqrt(1.0 + t * t);
+        double s = c * t;
+        cd e = g / ag;
+        cd se = s * e, sec = s * std::conj(e);
+        for (int r = 0; r < q; ++r) {
+          cd x = bi[r], y = bj[r];
+          bi[r] = c * x - sec * y;
+          bj[r] = se * x + c * y;
+        }
+        cd* xi = &X[(size_t)p * i];
+        cd* xj = &X[(size_t)p * j];
+        for (int r = 0; r < p; ++r) {
+          cd x = xi[r], y = xj[r];
+          xi[r] = c * x - sec * y;
+          xj[r] = se * x + c * y;
+        }
+      }
+      // rotate slots 1..pe-1 (slot 0 fixed)
+      int last = slots[pe - 1];
+      for (int i = pe - 1; i > 1; --i) slots[i] = slots[i - 1];
+      slots[1] = last;
+    }
+    if (rotations == 0) break;
+  }
+  vector<double> sig(p);
+  for (int c = 0; c < p; ++c) sig[c] = nrm2(&B[(size_t)q * c], q);
+  vector<int> ord(p);
+  for (int i = 0; i < p; ++i) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return sig[a] > sig[b]; });
+  const double smax = p > 0 ? sig[ord[0]] : 0.0;
+  // left vectors Y (q x p) = B / sigma, right vectors Z (p x p) = X (sorted)
+  vector<cd> Y((size_t)q * p, 0.0), Z((size_t)p * p, 0.0);
+  S.assign(p, 0.0);
+  vector<int> good;
+  vector<int> nulls;
+  for (int k = 0; k < p; ++k) {
+    int c = ord[k];
+    double s = sig[c];
+    if (smax > 0 && s > kSvdNullTol * smax) {
+      S[k] = s;
+      for (int r = 0; r < q; ++r) Y[(size_t)q * k + r] = B[(size_t)q * c + r] / s;
+      for (int r = 0; r < p; ++r) Z[(size_t)p * k + r] = X[(size_t)p * c + r];
+      good.push_back(k);
+    } else {
+      S[k] = 0.0;
+      nulls.push_back(k);
+    }
+  }
+  vector<int> haveY = good, haveZ = good;
+  for (int k : nulls) {
+    complete_column(q, Y, haveY, k);
+    haveY.push_back(k);
+    complete_column(p, Z, haveZ, k);
+    haveZ.push_back(k);
+  }
+  // M = U S V^H.  !tr: U = Y (m=q), V = Z (n=p).  tr: U = Z (m=p), V = Y (n=q).
+  const int k = p;
+  U.assign((size_t)m * k, 0.0);
+  Vt.assign((size_t)k * n, 0.0);
+  const vector<cd>& Uc = tr ? Z : Y;
+  const vector<cd>& Vc = tr ? Y : Z;
+  for (int j = 0; j < k; ++j) {
+    for (int i = 0; i < m; ++i) U[i + (size_t)m * j] = Uc[i + (size_t)m * j];
+    for (int i = 0; i < n; ++i) Vt[j + (size_t)k * i] = std::conj(Vc[i + (size_t)n * j]);
+  }
+}
+
+// Truncation rules (each restates one call site).
+// split_mps_tensor_svd (Algorithms.jl:423-438) and two_site_svd
+// (Decompositions.jl:121-149): absolute, keep the crossing value, min 2.
+int keep_tdvp(const vector<double>& S, double thr, int max_bond) {
+  int n = (int)S.size();
+  double disc = 0;
+  int keep = n;
+  for (int k = n; k >= 1; --k) {
+    disc += S[k - 1] * S[k - 1];
+    if (disc >= thr) {
+      keep = std::max(k, 2);
+      break;
+    }
+  }
+  return std::max(1, std::min(keep, max_bond));
+}
+// Dissipation.jl:290-303 and StochasticProcess.jl:288-300: relative, min 1.
+int keep_relative(const vector<double>& S, double thr, int max_bond) {
+  int n = (int)S.size();
+  double nsq = 0;
+  for (double s : S) nsq += s * s;
+  double cur = 0;
+  int rank = n;
+  for (int k = n; k >= 1; --k) {
+    cur += S[k - 1] * S[k - 1];
+    if (cur > thr * nsq) {
+      rank = k;
+      break;
+    }
+  }
+  return std::max(1, std::min(rank, max_bond));
+}
+
+// ---------------------------------------------------------------------------
+// Small symmetric eigensolver (cyclic Jacobi) for the Lanczos matrix.
+// ---------------------------------------------------------------------------
+void sym_eig(int n, vector<double>& A, vector<double>& V) {  // A (n x n) -> diag, V eigenvectors
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + (size_t)n * i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0, tot = 0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        double x = A[i + (size_t)n * j] * A[i + (size_t)n * j];
+        tot += x;
+        if (i != j) off += x;
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = A[p + (size_t)n * q];
+        if (apq == 0.0) continue;
+        double app = A[p + (size_t)n * p], aqq = A[q + (size_t)n * q];
+        double zeta = (aqq - app) / (2.0 * apq);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
+        for (int k = 0; k < n; ++k) {  // columns p,q
+          double akp = A[k + (size_t)n * p], akq = A[k + (size_t)n * q];
+          A[k + (size_t)n * p] = c * akp - s * akq;
+          A[k + (size_t)n * q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p,q
+          double apk = A[p + (size_t)n * k], aqk = A[q + (size_t)n * k];
+          A[p + (size_t)n * k] = c * apk - s * aqk;
+          A[q + (size_t)n * k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          double vkp = V[k + (size_t)n * p], vkq = V[k + (size_t)n * q];
+          V[k + (size_t)n * p] = c * vkp - s * vkq;
+          V[k + (size_t)n * q] = s * vkp + c * vkq;
+        }
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov exponential (restates expm_krylov, Algorithms.jl:144-187, and the
+// KrylovKit exponentiate call at :185): returns exp(-i*dt*H) v.
+// ---------------------------------------------------------------------------
+struct KrylovParams {
+  int kdim = 25;
+  double tol = 1e-10;
+  double exit_tol = 0.0;
+};
+
+struct Counters {
+  long long matvecs = 0, solves = 0, svds = 0, jumps = 0, nonfinite = 0;
+  double flops = 0;
+};
+
+template <class Op>
+vector<cd> expm_krylov(Op&& op, const vector<cd>& v, double dt, const KrylovParams& kp, Counters& cnt) {
+  const long n = (long)v.size();
+  const double beta0 = nrm2(v.data(), n);
+  if (beta0 == 0.0) return v;
+  cnt.solves++;
+  const double tau = std::fabs(dt);
+  vector<vector<cd>> Q;
+  Q.reserve(kp.kdim + 1);
+  vector<cd> q0(n);
+  for (long i = 0; i < n; ++i) q0[i] = v[i] / beta0;
+  Q.push_back(std::move(q0));
+  vector<double> alpha, beta;
+  double bound = 1.0;
+  int m = 0;
+  vector<cd> w(n);
+  for (int k = 1; k <= kp.kdim; ++k) {
+    op(Q[k - 1], w);
+    cnt.matvecs++;
+    // two-pass classical Gram-Schmidt against q_1..q_k
+    double a_k = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+      vector<cd> h(k);
+      for (int j = 0; j < k; ++j) {
+        cd s = 0;
+        const cd* qj = Q[j].data();
+        for (long i = 0; i < n; ++i) s += std::conj(qj[i]) * w[i];
+        h[j] = s;
+      }
+      for (int j = 0; j < k; ++j) {
+        const cd* qj = Q[j].data();
+        cd hj = h[j];
+        for (long i = 0; i < n; ++i) w[i] -= hj * qj[i];
+      }
+      a_k += h[k - 1].real();
+    }
+    alpha.push_back(a_k);
+    double b_k = nrm2(w.data(), n);
+    m = k;
+    if (b_k <= tau * kp.tol) break;  // invariant subspace (KrylovKit normres test)
+    if (k == kp.kdim) break;
+    bound *= b_k * tau / k;
+    if (kp.exit_tol > 0.0 && bound <= kp.exit_tol) break;
+    beta.push_back(b_k);
+    vector<cd> qn(n);
+    for (long i = 0; i < n; ++i) qn[i] = w[i] / b_k;
+    Q.push_back(std::move(qn));
+  }
+  // T (m x m) symmetric tridiagonal
+  vector<double> T((size_t)m * m, 0.0), V;
+  for (int i = 0; i < m; ++i) T[i + (size_t)m * i] = alpha[i];
+  for (int i = 0; i + 1 < m; ++i) {
+    T[i + (size_t)m * (i + 1)] = beta[i];
+    T[(i + 1) + (size_t)m * i] = beta[i];
+  }
+  sym_eig(m, T, V);
+  vector<cd> y(m, 0.0);
+  for (int e = 0; e < m; ++e) {
+    double lam = T[e + (size_t)m * e];
+    cd ph = std::exp(cd(0.0, -dt * lam)) * V[0 + (size_t)m * e];
+    for (int j = 0; j < m; ++j) y[j] += V[j + (size_t)m * e] * ph;
+  }
+  vector<cd> out(n, 0.0);
+  for (int j = 0; j < m; ++j) {
+    cd c = y[j] * beta0;
+    const cd* qj = Q[j].data();
+    for (long i = 0; i < n; ++i) out[i] += c * qj[i];
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// Environments and projected operators (Algorithms.jl:191-226)
+// ---------------------------------------------------------------------------
+Env identity_env(int dim, int w) {  // make_identity_env, Algorithms.jl:191-197
+  Env E(dim, w, dim);
+  for (int i = 0; i < dim; ++i) E.at(i, 0, i) = 1.0;
+  return E;
+}
+
+// update_left_environment (Algorithms.jl:199-204)
+Env update_left(const Ten& A, const Wt& W, const Env& E) {
+  const int bl = A.l, d = A.d, br = A.r, wl = W.wl, wr = W.wr;
+  // T1[bra_l, ml, pin, ket_r] = sum_k E[bra_l, ml, k] A[k, pin, ket_r]
+  vector<cd> T1((size_t)bl * wl * d * br);
+  matmul(bl * wl, d * br, bl, E.v.data(), A.v.data(), T1.data());
+  // T2[bra_l, ket_r, pout, mr] = sum T1[bra_l, ml, pin, ket_r] W[ml, pout, pin, mr]
+  vector<cd> T2((size_t)bl * br * d * wr, 0.0);
+  for (int kr = 0; kr < br; ++kr)
+    for (int mr = 0; mr < wr; ++mr)
+      for (int po = 0; po < d; ++po)
+        for (int ml = 0; ml < wl; ++ml)
+          for (int pi = 0; pi < d; ++pi) {
+            cd w = W.at(ml, po, pi, mr);
+            if (w == cd(0)) continue;
+            const cd* t1 = &T1[(size_t)bl * (ml + (size_t)wl * (pi + (size_t)d * kr))];
+            cd* t2 = &T2[(size_t)bl * (kr + (size_t)br * (po + (size_t)d * mr))];
+            for (int a = 0; a < bl; ++a) t2[a] += t1[a] * w;
+          }
+  // E'[bra_r, mr, ket_r] = sum T2[bl, ket_r, pout, mr] conj(A[bl, pout, bra_r])
+  Env En(br, wr, br);
+  for (int kr = 0; kr < br; ++kr)
+    for (int mr = 0; mr < wr; ++mr)
+      for (int b = 0; b < br; ++b) {
+        cd s = 0;
+        for (int po = 0; po < d; ++po) {
+          const cd* t2 = &T2[(size_t)bl * (kr + (size_t)br * (po + (size_t)d * mr))];
+          for (int a = 0; a < bl; ++a) s += t2[a] * std::conj(A.at(a, po, b));
+        }
+        En.at(b, mr, kr) = s;
+      }
+  return En;
+}
+
+// update_right_environment (Algorithms.jl:206-211)
+Env update_right(const Ten& A, const Wt& W, const Env& E) {
+  const int kl = A.l, d = A.d, kr = A.r, wl = W.wl, wr = W.wr;
+  // T1[ket_l, pin, bra_r, mr] = sum_k A[ket_l, pin, k] E[bra_r, mr, k]
+  vector<cd> T1((size_t)kl * d * kr * wr, 0.0);
+  for (int k = 0; k < kr; ++k)
+    for (int mr = 0; mr < wr; ++mr)
+      for (int b = 0; b < kr; ++b) {
+        cd e = E.at(b, mr, k);
+        if (e == cd(0)) continue;
+        for (int pi = 0; pi < d; ++pi) {
+          cd* t1 = &T1[(size_t)kl * (pi + (size_t)d * (b + (size_t)kr * mr))];
+          for (int a = 0; a < kl; ++a) t1[a] += A.at(a, pi, k) * e;
+        }
+      }
+  // T2[ml, pout, ket_l, bra_r] = sum W[ml, pout, pin, mr] T1[ket_l, pin, bra_r, mr]
+  vector<cd> T2((size_t)wl * d * kl * kr, 0.0);
+  for (int b = 0; b < kr; ++b)
+    for (int a = 0; a < kl; ++a)
+      for (int ml = 0; ml < wl; ++ml)
+        for (int po = 0; po < d; ++po) {
+          cd s = 0;
+          for (int mr = 0; mr < wr; ++mr)
+            for (int pi = 0; pi < d; ++pi) {
+              cd w = W.at(ml, po, pi, mr);
+              if (w == cd(0)) continue;
+              s += w * T1[a + (size_t)kl * (pi + (size_t)d * (b + (size_t)kr * mr))];
+            }
+          T2[ml + (size_t)wl * (po + (size_t)d * (a + (size_t)kl * b))] = s;
+        }
+  // E'[bra_l, ml, ket_l] = sum T2[ml, pout, ket_l, br] conj(A[bra_l, pout, br])
+  Env En(kl, wl, kl);
+  for (int a = 0; a < kl; ++a)
+    for (int ml = 0; ml < wl; ++ml)
+      for (int x = 0; x < kl; ++x) {
+        cd s = 0;
+        for (int b = 0; b < kr; ++b)
+          for (int po = 0; po < d; ++po)
+            s += T2[ml + (size_t)wl * (po + (size_t)d * (a + (size_t)kl * b))] * std::conj(A.at(x, po, b));
+        En.at(x, ml, a) = s;
+      }
+  return En;
+}
+
+// project_site (Algorithms.jl:215-220, workspace form :330-361).
+// x is (chil, D, chir); out is (chil, D, chir).
+void project_site(const Env& Le, const Env& Re, const Wt& W, int chil, int D, int chir, const vector<cd>& x,
+                  vector<cd>& out) {
+  const int wl = W.wl, wr = W.wr;
+  // T1[a, ml, pin, c] = sum_k L[a, ml, k] x[k, pin, c]
+  vector<cd> T1((size_t)chil * wl * D * chir);
+  matmul(chil * wl, D * chir, chil, Le.v.data(), x.data(), T1.data());
+  // T2[a, c, pout, mr] = sum T1[a, ml, pin, c] W[ml, pout, pin, mr]
+  vector<cd> T2((size_t)chil * chir * D * wr, 0.0);
+  for (int c = 0; c < chir; ++c)
+    for (int mr = 0; mr < wr; ++mr)
+      for (int po = 0; po < D; ++po)
+        for (int ml = 0; ml < wl; ++ml)
+          for (int pi = 0; pi < D; ++pi) {
+            cd w = W.at(ml, po, pi, mr);
+            if (w == cd(0)) continue;
+            const cd* t1 = &T1[(size_t)chil * (ml + (size_t)wl * (pi + (size_t)D * c))];
+            cd* t2 = &T2[(size_t)chil * (c + (size_t)chir * (po + (size_t)D * mr))];
+            for (int a = 0; a < chil; ++a) t2[a] += t1[a] * w;
+          }
+  // out[a, pout, b] = sum T2[a, c, pout, mr] R[b, mr, c]
+  out.assign((size_t)chil * D * chir, 0.0);
+  for (int b = 0; b < chir; ++b)
+    for (int po = 0; po < D; ++po) {
+      cd* o = &out[(size_t)chil * (po + (size_t)D * b)];
+      for (int mr = 0; mr < wr; ++mr)
+        for (int c = 0; c < chir; ++c) {
+          cd r = Re.at(b, mr, c);
+          if (r == cd(0)) continue;
+          const cd* t2 = &T2[(size_t)chil * (c + (size_t)chir * (po + (size_t)D * mr))];
+          for (int a = 0; a < chil; ++a) o[a] += t2[a] * r;
+        }
+    }
+}
+
+inline double heff_flops(int chil, int wl, int D, int chir, int wr) {
+  return 8.0 * ((double)chil * chil * wl * D * chir + (double)chil * chir * D * D * wl * wr +
+                (double)chil * D * chir * chir * wr);
+}
+
+// ---------------------------------------------------------------------------
+// MPS gauge operations (MPS.jl:182-311)
+// ---------------------------------------------------------------------------
+void shift_oc(State& s, int nc) {  // shift_orthogonality_center!, MPS.jl:182-266
+  int oc = s.oc;
+  if (oc == nc) return;
+  if (nc > oc) {
+    for (int i = oc; i < nc; ++i) {
+      Ten& A = s.t[i];
+      vector<cd> Q, R;
+      house_qr(A.l * A.d, A.r, A.v.data(), Q, R);
+      int rn = std::min(A.l * A.d, A.r);
+      Ten An(A.l, A.d, rn);
+      An.v = Q;
+      Ten& N = s.t[i + 1];
+      Ten Nn(rn, N.d, N.r);
+      matmul(rn, N.d * N.r, A.r, R.data(), N.v.data(), Nn.v.data());
+      A = std::move(An);
+      N = std::move(Nn);
+    }
+  } else {
+    for (int i = oc; i > nc; --i) {
+      Ten& A = s.t[i];
+      vector<cd> Lm, Qm;
+      house_lq(A.l, A.d * A.r, A.v.data(), Lm, Qm);
+      int rn = std::min(A.l, A.d * A.r);
+      Ten An(rn, A.d, A.r);
+      An.v = Qm;
+      Ten& P = s.t[i - 1];
+      Ten Pn(P.l, P.d, rn);
+      matmul(P.l * P.d, rn, P.r, P.v.data(), Lm.data(), Pn.v.data());
+      A = std::move(An);
+      P = std::move(Pn);
+    }
+  }
+  s.oc = nc;
+}
+
+void normalize_mps(State& s) {  // normalize!, MPS.jl:274-311
+  for (int i = s.L - 1; i >= 1; --i) {
+    Ten& A = s.t[i];
+    vector<cd> Lm, Qm;
+    house_lq(A.l, A.d * A.r, A.v.data(), Lm, Qm);
+    int rn = std::min(A.l, A.d * A.r);
+    Ten An(rn, A.d, A.r);
+    An.v = Qm;
+    Ten& P = s.t[i - 1];
+    Ten Pn(P.l, P.d, rn);
+    matmul(P.l * P.d, rn, P.r, P.v.data(), Lm.data(), Pn.v.data());
+    A = std::move(An);
+    P = std::move(Pn);
+  }
+  Ten& A1 = s.t[0];
+  double nr = nrm2(A1.v.data(), (long)A1.v.size());
+  if (nr > 1e-13)
+    for (auto& x : A1.v) x *= (1.0 / nr);
+  s.oc = 0;
+}
+
+cd scalar_product(const State& s) {  // scalar_product(psi, psi), MPS.jl:528-585
+  vector<cd> E(1, 1.0);
+  int eb = 1;
+  for (int i = 0; i < s.L; ++i) {
+    const Ten& A = s.t[i];
+    // E'[ra, rb] = sum E[la, lb] A[la, p, ra] conj(A[lb, p, rb])
+    vector<cd> T1((size_t)A.l * A.d * A.r, 0.0);  // T1[lb, p, ra] = sum_la E[la, lb] A[la, p, ra]
+    for (int ra = 0; ra < A.r; ++ra)
+      for (int p = 0; p < A.d; ++p)
+        for (int lb = 0; lb < A.l; ++lb) {
+          cd sacc = 0;
+          for (int la = 0; la < A.l; ++la) sacc += E[la + (size_t)eb * lb] * A.at(la, p, ra);
+          T1[lb + (size_t)A.l * (p + (size_t)A.d * ra)] = sacc;
+        }
+    vector<cd> En((size_t)A.r * A.r, 0.0);
+    for (int rb = 0; rb < A.r; ++rb)
+      for (int ra = 0; ra < A.r; ++ra) {
+        cd sacc = 0;
+        for (int p = 0; p < A.d; ++p)
+          for (int lb = 0; lb < A.l; ++lb)
+            sacc += T1[lb + (size_t)A.l * (p + (size_t)A.d * ra)] * std::conj(A.at(lb, p, rb));
+        En[ra + (size_t)A.r * rb] = sacc;
+      }
+    E.swap(En);
+    eb = A.r;
+  }
+  return E[0];
+}
+
+void apply_1site(Ten& A, const cd* op) {  // T[l,p,r] <- sum_k op[p,k] T[l,k,r]
+  Ten B(A.l, A.d, A.r);
+  for (int r = 0; r < A.r; ++r)
+    for (int p = 0; p < A.d; ++p)
+      for (int l = 0; l < A.l; ++l) {
+        cd sacc = 0;
+        for (int k = 0; k < A.d; ++k) sacc += op[p + A.d * k] * A.at(l, k, r);
+        B.at(l, p, r) = sacc;
+      }
+  A = std::move(B);
+}
+
+Ten merge(const Ten& A1, const Ten& A2) {  // Theta[l, p1, p2, r] as (l, 4, r), p = p1 + 2 p2
+  Ten T(A1.l, A1.d * A2.d, A2.r);
+  matmul(A1.l * A1.d, A2.d * A2.r, A1.r, A1.v.data(), A2.v.data(), T.v.data());
+  return T;
+}
+
+void apply_2site(Ten& T, const cd* op) {  // op (4x4) on the merged index p1 + 2 p2
+  Ten B(T.l, T.d, T.r);
+  for (int r = 0; r < T.r; ++r)
+    for (int p = 0; p < T.d; ++p)
+      for (int l = 0; l < T.l; ++l) {
+        cd sacc = 0;
+        for (int k = 0; k < T.d; ++k) sacc += op[p + T.d * k] * T.at(l, k, r);
+        B.at(l, p, r) = sacc;
+      }
+  T = std::move(B);
+}
+
+double tnorm2(const Ten& A) {
+  double s = 0;
+  for (auto& x : A.v) s += std::norm(x);
+  return s;
+}
+
+// Split Theta (l, 4, r) by SVD; rule 0 = TDVP, 1 = relative.  Returns U (l,2,k), S, Vt (k,2,r).
+void split_theta(const Ten& Th, int rule, double thr, int max_bond, Ten& Uo, vector<double>& So, Ten& Vo,
+                 Counters& cnt) {
+  const int m = Th.l * 2, n = 2 * Th.r;
+  vector<cd> M = Th.v;
+  bool bad = false;
+  for (auto& x : M)
+    if (!std::isfinite(x.real()) || !std::isfinite(x.imag())) {
+      x = 0.0;
+      bad = true;
+    }
+  if (bad) cnt.nonfinite++;
+  vector<cd> U, Vt;
+  vector<double> S;
+  jacobi_svd(m, n, M.data(), U, S, Vt);
+  cnt.svds++;
+  int keep = (rule == 0) ? keep_tdvp(S, thr, max_bond) : keep_relative(S, thr, max_bond);
+  const int k = (int)S.size();
+  Uo = Ten(Th.l, 2, keep);
+  for (int j = 0; j < keep; ++j)
+    for (int i = 0; i < m; ++i) Uo.v[i + (size_t)m * j] = U[i + (size_t)m * j];
+  Vo = Ten(keep, 2, Th.r);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < keep; ++i) Vo.v[i + (size_t)keep * j] = Vt[i + (size_t)k * j];
+  So.assign(S.begin(), S.begin() + keep);
+}
+
+// ---------------------------------------------------------------------------
+// Problem definition (host copies of the C-ABI descriptors)
+// ---------------------------------------------------------------------------
+struct NoiseProc {
+  int nsites;
+  int s0, s1;
+  double gamma;
+  cd mat[16];
+  bool pauli_name, pauli_proc;
+  cd diss_half[16];  // expm(-0.5*dt*gamma*L^dag L) for dt/2 (computed per run)
+  cd diss_full[16];  // ... for dt
+};
+
+struct Obs {
+  int kind;
+  int s0, s1;
+  cd mat[16];
+};
+
+struct Problem {
+  int L;
+  vector<Wt> W;
+  vector<Wt> W2;  // merged two-site W_group (Algorithms.jl:639-643), index i for sites (i, i+1)
+  State psi0;
+  bool noise_present = false;
+  vector<NoiseProc> procs;
+  bool all_zero = true;
+  vector<Obs> obs;
+  double dt;
+  int n_times, num_traj, max_bond, order;
+  double thr;
+  bool sample_timesteps;
+  KrylovParams kp;
+  int rng_mode;
+  uint64_t seed;
+  const double* uniforms;
+  long long stride;
+  int traj_offset;
+};
+
+// Hermitian matrix exponential exp(c * H) for small H (n<=4) via Jacobi on
+// the 2n x 2n real embedding-free approach: eigendecompose Hermitian H with
+// complex Jacobi rotations.
+void herm_expm(int n, const cd* H, double c, cd* out) {
+  vector<cd> A(H, H + n * n), V(n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + n * i] = 1.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
+        if (i != j) off += std::norm(A[i + n * j]);
+    if (off < 1e-34) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        cd apq = A[p + n * q];
+        double ag = std::abs(apq);
+        if (ag == 0.0) continue;
+        double app = A[p + n * p].real(), aqq = A[q + n * q].real();
+        double zeta = (aqq - app) / (2.0 * ag);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        double cc = 1.0 / std::sqrt(1.0 + t * t), s = cc * t;
+        cd e = apq / ag;
+        // J = [[cc, s e],[-s conj(e), cc]] acting on columns p,q: A <- J^H A J
+        for (int k = 0; k < n; ++k) {
+          cd x = A[k + n * p], y = A[k + n * q];
+          A[k + n * p] = cc * x - s * std::conj(e) * y;
+          A[k + n * q] = s * e * x + cc * y;
+        }
+        for (int k = 0; k < n; ++k) {
+          cd x = A[p + n * k], y = A[q + n * k];
+          A[p + n * k] = cc * x - s * e * y;
+          A[q + n * k] = s * std::conj(e) * x + cc * y;
+        }
+        for (int k = 0; k < n; ++k) {
+          cd x = V[k + n * p], y = V[k + n * q];
+          V[k + n * p] = cc * x - s * std::conj(e) * y;
+          V[k + n * q] = s * e * x + cc * y;
+        }
+      }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      cd sacc = 0;
+      for (int k = 0; k < n; ++k) sacc += V[i + n * k] * std::exp(c * A[k + n * k].real()) * std::conj(V[j + n * k]);
+      out[i + n * j] = sacc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Uniform draws
+// ---------------------------------------------------------------------------
+inline void philox_round(uint32_t* c, const uint32_t* k) {
+  const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+  const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+  uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+  uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+  uint32_t n0 = hi1 ^ c[1] ^ k[0];
+  uint32_t n1 = lo1;
+  uint32_t n2 = hi0 ^ c[3] ^ k[1];
+  uint32_t n3 = lo0;
+  c[0] = n0;
+  c[1] = n1;
+  c[2] = n2;
+  c[3] = n3;
+}
+
+// Philox-4x32-10 (Salmon et al., SC'11).  Counter = (draw lo, draw hi,
+// stream lo, stream hi), key = seed.  Returns a 53-bit double in [0,1).
+double philox_uniform(uint64_t seed, uint64_t stream, uint64_t draw) {
+  uint32_t c[4] = {(uint32_t)draw, (uint32_t)(draw >> 32), (uint32_t)stream, (uint32_t)(stream >> 32)};
+  uint32_t k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int r = 0; r < 10; ++r) {
+    philox_round(c, k);
+    if (r < 9) {
+      k[0] += 0x9E3779B9u;
+      k[1] += 0xBB67AE85u;
+    }
+  }
+  uint64_t bits = ((uint64_t)c[1] << 32) | c[0];
+  return (double)(bits >> 11) * (1.0 / 9007199254740992.0);
+}
+
+struct Draws {
+  const Problem* P;
+  long long traj;
+  long long pos = 0;
+  bool exhausted = false;
+  double next() {
+    if (P->rng_mode == YAQS_RNG_INJECTED) {
+      if (pos >= P->stride) {
+        exhausted = true;
+        return 1.0;
+      }
+      return P->uniforms[traj * P->stride + pos++];
+    }
+    return philox_uniform(P->seed, (uint64_t)(P->traj_offset + traj), (uint64_t)pos++);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Two-site TDVP, Hamiltonian symmetric sweep (Algorithms.jl:580-603, 631-760)
+// ---------------------------------------------------------------------------
+struct Sweeper {
+  const Problem& P;
+  Counters& cnt;
+  vector<Env> EL, ER;
+
+  Sweeper(const Problem& p, Counters& c) : P(p), cnt(c) {}
+
+  vector<cd> evolve(const Env& Le, const Env& Re, const Wt& W, const Ten& x, double dt) {
+    auto op = [&](const vector<cd>& in, vector<cd>& out) {
+      project_site(Le, Re, W, x.l, x.d, x.r, in, out);
+      cnt.flops += heff_flops(x.l, W.wl, x.d, x.r, W.wr);
+    };
+    return expm_krylov(op, x.v, dt, P.kp, cnt);
+  }
+
+  void init_envs(State& s) {  // _init_envs, Algorithms.jl:802-819
+    const int L = s.L;
+    ER.assign(L + 1, Env());
+    EL.assign(L + 1, Env());
+    ER[L] = identity_env(s.t[L - 1].r, P.W[L - 1].wr);
+    for (int i = L - 1; i >= 1; --i) ER[i] = update_right(s.t[i], P.W[i], ER[i + 1]);
+    EL[0] = identity_env(s.t[0].l, P.W[0].wl);
+  }
+
+  // _two_site_update_forward! (Algorithms.jl:631-672), evolve_back = true
+  void forward(State& s, int i, double dts) {
+    Ten Th = merge(s.t[i], s.t[i + 1]);
+    Th.v = evolve(EL[i], ER[i + 2], P.W2[i], Th, dts);
+    Ten U, V;
+    vector<double> S;
+    split_theta(Th, 0, P.thr, P.max_bond, U, S, V, cnt);
+    s.t[i] = U;
+    EL[i + 1] = update_left(s.t[i], P.W[i], EL[i]);
+    for (int b = 0; b < V.r; ++b)
+      for (int p = 0; p < 2; ++p)
+        for (int a = 0; a < V.l; ++a) V.at(a, p, b) *= S[a];
+    V.v = evolve(EL[i + 1], ER[i + 2], P.W[i + 1], V, -dts);
+    s.t[i + 1] = V;
+  }
+
+  // _two_site_update_edge_hamiltonian! (Algorithms.jl:674-711) and the
+  // second half of _two_site_update_backward_precorrect! (:729-759).
+  void split_left(State& s, int i, double dts) {
+    Ten Th = merge(s.t[i], s.t[i + 1]);
+    Th.v = evolve(EL[i], ER[i + 2], P.W2[i], Th, dts);
+    Ten U, V;
+    vector<double> S;
+    split_theta(Th, 0, P.thr, P.max_bond, U, S, V, cnt);
+    s.t[i + 1] = V;
+    ER[i + 1] = update_right(s.t[i + 1], P.W[i + 1], ER[i + 2]);
+    for (int j = 0; j < U.r; ++j)
+      for (int p = 0; p < 2; ++p)
+        for (int a = 0; a < U.l; ++a) U.at(a, p, j) *= S[j];
+    s.t[i] = U;
+  }
+
+  void backward(State& s, int i, double dts) {  // Algorithms.jl:713-760
+    s.t[i + 1].v = evolve(EL[i + 1], ER[i + 2], P.W[i + 1], s.t[i + 1], -dts);
+    split_left(s, i, dts);
+  }
+
+  void sweep(State& s) {  // _tdvp_sweep_hamiltonian_2site!, Algorithms.jl:580-603
+    shift_oc(s, 0);
+    const int L = s.L;
+    const double dt = P.dt;
+    init_envs(s);
+    for (int i = 0; i <= L - 3; ++i) forward(s, i, dt / 2);
+    if (L >= 2) split_left(s, L - 2, dt);
+    for (int i = L - 3; i >= 0; --i) backward(s, i, dt / 2);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Dissipation (Dissipation.jl:37-159), local processes
+// ---------------------------------------------------------------------------
+void apply_dissipation(const Problem& P, State& s, bool full_dt, double dt, Counters& cnt) {
+  const int L = s.L;
+  if (!P.noise_present || P.all_zero) {  // :39-47
+    for (int i = L - 1; i >= 1; --i) shift_oc(s, i - 1);
+    return;
+  }
+  for (int i = L - 1; i >= 0; --i) {
+    for (const auto& pr : P.procs) {
+      if (pr.nsites == 1 && pr.s0 == i) {
+        if (pr.pauli_name) {
+          double f = std::exp(-0.5 * dt * pr.gamma);
+          for (auto& x : s.t[i].v) x *= f;
+        } else {
+          apply_1site(s.t[i], full_dt ? pr.diss_full : pr.diss_half);
+        }
+      }
+    }
+    if (i > 0) {
+      for (const auto& pr : P.procs) {
+        if (pr.nsites == 2 && pr.s1 == i) {
+          if (pr.pauli_name) {
+            double f = std::exp(-0.5 * dt * pr.gamma);
+            for (auto& x : s.t[i].v) x *= f;
+          } else {
+            Ten Th = merge(s.t[i - 1], s.t[i]);
+            apply_2site(Th, full_dt ? pr.diss_full : pr.diss_half);
+            Ten U, V;
+            vector<double> S;
+            split_theta(Th, 1, P.thr, P.max_bond, U, S, V, cnt);
+            for (int b = 0; b < V.r; ++b)
+              for (int p = 0; p < 2; ++p)
+                for (int a = 0; a < V.l; ++a) V.at(a, p, b) *= S[a];
+            s.t[i - 1] = U;
+            s.t[i] = V;
+          }
+        }
+      }
+      shift_oc(s, i - 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stochastic process (StochasticProcess.jl:35-38, 89-212, 219-330)
+// ---------------------------------------------------------------------------
+struct Cand {
+  const NoiseProc* pr;
+  double dp;
+};
+
+bool stochastic_process(const Problem& P, State& s, double dt, Draws& rng, Counters& cnt) {
+  const int L = s.L;
+  double dp = 1.0 - scalar_product(s).real();
+  if (P.procs.empty() || rng.next() >= dp) {
+    shift_oc(s, 0);
+    normalize_mps(s);
+    return false;
+  }
+  // create_probability_distribution
+  vector<Cand> cands;
+  for (int site = 0; site < L; ++site) {
+    shift_oc(s, site);
+    for (const auto& pr : P.procs) {
+      if (pr.nsites == 1 && pr.s0 == site) {
+        double nr;
+        if (pr.pauli_proc) {
+          nr = tnorm2(s.t[site]);
+        } else {
+          Ten T = s.t[site];
+          apply_1site(T, pr.mat);
+          nr = tnorm2(T);
+        }
+        cands.push_back({&pr, dt * pr.gamma * nr});
+      }
+    }
+    if (site < L - 1) {
+      for (const auto& pr : P.procs) {
+        if (pr.nsites == 2 && pr.s0 == site) {
+          double nr;
+          if (pr.pauli_proc) {
+            nr = tnorm2(s.t[site]);
+          } else {
+            Ten Th = merge(s.t[site], s.t[site + 1]);
+            apply_2site(Th, pr.mat);
+            nr = tnorm2(Th);
+          }
+          cands.push_back({&pr, dt * pr.gamma * nr});
+        }
+      }
+    }
+  }
+  double total = 0;
+  for (auto& c : cands) total += c.dp;
+  if (total == 0.0) {
+    shift_oc(s, 0);
+    normalize_mps(s);
+    return false;
+  }
+  double r = rng.next();
+  double acc = 0;
+  size_t chosen = 0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    acc += cands[i].dp / total;
+    if (r <= acc) {
+      chosen = i;
+      break;
+    }
+  }
+  const NoiseProc& pr = *cands[chosen].pr;
+  if (pr.nsites == 1) {
+    shift_oc(s, pr.s0);
+    apply_1site(s.t[pr.s0], pr.mat);
+  } else {
+    shift_oc(s, pr.s0);
+    Ten Th = merge(s.t[pr.s0], s.t[pr.s0 + 1]);
+    apply_2site(Th, pr.mat);
+    Ten U, V;
+    vector<double> S;
+    split_theta(Th, 1, P.thr, P.max_bond, U, S, V, cnt);
+    for (int b = 0; b < V.r; ++b)
+      for (int p = 0; p < 2; ++p)
+        for (int a = 0; a < V.l; ++a) V.at(a, p, b) *= S[a];
+    s.t[pr.s0] = U;
+    s.t[pr.s0 + 1] = V;
+  }
+  cnt.jumps++;
+  normalize_mps(s);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Observables (SimulationConfigs.jl:42-56, MPS.jl:608-651)
+// ---------------------------------------------------------------------------
+double measure(const Obs& o, State& s) {
+  if (o.kind == YAQS_OBS_LOCAL1) {
+    shift_oc(s, o.s0);
+    const Ten& A = s.t[o.s0];
+    cd acc = 0;
+    for (int r = 0; r < A.r; ++r)
+      for (int l = 0; l < A.l; ++l)
+        for (int p = 0; p < 2; ++p) {
+          cd oa = 0;
+          for (int k = 0; k < 2; ++k) oa += o.mat[p + 2 * k] * A.at(l, k, r);
+          acc += std::conj(A.at(l, p, r)) * oa;
+        }
+    return acc.real();
+  }
+  if (o.kind == YAQS_OBS_LOCAL2) {
+    shift_oc(s, o.s0);
+    Ten Th = merge(s.t[o.s0], s.t[o.s0 + 1]);
+    cd acc = 0;
+    for (int r = 0; r < Th.r; ++r)
+      for (int l = 0; l < Th.l; ++l)
+        for (int p = 0; p < 4; ++p) {
+          cd oa = 0;
+          for (int k = 0; k < 4; ++k) oa += o.mat[p + 4 * k] * Th.at(l, k, r);
+          acc += std::conj(Th.at(l, p, r)) * oa;
+        }
+    return acc.real();
+  }
+  // ENTROPY across the bond (s0, s0+1): Schmidt values of the center tensor.
+  shift_oc(s, o.s0);
+  const Ten& A = s.t[o.s0];
+  vector<cd> U, Vt;
+  vector<double> S;
+  jacobi_svd(A.l * A.d, A.r, A.v.data(), U, S, Vt);
+  double nsq = 0;
+  for (double x : S) nsq += x * x;
+  double ent = 0;
+  for (double x : S) {
+    double p = x * x / nsq;
+    if (p > 0) ent -= p * std::log(p);
+  }
+  return ent;
+}
+
+int max_bond(const State& s) {  // write_max_bond_dim, MPS.jl:168-174
+  int m = 0;
+  for (const auto& t : s.t) m = std::max(m, std::max(t.l, t.r));
+  return m;
+}
+
+void evaluate(const Problem& P, State& s, double* out, int col, int ncols, int* chi_out) {
+  for (size_t k = 0; k < P.obs.size(); ++k) out[k * ncols + col] = measure(P.obs[k], s);
+  if (chi_out) chi_out[col] = max_bond(s);
+}
+
+// ---------------------------------------------------------------------------
+// Trajectories (AnalogTJM.jl:21-176)
+// ---------------------------------------------------------------------------
+int run_trajectory(const Problem& P, long long traj, double* out, int* chi_out, Counters& cnt) {
+  State s = P.psi0;  // deepcopy (AnalogTJM.jl:110)
+  normalize_mps(s);  // Simulator.run normalises psi0 (Simulator.jl:128)
+  Draws rng{&P, traj};
+  const int nobs = (int)P.obs.size();
+  const int ncols = P.sample_timesteps ? P.n_times : 1;
+  const double dt = P.dt;
+  Sweeper sw(P, cnt);
+  if (P.order == 2) {
+    if (P.sample_timesteps) evaluate(P, s, out, 0, ncols, chi_out);
+    // initialize (AnalogTJM.jl:21-33)
+    apply_dissipation(P, s, false, dt / 2, cnt);
+    if (P.noise_present) stochastic_process(P, s, dt, rng, cnt);
+    auto sample = [&](int j) {  // AnalogTJM.jl:62-81
+      State psi = s;
+      sw.sweep(psi);
+      apply_dissipation(P, psi, false, dt / 2, cnt);
+      if (P.noise_present) stochastic_process(P, psi, dt, rng, cnt);
+      evaluate(P, psi, out, P.sample_timesteps ? j : 0, ncols, chi_out);
+    };
+    if (P.sample_timesteps && P.n_times > 1) sample(1);
+    for (int j = 2; j < P.n_times; ++j) {
+      sw.sweep(s);  // step_through (AnalogTJM.jl:40-55)
+      apply_dissipation(P, s, true, dt, cnt);
+      if (P.noise_present) stochastic_process(P, s, dt, rng, cnt);
+      if (P.sample_timesteps || j == P.n_times - 1) sample(j);
+    }
+  } else {
+    if (P.sample_timesteps) evaluate(P, s, out, 0, ncols, chi_out);
+    for (int j = 1; j < P.n_times; ++j) {
+      sw.sweep(s);
+      if (P.noise_present) {
+        apply_dissipation(P, s, true, dt, cnt);
+        stochastic_process(P, s, dt, rng, cnt);
+      }
+      if (P.sample_timesteps)
+        evaluate(P, s, out, j, ncols, chi_out);
+      else if (j == P.n_times - 1)
+        evaluate(P, s, out, 0, ncols, chi_out);
+    }
+  }
+  (void)nobs;
+  return rng.exhausted ? YAQS_E_RNG : YAQS_OK;
+}
+
+std::string g_err;
+std::mutex g_err_mu;
+
+int fail(int code, const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_err = msg;
+  return code;
+}
+
+bool load_problem(Problem& P, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                  const yaqs_obs_desc* obs, int n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                  std::string& err) {
+  if (!psi0 || !H || !cfg || !rng) {
+    err = "null descriptor";
+    return false;
+  }
+  const int L = psi0->L;
+  if (L < 2 || H->L != L) {
+    err = "need L >= 2 and matching MPO length";
+    return false;
+  }
+  P.L = L;
+  P.psi0.L = L;
+  P.psi0.oc = 0;
+  P.psi0.t.resize(L);
+  for (int i = 0; i < L; ++i) {
+    int l = psi0->chi[i], r = psi0->chi[i + 1];
+    Ten T(l, 2, r);
+    const double* src = psi0->tensors[i];
+    for (size_t k = 0; k < T.v.size(); ++k) T.v[k] = cd(src[2 * k], src[2 * k + 1]);
+    P.psi0.t[i] = std::move(T);
+  }
+  P.W.resize(L);
+  for (int i = 0; i < L; ++i) {
+    Wt W(H->w[i], 2, H->w[i + 1]);
+    const double* src = H->tensors[i];
+    for (size_t k = 0; k < W.v.size(); ++k) W.v[k] = cd(src[2 * k], src[2 * k + 1]);
+    P.W[i] = std::move(W);
+  }
+  P.W2.resize(L - 1);
+  for (int i = 0; i + 1 < L; ++i) {  // W_group, Algorithms.jl:639-643
+    const Wt &W1 = P.W[i], &Wn = P.W[i + 1];
+    Wt G(W1.wl, 4, Wn.wr);
+    for (int l = 0; l < W1.wl; ++l)
+      for (int r = 0; r < Wn.wr; ++r)
+        for (int p1o = 0; p1o < 2; ++p1o)
+          for (int p2o = 0; p2o < 2; ++p2o)
+            for (int p1i = 0; p1i < 2; ++p1i)
+              for (int p2i = 0; p2i < 2; ++p2i) {
+                cd sacc = 0;
+                for (int k = 0; k < W1.wr; ++k) sacc += W1.at(l, p1o, p1i, k) * Wn.at(k, p2o, p2i, r);
+                G.at(l, p1o + 2 * p2o, p1i + 2 * p2i, r) = sacc;
+              }
+    P.W2[i] = std::move(G);
+  }
+  P.dt = cfg->dt;
+  P.n_times = cfg->n_times;
+  P.num_traj = cfg->num_traj;
+  P.max_bond = cfg->max_bond_dim;
+  P.thr = cfg->truncation_threshold;
+  P.order = cfg->order;
+  P.sample_timesteps = cfg->sample_timesteps != 0;
+  P.kp.kdim = cfg->krylov_dim;
+  P.kp.tol = cfg->krylov_tol;
+  P.kp.exit_tol = cfg->krylov_exit_tol;
+  P.traj_offset = cfg->traj_offset;
+  if (P.n_times < 1 || P.num_traj < 1 || P.max_bond < 1 || P.kp.kdim < 1) {
+    err = "bad config";
+    return false;
+  }
+  P.noise_present = noise && noise->present;
+  P.all_zero = true;
+  if (P.noise_present) {
+    for (int k = 0; k < noise->n; ++k) {
+      const yaqs_noise_proc& q = noise->procs[k];
+      NoiseProc pr{};
+      pr.nsites = q.nsites;
+      pr.s0 = q.site[0];
+      pr.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
+      pr.gamma = q.strength;
+      pr.pauli_name = q.pauli_name != 0;
+      pr.pauli_proc = q.pauli_proc != 0;
+      if (q.nsites == 2 && pr.s1 != pr.s0 + 1) {
+        err = "only adjacent 2-site processes are supported";
+        return false;
+      }
+      int dd = q.nsites == 1 ? 2 : 4;
+      for (int e = 0; e < dd * dd; ++e) pr.mat[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);
+      cd LdL[16];
+      for (int i = 0; i < dd; ++i)
+        for (int j = 0; j < dd; ++j) {
+          cd sacc = 0;
+          for (int k = 0; k < dd; ++k) sacc += std::conj(pr.mat[k + dd * i]) * pr.mat[k + dd * j];
+          LdL[i + dd * j] = sacc;
+        }
+      herm_expm(dd, LdL, -0.5 * (P.dt / 2) * pr.gamma, pr.diss_half);
+      herm_expm(dd, LdL, -0.5 * P.dt * pr.gamma, pr.diss_full);
+      if (pr.gamma != 0.0) P.all_zero = false;
+      P.procs.push_back(pr);
+    }
+  }
+  for (int k = 0; k < n_obs; ++k) {
+    Obs o{};
+    o.kind = obs[k].kind;
+    o.s0 = obs[k].site[0];
+    o.s1 = obs[k].site[1];
+    int dd = o.kind == YAQS_OBS_LOCAL2 ? 4 : 2;
+    for (int e = 0; e < dd * dd; ++e) o.mat[e] = cd(obs[k].matrix[2 * e], obs[k].matrix[2 * e + 1]);
+    P.obs.push_back(o);
+  }
+  P.rng_mode = rng->mode;
+  P.seed = rng->seed;
+  P.uniforms = rng->uniforms;
+  P.stride = rng->stride;
+  return true;
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C" API of the oracle (ctypes, tests only)
+// ===========================================================================
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+// Runs trajectories [t_begin, t_end) of the problem on nthreads host threads.
+// traj_out is [num_traj][n_obs][n_out] indexed by the absolute trajectory.
+int orc_analog_run(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                   const yaqs_obs_desc* obs, int32_t n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                   int32_t t_begin, int32_t t_end, int32_t nthreads, double* traj_out, int32_t* maxchi_out,
+                   yaqs_run_stats* stats) {
+  Problem P;
+  std::string err;
+  if (!load_problem(P, psi0, H, noise, obs, n_obs, cfg, rng, err)) return fail(YAQS_E_ARG, err);
+  const int ncols = P.sample_timesteps ? P.n_times : 1;
+  if (t_begin < 0 || t_end > P.num_traj || t_begin > t_end) return fail(YAQS_E_ARG, "bad trajectory range");
+  std::atomic<int> next(t_begin);
+  std::atomic<int> status(YAQS_OK);
+  std::mutex mu;
+  Counters total;
+  auto worker = [&]() {
+    Counters c;
+    for (;;) {
+      int t = next.fetch_add(1);
+      if (t >= t_end) break;
+      vector<double> out((size_t)n_obs * ncols, 0.0);
+      vector<int> chi(ncols, 0);
+      int st = run_trajectory(P, t, out.data(), chi.data(), c);
+      if (st != YAQS_OK) status.store(st);
+      if (traj_out) std::copy(out.begin(), out.end(), traj_out + (size_t)t * n_obs * ncols);
+      if (maxchi_out) std::copy(chi.begin(), chi.end(), maxchi_out + (size_t)t * ncols);
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    total.matvecs += c.matvecs;
+    total.solves += c.solves;
+    total.svds += c.svds;
+    total.jumps += c.jumps;
+    total.nonfinite += c.nonfinite;
+    total.flops += c.flops;
+  };
+  int nt = std::max(1, (int)nthreads);
+  vector<std::thread> th;
+  for (int i = 0; i < nt; ++i) th.emplace_back(worker);
+  for (auto& x : th) x.join();
+  if (stats) {
+    stats->matvecs = total.matvecs;
+    stats->krylov_solves = total.solves;
+    stats->svds = total.svds;
+    stats->jumps = total.jumps;
+    stats->nonfinite_fixes = total.nonfinite;
+    stats->flops = total.flops;
+    stats->device_ms = 0;
+  }
+  if (status.load() != YAQS_OK) return fail(status.load(), "injected uniform stream exhausted");
+  return YAQS_OK;
+}
+
+// Plain 2TDVP evolution without noise: n_steps sweeps of two_site_tdvp!, with
+// local_expect of the given 1-site observables after every sweep (the loop
+// of test/benchmark_tdvp.jl:195-212 and test/simulate_large_ising.jl:69-81).
+// out is [n_steps+1][n_obs].
+int orc_tdvp_evolve(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_obs_desc* obs, int32_t n_obs,
+                    const yaqs_tev_config* cfg, int32_t n_steps, double* out) {
+  Problem P;
+  std::string err;
+  yaqs_rng_desc rng{YAQS_RNG_PHILOX, 0, nullptr, 0};
+  if (!load_problem(P, psi0, H, nullptr, obs, n_obs, cfg, &rng, err)) return fail(YAQS_E_ARG, err);
+  Counters c;
+  State s = P.psi0;
+  Sweeper sw(P, c);
+  for (int k = 0; k < n_obs; ++k) out[k] = measure(P.obs[k], s);
+  for (int t = 1; t <= n_steps; ++t) {
+    sw.sweep(s);
+    for (int k = 0; k < n_obs; ++k) out[(size_t)t * n_obs + k] = measure(P.obs[k], s);
+  }
+  return YAQS_OK;
+}
+
+// Component entry points used by the unit tests.
+int orc_svd(int32_t m, int32_t n, const double* M, double* U, double* S, double* Vt) {
+  vector<cd> A((size_t)m * n);
+  for (size_t k = 0; k < A.size(); ++k) A[k] = cd(M[2 * k], M[2 * k + 1]);
+  vector<cd> u, vt;
+  vector<double> s;
+  jacobi_svd(m, n, A.data(), u, s, vt);
+  std::memcpy(U, u.data(), u.size() * sizeof(cd));
+  std::memcpy(Vt, vt.data(), vt.size() * sizeof(cd));
+  std::memcpy(S, s.data(), s.size() * sizeof(double));
+  return YAQS_OK;
+}
+
+int orc_qr(int32_t m, int32_t n, const double* M, double* Q, double* R) {
+  vector<cd> A((size_t)m * n);
+  for (size_t k = 0; k < A.size(); ++k) A[k] = cd(M[2 * k], M[2 * k + 1]);
+  vector<cd> q, r;
+  house_qr(m, n, A.data(), q, r);
+  std::memcpy(Q, q.data(), q.size() * sizeof(cd));
+  std::memcpy(R, r.data(), r.size() * sizeof(cd));
+  return YAQS_OK;
+}
+
+int orc_truncation_rank(int32_t n, const double* S, double thr, int32_t max_bond, int32_t rule) {
+  vector<double> s(S, S + n);
+  return rule == 0 ? keep_tdvp(s, thr, max_bond) : keep_relative(s, thr, max_bond);
+}
+
+// exp(-i dt H_eff) x for H_eff = project_site(L, R, W) with (chil, D, chir) x.
+// L: (chil, wl, chil), R: (chir, wr, chir), W: (wl, D, D, wr).
+int orc_expm_site(int32_t chil, int32_t D, int32_t chir, int32_t wl, int32_t wr, const double* Lp, const double* Rp,
+                  const double* Wp, const double* x, double dt, int32_t kdim, double tol, double exit_tol, double* out,
+                  int32_t* matvecs) {
+  Env Le(chil, wl, chil), Re(chir, wr, chir);
+  for (size_t k = 0; k < Le.v.size(); ++k) Le.v[k] = cd(Lp[2 * k], Lp[2 * k + 1]);
+  for (size_t k = 0; k < Re.v.size(); ++k) Re.v[k] = cd(Rp[2 * k], Rp[2 * k + 1]);
+  Wt W(wl, D, wr);
+  for (size_t k = 0; k < W.v.size(); ++k) W.v[k] = cd(Wp[2 * k], Wp[2 * k + 1]);
+  vector<cd> v((size_t)chil * D * chir);
+  for (size_t k = 0; k < v.size(); ++k) v[k] = cd(x[2 * k], x[2 * k + 1]);
+  KrylovParams kp;
+  kp.kdim = kdim;
+  kp.tol = tol;
+  kp.exit_tol = exit_tol;
+  Counters c;
+  auto op = [&](const vector<cd>& in, vector<cd>& o) { project_site(Le, Re, W, chil, D, chir, in, o); };
+  vector<cd> r = expm_krylov(op, v, dt, kp, c);
+  std::memcpy(out, r.data(), r.size() * sizeof(cd));
+  if (matvecs) *matvecs = (int32_t)c.matvecs;
+  return YAQS_OK;
+}
+
+int orc_project_site(int32_t chil, int32_t D, int32_t chir, int32_t wl, int32_t wr, const double* Lp,
+                     const double* Rp, const double* Wp, const double* x, double* out) {
+  Env Le(chil, wl, chil), Re(chir, wr, chir);
+  for (size_t k = 0; k < Le.v.size(); ++k) Le.v[k] = cd(Lp[2 * k], Lp[2 * k + 1]);
+  for (size_t k = 0; k < Re.v.size(); ++k) Re.v[k] = cd(Rp[2 * k], Rp[2 * k + 1]);
+  Wt W(wl, D, wr);
+  for (size_t k = 0; k < W.v.size(); ++k) W.v[k] = cd(Wp[2 * k], Wp[2 * k + 1]);
+  vector<cd> v((size_t)chil * D * chir), o;
+  for (size_t k = 0; k < v.size(); ++k) v[k] = cd(x[2 * k], x[2 * k + 1]);
+  project_site(Le, Re, W, chil, D, chir, v, o);
+  std::memcpy(out, o.data(), o.size() * sizeof(cd));
+  return YAQS_OK;
+}
+
+double orc_philox_uniform(uint64_t seed, uint64_t stream, uint64_t draw) { return philox_uniform(seed, stream, draw); }
+
+}  // extern "C"
+
+extern "C" {
+// Raw Philox-4x32-10 block for known-answer tests.
+void orc_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  uint32_t k[2] = {key[0], key[1]};
+  for (int r = 0; r < 10; ++r) {
+    philox_round(c, k);
+    if (r < 9) {
+      k[0] += 0x9E3779B9u;
+      k[1] += 0xBB67AE85u;
+    }
+  }
+  for (int i = 0; i < 4; ++i) out[i] = c[i];
+}
+}

@@ -1,0 +1,103 @@
+"""The CPU oracle against the reference's own committed outputs.
+
+Fixtures come from tests/golden/make_golden.py (copies of CSVs the
+reference committed; Julia cannot run here).
+"""
+import csv
+import os
+
+import numpy as np
+import pytest
+
+from yaqs_julia_b200 import api
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _tdvp_golden(model, method):
+    rows = [r for r in csv.DictReader(open(os.path.join(GOLD, "tdvp_benchmark.csv")))
+            if r["Model"] == model and r["Method"] == method]
+    times = sorted({float(r["Time"]) for r in rows})
+    out = np.zeros((len(times), 3))
+    for r in rows:
+        out[times.index(float(r["Time"])), [1, 3, 6].index(int(r["Site"]))] = float(r["ExpVal"])
+    return out
+
+
+MODELS = {
+    # test/benchmark_tdvp.jl:105-123; the Heisenberg exact H there is
+    # -sum(XX+YY+ZZ) - 0.5 sum Z, i.e. init_general_hamiltonian(L,-1,-1,-1,0,0,-0.5)
+    "Ising_Ferro": lambda L: api.init_ising(L, 1.0, 0.5),
+    "Ising_Disordered": lambda L: api.init_ising(L, [0.6, 1.2, 0.8, 1.4, 0.9], [0.7, 1.3, 0.5, 1.1, 0.8, 1.2]),
+    "Heisenberg": lambda L: api.init_general_hamiltonian(L, -1.0, -1.0, -1.0, 0, 0, -0.5),
+}
+
+
+def _run_tdvp(oracle, H, L, sites, steps, dt, max_bond, thr, exit_tol=1e-12, state="zeros"):
+    obs = [api.Observable(f"Z{s}", api.Z, s) for s in sites]
+    cfg = api.TimeEvolutionConfig(obs, steps * dt, dt=dt, max_bond_dim=max_bond, truncation_threshold=thr)
+    d = api.Descriptors(api.MPS(L, state=state), H, cfg, None, krylov_exit_tol=exit_tol)
+    return oracle.tdvp_evolve(d, steps)
+
+
+@pytest.mark.parametrize("model", list(MODELS))
+def test_tdvp_benchmark_golden_untruncated(oracle, model):
+    # The committed 2TDVP rows agree with exact evolution to 7e-14, which the
+    # current split_mps_tensor_svd rule (absolute 1e-9 discard) cannot reach
+    # (it drops Schmidt values that later grow); without truncation the
+    # restatement reproduces them to 1e-11.
+    res = _run_tdvp(oracle, MODELS[model](6), 6, [1, 3, 6], 40, 0.05, 16, 0.0)
+    assert np.abs(res - _tdvp_golden(model, "2TDVP")).max() < 1e-11
+    assert np.abs(res - _tdvp_golden(model, "Exact")).max() < 1e-11
+
+
+@pytest.mark.parametrize("model", ["Ising_Ferro", "Ising_Disordered"])
+def test_tdvp_benchmark_golden_default_threshold(oracle, model):
+    res = _run_tdvp(oracle, MODELS[model](6), 6, [1, 3, 6], 40, 0.05, 16, 1e-9)
+    err = np.abs(res - _tdvp_golden(model, "Exact")).max(axis=1)
+    assert err[:5].max() < 1e-12      # before any Schmidt value falls under the cut
+    assert err.max() < 1e-4
+
+
+def test_large_ising_golden(oracle):
+    # test/simulate_large_ising.jl:31-98: L=30, chi<=32, default threshold.
+    rows = list(csv.DictReader(open(os.path.join(GOLD, "large_ising.csv"))))
+    g = np.zeros((41, 3))
+    for r in rows:
+        g[int(round(float(r["Time"]) / 0.05)), [1, 16, 30].index(int(r["Site"]))] = float(r["ExpVal"])
+    res = _run_tdvp(oracle, api.init_ising(30, 1.0, 0.5), 30, [1, 16, 30], 40, 0.05, 32, 1e-9)
+    err = np.abs(res - g).max(axis=1)
+    assert err[1] < 2e-9
+    assert err[:11].max() < 1e-6
+    assert err.max() < 1e-5
+
+
+def test_dense_lindblad_matches_qutip_golden():
+    from oracle import dense as D
+    L = 6
+    Hm = api.init_ising(L, 1.0, 0.5).to_matrix()
+    Zs = [D.site_op(api.Z, s, L) for s in range(1, L + 1)]
+    jumps = [np.sqrt(0.1) * D.site_op(api.RAISING, s, L) for s in range(1, L + 1)]
+    ex = D.lindblad(Hm, D.product_state([[1, 0]] * L), jumps, 0.05, 40, Zs, substeps=10)
+    for name in ("tjm_vs_qutip_a.csv", "tjm_vs_qutip_b.csv"):
+        g = np.loadtxt(os.path.join(GOLD, name), delimiter=",")
+        assert np.abs(ex - g[:, 8:14]).max() < 1e-7
+
+
+def test_tjm_ensemble_within_3se_of_exact_lindblad(oracle):
+    # Setup of benchmark_analog_tjm.jl:90-227 (L=6 Ising, raising 0.1, dt=0.05, T=2).
+    from oracle import dense as D
+    L = 6
+    H = api.init_ising(L, 1.0, 0.5)
+    Zs = [D.site_op(api.Z, s, L) for s in range(1, L + 1)]
+    jumps = [np.sqrt(0.1) * D.site_op(api.RAISING, s, L) for s in range(1, L + 1)]
+    ex = D.lindblad(H.to_matrix(), D.product_state([[1, 0]] * L), jumps, 0.05, 40, Zs, substeps=10)
+    obs = [api.Observable(f"Z{s}", api.Z, s) for s in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 2.0, dt=0.05, num_traj=800, max_bond_dim=8)
+    nm = api.NoiseModel([{"name": "raising", "sites": [i], "strength": 0.1} for i in range(1, L + 1)], L)
+    traj, _, st = oracle.analog_run(api.Descriptors(api.MPS(L, state="zeros"), H, cfg, nm, seed=20241203))
+    mean = traj.mean(0).T
+    se = traj.std(0, ddof=1).T / np.sqrt(traj.shape[0])
+    z = np.abs(mean - ex)[1:] / np.maximum(se[1:], 1e-12)
+    assert st["jumps"] > 0
+    assert (z > 3).mean() < 0.03 and z.max() < 5

@@ -1,0 +1,451 @@
+"""Host-side mirror of the Yaqs.jl API for the analog TJM path.
+
+Names, argument meaning and defaults follow the reference so code written
+against Yaqs.jl reads the same here:
+
+* ``MPS(length; state=...)``            — src/MPS.jl:52-144
+* ``init_ising``, ``init_general_hamiltonian`` — src/MPO.jl:92-260
+* ``NoiseModel(processes, num_qubits)`` — src/Noise.jl:299-420 (standard
+  unraveling of local processes)
+* ``Observable``, ``TimeEvolutionConfig`` — src/SimulationConfigs.jl:23-92
+* ``run(initial_state, H, sim_params, noise_model)`` — src/Simulator.jl:127-141
+
+Sites are 1-based, as in Julia.  Tensors are numpy arrays in the
+reference's index order, (left, phys, right) for MPS and
+(left, phys_out, phys_in, right) for MPO, stored column-major
+(Fortran order) so their buffers are exactly what a Julia caller passes
+through the C-ABI.
+
+``run`` executes on the GPU through ``libyaqs_b200.so``; there is no CPU
+path.  If the library or a CUDA device is missing it raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi as A
+
+# ---------------------------------------------------------------------------
+# Gate library (src/GateLibrary.jl).  Matrices as in the reference; 4x4
+# operators use the basis index p1 + 2*p2 (first site fastest).
+# ---------------------------------------------------------------------------
+I2 = np.eye(2, dtype=np.complex128)
+X = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+Y = np.array([[0, -1j], [1j, 0]], dtype=np.complex128)
+Z = np.array([[1, 0], [0, -1]], dtype=np.complex128)
+H = np.array([[1, 1], [1, -1]], dtype=np.complex128) / math.sqrt(2)
+RAISING = np.array([[0, 0], [1, 0]], dtype=np.complex128)   # GateLibrary.jl:77-78
+LOWERING = np.array([[0, 1], [0, 0]], dtype=np.complex128)  # GateLibrary.jl:80-81
+
+
+def Rx(theta):
+    c, s = math.cos(theta / 2), -1j * math.sin(theta / 2)
+    return np.array([[c, s], [s, c]], dtype=np.complex128)
+
+
+def Rz(theta):
+    return np.diag([np.exp(-0.5j * theta), np.exp(0.5j * theta)]).astype(np.complex128)
+
+
+def Rzz(theta):
+    em, ep = np.exp(-0.5j * theta), np.exp(0.5j * theta)
+    return np.diag([em, ep, ep, em]).astype(np.complex128)
+
+
+SWAP = np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, 1, 0, 0], [0, 0, 0, 1]], dtype=np.complex128)
+
+
+def kron2(a, b):
+    """Julia's kron(a, b) reshaped to the (p1_out, p2_out, p1_in, p2_in)
+    convention: kron(A, B) acts with B on the FIRST site (Noise.jl:47-57)."""
+    return np.kron(a, b)
+
+
+GATES = {"x": X, "y": Y, "z": Z, "h": H, "id": I2, "raising": RAISING, "lowering": LOWERING}
+
+
+def _pauli(c):
+    return {"x": X, "y": Y, "z": Z}[c]
+
+
+def get_operator(name: str) -> np.ndarray:
+    """Noise.get_operator (src/Noise.jl:41-61)."""
+    if name == "pauli_x":
+        return X.copy()
+    if name == "pauli_y":
+        return Y.copy()
+    if name == "pauli_z":
+        return Z.copy()
+    if name == "raising":
+        return RAISING.copy()
+    if name == "lowering":
+        return LOWERING.copy()
+    if name == "raising_two":
+        return np.kron(RAISING, RAISING)
+    if name == "lowering_two":
+        return np.kron(LOWERING, LOWERING)
+    if name.startswith("crosstalk_") and len(name) == 12:
+        return np.kron(_pauli(name[10]), _pauli(name[11]))
+    raise ValueError(f"Unknown operator: {name}")
+
+
+_PAULI_NAMES = {"pauli_x", "pauli_y", "pauli_z", "crosstalk_xx", "crosstalk_yy", "crosstalk_zz",
+                "crosstalk_xy", "crosstalk_yx", "crosstalk_zy", "crosstalk_zx", "crosstalk_yz",
+                "crosstalk_xz"}
+
+
+def is_pauli_name(name: str) -> bool:
+    """DissipationModule.is_pauli (src/Dissipation.jl:14-21)."""
+    return name in _PAULI_NAMES
+
+
+def is_pauli_matrix(op: np.ndarray) -> bool:
+    """StochasticProcessModule.is_pauli (src/StochasticProcess.jl:336-341)."""
+    d = op.shape[0]
+    return bool(np.allclose(op.conj().T @ op, np.eye(d), rtol=0.0, atol=1e-10))
+
+
+def is_pauli_proc(name: str, op: np.ndarray) -> bool:
+    """StochasticProcessModule.is_pauli_proc (src/StochasticProcess.jl:343-357)."""
+    if ("pauli" in name or "crosstalk" in name) and "projector" not in name:
+        return True
+    return is_pauli_matrix(op)
+
+
+# ---------------------------------------------------------------------------
+# MPS (src/MPS.jl)
+# ---------------------------------------------------------------------------
+class MPS:
+    """Matrix product state; tensors are (left, phys, right) arrays."""
+
+    def __init__(self, length: int, tensors=None, physical_dimensions=None, state: str = "zeros",
+                 basis_string: str | None = None):
+        self.length = int(length)
+        if physical_dimensions not in (None, 2) and not (
+                isinstance(physical_dimensions, (list, tuple)) and set(physical_dimensions) == {2}):
+            raise NotImplementedError("only qubits (d = 2) are served")
+        self.phys_dims = [2] * self.length
+        self.orth_center = 1
+        if tensors is not None:
+            assert len(tensors) == self.length
+            self.tensors = [np.asfortranarray(np.asarray(t, dtype=np.complex128)) for t in tensors]
+            return
+        ts = []
+        for i in range(1, self.length + 1):  # MPS.jl:105-134
+            v = np.zeros(2, dtype=np.complex128)
+            if state == "basis":
+                assert basis_string is not None and len(basis_string) == self.length
+                v[int(basis_string[i - 1])] = 1.0
+            elif state == "zeros":
+                v[0] = 1.0
+            elif state == "ones":
+                v[1] = 1.0
+            elif state == "x+":
+                v[:] = [1 / math.sqrt(2), 1 / math.sqrt(2)]
+            elif state == "x-":
+                v[:] = [1 / math.sqrt(2), -1 / math.sqrt(2)]
+            elif state == "y+":
+                v[:] = [1 / math.sqrt(2), 1j / math.sqrt(2)]
+            elif state == "y-":
+                v[:] = [1 / math.sqrt(2), -1j / math.sqrt(2)]
+            elif state == "Neel":
+                v[0 if i % 2 != 0 else 1] = 1.0
+            elif state == "wall":
+                v[0 if i <= self.length // 2 else 1] = 1.0
+            else:
+                raise ValueError(f"Unknown state: {state}")
+            ts.append(np.asfortranarray(v.reshape(1, 2, 1)))
+        self.tensors = ts
+
+    @property
+    def bond_dims(self):
+        return [1] + [t.shape[2] for t in self.tensors]
+
+    def to_vec(self) -> np.ndarray:
+        """MPS.to_vec (src/MPS.jl:766-775): site 1 is the fastest index."""
+        v = self.tensors[0]
+        for t in self.tensors[1:]:
+            l, p, _ = v.shape
+            v = np.einsum("lpk,kqr->lpqr", v, t).reshape(l, p * t.shape[1], t.shape[2], order="F")
+        return v.reshape(-1, order="F")
+
+
+# ---------------------------------------------------------------------------
+# MPO (src/MPO.jl)
+# ---------------------------------------------------------------------------
+class MPO:
+    """Matrix product operator; tensors are (left, out, in, right) arrays."""
+
+    def __init__(self, length: int, tensors):
+        self.length = int(length)
+        self.tensors = [np.asfortranarray(np.asarray(t, dtype=np.complex128)) for t in tensors]
+        self.phys_dims = [2] * self.length
+
+    @property
+    def bond_dims(self):
+        return [1] + [t.shape[3] for t in self.tensors]
+
+    def to_matrix(self) -> np.ndarray:
+        """Dense operator in the to_vec basis (site 1 fastest); tests only."""
+        W = self.tensors[0][0]  # (out, in, r)
+        op = W
+        for t in self.tensors[1:]:
+            # op[(o1..), (i1..), k] * t[k, o, i, r]
+            do, di, _ = op.shape
+            op = np.einsum("abk,kcdr->acbdr", op, t).reshape(do * 2, di * 2, t.shape[3], order="F")
+        return op[:, :, 0]
+
+
+def _block_to_tensor(blocks):
+    rows, cols = len(blocks), len(blocks[0])
+    T = np.zeros((rows, 2, 2, cols), dtype=np.complex128, order="F")
+    for r in range(rows):
+        for c in range(cols):
+            T[r, :, :, c] = blocks[r][c]
+    return T
+
+
+def _param(p, i):  # 1-based site i; vectors shorter than L give 0 (MPO.jl:102,186)
+    if isinstance(p, (list, tuple, np.ndarray)):
+        return float(p[i - 1]) if i <= len(p) else 0.0
+    return float(p)
+
+
+def init_ising(length: int, J, g) -> MPO:
+    """H = -sum J Z_i Z_{i+1} - sum g X_i (src/MPO.jl:92-163), bond width 3."""
+    Zr = np.zeros((2, 2), dtype=np.complex128)
+    L = int(length)
+    if L == 1:
+        return MPO(1, [(-_param(g, 1) * X).reshape(1, 2, 2, 1)])
+    ts = [_block_to_tensor([[I2, -_param(J, 1) * Z, -_param(g, 1) * X]])]
+    for i in range(2, L):
+        W = [[Zr] * 3 for _ in range(3)]
+        W[0][0] = I2
+        W[0][1] = -_param(J, i) * Z
+        W[0][2] = -_param(g, i) * X
+        W[1][2] = Z
+        W[2][2] = I2
+        ts.append(_block_to_tensor(W))
+    ts.append(_block_to_tensor([[-_param(g, L) * X], [Z], [I2]]))
+    return MPO(L, ts)
+
+
+def init_general_hamiltonian(length: int, Jxx, Jyy, Jzz, hx, hy, hz) -> MPO:
+    """H = sum(Jxx XX + Jyy YY + Jzz ZZ) + sum(hx X + hy Y + hz Z)
+    (src/MPO.jl:175-260), bond width 5, signs as written (positive)."""
+    Zr = np.zeros((2, 2), dtype=np.complex128)
+    L = int(length)
+    ts = []
+    for i in range(1, L + 1):
+        jxx = _param(Jxx, i) if i < L else 0.0
+        jyy = _param(Jyy, i) if i < L else 0.0
+        jzz = _param(Jzz, i) if i < L else 0.0
+        loc = _param(hx, i) * X + _param(hy, i) * Y + _param(hz, i) * Z
+        W = [[Zr] * 5 for _ in range(5)]
+        W[0][0] = I2
+        W[0][1] = jxx * X
+        W[0][2] = jyy * Y
+        W[0][3] = jzz * Z
+        W[0][4] = loc
+        W[1][4] = X
+        W[2][4] = Y
+        W[3][4] = Z
+        W[4][4] = I2
+        if i == 1:
+            ts.append(loc.reshape(1, 2, 2, 1) if L == 1 else _block_to_tensor([W[0]]))
+        elif i == L:
+            ts.append(_block_to_tensor([[W[r][4]] for r in range(5)]))
+        else:
+            ts.append(_block_to_tensor(W))
+    return MPO(L, ts)
+
+
+# ---------------------------------------------------------------------------
+# Noise (src/Noise.jl)
+# ---------------------------------------------------------------------------
+class LocalNoiseProcess:
+    def __init__(self, name, sites, strength, matrix):
+        self.name = name
+        self.sites = list(sites)
+        self.strength = float(strength)
+        self.matrix = np.asarray(matrix, dtype=np.complex128)
+
+
+class NoiseModel:
+    """NoiseModel(processes_info, num_qubits) with the "standard" unraveling
+    (src/Noise.jl:299-420).  Long-range and unraveling expansions are not
+    served by this engine and raise NotImplementedError."""
+
+    def __init__(self, processes, num_qubits: int | None = None):
+        self.processes = []
+        for p in processes:
+            if isinstance(p, LocalNoiseProcess):
+                self.processes.append(p)
+                continue
+            name = p["name"]
+            sites = list(p["sites"])
+            unravel = p.get("unraveling", "standard")
+            if unravel not in ("standard",):
+                raise NotImplementedError(f"unraveling {unravel!r} is not served")
+            if len(sites) == 2:
+                sites = sorted(sites)
+            if not sites or len(sites) > 2:
+                raise ValueError("Invalid sites")
+            if len(sites) == 2 and sites[1] - sites[0] > 1:
+                raise NotImplementedError("long-range (MPO) noise processes are not served")
+            mat = np.asarray(p["matrix"], dtype=np.complex128) if "matrix" in p else get_operator(name)
+            self.processes.append(LocalNoiseProcess(name, sites, p["strength"], mat))
+
+
+# ---------------------------------------------------------------------------
+# Observables and configs (src/SimulationConfigs.jl)
+# ---------------------------------------------------------------------------
+class Observable:
+    """Observable(name, op, sites).  op is a 2x2 / 4x4 matrix or a gate name
+    ("x", "y", "z", ...).  kind="entropy" measures the von Neumann entropy
+    across the bond right of sites[0] (an addition to the reference)."""
+
+    def __init__(self, name, op=None, sites=None, kind=None):
+        self.name = name
+        if isinstance(sites, int):
+            sites = [sites]
+        self.sites = list(sites)
+        self.kind = kind or ("local" if op is not None else "entropy")
+        if isinstance(op, str):
+            op = GATES[op.lower()]
+        self.op = None if op is None else np.asarray(op, dtype=np.complex128)
+        self.results = np.zeros(0)
+        self.trajectories = np.zeros((0, 0))
+
+
+def _range_len(total_time: float, dt: float) -> int:
+    """length(0.0:dt:total_time) (SimulationConfigs.jl:89)."""
+    n = total_time / dt
+    r = round(n)
+    if abs(n - r) <= 1e-10 * max(1.0, abs(n)):
+        return int(r) + 1
+    return int(math.floor(n)) + 1
+
+
+class TimeEvolutionConfig:
+    def __init__(self, observables, total_time: float, dt: float = 0.1, num_traj: int = 1000,
+                 max_bond_dim: int = 4096, min_bond_dim: int = 2, truncation_threshold: float = 1e-9,
+                 sample_timesteps: bool = True, order: int = 2):
+        self.observables = list(observables)
+        self.total_time = float(total_time)
+        self.dt = float(dt)
+        n = _range_len(self.total_time, self.dt)
+        self.times = np.arange(n) * self.dt
+        self.num_traj = int(num_traj)
+        self.max_bond_dim = int(max_bond_dim)
+        self.min_bond_dim = int(min_bond_dim)
+        self.truncation_threshold = float(truncation_threshold)
+        self.sample_timesteps = bool(sample_timesteps)
+        self.order = int(order)
+
+
+# ---------------------------------------------------------------------------
+# Descriptor packing (what the Julia shim does before ccall)
+# ---------------------------------------------------------------------------
+def _c64(a) -> np.ndarray:
+    """Column-major complex128 buffer viewed as interleaved doubles."""
+    f = np.asfortranarray(np.asarray(a, dtype=np.complex128))
+    return f.reshape(-1, order="F").view(np.float64)
+
+
+class Descriptors:
+    """Owns every buffer referenced by the C descriptors of one run."""
+
+    def __init__(self, psi0: MPS, H: MPO, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None,
+                 *, rng_mode: int = A.YAQS_RNG_PHILOX, seed: int = 0, uniforms: np.ndarray | None = None,
+                 krylov_dim: int = 25, krylov_tol: float = 1e-10, krylov_exit_tol: float = 1e-12,
+                 precision: int = A.YAQS_PREC_FP64, traj_offset: int = 0, num_traj: int | None = None):
+        L = psi0.length
+        if H.length != L:
+            raise ValueError("MPO and MPS lengths differ")
+        self._keep = []
+        # MPS
+        chi = np.array([1] + [t.shape[2] for t in psi0.tensors], dtype=np.int32)
+        for i, t in enumerate(psi0.tensors):
+            if t.shape[0] != chi[i] or t.shape[1] != 2:
+                raise ValueError(f"bond dimension mismatch at site {i + 1}")
+        bufs = [_c64(t) for t in psi0.tensors]
+        ptrs = (A.DPTR * L)(*[A.dptr(b) for b in bufs])
+        self._keep += [chi, bufs, ptrs]
+        self.mps = A.MpsDesc(L, chi.ctypes.data_as(C.POINTER(C.c_int32)), ptrs)
+        # MPO
+        w = np.array([1] + [t.shape[3] for t in H.tensors], dtype=np.int32)
+        wb = [_c64(t) for t in H.tensors]
+        wp = (A.DPTR * L)(*[A.dptr(b) for b in wb])
+        self._keep += [w, wb, wp]
+        self.mpo = A.MpoDesc(L, w.ctypes.data_as(C.POINTER(C.c_int32)), wp)
+        # noise
+        procs = noise_model.processes if noise_model is not None else []
+        arr = (A.NoiseProc * max(1, len(procs)))()
+        for k, p in enumerate(procs):
+            q = arr[k]
+            q.nsites = len(p.sites)
+            q.site[0] = p.sites[0] - 1
+            q.site[1] = (p.sites[1] - 1) if len(p.sites) == 2 else (p.sites[0] - 1)
+            q.strength = p.strength
+            m = _c64(p.matrix)
+            for e in range(m.size):
+                q.matrix[e] = m[e]
+            q.pauli_name = int(is_pauli_name(p.name))
+            q.pauli_proc = int(is_pauli_matrix(p.matrix) if len(p.sites) == 1 else is_pauli_proc(p.name, p.matrix))
+        self._keep.append(arr)
+        self.noise = A.NoiseDesc(int(noise_model is not None), len(procs), arr)
+        self.all_zero = all(p.strength == 0 for p in procs)
+        # observables
+        obs = sim_params.observables
+        oarr = (A.ObsDesc * max(1, len(obs)))()
+        for k, o in enumerate(obs):
+            d = oarr[k]
+            if o.kind == "entropy":
+                d.kind = A.YAQS_OBS_ENTROPY
+                d.site[0] = d.site[1] = o.sites[0] - 1
+            elif len(o.sites) == 1:
+                d.kind = A.YAQS_OBS_LOCAL1
+                d.site[0] = d.site[1] = o.sites[0] - 1
+            elif len(o.sites) == 2:
+                s1, s2 = sorted(o.sites)
+                if s2 != s1 + 1:
+                    raise ValueError("Only nearest neighbor supported efficiently")  # MPS.jl:627
+                d.kind = A.YAQS_OBS_LOCAL2
+                d.site[0], d.site[1] = s1 - 1, s2 - 1
+            else:
+                raise ValueError("Only 1 or 2 site observables supported")
+            if o.op is not None:
+                m = _c64(o.op)
+                for e in range(m.size):
+                    d.matrix[e] = m[e]
+        self._keep.append(oarr)
+        self.obs = oarr
+        self.n_obs = len(obs)
+        # config
+        nt = sim_params.num_traj if num_traj is None else num_traj
+        self.cfg = A.TevConfig(sim_params.dt, len(sim_params.times), nt, sim_params.max_bond_dim,
+                               sim_params.truncation_threshold, sim_params.order,
+                               int(sim_params.sample_timesteps), krylov_dim, krylov_tol, krylov_exit_tol,
+                               precision, traj_offset)
+        self.n_out = len(sim_params.times) if sim_params.sample_timesteps else 1
+        # rng
+        if rng_mode == A.YAQS_RNG_INJECTED:
+            u = np.ascontiguousarray(uniforms, dtype=np.float64)
+            if u.ndim != 2 or u.shape[0] < nt:
+                raise ValueError("uniforms must be [num_traj, stride]")
+            self._keep.append(u)
+            self.rng = A.RngDesc(rng_mode, seed, A.dptr(u), u.shape[1])
+        else:
+            self.rng = A.RngDesc(rng_mode, seed, None, 0)
+        self.num_traj = nt
+
+
+def max_draws(sim_params: TimeEvolutionConfig) -> int:
+    """Upper bound on uniforms one trajectory consumes (2 per stochastic step)."""
+    n = len(sim_params.times)
+    steps = (2 * n - 2) if sim_params.order == 2 else (n - 1)
+    return 2 * max(steps, 1)
