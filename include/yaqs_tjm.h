@@ -187,6 +187,28 @@ int yaqs_analog_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0,
                     double* traj_out, double* mean_out, int32_t* maxchi_out,
                     yaqs_run_stats* stats);
 
+/*
+ * The same run in steps, for callers that interleave other work or time
+ * individual time indices.  yaqs_analog_begin validates the descriptors,
+ * copies every input to the device and sizes the workspaces; nothing is
+ * evolved yet.  yaqs_analog_advance runs the next n recorded time indices
+ * (the first one also performs the t = 0 measurement and the initial
+ * half-step, AnalogTJM.jl:114-126) and waits for them; *device_ms receives
+ * their device time.  yaqs_analog_remaining tells how many are left.
+ * yaqs_analog_finish copies the outputs back (as yaqs_analog_run) and frees
+ * the run; it must be called exactly once, also after an error.
+ */
+typedef struct yaqs_run yaqs_run;
+int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0,
+                      const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                      const yaqs_obs_desc* obs, int32_t n_obs,
+                      const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                      yaqs_run** out);
+int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms);
+int yaqs_analog_remaining(const yaqs_run* run);
+int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out,
+                       int32_t* maxchi_out, yaqs_run_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,53 @@
+/*
+ * yaqs_tjm_components.h — batched device kernels of the TJM engine exposed
+ * one at a time.  Each runs one CTA per problem of the batch, on host
+ * buffers (copied in and out), with the same device code the trajectory
+ * engine uses.  Layouts are column-major interleaved complex, as in
+ * yaqs_tjm.h.  They replace, one for one, the reference's per-call numerics:
+ *
+ *   yaqs_batched_svd          svd(Mat) in split_mps_tensor_svd
+ *                             (src/Algorithms.jl:409-445), thin factors,
+ *                             singular values descending.
+ *   yaqs_batched_qr           qr(Mat) of right_qr / shift_orthogonality_center!
+ *                             (src/Decompositions.jl:18-36, src/MPS.jl:197-202).
+ *   yaqs_batched_project_site project_site / _project_site_ws!
+ *                             (src/Algorithms.jl:215-220, :330-361).
+ *   yaqs_batched_expm_site    expm_krylov(project_site, x, dt, 25)
+ *                             (src/Algorithms.jl:144-187).
+ */
+#ifndef YAQS_TJM_COMPONENTS_H
+#define YAQS_TJM_COMPONENTS_H
+
+#include <stdint.h>
+
+#include "yaqs_tjm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* M: batch x (m x n); U: batch x (m x k); S: batch x k; Vt: batch x (k x n); k = min(m, n) <= 256. */
+int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* U,
+                     double* S, double* Vt);
+
+/* M: batch x (m x n); Q: batch x (m x k); R: batch x (k x n). */
+int yaqs_batched_qr(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* Q,
+                    double* R);
+
+/* L: batch x (chil, wl, chil); R: batch x (chir, wr, chir); W: (wl, D, D, wr) shared;
+ * x, out: batch x (chil, D, chir).  D is 2 (one site) or 4 (two merged sites). */
+int yaqs_batched_project_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, int32_t chir,
+                              int32_t wl, int32_t wr, const double* L, const double* R, const double* W,
+                              const double* x, double* out);
+
+/* out = exp(-i dt H_eff) x; matvecs (optional) receives the Lanczos length per problem. */
+int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, int32_t chir,
+                           int32_t wl, int32_t wr, const double* L, const double* R, const double* W,
+                           const double* x, double dt, int32_t krylov_dim, double krylov_tol,
+                           double krylov_exit_tol, double* out, int32_t* matvecs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YAQS_TJM_COMPONENTS_H */

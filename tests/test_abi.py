@@ -1,0 +1,73 @@
+"""The C-ABI library builds, loads and exports every declared symbol (CPU only, no device calls)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"^\s*(?:int|const char\*|double)\s+(yaqs_\w+)\s*\(", src, flags=re.M))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    assert {"yaqs_analog_run", "yaqs_ctx_create", "yaqs_batched_svd", "yaqs_batched_expm_site"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    from yaqs_julia_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("engine not built")
+    lib = C.CDLL(_lib.LIB_PATH)
+    for n in sorted(_declared()):
+        assert hasattr(lib, n), n
+    assert b"sm_100a" in _lib.lib().yaqs_version()
+
+
+def test_abi_struct_layouts_match_header(tmp_path):
+    """ctypes mirrors match the C compiler's sizeof/offsetof for every struct."""
+    import shutil
+    import subprocess
+    from yaqs_julia_b200 import _abi as A
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    structs = {"yaqs_mps_desc": A.MpsDesc, "yaqs_mpo_desc": A.MpoDesc, "yaqs_noise_proc": A.NoiseProc,
+               "yaqs_noise_desc": A.NoiseDesc, "yaqs_obs_desc": A.ObsDesc, "yaqs_rng_desc": A.RngDesc,
+               "yaqs_tev_config": A.TevConfig, "yaqs_run_stats": A.RunStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "yaqs_tjm.h"', "int main(void){"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split("\n")
+               if line)
+    for cname, py in structs.items():
+        assert int(out[cname]) == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(out[f"{cname}.{f}"]) == getattr(py, f).offset, (cname, f)
+
+
+def test_descriptor_validation_host_side():
+    from yaqs_julia_b200 import api
+    with pytest.raises(NotImplementedError):
+        api.NoiseModel([{"name": "pauli_z", "sites": [1, 3], "strength": 0.1}], 4)
+    with pytest.raises(ValueError):
+        H = api.init_ising(4, 1, 1)
+        cfg = api.TimeEvolutionConfig([api.Observable("zz", np.kron(api.Z, api.Z), [1, 3])], 1.0)
+        api.Descriptors(api.MPS(4), H, cfg, None)
+
+
+import numpy as np  # noqa: E402

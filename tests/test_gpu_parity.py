@@ -1,0 +1,180 @@
+"""CUDA engine vs the CPU oracle, through the C-ABI (needs a B200)."""
+import numpy as np
+import pytest
+
+from yaqs_julia_b200 import _abi as A
+from yaqs_julia_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from yaqs_julia_b200 import _lib
+    return _lib.default_context()
+
+
+def _rand(rng, *shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def _f(a):
+    return np.asfortranarray(a, dtype=np.complex128).reshape(-1, order="F").view(np.float64)
+
+
+@pytest.mark.parametrize("m,n,rank", [(2, 2, 2), (4, 16, 4), (16, 4, 4), (33, 20, 20), (64, 64, 64),
+                                      (128, 128, 128), (12, 12, 3), (128, 64, 64)])
+def test_svd_matches_oracle(ctx, oracle, m, n, rank):
+    rng = np.random.default_rng(m * 1000 + n + rank)
+    batch = 3
+    Ms = [(_rand(rng, m, rank) @ _rand(rng, rank, n)) for _ in range(batch)]
+    k = min(m, n)
+    U = np.zeros(batch * m * k * 2)
+    S = np.zeros(batch * k)
+    Vt = np.zeros(batch * k * n * 2)
+    Mb = np.concatenate([_f(M) for M in Ms])
+    ctx.check(ctx._lib.yaqs_batched_svd(ctx.handle, batch, m, n, A.dptr(Mb), A.dptr(U), A.dptr(S), A.dptr(Vt)))
+    U = U.view(np.complex128).reshape(batch, k, m).transpose(0, 2, 1)
+    Vt = Vt.view(np.complex128).reshape(batch, n, k).transpose(0, 2, 1)
+    S = S.reshape(batch, k)
+    for b, M in enumerate(Ms):
+        Uo, So, Vto = oracle.svd(M)
+        scale = np.abs(M).max()
+        assert np.abs(S[b] - So).max() < 1e-12 * scale * max(m, n)
+        assert np.abs(U[b] @ np.diag(S[b]) @ Vt[b] - M).max() < 1e-11 * scale * max(m, n)
+        assert np.abs(U[b].conj().T @ U[b] - np.eye(k)).max() < 1e-12 * max(m, n)
+        assert np.abs(Vt[b] @ Vt[b].conj().T - np.eye(k)).max() < 1e-12 * max(m, n)
+        # same gauge as the oracle for well separated singular values
+        gap_ok = [j for j in range(min(rank, k)) if all(abs(So[j] - So[i]) > 1e-6 * So[0] for i in range(k) if i != j)]
+        for j in gap_ok:
+            assert np.abs(U[b][:, j] - Uo[:, j]).max() < 1e-9
+            assert np.abs(Vt[b][j] - Vto[j]).max() < 1e-9
+
+
+@pytest.mark.parametrize("m,n", [(4, 2), (2, 4), (128, 64), (64, 128), (7, 7)])
+def test_qr_matches_oracle(ctx, oracle, m, n):
+    rng = np.random.default_rng(m + 31 * n)
+    M = _rand(rng, m, n)
+    k = min(m, n)
+    Q = np.zeros(m * k * 2)
+    R = np.zeros(k * n * 2)
+    ctx.check(ctx._lib.yaqs_batched_qr(ctx.handle, 1, m, n, A.dptr(_f(M)), A.dptr(Q), A.dptr(R)))
+    Q = Q.view(np.complex128).reshape(k, m).T
+    R = R.view(np.complex128).reshape(n, k).T
+    Qo, Ro = oracle.qr(M)
+    assert np.abs(Q - Qo).max() < 1e-12 * max(m, n)
+    assert np.abs(R - Ro).max() < 1e-12 * max(m, n) * np.abs(M).max()
+
+
+def _herm_env(rng, chi, w):
+    E = _rand(rng, chi, w, chi)
+    return E + E.transpose(2, 1, 0).conj()
+
+
+@pytest.mark.parametrize("chil,D,chir,wl,wr", [(1, 2, 1, 1, 3), (3, 2, 5, 3, 3), (8, 4, 8, 5, 5), (16, 4, 9, 3, 3),
+                                               (33, 2, 17, 5, 5), (64, 4, 64, 5, 5)])
+def test_project_site_and_expm_match_oracle(ctx, oracle, chil, D, chir, wl, wr):
+    rng = np.random.default_rng(chil * 7 + chir + D)
+    Lh = _herm_env(rng, chil, wl)
+    Rh = _herm_env(rng, chir, wr)
+    W = _rand(rng, wl, D, D, wr)
+    W = W + W.transpose(0, 2, 1, 3).conj()
+    x = _rand(rng, chil, D, chir)
+    n = chil * D * chir
+    out = np.zeros(2 * n)
+    ctx.check(ctx._lib.yaqs_batched_project_site(ctx.handle, 1, chil, D, chir, wl, wr, A.dptr(_f(Lh)),
+                                                 A.dptr(_f(Rh)), A.dptr(_f(W)), A.dptr(_f(x)), A.dptr(out)))
+    ref = oracle.project_site(Lh, Rh, W, x).reshape(-1, order="F")
+    got = out.view(np.complex128)
+    assert np.abs(got - ref).max() < 1e-12 * np.abs(ref).max()
+    for dt, ex in ((0.01, 0.0), (0.025, 1e-12), (-0.05, 1e-12)):
+        import ctypes as C
+        mv = C.c_int32(0)
+        ctx.check(ctx._lib.yaqs_batched_expm_site(ctx.handle, 1, chil, D, chir, wl, wr, A.dptr(_f(Lh)),
+                                                  A.dptr(_f(Rh)), A.dptr(_f(W)), A.dptr(_f(x)), dt, 25, 1e-10, ex,
+                                                  A.dptr(out), C.byref(mv)))
+        ref, mvo = oracle.expm_site(Lh, Rh, W, x, dt, exit_tol=ex)
+        ref = ref.reshape(-1, order="F")
+        assert mv.value == mvo
+        assert np.abs(out.view(np.complex128) - ref).max() < 1e-11 * np.abs(ref).max()
+
+
+def _cfg1(L=6, num_traj=6, T=1.0, dt=0.1, chi=16, thr=1e-10, order=2, state="zeros"):
+    H = api.init_ising(L, 1.0, 0.5)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, T, dt=dt, num_traj=num_traj, max_bond_dim=chi, truncation_threshold=thr,
+                                  order=order)
+    nm = api.NoiseModel([{"name": "lowering", "sites": [i], "strength": 0.1} for i in range(1, L + 1)] +
+                        [{"name": "pauli_z", "sites": [i], "strength": 0.1} for i in range(1, L + 1)], L)
+    return api.MPS(L, state=state), H, cfg, nm
+
+
+def _compare(oracle, psi, H, cfg, nm, uniforms=None, seed=7, rtol=1e-10):
+    mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
+    d = api.Descriptors(psi, H, cfg, nm, rng_mode=mode, seed=seed, uniforms=uniforms)
+    ref, chi_ref, st_ref = oracle.analog_run(d)
+    got = api.run_descriptors(d)
+    err = np.abs(got.trajectories - ref)
+    assert err.max() <= rtol * max(1.0, np.abs(ref).max()), err.max()
+    assert np.array_equal(got.max_bond, chi_ref)
+    assert got.stats["jumps"] == st_ref["jumps"]
+    return got, ref
+
+
+def test_noiseless_tdvp_matches_oracle(oracle):
+    psi, H, cfg, _ = _cfg1(num_traj=1, T=2.0, dt=0.05)
+    _compare(oracle, psi, H, cfg, None)
+
+
+@pytest.mark.parametrize("order", [2, 1])
+def test_trajectories_with_injected_draws_match_oracle(oracle, order):
+    psi, H, cfg, nm = _cfg1(num_traj=8, T=1.0, order=order)
+    u = np.random.default_rng(11).random((8, api.max_draws(cfg)))
+    got, _ = _compare(oracle, psi, H, cfg, nm, uniforms=u)
+    assert got.stats["jumps"] > 0
+
+
+def test_trajectories_with_philox_draws_match_oracle(oracle):
+    psi, H, cfg, nm = _cfg1(num_traj=6, T=0.6)
+    _compare(oracle, psi, H, cfg, nm, seed=0xC0FFEE01)
+
+
+def test_heisenberg_neel_dephasing_entropy_and_two_site(oracle):
+    L = 10
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = ([api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)] +
+           [api.Observable("S_half", None, L // 2, kind="entropy"),
+            api.Observable("ZZ45", np.kron(api.Z, api.Z), [4, 5])])
+    cfg = api.TimeEvolutionConfig(obs, 0.5, dt=0.05, num_traj=4, max_bond_dim=16)
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    _compare(oracle, api.MPS(L, state="Neel"), H, cfg, nm, seed=3)
+
+
+def test_two_site_noise_processes(oracle):
+    L = 5
+    H = api.init_ising(L, 1.0, 0.7)
+    obs = [api.Observable(f"X{i}", api.X, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.4, dt=0.1, num_traj=5, max_bond_dim=8)
+    nm = api.NoiseModel([{"name": "crosstalk_xz", "sites": [2, 3], "strength": 0.3},
+                         {"name": "lowering_two", "sites": [3, 4], "strength": 0.5},
+                         {"name": "raising", "sites": [1], "strength": 0.2}], L)
+    u = np.random.default_rng(2).random((5, api.max_draws(cfg)))
+    _compare(oracle, api.MPS(L, state="x+"), H, cfg, nm, uniforms=u)
+
+
+def test_rng_exhaustion_reports_status(oracle):
+    psi, H, cfg, nm = _cfg1(num_traj=2, T=0.5)
+    u = np.random.default_rng(0).random((2, 1))
+    d = api.Descriptors(psi, H, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=u)
+    from yaqs_julia_b200._lib import EngineError
+    with pytest.raises(EngineError, match="YAQS_E_RNG"):
+        api.run_descriptors(d)
+
+
+def test_run_fills_observables_like_reference():
+    psi, H, cfg, nm = _cfg1(num_traj=4, T=0.3)
+    res = api.run(psi, H, cfg, nm, seed=5)
+    for k, o in enumerate(cfg.observables):
+        assert o.trajectories.shape == (4, len(cfg.times))
+        assert np.allclose(o.results, res.trajectories[:, k, :].mean(0))
+    assert np.allclose(cfg.observables[0].trajectories[:, 0], 1.0)

@@ -449,3 +449,49 @@ def max_draws(sim_params: TimeEvolutionConfig) -> int:
     n = len(sim_params.times)
     steps = (2 * n - 2) if sim_params.order == 2 else (n - 1)
     return 2 * max(steps, 1)
+
+
+# ---------------------------------------------------------------------------
+# Simulator.run (src/Simulator.jl:22-69, 127-141) on the GPU engine
+# ---------------------------------------------------------------------------
+class RunResult:
+    def __init__(self, traj, mean, maxchi, stats):
+        self.trajectories = traj      # [num_traj, n_obs, n_out]
+        self.mean = mean              # [n_obs, n_out]
+        self.max_bond = maxchi        # [num_traj, n_out]
+        self.stats = stats
+
+
+def run_descriptors(desc: Descriptors, ctx=None) -> RunResult:
+    """Runs a packed problem through yaqs_analog_run."""
+    from . import _lib
+    ctx = ctx or _lib.default_context()
+    nt, nobs, nout = desc.num_traj, desc.n_obs, desc.n_out
+    traj = np.zeros((nt, max(nobs, 1), nout))
+    mean = np.zeros((max(nobs, 1), nout))
+    chi = np.zeros((nt, nout), dtype=np.int32)
+    st = A.RunStats()
+    ctx.check(ctx._lib.yaqs_analog_run(ctx.handle, C.byref(desc.mps), C.byref(desc.mpo), C.byref(desc.noise),
+                                       desc.obs, nobs, C.byref(desc.cfg), C.byref(desc.rng), A.dptr(traj),
+                                       A.dptr(mean), chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st)))
+    return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
+
+
+def run(initial_state: MPS, operator: MPO, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
+        *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12, ctx=None) -> RunResult:
+    """Simulator.run for an MPO (analog TJM).  Fills every observable's
+    ``trajectories`` [num_traj, n_out] and ``results`` [n_out] like
+    _run_analog.  As in the reference, a noiseless model runs one trajectory
+    and mutates ``sim_params.num_traj`` (Simulator.jl:27-29)."""
+    if not isinstance(operator, MPO):
+        raise TypeError("Simulation requires MPO (Analog).")
+    if noise_model is None or all(p.strength == 0 for p in noise_model.processes):
+        sim_params.num_traj = 1
+    mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
+    desc = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
+                       uniforms=uniforms, krylov_exit_tol=krylov_exit_tol)
+    res = run_descriptors(desc, ctx)
+    for k, o in enumerate(sim_params.observables):
+        o.trajectories = res.trajectories[:, k, :].astype(np.complex128)
+        o.results = res.mean[k].copy()
+    return res

@@ -1,0 +1,117 @@
+// common.cuh — complex FP64 helpers and CTA-collective reductions.
+//
+// Every function marked "CTA-collective" must be called by all NT threads of
+// the block with identical arguments; decisions derived from reductions are
+// broadcast through shared memory so control flow stays uniform.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define NT 256
+#define NW (NT / 32)
+
+typedef double2 cplx;
+
+__device__ __forceinline__ cplx cmk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ cplx cconj(cplx a) { return make_double2(a.x, -a.y); }
+// conj(a) * b
+__device__ __forceinline__ cplx cmulc(cplx a, cplx b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ cplx cscale(cplx a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double cabs2(cplx a) { return a.x * a.x + a.y * a.y; }
+// c += a * b
+__device__ __forceinline__ void cfma(cplx& c, cplx a, cplx b) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+}
+// c += conj(a) * b
+__device__ __forceinline__ void cfmac(cplx& c, cplx a, cplx b) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(-a.y, b.x, c.y);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Shared scratch used by the reductions (NW*16+16 doubles).
+struct RedScratch {
+  double v[NW * 16 + 16];
+};
+
+// CTA-collective sum of NV values per thread; result broadcast to every thread.
+template <int NV>
+__device__ __forceinline__ void block_sum_n(double (&x)[NV], RedScratch& rs) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) x[k] = warp_sum(x[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) rs.v[wid * NV + k] = x[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int w = 0; w < NW; ++w) s += rs.v[w * NV + threadIdx.x];
+    rs.v[NW * 16 + threadIdx.x] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) x[k] = rs.v[NW * 16 + k];
+  __syncthreads();
+}
+
+__device__ __forceinline__ double block_sum(double v, RedScratch& rs) {
+  double x[1] = {v};
+  block_sum_n<1>(x, rs);
+  return x[0];
+}
+
+__device__ __forceinline__ double block_max(double v, RedScratch& rs) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_max(v);
+  if (lane == 0) rs.v[wid] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = rs.v[0];
+    for (int w = 1; w < NW; ++w) s = fmax(s, rs.v[w]);
+    rs.v[NW * 16] = s;
+  }
+  __syncthreads();
+  v = rs.v[NW * 16];
+  __syncthreads();
+  return v;
+}
+
+// CTA-collective copy / fill helpers.
+__device__ __forceinline__ void cta_copy(cplx* __restrict__ dst, const cplx* __restrict__ src, long long n) {
+  for (long long i = threadIdx.x; i < n; i += NT) dst[i] = src[i];
+}
+__device__ __forceinline__ void cta_zero(cplx* dst, long long n) {
+  for (long long i = threadIdx.x; i < n; i += NT) dst[i] = make_double2(0.0, 0.0);
+}
+__device__ __forceinline__ void cta_scale(cplx* x, long long n, double s) {
+  for (long long i = threadIdx.x; i < n; i += NT) x[i] = cscale(x[i], s);
+}
+__device__ __forceinline__ double cta_norm2(const cplx* x, long long n, RedScratch& rs) {
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < n; i += NT) s += cabs2(x[i]);
+  return block_sum(s, rs);
+}

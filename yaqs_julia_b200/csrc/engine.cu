@@ -1,0 +1,963 @@
+// engine.cu — kernels and C-ABI of the B200 TJM trajectory engine.
+//
+// One persistent kernel launch per recorded time index.  Each CTA (256
+// threads) owns a workspace slot and pulls trajectories from an atomic queue;
+// for each it runs that trajectory's share of analog_tjm_2 / analog_tjm_1
+// (AnalogTJM.jl:21-176) entirely on the device, with the MPS of every
+// trajectory resident in HBM between launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/yaqs_tjm.h"
+#include "../../include/yaqs_tjm_components.h"
+#include "tjm.cuh"
+
+// ---------------------------------------------------------------------------
+// Device program
+// ---------------------------------------------------------------------------
+__device__ void copy_state(Ctx& c, const DState& dst, const DState& src) {
+  cta_copy(dst.a, src.a, c.P.mps_size);
+  for (int b = threadIdx.x; b <= c.P.L; b += NT) dst.chi[b] = src.chi[b];
+  if (threadIdx.x == 0) *dst.oc = *src.oc;
+  __syncthreads();
+}
+
+__device__ void sample(Ctx& c, const DState& phi, const DState& psi, int col) {
+  copy_state(c, psi, phi);
+  tdvp_sweep(c, psi);
+  if (c.sm.fail) return;
+  apply_dissipation(c, psi, false, c.P.dt / 2);
+  if (c.sm.fail) return;
+  if (c.P.noise_present) stochastic_process(c, psi, c.P.dt);
+  if (c.sm.fail) return;
+  evaluate(c, psi, col);
+}
+
+__device__ void run_step(Ctx& c, int j) {
+  const DevParams& P = c.P;
+  const int L = P.L;
+  DState phi{P.phi + (long long)c.traj * P.mps_size, P.phi_chi + (long long)c.traj * (L + 1), P.phi_oc + c.traj};
+  DState psi{c.ws + P.lay.psi, c.wsi + P.lay.i_chi, c.wsi + P.lay.i_oc};
+  if (j == 0) {
+    cta_copy(phi.a, P.psi0, P.mps_size);
+    for (int b = threadIdx.x; b <= L; b += NT) phi.chi[b] = P.chi0[b];
+    if (threadIdx.x == 0) *phi.oc = 0;
+    __syncthreads();
+    normalize_state(c, phi);  // Simulator.jl:128
+    if (P.sample_ts) evaluate(c, phi, 0);
+    if (P.order == 2) {
+      apply_dissipation(c, phi, false, P.dt / 2);  // initialize, AnalogTJM.jl:21-33
+      if (c.sm.fail) return;
+      if (P.noise_present) stochastic_process(c, phi, P.dt);
+      if (c.sm.fail) return;
+      if (P.sample_ts && P.n_times > 1) sample(c, phi, psi, 1);
+    }
+    return;
+  }
+  tdvp_sweep(c, phi);
+  if (c.sm.fail) return;
+  if (P.order == 2) {
+    apply_dissipation(c, phi, true, P.dt);  // step_through, AnalogTJM.jl:40-55
+    if (c.sm.fail) return;
+    if (P.noise_present) stochastic_process(c, phi, P.dt);
+    if (c.sm.fail) return;
+    if (P.sample_ts || j == P.n_times - 1) sample(c, phi, psi, P.sample_ts ? j : 0);
+  } else {
+    if (P.noise_present) {  // AnalogTJM.jl:160-173
+      apply_dissipation(c, phi, true, P.dt);
+      if (c.sm.fail) return;
+      stochastic_process(c, phi, P.dt);
+      if (c.sm.fail) return;
+    }
+    if (P.sample_ts)
+      evaluate(c, phi, j);
+    else if (j == P.n_times - 1)
+      evaluate(c, phi, 0);
+  }
+}
+
+__global__ void __launch_bounds__(NT, 1) tjm_step_kernel(const DevParams P, int j) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+  const int slot = blockIdx.x;
+  cplx* ws = P.ws + (long long)slot * P.lay.total;
+  int* wsi = P.wsi + (long long)slot * P.lay.itotal;
+  for (;;) {
+    if (threadIdx.x == 0) sm.bcast_i[7] = atomicAdd(&P.queue[j], 1);
+    __syncthreads();
+    const int t = sm.bcast_i[7];
+    __syncthreads();
+    if (t >= P.num_traj) break;
+    if (P.status[t] != 0) continue;
+    if (threadIdx.x == 0) sm.fail = 0;
+    __syncthreads();
+    Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
+    run_step(c, j);
+    __syncthreads();
+    if (threadIdx.x == 0 && sm.fail) P.status[t] = sm.fail;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Component kernels (one CTA per problem) used by the parity tests
+// ---------------------------------------------------------------------------
+struct CompSmem {
+  EngineSmem e;
+  LinalgSmem la;
+};
+
+__global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M, cplx* U, double* S, cplx* Vt,
+                                                    cplx* work, long long wstride, int* iwork) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
+  const int b = blockIdx.x;
+  const int k = min(m, n);
+  const long long big = (long long)max(m, n) * max(m, n);
+  cplx* w0 = work + wstride * b;
+  SvdWork w;
+  w.B = w0;
+  w.X = w0 + big;
+  w.Yo = w0 + 2 * big;
+  w.Zo = w0 + 3 * big;
+  w.y = w0 + 4 * big;
+  w.sig = reinterpret_cast<double*>(w0 + 4 * big + max(m, n));
+  w.ord = iwork + (long long)b * SVD_MAX_COLS;
+  SvdResult r = dev_svd(M + (long long)m * n * b, m, n, w, sm.la, sm.e.r);
+  dev_svd_vectors(r, k, w, sm.e.r);
+  dev_svd_write(r, w, m, n, k, U + (long long)m * k * b, false, Vt + (long long)k * n * b, false);
+  for (int e = threadIdx.x; e < k; e += NT) S[(long long)k * b + e] = w.sig[e];
+}
+
+__global__ void __launch_bounds__(NT, 1) qr_kernel(int m, int n, const cplx* M, cplx* Q, cplx* R, cplx* work) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
+  const int b = blockIdx.x;
+  const int k = min(m, n);
+  cplx* H = work + (long long)m * n * b;
+  cta_copy(H, M + (long long)m * n * b, (long long)m * n);
+  __syncthreads();
+  dev_qr_factor(H, m, n, sm.la, sm.e.r);
+  dev_qr_formq(H, m, n, Q + (long long)m * k * b, sm.la);
+  dev_qr_extract_r(H, m, n, R + (long long)k * n * b);
+}
+
+__global__ void __launch_bounds__(NT, 1) expm_kernel(int chil, int D, int chir, int wl, int wr, const cplx* Lb,
+                                                     const cplx* Rb, const WMat W, cplx* x, double dt, KrylovCfg kc,
+                                                     cplx* work, long long wstride, int* matvecs, int heff_only,
+                                                     cplx* out) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
+  const int b = blockIdx.x;
+  const long long n = (long long)chil * D * chir;
+  const long long tsz = (long long)chil * chir * max(wl, wr) * D;
+  cplx* w0 = work + wstride * b;
+  HeffOp h;
+  h.L = Lb + (long long)chil * wl * chil * b;
+  h.R = Rb + (long long)chir * wr * chir * b;
+  h.W = W;
+  h.chil = chil;
+  h.D = D;
+  h.chir = chir;
+  h.wl = wl;
+  h.wr = wr;
+  h.T1 = w0;
+  h.T2 = w0 + tsz;
+  cplx* Q = w0 + 2 * tsz;
+  cplx* xb = x + n * b;
+  if (heff_only) {
+    dev_heff(h, xb, out + n * b, sm.e);
+    return;
+  }
+  int mv = dev_expm_krylov(h, xb, dt, kc, Q, n, sm.e);
+  if (threadIdx.x == 0) matvecs[b] = mv;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+using hcd = std::complex<double>;
+
+struct yaqs_ctx {
+  int device = 0;
+  int sms = 0;
+  std::string err;
+  std::mutex mu;
+};
+
+namespace {
+
+thread_local std::string g_static_err;
+
+int set_err(yaqs_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  else g_static_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, x)                                                                  \
+  do {                                                                                    \
+    cudaError_t e_ = (x);                                                                 \
+    if (e_ != cudaSuccess) return set_err(ctx, YAQS_E_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Device allocations owned by one call; freed on scope exit.
+struct DevMem {
+  std::vector<void*> ptrs;
+  ~DevMem() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  cudaError_t alloc(T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) {
+      ptrs.push_back(q);
+      *p = reinterpret_cast<T*>(q);
+    }
+    return e;
+  }
+};
+
+// Sparse M[o, i] built from a dense lambda, in CSR.
+struct HostWMat {
+  int no = 0, ni = 0;
+  std::vector<int> rowp, col;
+  std::vector<hcd> val;
+};
+
+template <class F>
+HostWMat build_wmat(int no, int ni, F f) {
+  HostWMat m;
+  m.no = no;
+  m.ni = ni;
+  m.rowp.push_back(0);
+  for (int o = 0; o < no; ++o) {
+    for (int i = 0; i < ni; ++i) {
+      hcd v = f(o, i);
+      if (v != hcd(0.0)) {
+        m.col.push_back(i);
+        m.val.push_back(v);
+      }
+    }
+    m.rowp.push_back((int)m.col.size());
+  }
+  return m;
+}
+
+// exp(c * H) for a small Hermitian H (cyclic complex Jacobi).
+void herm_expm(int n, const hcd* Hm, double c, hcd* out) {
+  std::vector<hcd> A(Hm, Hm + n * n), V(n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + n * i] = 1.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
+        if (i != j) off += std::norm(A[i + n * j]);
+    if (off < 1e-34) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        hcd apq = A[p + n * q];
+        double ag = std::abs(apq);
+        if (ag == 0.0) continue;
+        double zeta = (A[q + n * q].real() - A[p + n * p].real()) / (2.0 * ag);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        double cc = 1.0 / std::sqrt(1.0 + t * t), s = cc * t;
+        hcd e = apq / ag;
+        for (int k = 0; k < n; ++k) {
+          hcd x = A[k + n * p], y = A[k + n * q];
+          A[k + n * p] = cc * x - s * std::conj(e) * y;
+          A[k + n * q] = s * e * x + cc * y;
+        }
+        for (int k = 0; k < n; ++k) {
+          hcd x = A[p + n * k], y = A[q + n * k];
+          A[p + n * k] = cc * x - s * e * y;
+          A[q + n * k] = s * std::conj(e) * x + cc * y;
+        }
+        for (int k = 0; k < n; ++k) {
+          hcd x = V[k + n * p], y = V[k + n * q];
+          V[k + n * p] = cc * x - s * std::conj(e) * y;
+          V[k + n * q] = s * e * x + cc * y;
+        }
+      }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      hcd sacc = 0;
+      for (int k = 0; k < n; ++k) sacc += V[i + n * k] * std::exp(c * A[k + n * k].real()) * std::conj(V[j + n * k]);
+      out[i + n * j] = sacc;
+    }
+}
+
+struct UploadedWMats {
+  std::vector<WMat> heff1, heff2, envL, envR;
+};
+
+// Copies all CSR matrices into one device buffer and fills WMat views.
+int upload_wmats(yaqs_ctx* ctx, DevMem& dm, const std::vector<HostWMat>& all, std::vector<WMat>& views) {
+  size_t nint = 0, nval = 0;
+  for (auto& m : all) {
+    nint += m.rowp.size() + m.col.size();
+    nval += m.val.size();
+  }
+  int* di = nullptr;
+  cplx* dv = nullptr;
+  CUDA_TRY(ctx, dm.alloc(&di, nint));
+  CUDA_TRY(ctx, dm.alloc(&dv, nval));
+  std::vector<int> hi;
+  std::vector<hcd> hv;
+  hi.reserve(nint);
+  hv.reserve(nval);
+  views.clear();
+  for (auto& m : all) {
+    WMat w;
+    w.no = m.no;
+    w.ni = m.ni;
+    w.nnz = (int)m.val.size();
+    w.rowp = di + hi.size();
+    hi.insert(hi.end(), m.rowp.begin(), m.rowp.end());
+    w.col = di + hi.size();
+    hi.insert(hi.end(), m.col.begin(), m.col.end());
+    w.val = dv + hv.size();
+    hv.insert(hv.end(), m.val.begin(), m.val.end());
+    views.push_back(w);
+  }
+  CUDA_TRY(ctx, cudaMemcpy(di, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(dv, hv.data(), hv.size() * sizeof(hcd), cudaMemcpyHostToDevice));
+  return YAQS_OK;
+}
+
+inline hcd cload(const double* p, size_t k) { return hcd(p[2 * k], p[2 * k + 1]); }
+
+}  // namespace
+
+// One analog run held on the device between yaqs_analog_begin and
+// yaqs_analog_finish: trajectory states, workspaces and outputs.
+struct yaqs_run {
+  yaqs_ctx* ctx = nullptr;
+  DevMem dm;
+  DevParams P;
+  int slots = 0;
+  size_t smem = 0;
+  int num_traj = 0, n_obs = 0, ncols = 0;
+  std::vector<int> launches;
+  size_t next = 0;
+  double device_ms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double* d_traj_out = nullptr;
+  int* d_chi_out = nullptr;
+  int* d_status = nullptr;
+  unsigned long long* d_counters = nullptr;
+  double* d_flops = nullptr;
+  ~yaqs_run() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" {
+
+const char* yaqs_version(void) { return "yaqs-b200 0.1.0 (sm_100a, FP64 trajectory engine)"; }
+
+int yaqs_ctx_create(int32_t device, yaqs_ctx** out) {
+  if (!out) return set_err(nullptr, YAQS_E_ARG, "null out pointer");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return set_err(nullptr, YAQS_E_CUDA, "no CUDA device visible");
+  if (device < 0 || device >= n) return set_err(nullptr, YAQS_E_ARG, "device index out of range");
+  yaqs_ctx* c = new yaqs_ctx();
+  c->device = device;
+  cudaSetDevice(device);
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  *out = c;
+  return YAQS_OK;
+}
+
+int yaqs_ctx_destroy(yaqs_ctx* ctx) {
+  delete ctx;
+  return YAQS_OK;
+}
+
+const char* yaqs_last_error(const yaqs_ctx* ctx) { return ctx ? ctx->err.c_str() : g_static_err.c_str(); }
+
+int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                      const yaqs_obs_desc* obs, int32_t n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                      yaqs_run** out) {
+  if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
+  if (!out) return set_err(ctx, YAQS_E_ARG, "null run handle");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!psi0 || !H || !cfg || !rng || (n_obs > 0 && !obs)) return set_err(ctx, YAQS_E_ARG, "null descriptor");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int L = psi0->L;
+  if (L < 2 || L > MAX_L || H->L != L) return set_err(ctx, YAQS_E_ARG, "need 2 <= L <= 256 and matching MPO length");
+  if (!psi0->chi || !psi0->tensors || !H->w || !H->tensors) return set_err(ctx, YAQS_E_ARG, "null tensor arrays");
+  if (psi0->chi[0] != 1 || psi0->chi[L] != 1 || H->w[0] != 1 || H->w[L] != 1)
+    return set_err(ctx, YAQS_E_ARG, "boundary bond dimensions must be 1");
+  for (int b = 0; b <= L; ++b) {
+    if (psi0->chi[b] < 1) return set_err(ctx, YAQS_E_ARG, "bond dimension < 1");
+    if (H->w[b] < 1 || H->w[b] > 8) return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO bond width must be in [1, 8]");
+  }
+  if (cfg->n_times < 1 || cfg->num_traj < 1 || cfg->max_bond_dim < 1 || !(cfg->dt == cfg->dt))
+    return set_err(ctx, YAQS_E_ARG, "bad config (n_times, num_traj, max_bond_dim, dt)");
+  if (cfg->krylov_dim < 1 || cfg->krylov_dim > KRYLOV_MAX) return set_err(ctx, YAQS_E_ARG, "krylov_dim must be in [1, 32]");
+  if (cfg->order != 1 && cfg->order != 2) return set_err(ctx, YAQS_E_ARG, "order must be 1 or 2");
+  if (cfg->precision != YAQS_PREC_FP64)
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "only the ComplexF64 form is served by this build");
+  if (n_obs < 0 || n_obs > MAX_OBS) return set_err(ctx, YAQS_E_ARG, "n_obs out of range");
+  if (rng->mode != YAQS_RNG_PHILOX && rng->mode != YAQS_RNG_INJECTED) return set_err(ctx, YAQS_E_ARG, "bad rng mode");
+  if (rng->mode == YAQS_RNG_INJECTED && (!rng->uniforms || rng->stride < 1))
+    return set_err(ctx, YAQS_E_ARG, "injected uniforms need a buffer and stride >= 1");
+  const int nprocs = (noise && noise->present) ? noise->n : 0;
+  if (nprocs < 0 || nprocs > MAX_PROCS || (nprocs > 0 && !noise->procs)) return set_err(ctx, YAQS_E_ARG, "bad noise descriptor");
+
+  // ---- capacities and layouts ----
+  std::vector<int> cap(L + 1), chi0(psi0->chi, psi0->chi + L + 1), w(H->w, H->w + L + 1);
+  for (int b = 0; b <= L; ++b) {
+    long long s = 1;
+    int e = std::min(b, L - b);
+    for (int k = 0; k < e && s < (1 << 20); ++k) s *= 2;
+    long long structural = std::min<long long>(s, cfg->max_bond_dim);
+    cap[b] = (int)std::max<long long>(structural, chi0[b]);
+    if (2 * cap[b] > SVD_MAX_COLS) return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
+  }
+  int capmax = *std::max_element(cap.begin(), cap.end());
+  int wmax = *std::max_element(w.begin(), w.end());
+  std::vector<long long> mps_off(L), env_off(L + 1);
+  long long mps_size = 0, env_size = 0, kry_n = 0, t_size = 0;
+  for (int i = 0; i < L; ++i) {
+    mps_off[i] = mps_size;
+    mps_size += (long long)cap[i] * 2 * cap[i + 1];
+  }
+  for (int b = 0; b <= L; ++b) {
+    env_off[b] = env_size;
+    env_size += (long long)cap[b] * cap[b] * w[b];
+  }
+  for (int i = 0; i < L; ++i) {
+    kry_n = std::max(kry_n, (long long)cap[i] * 2 * cap[i + 1]);
+    t_size = std::max(t_size, (long long)cap[i] * cap[i + 1] * 2 * std::max(w[i], w[i + 1]));
+    if (i + 2 <= L) {
+      kry_n = std::max(kry_n, (long long)cap[i] * 4 * cap[i + 2]);
+      t_size = std::max(t_size, (long long)cap[i] * cap[i + 2] * 4 * std::max(w[i], w[i + 2]));
+    }
+  }
+  const long long tmp = 4LL * capmax * capmax + 16;
+  WsLayout lay;
+  long long off = 0;
+  auto take = [&](long long n) {
+    long long o = off;
+    off += (n + 1) & ~1LL;  // keep 32-byte alignment
+    return o;
+  };
+  lay.psi = take(mps_size);
+  lay.EL = take(env_size);
+  lay.ER = take(env_size);
+  lay.Q = take((long long)(cfg->krylov_dim + 1) * kry_n);
+  lay.T1 = take(t_size);
+  lay.T2 = take(t_size);
+  lay.tA = take(tmp);
+  lay.tB = take(tmp);
+  lay.tC = take(tmp);
+  lay.th = take(kry_n);
+  lay.B = take(tmp);
+  lay.X = take(tmp);
+  lay.Yo = take(tmp);
+  lay.Zo = take(tmp);
+  lay.y = take(2 * capmax + 16);
+  lay.dbl = take((SVD_MAX_COLS + MAX_PROCS) / 2 + 8);
+  lay.total = off;
+  long long ioff = 0;
+  lay.i_chi = ioff;
+  ioff += L + 1;
+  lay.i_oc = ioff;
+  ioff += 1;
+  lay.i_ord = ioff;
+  ioff += SVD_MAX_COLS;
+  lay.i_cand = ioff;
+  ioff += MAX_PROCS;
+  lay.itotal = (ioff + 31) & ~31LL;
+
+  // ---- MPO sparse matrices (merged two-site W of Algorithms.jl:639-643) ----
+  auto Wat = [&](int i, int m, int po, int pi, int mr) {
+    return cload(H->tensors[i], (size_t)m + (size_t)w[i] * (po + 2 * (pi + 2 * (size_t)mr)));
+  };
+  std::vector<HostWMat> all;
+  for (int i = 0; i < L; ++i) {  // heff1
+    int wl = w[i], wr = w[i + 1];
+    all.push_back(build_wmat(2 * wr, wl * 2, [&](int o, int in) {
+      int pp = o % 2, mp = o / 2, m = in % wl, p = in / wl;
+      return Wat(i, m, pp, p, mp);
+    }));
+  }
+  for (int i = 0; i + 1 < L; ++i) {  // heff2 (merged)
+    int wl = w[i], wm = w[i + 1], wr = w[i + 2];
+    std::vector<hcd> G((size_t)wl * 16 * wr, 0.0);
+    for (int l = 0; l < wl; ++l)
+      for (int r = 0; r < wr; ++r)
+        for (int p1o = 0; p1o < 2; ++p1o)
+          for (int p2o = 0; p2o < 2; ++p2o)
+            for (int p1i = 0; p1i < 2; ++p1i)
+              for (int p2i = 0; p2i < 2; ++p2i) {
+                hcd s = 0;
+                for (int k = 0; k < wm; ++k) s += Wat(i, l, p1o, p1i, k) * Wat(i + 1, k, p2o, p2i, r);
+                G[l + (size_t)wl * ((p1o + 2 * p2o) + 4 * ((p1i + 2 * p2i) + 4 * (size_t)r))] = s;
+              }
+    all.push_back(build_wmat(4 * wr, wl * 4, [&](int o, int in) {
+      int pp = o % 4, mp = o / 4, m = in % wl, p = in / wl;
+      return G[m + (size_t)wl * (pp + 4 * (p + 4 * (size_t)mp))];
+    }));
+  }
+  for (int i = 0; i < L; ++i) {  // envL: M[(po + 2 m'), (ml + wl pi)]
+    int wl = w[i], wr = w[i + 1];
+    all.push_back(build_wmat(2 * wr, wl * 2, [&](int o, int in) {
+      int po = o % 2, mp = o / 2, ml = in % wl, pi = in / wl;
+      return Wat(i, ml, po, pi, mp);
+    }));
+  }
+  for (int i = 0; i < L; ++i) {  // envR: M[(po + 2 ml), (pi + 2 mr)]
+    int wl = w[i], wr = w[i + 1];
+    all.push_back(build_wmat(2 * wl, 2 * wr, [&](int o, int in) {
+      int po = o % 2, ml = o / 2, pi = in % 2, mr = in / 2;
+      return Wat(i, ml, po, pi, mr);
+    }));
+  }
+  for (auto& m : all)
+    if (m.ni > WAPPLY_MAXI || m.no > WAPPLY_MAXI || (int)m.val.size() > WAPPLY_MAXNNZ)
+      return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO too wide for the sparse MPO apply");
+
+  // ---- noise and observables ----
+  std::vector<DevProc> hp(std::max(nprocs, 1));
+  bool all_zero = true;
+  for (int k = 0; k < nprocs; ++k) {
+    const yaqs_noise_proc& q = noise->procs[k];
+    DevProc& d = hp[k];
+    memset(&d, 0, sizeof(d));
+    d.nsites = q.nsites;
+    d.s0 = q.site[0];
+    d.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
+    if (q.nsites < 1 || q.nsites > 2 || d.s0 < 0 || d.s1 >= L || (q.nsites == 2 && d.s1 != d.s0 + 1))
+      return set_err(ctx, q.nsites == 2 ? YAQS_E_UNSUPPORTED : YAQS_E_ARG,
+                     "noise processes must be 1-site or adjacent 2-site with sites in range");
+    d.gamma = q.strength;
+    d.pauli_name = q.pauli_name;
+    d.pauli_proc = q.pauli_proc;
+    if (q.strength != 0.0) all_zero = false;
+    const int dd = q.nsites == 1 ? 2 : 4;
+    hcd M[16], LdL[16], e1[16], e2[16];
+    for (int e = 0; e < dd * dd; ++e) M[e] = cload(q.matrix, e);
+    for (int i = 0; i < dd; ++i)
+      for (int j = 0; j < dd; ++j) {
+        hcd s = 0;
+        for (int kk = 0; kk < dd; ++kk) s += std::conj(M[kk + dd * i]) * M[kk + dd * j];
+        LdL[i + dd * j] = s;
+      }
+    herm_expm(dd, LdL, -0.5 * (cfg->dt / 2) * q.strength, e1);
+    herm_expm(dd, LdL, -0.5 * cfg->dt * q.strength, e2);
+    for (int e = 0; e < dd * dd; ++e) {
+      d.mat[e] = make_double2(M[e].real(), M[e].imag());
+      d.diss_half[e] = make_double2(e1[e].real(), e1[e].imag());
+      d.diss_full[e] = make_double2(e2[e].real(), e2[e].imag());
+    }
+  }
+  std::vector<DevObs> ho(std::max(n_obs, 1));
+  for (int k = 0; k < n_obs; ++k) {
+    const yaqs_obs_desc& o = obs[k];
+    DevObs& d = ho[k];
+    memset(&d, 0, sizeof(d));
+    d.kind = o.kind;
+    d.s0 = o.site[0];
+    d.s1 = o.site[1];
+    bool ok = (o.kind == YAQS_OBS_LOCAL1 && d.s0 >= 0 && d.s0 < L) ||
+              (o.kind == YAQS_OBS_LOCAL2 && d.s0 >= 0 && d.s0 + 1 < L && d.s1 == d.s0 + 1) ||
+              (o.kind == YAQS_OBS_ENTROPY && d.s0 >= 0 && d.s0 + 1 < L);
+    if (!ok) return set_err(ctx, YAQS_E_ARG, "bad observable descriptor");
+    const int dd = o.kind == YAQS_OBS_LOCAL2 ? 4 : 2;
+    for (int e = 0; e < dd * dd; ++e) d.mat[e] = make_double2(o.matrix[2 * e], o.matrix[2 * e + 1]);
+  }
+
+  // ---- slots and memory admission ----
+  const int num_traj = cfg->num_traj;
+  const int ncols = cfg->sample_timesteps ? cfg->n_times : 1;
+  const size_t smem = sizeof(CtaSmem);
+  CUDA_TRY(ctx, cudaFuncSetAttribute(tjm_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tjm_step_kernel, NT, smem));
+  if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
+  size_t free_b = 0, total_b = 0;
+  CUDA_TRY(ctx, cudaMemGetInfo(&free_b, &total_b));
+  const size_t per_traj = (size_t)mps_size * sizeof(cplx) + (L + 2) * sizeof(int) + 64 +
+                          (size_t)n_obs * ncols * sizeof(double) + ncols * sizeof(int);
+  const size_t per_slot = (size_t)lay.total * sizeof(cplx) + lay.itotal * sizeof(int) + 8 * 8 + 8;
+  const size_t fixed = (size_t)mps_size * sizeof(cplx) + (64u << 20);
+  const size_t budget = free_b > (size_t)(1u << 30) ? free_b - (size_t)(1u << 30) : 0;
+  if (fixed + (size_t)num_traj * per_traj + per_slot > budget)
+    return set_err(ctx, YAQS_E_OOM, "trajectory states do not fit in device memory");
+  int slots = std::min(num_traj, ctx->sms * per_sm);
+  while (slots > 1 && fixed + (size_t)num_traj * per_traj + (size_t)slots * per_slot > budget) --slots;
+
+  yaqs_run* run = new yaqs_run();
+  std::unique_ptr<yaqs_run> guard(run);
+  run->ctx = ctx;
+  DevMem& dm = run->dm;
+  DevParams& P = run->P;
+  memset(&P, 0, sizeof(P));
+  P.L = L;
+  P.n_times = cfg->n_times;
+  P.order = cfg->order;
+  P.sample_ts = cfg->sample_timesteps != 0;
+  P.max_bond = cfg->max_bond_dim;
+  P.nobs = n_obs;
+  P.nprocs = nprocs;
+  P.noise_present = (noise && noise->present) ? 1 : 0;
+  P.all_zero = all_zero ? 1 : 0;
+  P.rng_mode = rng->mode;
+  P.num_traj = num_traj;
+  P.traj_offset = cfg->traj_offset;
+  P.ncols = ncols;
+  P.dt = cfg->dt;
+  P.thr = cfg->truncation_threshold;
+  P.kc.kdim = cfg->krylov_dim;
+  P.kc.tol = cfg->krylov_tol;
+  P.kc.exit_tol = cfg->krylov_exit_tol;
+  P.seed = rng->seed;
+  P.stride = rng->stride;
+  P.mps_size = mps_size;
+  P.kry_n = kry_n;
+  P.lay = lay;
+
+  int *d_cap, *d_w, *d_chi0;
+  long long *d_mps_off, *d_env_off;
+  CUDA_TRY(ctx, dm.alloc(&d_cap, L + 1));
+  CUDA_TRY(ctx, dm.alloc(&d_w, L + 1));
+  CUDA_TRY(ctx, dm.alloc(&d_chi0, L + 1));
+  CUDA_TRY(ctx, dm.alloc(&d_mps_off, L));
+  CUDA_TRY(ctx, dm.alloc(&d_env_off, L + 1));
+  CUDA_TRY(ctx, cudaMemcpy(d_cap, cap.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_w, w.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_chi0, chi0.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_mps_off, mps_off.data(), L * sizeof(long long), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_env_off, env_off.data(), (L + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+  P.cap = d_cap;
+  P.w = d_w;
+  P.chi0 = d_chi0;
+  P.mps_off = d_mps_off;
+  P.env_off = d_env_off;
+
+  std::vector<WMat> views;
+  int st = upload_wmats(ctx, dm, all, views);
+  if (st != YAQS_OK) return st;
+  WMat* d_views;
+  CUDA_TRY(ctx, dm.alloc(&d_views, views.size()));
+  CUDA_TRY(ctx, cudaMemcpy(d_views, views.data(), views.size() * sizeof(WMat), cudaMemcpyHostToDevice));
+  P.wm_heff1 = d_views;
+  P.wm_heff2 = d_views + L;
+  P.wm_envL = d_views + L + (L - 1);
+  P.wm_envR = d_views + L + (L - 1) + L;
+
+  DevProc* d_procs;
+  DevObs* d_obs;
+  CUDA_TRY(ctx, dm.alloc(&d_procs, hp.size()));
+  CUDA_TRY(ctx, dm.alloc(&d_obs, ho.size()));
+  CUDA_TRY(ctx, cudaMemcpy(d_procs, hp.data(), hp.size() * sizeof(DevProc), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_obs, ho.data(), ho.size() * sizeof(DevObs), cudaMemcpyHostToDevice));
+  P.procs = d_procs;
+  P.obs = d_obs;
+
+  // initial state arena (compact tensors at the site slots)
+  std::vector<hcd> arena((size_t)mps_size, 0.0);
+  for (int i = 0; i < L; ++i) {
+    const size_t n = (size_t)chi0[i] * 2 * chi0[i + 1];
+    if (!psi0->tensors[i]) return set_err(ctx, YAQS_E_ARG, "null MPS tensor");
+    for (size_t e = 0; e < n; ++e) arena[mps_off[i] + e] = cload(psi0->tensors[i], e);
+  }
+  cplx* d_psi0;
+  CUDA_TRY(ctx, dm.alloc(&d_psi0, mps_size));
+  CUDA_TRY(ctx, cudaMemcpy(d_psi0, arena.data(), mps_size * sizeof(cplx), cudaMemcpyHostToDevice));
+  P.psi0 = d_psi0;
+
+  cplx* d_phi;
+  int *d_phi_chi, *d_phi_oc, *d_status, *d_queue, *d_chi_out, *d_wsi;
+  long long* d_rng_pos;
+  double *d_traj_out, *d_flops, *d_uniforms = nullptr;
+  unsigned long long* d_counters;
+  cplx* d_ws;
+  CUDA_TRY(ctx, dm.alloc(&d_phi, (size_t)num_traj * mps_size));
+  CUDA_TRY(ctx, dm.alloc(&d_phi_chi, (size_t)num_traj * (L + 1)));
+  CUDA_TRY(ctx, dm.alloc(&d_phi_oc, num_traj));
+  CUDA_TRY(ctx, dm.alloc(&d_status, num_traj));
+  CUDA_TRY(ctx, dm.alloc(&d_queue, cfg->n_times));
+  CUDA_TRY(ctx, dm.alloc(&d_chi_out, (size_t)num_traj * ncols));
+  CUDA_TRY(ctx, dm.alloc(&d_rng_pos, num_traj));
+  CUDA_TRY(ctx, dm.alloc(&d_traj_out, (size_t)num_traj * std::max(n_obs, 1) * ncols));
+  CUDA_TRY(ctx, dm.alloc(&d_flops, slots));
+  CUDA_TRY(ctx, dm.alloc(&d_counters, (size_t)slots * 8));
+  CUDA_TRY(ctx, dm.alloc(&d_ws, (size_t)slots * lay.total));
+  CUDA_TRY(ctx, dm.alloc(&d_wsi, (size_t)slots * lay.itotal));
+  CUDA_TRY(ctx, cudaMemset(d_status, 0, num_traj * sizeof(int)));
+  CUDA_TRY(ctx, cudaMemset(d_queue, 0, cfg->n_times * sizeof(int)));
+  CUDA_TRY(ctx, cudaMemset(d_rng_pos, 0, num_traj * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(d_traj_out, 0, (size_t)num_traj * std::max(n_obs, 1) * ncols * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(d_chi_out, 0, (size_t)num_traj * ncols * sizeof(int)));
+  CUDA_TRY(ctx, cudaMemset(d_flops, 0, slots * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(d_counters, 0, (size_t)slots * 8 * sizeof(unsigned long long)));
+  if (rng->mode == YAQS_RNG_INJECTED) {
+    CUDA_TRY(ctx, dm.alloc(&d_uniforms, (size_t)num_traj * rng->stride));
+    CUDA_TRY(ctx, cudaMemcpy(d_uniforms, rng->uniforms, (size_t)num_traj * rng->stride * sizeof(double),
+                             cudaMemcpyHostToDevice));
+  }
+  P.phi = d_phi;
+  P.phi_chi = d_phi_chi;
+  P.phi_oc = d_phi_oc;
+  P.status = d_status;
+  P.queue = d_queue;
+  P.chi_out = d_chi_out;
+  P.rng_pos = d_rng_pos;
+  P.traj_out = d_traj_out;
+  P.flops = d_flops;
+  P.counters = d_counters;
+  P.ws = d_ws;
+  P.wsi = d_wsi;
+  P.uniforms = d_uniforms;
+
+  run->slots = slots;
+  run->smem = smem;
+  run->num_traj = num_traj;
+  run->n_obs = n_obs;
+  run->ncols = ncols;
+  run->d_traj_out = d_traj_out;
+  run->d_chi_out = d_chi_out;
+  run->d_status = d_status;
+  run->d_counters = d_counters;
+  run->d_flops = d_flops;
+  run->launches.push_back(0);
+  for (int j = (cfg->order == 2 ? 2 : 1); j < cfg->n_times; ++j) run->launches.push_back(j);
+  CUDA_TRY(ctx, cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking));
+  CUDA_TRY(ctx, cudaEventCreate(&run->e0));
+  CUDA_TRY(ctx, cudaEventCreate(&run->e1));
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  *out = guard.release();
+  return YAQS_OK;
+}
+
+int yaqs_analog_remaining(const yaqs_run* run) {
+  return run ? (int)(run->launches.size() - run->next) : 0;
+}
+
+int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms) {
+  if (!run) return set_err(nullptr, YAQS_E_ARG, "null run");
+  yaqs_ctx* ctx = run->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (n < 0) return set_err(ctx, YAQS_E_ARG, "negative step count");
+  const int avail = (int)(run->launches.size() - run->next);
+  n = std::min(n, avail);
+  CUDA_TRY(ctx, cudaEventRecord(run->e0, run->stream));
+  for (int k = 0; k < n; ++k) {
+    const int j = run->launches[run->next++];
+    tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, j);
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return set_err(ctx, YAQS_E_CUDA, std::string("launch: ") + cudaGetErrorString(le));
+  }
+  CUDA_TRY(ctx, cudaEventRecord(run->e1, run->stream));
+  cudaError_t se = cudaEventSynchronize(run->e1);
+  if (se != cudaSuccess) return set_err(ctx, YAQS_E_CUDA, std::string("run: ") + cudaGetErrorString(se));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, run->e0, run->e1);
+  run->device_ms += ms;
+  if (device_ms) *device_ms = ms;
+  return YAQS_OK;
+}
+
+int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out, int32_t* maxchi_out,
+                       yaqs_run_stats* stats) {
+  if (!run) return set_err(nullptr, YAQS_E_ARG, "null run");
+  std::unique_ptr<yaqs_run> guard(run);
+  yaqs_ctx* ctx = run->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(run->stream));
+  const int num_traj = run->num_traj, n_obs = run->n_obs, ncols = run->ncols, slots = run->slots;
+  std::vector<double> out((size_t)num_traj * std::max(n_obs, 1) * ncols);
+  std::vector<int> status(num_traj);
+  CUDA_TRY(ctx, cudaMemcpy(out.data(), run->d_traj_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(status.data(), run->d_status, num_traj * sizeof(int), cudaMemcpyDeviceToHost));
+  if (maxchi_out)
+    CUDA_TRY(ctx, cudaMemcpy(maxchi_out, run->d_chi_out, (size_t)num_traj * ncols * sizeof(int), cudaMemcpyDeviceToHost));
+  if (traj_out) memcpy(traj_out, out.data(), (size_t)num_traj * n_obs * ncols * sizeof(double));
+  if (mean_out) {
+    for (int k = 0; k < n_obs; ++k)
+      for (int c = 0; c < ncols; ++c) {
+        double s = 0;
+        for (int t = 0; t < num_traj; ++t) s += out[((size_t)t * n_obs + k) * ncols + c];
+        mean_out[(size_t)k * ncols + c] = s / num_traj;
+      }
+  }
+  if (stats) {
+    std::vector<unsigned long long> cnt((size_t)slots * 8);
+    std::vector<double> fl(slots);
+    CUDA_TRY(ctx, cudaMemcpy(cnt.data(), run->d_counters, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    CUDA_TRY(ctx, cudaMemcpy(fl.data(), run->d_flops, fl.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    memset(stats, 0, sizeof(*stats));
+    for (int s = 0; s < slots; ++s) {
+      stats->matvecs += cnt[s * 8 + 0];
+      stats->krylov_solves += cnt[s * 8 + 1];
+      stats->svds += cnt[s * 8 + 2];
+      stats->jumps += cnt[s * 8 + 3];
+      stats->nonfinite_fixes += cnt[s * 8 + 4];
+      stats->flops += fl[s];
+    }
+    stats->device_ms = run->device_ms;
+  }
+  for (int t = 0; t < num_traj; ++t) {
+    if (status[t] != 0) {
+      const char* why = status[t] == ST_RNG ? "injected uniform stream exhausted"
+                        : status[t] == ST_UNSUPPORTED ? "bond dimension exceeded its planned capacity"
+                                                      : "trajectory failed";
+      return set_err(ctx, status[t], std::string(why) + " (trajectory " + std::to_string(t) + ")");
+    }
+  }
+  return YAQS_OK;
+}
+
+int yaqs_analog_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                    const yaqs_obs_desc* obs, int32_t n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                    double* traj_out, double* mean_out, int32_t* maxchi_out, yaqs_run_stats* stats) {
+  yaqs_run* run = nullptr;
+  int st = yaqs_analog_begin(ctx, psi0, H, noise, obs, n_obs, cfg, rng, &run);
+  if (st != YAQS_OK) return st;
+  st = yaqs_analog_advance(run, yaqs_analog_remaining(run), nullptr);
+  if (st != YAQS_OK) {
+    yaqs_analog_finish(run, nullptr, nullptr, nullptr, nullptr);
+    return st;
+  }
+  return yaqs_analog_finish(run, traj_out, mean_out, maxchi_out, stats);
+}
+
+// ---- component entry points ----
+int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* U, double* S,
+                     double* Vt) {
+  if (!ctx || batch < 1 || m < 1 || n < 1 || std::min(m, n) > SVD_MAX_COLS || !M || !U || !S || !Vt)
+    return set_err(ctx, YAQS_E_ARG, "bad svd arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int k = std::min(m, n);
+  const long long big = (long long)std::max(m, n) * std::max(m, n);
+  const long long wstride = 4 * big + std::max(m, n) + SVD_MAX_COLS;
+  DevMem dm;
+  cplx *dM, *dU, *dVt, *dw;
+  double* dS;
+  int* di;
+  CUDA_TRY(ctx, dm.alloc(&dM, (size_t)batch * m * n));
+  CUDA_TRY(ctx, dm.alloc(&dU, (size_t)batch * m * k));
+  CUDA_TRY(ctx, dm.alloc(&dVt, (size_t)batch * k * n));
+  CUDA_TRY(ctx, dm.alloc(&dS, (size_t)batch * k));
+  CUDA_TRY(ctx, dm.alloc(&dw, (size_t)batch * wstride));
+  CUDA_TRY(ctx, dm.alloc(&di, (size_t)batch * SVD_MAX_COLS));
+  CUDA_TRY(ctx, cudaMemcpy(dM, M, (size_t)batch * m * n * sizeof(cplx), cudaMemcpyHostToDevice));
+  const size_t smem = sizeof(CompSmem);
+  CUDA_TRY(ctx, cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  svd_kernel<<<batch, NT, smem>>>(m, n, dM, dU, dS, dVt, dw, wstride, di);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  CUDA_TRY(ctx, cudaMemcpy(U, dU, (size_t)batch * m * k * sizeof(cplx), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(Vt, dVt, (size_t)batch * k * n * sizeof(cplx), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(S, dS, (size_t)batch * k * sizeof(double), cudaMemcpyDeviceToHost));
+  return YAQS_OK;
+}
+
+int yaqs_batched_qr(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* Q, double* R) {
+  if (!ctx || batch < 1 || m < 1 || n < 1 || std::min(m, n) > SVD_MAX_COLS || !M || !Q || !R)
+    return set_err(ctx, YAQS_E_ARG, "bad qr arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int k = std::min(m, n);
+  DevMem dm;
+  cplx *dM, *dQ, *dR, *dw;
+  CUDA_TRY(ctx, dm.alloc(&dM, (size_t)batch * m * n));
+  CUDA_TRY(ctx, dm.alloc(&dQ, (size_t)batch * m * k));
+  CUDA_TRY(ctx, dm.alloc(&dR, (size_t)batch * k * n));
+  CUDA_TRY(ctx, dm.alloc(&dw, (size_t)batch * m * n));
+  CUDA_TRY(ctx, cudaMemcpy(dM, M, (size_t)batch * m * n * sizeof(cplx), cudaMemcpyHostToDevice));
+  const size_t smem = sizeof(CompSmem);
+  CUDA_TRY(ctx, cudaFuncSetAttribute(qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  qr_kernel<<<batch, NT, smem>>>(m, n, dM, dQ, dR, dw);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  CUDA_TRY(ctx, cudaMemcpy(Q, dQ, (size_t)batch * m * k * sizeof(cplx), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(R, dR, (size_t)batch * k * n * sizeof(cplx), cudaMemcpyDeviceToHost));
+  return YAQS_OK;
+}
+
+static int expm_common(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, int32_t chir, int32_t wl, int32_t wr,
+                       const double* Lh, const double* Rh, const double* Wh, const double* x, double dt,
+                       int32_t kdim, double tol, double exit_tol, double* out, int32_t* matvecs, int heff_only) {
+  if (!ctx || batch < 1 || chil < 1 || chir < 1 || (D != 2 && D != 4) || wl < 1 || wr < 1 || wl * D > WAPPLY_MAXI ||
+      wr * D > WAPPLY_MAXI || kdim < 1 || kdim > KRYLOV_MAX || !Lh || !Rh || !Wh || !x || !out)
+    return set_err(ctx, YAQS_E_ARG, "bad expm arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const long long n = (long long)chil * D * chir;
+  const long long tsz = (long long)chil * chir * std::max(wl, wr) * D;
+  const long long wstride = 2 * tsz + (long long)(kdim + 1) * n;
+  HostWMat hm = build_wmat(D * wr, wl * D, [&](int o, int in) {
+    int pp = o % D, mp = o / D, m = in % wl, p = in / wl;
+    return cload(Wh, (size_t)m + (size_t)wl * (pp + D * (p + D * (size_t)mp)));
+  });
+  if ((int)hm.val.size() > WAPPLY_MAXNNZ) return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO too dense");
+  DevMem dm;
+  std::vector<WMat> views;
+  int st = upload_wmats(ctx, dm, {hm}, views);
+  if (st != YAQS_OK) return st;
+  cplx *dL, *dR, *dx, *dw, *dout;
+  int* dmv;
+  CUDA_TRY(ctx, dm.alloc(&dL, (size_t)batch * chil * wl * chil));
+  CUDA_TRY(ctx, dm.alloc(&dR, (size_t)batch * chir * wr * chir));
+  CUDA_TRY(ctx, dm.alloc(&dx, (size_t)batch * n));
+  CUDA_TRY(ctx, dm.alloc(&dout, (size_t)batch * n));
+  CUDA_TRY(ctx, dm.alloc(&dw, (size_t)batch * wstride));
+  CUDA_TRY(ctx, dm.alloc(&dmv, batch));
+  CUDA_TRY(ctx, cudaMemcpy(dL, Lh, (size_t)batch * chil * wl * chil * sizeof(cplx), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(dR, Rh, (size_t)batch * chir * wr * chir * sizeof(cplx), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(dx, x, (size_t)batch * n * sizeof(cplx), cudaMemcpyHostToDevice));
+  KrylovCfg kc;
+  kc.kdim = kdim;
+  kc.tol = tol;
+  kc.exit_tol = exit_tol;
+  const size_t smem = sizeof(CompSmem);
+  CUDA_TRY(ctx, cudaFuncSetAttribute(expm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  expm_kernel<<<batch, NT, smem>>>(chil, D, chir, wl, wr, dL, dR, views[0], dx, dt, kc, dw, wstride, dmv, heff_only,
+                                   dout);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  CUDA_TRY(ctx, cudaMemcpy(out, heff_only ? dout : dx, (size_t)batch * n * sizeof(cplx), cudaMemcpyDeviceToHost));
+  if (matvecs && !heff_only) CUDA_TRY(ctx, cudaMemcpy(matvecs, dmv, batch * sizeof(int), cudaMemcpyDeviceToHost));
+  return YAQS_OK;
+}
+
+int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, int32_t chir, int32_t wl, int32_t wr,
+                           const double* L, const double* R, const double* W, const double* x, double dt,
+                           int32_t krylov_dim, double krylov_tol, double krylov_exit_tol, double* out,
+                           int32_t* matvecs) {
+  return expm_common(ctx, batch, chil, D, chir, wl, wr, L, R, W, x, dt, krylov_dim, krylov_tol, krylov_exit_tol, out,
+                     matvecs, 0);
+}
+
+int yaqs_batched_project_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, int32_t chir, int32_t wl,
+                              int32_t wr, const double* L, const double* R, const double* W, const double* x,
+                              double* out) {
+  return expm_common(ctx, batch, chil, D, chir, wl, wr, L, R, W, x, 0.0, 1, 0.0, 0.0, out, nullptr, 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,244 @@
+// krylov.cuh — effective-Hamiltonian product and Lanczos exponential.
+//
+// dev_heff restates project_site (Algorithms.jl:215-220, :330-361):
+//   T1[a,m,p,c]   = sum_k L[a,m,k] x[k,p,c]                    (GEMM)
+//   T2[a,p',m',c] = sum_{m,p} W[m,p',p,m'] T1[a,m,p,c]         (sparse MPO apply)
+//   y[a,p',b]     = sum_{m',c} T2[a,p',m',c] R[b,m',c]         (GEMM)
+// dev_expm_krylov restates expm_krylov (Algorithms.jl:144-187) / KrylovKit
+// exponentiate: Lanczos with two-pass classical Gram-Schmidt against the
+// whole basis, stopping at krylov_dim, at breakdown (beta <= |dt| tol), or
+// once prod(beta_i |dt|)/k! <= exit_tol; the small tridiagonal exponential
+// is taken on one warp by Taylor series over substeps of norm <= 1/2.
+#pragma once
+#include "common.cuh"
+#include "gemm.cuh"
+
+#define WAPPLY_PT 64
+#define WAPPLY_MAXI 32
+#define WAPPLY_MAXNNZ 1024
+#define KRYLOV_MAX 32
+
+// Sparse MPO matrix M[o, i] in CSR form (rows are outputs).
+struct WMat {
+  int no, ni, nnz;
+  const int* rowp;  // no+1
+  const int* col;   // nnz
+  const cplx* val;  // nnz
+};
+
+struct WApplyGeom {
+  int n0, n1;
+  long long is0, is1, ii1, ii2;
+  int ni1;
+  long long os0, os1, oo1, oo2;
+  int no1;
+};
+
+struct WApplySmem {
+  cplx in[WAPPLY_MAXI][WAPPLY_PT];
+  cplx val[WAPPLY_MAXNNZ];
+  int col[WAPPLY_MAXNNZ];
+  int rowp[WAPPLY_MAXI + 1];
+};
+
+// out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.
+__device__ __noinline__ void dev_wapply(const cplx* __restrict__ in, cplx* __restrict__ out, const WMat W,
+                                        const WApplyGeom g, WApplySmem& ws) {
+  const int tid = threadIdx.x;
+  for (int e = tid; e < W.nnz; e += NT) {
+    ws.val[e] = W.val[e];
+    ws.col[e] = W.col[e];
+  }
+  for (int e = tid; e <= W.no; e += NT) ws.rowp[e] = W.rowp[e];
+  const long long npair = (long long)g.n0 * g.n1;
+  for (long long base = 0; base < npair; base += WAPPLY_PT) {
+    __syncthreads();
+    for (int e = tid; e < WAPPLY_PT * W.ni; e += NT) {
+      int pl = e % WAPPLY_PT, i = e / WAPPLY_PT;
+      long long pair = base + pl;
+      cplx v = make_double2(0.0, 0.0);
+      if (pair < npair) {
+        long long q0 = pair % g.n0, q1 = pair / g.n0;
+        int i1 = i % g.ni1, i2 = i / g.ni1;
+        v = in[q0 * g.is0 + q1 * g.is1 + i1 * g.ii1 + i2 * g.ii2];
+      }
+      ws.in[i][pl] = v;
+    }
+    __syncthreads();
+    for (int e = tid; e < WAPPLY_PT * W.no; e += NT) {
+      int pl = e % WAPPLY_PT, o = e / WAPPLY_PT;
+      long long pair = base + pl;
+      if (pair >= npair) continue;
+      cplx acc = make_double2(0.0, 0.0);
+      for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) cfma(acc, ws.val[z], ws.in[ws.col[z]][pl]);
+      long long q0 = pair % g.n0, q1 = pair / g.n0;
+      int o1 = o % g.no1, o2 = o / g.no1;
+      out[q0 * g.os0 + q1 * g.os1 + o1 * g.oo1 + o2 * g.oo2] = acc;
+    }
+  }
+  __syncthreads();
+}
+
+struct HeffOp {
+  const cplx* L;  // (chil, wl, chil)
+  const cplx* R;  // (chir, wr, chir)
+  WMat W;         // rows p'+D m', cols m + wl p
+  int chil, D, chir, wl, wr;
+  cplx* T1;
+  cplx* T2;
+};
+
+struct KrySmem {
+  double alpha[KRYLOV_MAX + 1];
+  double beta[KRYLOV_MAX + 1];
+  cplx h[KRYLOV_MAX + 1];
+  cplx y[KRYLOV_MAX + 1];
+  int m;
+};
+
+struct EngineSmem {
+  GemmSmem g;
+  WApplySmem w;
+  RedScratch r;
+  KrySmem k;
+};
+
+// y = H_eff x.  CTA-collective.
+__device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, EngineSmem& sm) {
+  const int chil = h.chil, D = h.D, chir = h.chir, wl = h.wl, wr = h.wr;
+  cta_gemm(gemm_args(chil * wl, D * chir, chil, h.L, 1, (long long)chil * wl, x, 1, chil, h.T1, 1,
+                     (long long)chil * wl),
+           sm.g);
+  WApplyGeom g;
+  g.n0 = chil;
+  g.n1 = chir;
+  g.is0 = 1;
+  g.is1 = (long long)chil * wl * D;
+  g.ni1 = wl;
+  g.ii1 = chil;
+  g.ii2 = (long long)chil * wl;
+  g.os0 = 1;
+  g.os1 = (long long)chil * D * wr;
+  g.no1 = D;
+  g.oo1 = chil;
+  g.oo2 = (long long)chil * D;
+  dev_wapply(h.T1, h.T2, h.W, g, sm.w);
+  cta_gemm(gemm_args(chil * D, chir, wr * chir, h.T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
+                     (long long)chil * D),
+           sm.g);
+}
+
+__device__ __forceinline__ double heff_flops(int chil, int wl, int D, int chir, int wr) {
+  return 8.0 * ((double)chil * chil * wl * D * chir + (double)chil * chir * D * D * wl * wr +
+                (double)chil * D * chir * chir * wr);
+}
+
+struct KrylovCfg {
+  int kdim;
+  double tol;
+  double exit_tol;
+};
+
+// Warp 0: y = exp(-i dt T) e_1 for the m x m Lanczos matrix in ks.
+__device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
+  if (threadIdx.x >= 32) return;
+  const int j = threadIdx.x;
+  const bool on = j < m;
+  const double a = on ? ks.alpha[j] : 0.0;
+  const double bl = (on && j > 0) ? ks.beta[j - 1] : 0.0;
+  const double br = (on && j + 1 < m) ? ks.beta[j] : 0.0;
+  double rowsum = on ? fabs(a) + bl + br : 0.0;
+  const double tn = warp_max(rowsum) * fabs(dt);
+  int ns = (int)ceil(tn / 0.5);
+  if (ns < 1) ns = 1;
+  const double h = dt / ns;
+  cplx v = make_double2(j == 0 ? 1.0 : 0.0, 0.0);
+  for (int s = 0; s < ns; ++s) {
+    cplx term = v, acc = v;
+    for (int n = 1; n < 60; ++n) {
+      // term <- (-i h T) term / n
+      cplx tl = make_double2(__shfl_up_sync(0xffffffffu, term.x, 1), __shfl_up_sync(0xffffffffu, term.y, 1));
+      cplx tr = make_double2(__shfl_down_sync(0xffffffffu, term.x, 1), __shfl_down_sync(0xffffffffu, term.y, 1));
+      cplx tt = make_double2(a * term.x + bl * tl.x + br * tr.x, a * term.y + bl * tl.y + br * tr.y);
+      if (!on) tt = make_double2(0.0, 0.0);
+      // multiply by -i h / n:  (x + i y) * (-i c) = c y - i c x
+      const double c = h / n;
+      term = make_double2(c * tt.y, -c * tt.x);
+      acc = cadd(acc, term);
+      double tnorm = warp_sum(cabs2(term));
+      if (tnorm < 1e-40) break;
+    }
+    v = acc;
+  }
+  if (on) ks.y[j] = v;
+}
+
+// In place: x <- exp(-i dt H_eff) x.  Q holds kdim+1 vectors of stride qs.
+// Returns the number of H_eff products.  CTA-collective.
+__device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt, const KrylovCfg& kc, cplx* Q,
+                                            long long qs, EngineSmem& sm) {
+  const int tid = threadIdx.x;
+  const long long n = (long long)h.chil * h.D * h.chir;
+  const double beta0 = sqrt(cta_norm2(x, n, sm.r));
+  if (beta0 == 0.0) return 0;
+  const double tau = fabs(dt);
+  for (long long i = tid; i < n; i += NT) Q[i] = cscale(x[i], 1.0 / beta0);
+  __syncthreads();
+  double bound = 1.0;
+  int m = 0;
+  int mv = 0;
+  for (int k = 1; k <= kc.kdim; ++k) {
+    cplx* w = Q + qs * k;
+    dev_heff(h, Q + qs * (k - 1), w, sm);
+    ++mv;
+    double a_k = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int j0 = 0; j0 < k; j0 += 8) {
+        double d[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) d[e] = 0.0;
+        for (long long i = tid; i < n; i += NT) {
+          cplx wi = w[i];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            if (j0 + e < k) {
+              cplx p = cmulc(Q[qs * (j0 + e) + i], wi);
+              d[2 * e] += p.x;
+              d[2 * e + 1] += p.y;
+            }
+          }
+        }
+        block_sum_n<16>(d, sm.r);
+        if (tid < 8 && j0 + tid < k) sm.k.h[j0 + tid] = make_double2(d[2 * tid], d[2 * tid + 1]);
+      }
+      __syncthreads();
+      for (long long i = tid; i < n; i += NT) {
+        cplx v = w[i];
+        for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
+        w[i] = v;
+      }
+      a_k += sm.k.h[k - 1].x;
+      __syncthreads();
+    }
+    const double b_k = sqrt(cta_norm2(w, n, sm.r));
+    if (tid == 0) sm.k.alpha[k - 1] = a_k;
+    m = k;
+    if (b_k <= tau * kc.tol) break;
+    if (k == kc.kdim) break;
+    bound *= b_k * tau / k;
+    if (kc.exit_tol > 0.0 && bound <= kc.exit_tol) break;
+    if (tid == 0) sm.k.beta[k - 1] = b_k;
+    for (long long i = tid; i < n; i += NT) w[i] = cscale(w[i], 1.0 / b_k);
+    __syncthreads();
+  }
+  __syncthreads();
+  dev_tridiag_expm(m, dt, sm.k);
+  __syncthreads();
+  for (long long i = tid; i < n; i += NT) {
+    cplx v = make_double2(0.0, 0.0);
+    for (int j = 0; j < m; ++j) cfma(v, sm.k.y[j], Q[qs * j + i]);
+    x[i] = cscale(v, beta0);
+  }
+  __syncthreads();
+  return mv;
+}

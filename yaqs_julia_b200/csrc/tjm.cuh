@@ -1,0 +1,670 @@
+// tjm.cuh — per-trajectory TJM program executed by one CTA.
+//
+// Restates, for one trajectory held in HBM, the analog TJM step of
+// AnalogTJM.jl:21-176: the symmetric two-site TDVP sweep
+// (Algorithms.jl:580-819), apply_dissipation (Dissipation.jl:37-159),
+// stochastic_process! (StochasticProcess.jl:35-38, 89-330) and the
+// observables (SimulationConfigs.jl:42-56, MPS.jl:608-651), together with
+// the MPS gauge moves they rely on (MPS.jl:182-311, 528-585).
+#pragma once
+#include "common.cuh"
+#include "gemm.cuh"
+#include "krylov.cuh"
+#include "linalg.cuh"
+
+#define MAX_L 256
+#define MAX_PROCS 512
+#define MAX_OBS 512
+
+enum { OBS_LOCAL1 = 1, OBS_LOCAL2 = 2, OBS_ENTROPY = 3 };
+enum { ST_OK = 0, ST_ARG = 1, ST_NONFINITE = 3, ST_RNG = 7, ST_UNSUPPORTED = 8 };
+
+struct DevProc {
+  int nsites, s0, s1;
+  int pauli_name, pauli_proc;
+  double gamma;
+  cplx mat[16];
+  cplx diss_half[16];
+  cplx diss_full[16];
+};
+
+struct DevObs {
+  int kind, s0, s1;
+  cplx mat[16];
+};
+
+// Offsets (in cplx elements) of the parts of one slot's workspace.
+struct WsLayout {
+  long long psi, EL, ER, Q, T1, T2, tA, tB, tC, th, B, X, Yo, Zo, y, dbl;
+  long long total;
+  // int workspace (per slot)
+  long long i_chi, i_oc, i_ord, i_cand, itotal;
+};
+
+struct DevParams {
+  int L, n_times, order, sample_ts, max_bond, nobs, nprocs, noise_present, all_zero, rng_mode, num_traj,
+      traj_offset, ncols;
+  double dt, thr;
+  KrylovCfg kc;
+  unsigned long long seed;
+  long long stride;
+  const int* cap;            // [L+1]
+  const long long* mps_off;  // [L]
+  long long mps_size;
+  const int* w;              // [L+1]
+  const WMat* wm_heff1;      // [L]
+  const WMat* wm_heff2;      // [L-1]
+  const WMat* wm_envL;       // [L]
+  const WMat* wm_envR;       // [L]
+  const long long* env_off;  // [L+1]
+  long long kry_n;
+  const DevProc* procs;
+  const DevObs* obs;
+  const cplx* psi0;  // arena layout, compact tensors
+  const int* chi0;   // [L+1]
+  cplx* phi;         // [num_traj][mps_size]
+  int* phi_chi;      // [num_traj][L+1]
+  int* phi_oc;       // [num_traj]
+  cplx* ws;
+  int* wsi;
+  WsLayout lay;
+  const double* uniforms;
+  long long* rng_pos;  // [num_traj]
+  double* traj_out;    // [num_traj][nobs][ncols]
+  int* chi_out;        // [num_traj][ncols]
+  int* status;         // [num_traj]
+  unsigned long long* counters;  // [num_slots][8]
+  double* flops;                 // [num_slots]
+  int* queue;                    // [n_times]
+};
+
+struct CtaSmem {
+  EngineSmem e;
+  LinalgSmem la;
+  int bcast_i[8];
+  double bcast_d[8];
+  int fail;
+};
+
+struct Ctx {  // per-CTA view
+  const DevParams& P;
+  CtaSmem& sm;
+  cplx* ws;
+  int* wsi;
+  int slot;
+  int traj;
+  unsigned long long* cnt;
+  double* fl;
+};
+
+struct DState {
+  cplx* a;
+  int* chi;
+  int* oc;
+};
+
+__device__ __forceinline__ cplx* site_ptr(const Ctx& c, const DState& s, int i) { return s.a + c.P.mps_off[i]; }
+
+// ---------------------------------------------------------------------------
+// Philox-4x32-10 (Salmon et al., SC'11), one 53-bit double per counter.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double philox_uniform(unsigned long long seed, unsigned long long stream,
+                                                 unsigned long long draw) {
+  unsigned int c0 = (unsigned int)draw, c1 = (unsigned int)(draw >> 32), c2 = (unsigned int)stream,
+               c3 = (unsigned int)(stream >> 32);
+  unsigned int k0 = (unsigned int)seed, k1 = (unsigned int)(seed >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    unsigned int hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    unsigned int hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    unsigned int n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+    c0 = n0;
+    c1 = n1;
+    c2 = n2;
+    c3 = n3;
+    if (r < 9) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+  }
+  unsigned long long bits = ((unsigned long long)c1 << 32) | c0;
+  return (double)(bits >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Next uniform of this trajectory (CTA-collective; broadcast).
+__device__ double draw_uniform(Ctx& c) {
+  if (threadIdx.x == 0) {
+    long long pos = c.P.rng_pos[c.traj];
+    double u;
+    if (c.P.rng_mode == 1) {
+      if (pos >= c.P.stride) {
+        u = 1.0;
+        c.sm.fail = ST_RNG;
+      } else {
+        u = c.P.uniforms[(long long)c.traj * c.P.stride + pos];
+      }
+    } else {
+      u = philox_uniform(c.P.seed, (unsigned long long)(c.P.traj_offset + c.traj), (unsigned long long)pos);
+    }
+    c.P.rng_pos[c.traj] = pos + 1;
+    c.sm.bcast_d[0] = u;
+  }
+  __syncthreads();
+  double u = c.sm.bcast_d[0];
+  __syncthreads();
+  return u;
+}
+
+// ---------------------------------------------------------------------------
+// Gauge moves (MPS.jl:182-311)
+// ---------------------------------------------------------------------------
+__device__ void set_chi(Ctx& c, const DState& s, int b, int v) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (v > c.P.cap[b]) c.sm.fail = ST_UNSUPPORTED;
+    else s.chi[b] = v;
+  }
+  __syncthreads();
+}
+
+// site i: A = Q R, Q -> site i, R absorbed into site i+1.
+__device__ void qr_right(Ctx& c, const DState& s, int i) {
+  const int l = s.chi[i], r = s.chi[i + 1], m = 2 * l, rn = min(m, r);
+  const int r2 = s.chi[i + 2];
+  cplx* A = site_ptr(c, s, i);
+  cplx* An = site_ptr(c, s, i + 1);
+  cplx* H = c.ws + c.P.lay.tA;
+  cplx* Rb = c.ws + c.P.lay.tB;
+  cplx* T = c.ws + c.P.lay.tC;
+  cta_copy(H, A, (long long)m * r);
+  __syncthreads();
+  dev_qr_factor(H, m, r, c.sm.la, c.sm.e.r);
+  dev_qr_formq(H, m, r, A, c.sm.la);
+  dev_qr_extract_r(H, m, r, Rb);
+  cta_gemm(gemm_args(rn, 2 * r2, r, Rb, 1, rn, An, 1, r, T, 1, rn), c.sm.e.g);
+  cta_copy(An, T, (long long)rn * 2 * r2);
+  set_chi(c, s, i + 1, rn);
+}
+
+// site i: A = L Q, Q -> site i, L absorbed into site i-1.
+__device__ void lq_left(Ctx& c, const DState& s, int i) {
+  const int l = s.chi[i], r = s.chi[i + 1], n2 = 2 * r, rn = min(l, n2);
+  const int lp = s.chi[i - 1];
+  cplx* A = site_ptr(c, s, i);
+  cplx* Ap = site_ptr(c, s, i - 1);
+  cplx* H = c.ws + c.P.lay.tA;
+  cplx* Qh = c.ws + c.P.lay.tB;
+  cplx* Rb = c.ws + c.P.lay.tC;
+  for (long long e = threadIdx.x; e < (long long)n2 * l; e += NT) {
+    int cc = (int)(e % n2), ii = (int)(e / n2);
+    H[e] = cconj(A[ii + (long long)l * cc]);
+  }
+  __syncthreads();
+  dev_qr_factor(H, n2, l, c.sm.la, c.sm.e.r);
+  dev_qr_formq(H, n2, l, Qh, c.sm.la);
+  dev_qr_extract_r(H, n2, l, Rb);
+  for (long long e = threadIdx.x; e < (long long)rn * n2; e += NT) {
+    int k = (int)(e % rn), cc = (int)(e / rn);
+    A[e] = cconj(Qh[cc + (long long)n2 * k]);
+  }
+  __syncthreads();
+  cta_gemm(gemm_args(2 * lp, rn, l, Ap, 1, 2 * lp, Rb, rn, 1, H, 1, 2 * lp, false, true), c.sm.e.g);
+  cta_copy(Ap, H, (long long)2 * lp * rn);
+  set_chi(c, s, i, rn);
+}
+
+__device__ void shift_oc(Ctx& c, const DState& s, int nc) {
+  int oc = *s.oc;
+  __syncthreads();
+  if (oc == nc) return;
+  if (nc > oc) {
+    for (int i = oc; i < nc && !c.sm.fail; ++i) qr_right(c, s, i);
+  } else {
+    for (int i = oc; i > nc && !c.sm.fail; --i) lq_left(c, s, i);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *s.oc = nc;
+  __syncthreads();
+}
+
+__device__ void normalize_state(Ctx& c, const DState& s) {
+  for (int i = c.P.L - 1; i >= 1 && !c.sm.fail; --i) lq_left(c, s, i);
+  cplx* A = site_ptr(c, s, 0);
+  const long long n = (long long)s.chi[0] * 2 * s.chi[1];
+  double nr = sqrt(cta_norm2(A, n, c.sm.e.r));
+  if (nr > 1e-13) cta_scale(A, n, 1.0 / nr);
+  __syncthreads();
+  if (threadIdx.x == 0) *s.oc = 0;
+  __syncthreads();
+}
+
+// Re <psi|psi> by full contraction (scalar_product, MPS.jl:528-585).
+__device__ double scalar_product(Ctx& c, const DState& s) {
+  cplx* Ea = c.ws + c.P.lay.tA;
+  cplx* Eb = c.ws + c.P.lay.tB;
+  cplx* T = c.ws + c.P.lay.tC;
+  if (threadIdx.x == 0) Ea[0] = make_double2(1.0, 0.0);
+  __syncthreads();
+  for (int i = 0; i < c.P.L; ++i) {
+    const int l = s.chi[i], r = s.chi[i + 1];
+    const cplx* A = site_ptr(c, s, i);
+    cta_gemm(gemm_args(l, 2 * r, l, Ea, l, 1, A, 1, l, T, 1, l), c.sm.e.g);
+    cta_gemm(gemm_args(r, r, 2 * l, T, 2 * l, 1, A, 1, 2 * l, Eb, 1, r, false, true), c.sm.e.g);
+    cplx* t = Ea;
+    Ea = Eb;
+    Eb = t;
+  }
+  double v = Ea[0].x;
+  __syncthreads();
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Environments (Algorithms.jl:191-211)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ cplx* envL(const Ctx& c, int b) { return c.ws + c.P.lay.EL + c.P.env_off[b]; }
+__device__ __forceinline__ cplx* envR(const Ctx& c, int b) { return c.ws + c.P.lay.ER + c.P.env_off[b]; }
+
+__device__ void identity_env(Ctx& c, cplx* E, int dim, int w) {
+  for (long long e = threadIdx.x; e < (long long)dim * w * dim; e += NT) {
+    long long a = e % dim, rest = e / dim;
+    long long m = rest % w, k = rest / w;
+    E[e] = make_double2((m == 0 && a == k) ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+}
+
+// EL[i+1] from EL[i], A_i, W_i  (update_left_environment)
+__device__ void update_left(Ctx& c, const DState& s, int i) {
+  const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
+  const cplx* A = site_ptr(c, s, i);
+  cplx* T1 = c.ws + c.P.lay.T1;
+  cplx* T2 = c.ws + c.P.lay.T2;
+  cta_gemm(gemm_args(l * wl, 2 * r, l, envL(c, i), 1, (long long)l * wl, A, 1, l, T1, 1, (long long)l * wl),
+           c.sm.e.g);
+  WApplyGeom g;
+  g.n0 = l;
+  g.n1 = r;
+  g.is0 = 1;
+  g.is1 = (long long)l * wl * 2;
+  g.ni1 = wl;
+  g.ii1 = l;
+  g.ii2 = (long long)l * wl;
+  g.os0 = 1;
+  g.os1 = (long long)l * 2 * wr;
+  g.no1 = 2;
+  g.oo1 = l;
+  g.oo2 = 2 * l;
+  dev_wapply(T1, T2, c.P.wm_envL[i], g, c.sm.e.w);
+  cta_gemm(gemm_args(r, wr * r, 2 * l, A, 2 * l, 1, T2, 1, 2 * l, envL(c, i + 1), 1, r, true, false), c.sm.e.g);
+}
+
+// ER[i] from ER[i+1], A_i, W_i  (update_right_environment)
+__device__ void update_right(Ctx& c, const DState& s, int i) {
+  const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
+  const cplx* A = site_ptr(c, s, i);
+  cplx* T1 = c.ws + c.P.lay.T1;
+  cplx* T2 = c.ws + c.P.lay.T2;
+  cta_gemm(gemm_args(2 * l, r * wr, r, A, 1, 2 * l, envR(c, i + 1), (long long)r * wr, 1, T1, 1, 2 * l), c.sm.e.g);
+  WApplyGeom g;
+  g.n0 = l;
+  g.n1 = r;
+  g.is0 = 1;
+  g.is1 = 2 * l;
+  g.ni1 = 2;
+  g.ii1 = l;
+  g.ii2 = (long long)2 * l * r;
+  g.os0 = (long long)2 * r * wl;
+  g.os1 = 2;
+  g.no1 = 2;
+  g.oo1 = 1;
+  g.oo2 = 2 * r;
+  dev_wapply(T1, T2, c.P.wm_envR[i], g, c.sm.e.w);
+  cta_gemm(gemm_args(l, wl * l, 2 * r, A, 1, l, T2, 1, 2 * r, envR(c, i), 1, l, true, false), c.sm.e.g);
+}
+
+// ---------------------------------------------------------------------------
+// Two-site TDVP (Algorithms.jl:580-760)
+// ---------------------------------------------------------------------------
+__device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, const WMat& W, double dt) {
+  HeffOp h;
+  h.L = envL(c, bl);
+  h.R = envR(c, br);
+  h.W = W;
+  h.chil = l;
+  h.D = D;
+  h.chir = r;
+  h.wl = c.P.w[bl];
+  h.wr = c.P.w[br];
+  h.T1 = c.ws + c.P.lay.T1;
+  h.T2 = c.ws + c.P.lay.T2;
+  int mv = dev_expm_krylov(h, x, dt, c.P.kc, c.ws + c.P.lay.Q, c.P.kry_n, c.sm.e);
+  if (threadIdx.x == 0) {
+    c.cnt[0] += mv;
+    c.cnt[1] += (mv > 0);
+    *c.fl += mv * heff_flops(l, h.wl, D, r, h.wr);
+  }
+}
+
+// Theta (l,4,r) of sites i,i+1 into buffer th.
+__device__ void merge(Ctx& c, const DState& s, int i, cplx* th) {
+  const int l = s.chi[i], m = s.chi[i + 1], r = s.chi[i + 2];
+  cta_gemm(gemm_args(2 * l, 2 * r, m, site_ptr(c, s, i), 1, 2 * l, site_ptr(c, s, i + 1), 1, m, th, 1, 2 * l),
+           c.sm.e.g);
+}
+
+__device__ SvdWork svd_work(const Ctx& c) {
+  SvdWork w;
+  w.B = c.ws + c.P.lay.B;
+  w.X = c.ws + c.P.lay.X;
+  w.Yo = c.ws + c.P.lay.Yo;
+  w.Zo = c.ws + c.P.lay.Zo;
+  w.y = c.ws + c.P.lay.y;
+  w.sig = reinterpret_cast<double*>(c.ws + c.P.lay.dbl);
+  w.ord = c.wsi + c.P.lay.i_ord;
+  return w;
+}
+
+// NaN/Inf -> 0 before the SVD (Algorithms.jl:414-417).
+__device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
+  int bad = 0;
+  for (long long e = threadIdx.x; e < n; e += NT) {
+    cplx v = th[e];
+    if (!isfinite(v.x) || !isfinite(v.y)) {
+      th[e] = make_double2(0.0, 0.0);
+      bad = 1;
+    }
+  }
+  double b = block_sum((double)bad, c.sm.e.r);
+  if (b > 0 && threadIdx.x == 0) c.cnt[4] += 1;
+}
+
+// SVD split of theta (2l x 2r) into sites i (l,2,keep) and i+1 (keep,2,r).
+// rule 0: TDVP (absolute, min 2); rule 1: relative.  S goes left if s_left.
+__device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, int rule, bool s_left) {
+  const int m = 2 * l, n = 2 * r;
+  fix_nonfinite(c, th, (long long)m * n);
+  SvdWork w = svd_work(c);
+  SvdResult res = dev_svd(th, m, n, w, c.sm.la, c.sm.e.r);
+  if (threadIdx.x == 0) {
+    int keep = rule == 0 ? keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond)
+                         : keep_relative(w.sig, res.p, c.P.thr, c.P.max_bond);
+    c.sm.bcast_i[0] = keep;
+    c.cnt[2] += 1;
+  }
+  __syncthreads();
+  const int keep = c.sm.bcast_i[0];
+  __syncthreads();
+  if (keep > c.P.cap[i + 1]) {
+    if (threadIdx.x == 0) c.sm.fail = ST_UNSUPPORTED;
+    __syncthreads();
+    return;
+  }
+  dev_svd_vectors(res, keep, w, c.sm.e.r);
+  dev_svd_write(res, w, m, n, keep, site_ptr(c, s, i), s_left, site_ptr(c, s, i + 1), !s_left);
+  set_chi(c, s, i + 1, keep);
+}
+
+__device__ void tdvp_sweep(Ctx& c, const DState& s) {
+  const int L = c.P.L;
+  const double dt = c.P.dt;
+  shift_oc(c, s, 0);
+  cplx* th = c.ws + c.P.lay.th;
+  identity_env(c, envR(c, L), s.chi[L], c.P.w[L]);
+  for (int i = L - 1; i >= 1; --i) update_right(c, s, i);
+  identity_env(c, envL(c, 0), s.chi[0], c.P.w[0]);
+  // forward (Algorithms.jl:631-672)
+  for (int i = 0; i <= L - 3 && !c.sm.fail; ++i) {
+    const int l = s.chi[i], r = s.chi[i + 2];
+    merge(c, s, i, th);
+    evolve(c, th, l, 4, r, i, i + 2, c.P.wm_heff2[i], dt / 2);
+    split(c, s, i, th, l, r, 0, false);
+    if (c.sm.fail) break;
+    update_left(c, s, i);
+    evolve(c, site_ptr(c, s, i + 1), s.chi[i + 1], 2, r, i + 1, i + 2, c.P.wm_heff1[i + 1], -dt / 2);
+  }
+  // edge (Algorithms.jl:674-711) and backward (:713-760)
+  for (int i = L - 2; i >= 0 && !c.sm.fail; --i) {
+    const double dts = (i == L - 2) ? dt : dt / 2;
+    if (i < L - 2)
+      evolve(c, site_ptr(c, s, i + 1), s.chi[i + 1], 2, s.chi[i + 2], i + 1, i + 2, c.P.wm_heff1[i + 1], -dts);
+    const int l = s.chi[i], r = s.chi[i + 2];
+    merge(c, s, i, th);
+    evolve(c, th, l, 4, r, i, i + 2, c.P.wm_heff2[i], dts);
+    split(c, s, i, th, l, r, 0, true);
+    if (c.sm.fail) break;
+    update_right(c, s, i + 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Local operators
+// ---------------------------------------------------------------------------
+// A[l,p,r] <- sum_k op[p,k] A[l,k,r] for a d x d op (d = 2 or 4), in place.
+__device__ void apply_local(cplx* A, int l, int d, int r, const cplx* op) {
+  for (long long e = threadIdx.x; e < (long long)l * r; e += NT) {
+    long long a = e % l, b = e / l;
+    cplx v[4], o[4];
+    for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
+    for (int p = 0; p < d; ++p) {
+      cplx acc = make_double2(0.0, 0.0);
+      for (int k = 0; k < d; ++k) cfma(acc, op[p + d * k], v[k]);
+      o[p] = acc;
+    }
+    for (int p = 0; p < d; ++p) A[a + (long long)l * (p + (long long)d * b)] = o[p];
+  }
+  __syncthreads();
+}
+
+// sum |op . A|^2 (or sum |A|^2 when op == nullptr), d = 2 or 4.
+__device__ double local_norm2(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
+  double sacc = 0.0;
+  for (long long e = threadIdx.x; e < (long long)l * r; e += NT) {
+    long long a = e % l, b = e / l;
+    cplx v[4];
+    for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
+    for (int p = 0; p < d; ++p) {
+      if (op) {
+        cplx acc = make_double2(0.0, 0.0);
+        for (int k = 0; k < d; ++k) cfma(acc, op[p + d * k], v[k]);
+        sacc += cabs2(acc);
+      } else {
+        sacc += cabs2(v[p]);
+      }
+    }
+  }
+  return block_sum(sacc, c.sm.e.r);
+}
+
+// Re sum conj(A) (op A)
+__device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
+  double sacc = 0.0;
+  for (long long e = threadIdx.x; e < (long long)l * r; e += NT) {
+    long long a = e % l, b = e / l;
+    cplx v[4];
+    for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
+    for (int p = 0; p < d; ++p) {
+      cplx acc = make_double2(0.0, 0.0);
+      for (int k = 0; k < d; ++k) cfma(acc, op[p + d * k], v[k]);
+      sacc += v[p].x * acc.x + v[p].y * acc.y;
+    }
+  }
+  return block_sum(sacc, c.sm.e.r);
+}
+
+// ---------------------------------------------------------------------------
+// Dissipation (Dissipation.jl:37-159)
+// ---------------------------------------------------------------------------
+__device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt) {
+  const int L = c.P.L;
+  if (!c.P.noise_present || c.P.all_zero) {
+    for (int i = L - 1; i >= 1 && !c.sm.fail; --i) shift_oc(c, s, i - 1);
+    return;
+  }
+  cplx* th = c.ws + c.P.lay.th;
+  for (int i = L - 1; i >= 0 && !c.sm.fail; --i) {
+    for (int k = 0; k < c.P.nprocs; ++k) {
+      const DevProc& pr = c.P.procs[k];
+      if (pr.nsites == 1 && pr.s0 == i) {
+        cplx* A = site_ptr(c, s, i);
+        const long long n = (long long)s.chi[i] * 2 * s.chi[i + 1];
+        if (pr.pauli_name) {
+          cta_scale(A, n, exp(-0.5 * dt * pr.gamma));
+          __syncthreads();
+        } else {
+          apply_local(A, s.chi[i], 2, s.chi[i + 1], full ? pr.diss_full : pr.diss_half);
+        }
+      }
+    }
+    if (i > 0) {
+      for (int k = 0; k < c.P.nprocs && !c.sm.fail; ++k) {
+        const DevProc& pr = c.P.procs[k];
+        if (pr.nsites == 2 && pr.s1 == i) {
+          if (pr.pauli_name) {
+            cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * dt * pr.gamma));
+            __syncthreads();
+          } else {
+            const int l = s.chi[i - 1], r = s.chi[i + 1];
+            merge(c, s, i - 1, th);
+            apply_local(th, l, 4, r, full ? pr.diss_full : pr.diss_half);
+            split(c, s, i - 1, th, l, r, 1, false);
+          }
+        }
+      }
+      shift_oc(c, s, i - 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stochastic process (StochasticProcess.jl:219-330)
+// ---------------------------------------------------------------------------
+__device__ void stochastic_process(Ctx& c, const DState& s, double dt) {
+  const int L = c.P.L;
+  const double dp = 1.0 - scalar_product(c, s);
+  bool jump = false;
+  if (c.P.nprocs > 0) {
+    double u1 = draw_uniform(c);
+    jump = u1 < dp;
+  }
+  if (!jump) {
+    shift_oc(c, s, 0);
+    normalize_state(c, s);
+    return;
+  }
+  double* cand = reinterpret_cast<double*>(c.ws + c.P.lay.dbl) + SVD_MAX_COLS;
+  int* candp = c.wsi + c.P.lay.i_cand;
+  int nc = 0;
+  cplx* th = c.ws + c.P.lay.th;
+  for (int site = 0; site < L && !c.sm.fail; ++site) {
+    shift_oc(c, s, site);
+    for (int k = 0; k < c.P.nprocs; ++k) {
+      const DevProc& pr = c.P.procs[k];
+      if (pr.nsites == 1 && pr.s0 == site) {
+        double nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1],
+                                pr.pauli_proc ? nullptr : pr.mat);
+        if (threadIdx.x == 0) {
+          cand[nc] = dt * pr.gamma * nr;
+          candp[nc] = k;
+        }
+        ++nc;
+      }
+    }
+    if (site < L - 1) {
+      for (int k = 0; k < c.P.nprocs; ++k) {
+        const DevProc& pr = c.P.procs[k];
+        if (pr.nsites == 2 && pr.s0 == site) {
+          double nr;
+          if (pr.pauli_proc) {
+            nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1], nullptr);
+          } else {
+            merge(c, s, site, th);
+            nr = local_norm2(c, th, s.chi[site], 4, s.chi[site + 2], pr.mat);
+          }
+          if (threadIdx.x == 0) {
+            cand[nc] = dt * pr.gamma * nr;
+            candp[nc] = k;
+          }
+          ++nc;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double total = 0.0;
+  for (int e = 0; e < nc; ++e) total += cand[e];
+  if (total == 0.0) {
+    shift_oc(c, s, 0);
+    normalize_state(c, s);
+    return;
+  }
+  const double r = draw_uniform(c);
+  double acc = 0.0;
+  int chosen = 0;
+  for (int e = 0; e < nc; ++e) {
+    acc += cand[e] / total;
+    if (r <= acc) {
+      chosen = e;
+      break;
+    }
+  }
+  const DevProc& pr = c.P.procs[candp[chosen]];
+  __syncthreads();
+  if (pr.nsites == 1) {
+    shift_oc(c, s, pr.s0);
+    apply_local(site_ptr(c, s, pr.s0), s.chi[pr.s0], 2, s.chi[pr.s0 + 1], pr.mat);
+  } else {
+    shift_oc(c, s, pr.s0);
+    const int l = s.chi[pr.s0], rr = s.chi[pr.s0 + 2];
+    merge(c, s, pr.s0, th);
+    apply_local(th, l, 4, rr, pr.mat);
+    split(c, s, pr.s0, th, l, rr, 1, false);
+  }
+  if (threadIdx.x == 0) c.cnt[3] += 1;
+  normalize_state(c, s);
+}
+
+// ---------------------------------------------------------------------------
+// Observables
+// ---------------------------------------------------------------------------
+__device__ void evaluate(Ctx& c, const DState& s, int col) {
+  const int ncols = c.P.ncols;
+  for (int k = 0; k < c.P.nobs && !c.sm.fail; ++k) {
+    const DevObs& o = c.P.obs[k];
+    double val = 0.0;
+    if (o.kind == OBS_LOCAL1) {
+      shift_oc(c, s, o.s0);
+      val = local_expect(c, site_ptr(c, s, o.s0), s.chi[o.s0], 2, s.chi[o.s0 + 1], o.mat);
+    } else if (o.kind == OBS_LOCAL2) {
+      shift_oc(c, s, o.s0);
+      cplx* th = c.ws + c.P.lay.th;
+      merge(c, s, o.s0, th);
+      val = local_expect(c, th, s.chi[o.s0], 4, s.chi[o.s0 + 2], o.mat);
+    } else {
+      shift_oc(c, s, o.s0);
+      const int l = s.chi[o.s0], r = s.chi[o.s0 + 1];
+      SvdWork w = svd_work(c);
+      SvdResult res = dev_svd(site_ptr(c, s, o.s0), 2 * l, r, w, c.sm.la, c.sm.e.r);
+      if (threadIdx.x == 0) {
+        double nsq = 0.0;
+        for (int e = 0; e < res.p; ++e) nsq += w.sig[e] * w.sig[e];
+        double ent = 0.0;
+        for (int e = 0; e < res.p; ++e) {
+          double p = w.sig[e] * w.sig[e] / nsq;
+          if (p > 0.0) ent -= p * log(p);
+        }
+        c.sm.bcast_d[1] = ent;
+      }
+      __syncthreads();
+      val = c.sm.bcast_d[1];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) c.P.traj_out[((long long)c.traj * c.P.nobs + k) * ncols + col] = val;
+  }
+  if (threadIdx.x == 0) {
+    int mx = 0;
+    for (int b = 0; b <= c.P.L; ++b) mx = max(mx, s.chi[b]);
+    if (c.P.chi_out) c.P.chi_out[(long long)c.traj * ncols + col] = mx;
+  }
+  __syncthreads();
+}
