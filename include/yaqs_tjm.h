@@ -158,6 +158,7 @@ typedef struct {
   int64_t nonfinite_fixes; /* NaN/Inf replaced before an SVD (Algorithms.jl:414-417) */
   double flops;            /* algorithmic flops of the H_eff products       */
   double device_ms;        /* device time of the run (CUDA events)          */
+  int64_t svd_sweeps;      /* Jacobi sweeps summed over the two-site splits */
 } yaqs_run_stats;
 
 /* ---- context ---- */
@@ -208,6 +209,18 @@ int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms);
 int yaqs_analog_remaining(const yaqs_run* run);
 int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out,
                        int32_t* maxchi_out, yaqs_run_stats* stats);
+
+/*
+ * Device time per engine phase so far (clock cycles summed over CTAs, 16
+ * entries: GEMM, MPO apply, Lanczos orthogonalisation, tridiagonal
+ * exponential, SVD sweeps, SVD vectors, QR factor, QR form-Q, norm
+ * contraction, environment updates, dissipation, jump step, observables,
+ * TDVP sweep, whole step, state copy; nested phases overlap).  All zero
+ * unless the environment variable YAQS_PROFILE=1 was set at
+ * yaqs_analog_begin.  The analogue of the reference's Timing @t keys
+ * (src/Yaqs.jl:3-162).
+ */
+int yaqs_analog_profile(yaqs_run* run, double* cycles);
 
 #ifdef __cplusplus
 }

@@ -6,8 +6,9 @@
  * yaqs_tjm.h.  They replace, one for one, the reference's per-call numerics:
  *
  *   yaqs_batched_svd          svd(Mat) in split_mps_tensor_svd
- *                             (src/Algorithms.jl:409-445), thin factors,
- *                             singular values descending.
+ *                             (src/Algorithms.jl:409-445) in the split form
+ *                             the forward sweep uses: orthonormal U, the
+ *                             singular values descending and S*Vt = U^H M.
  *   yaqs_batched_qr           qr(Mat) of right_qr / shift_orthogonality_center!
  *                             (src/Decompositions.jl:18-36, src/MPS.jl:197-202).
  *   yaqs_batched_project_site project_site / _project_site_ws!
@@ -26,9 +27,10 @@
 extern "C" {
 #endif
 
-/* M: batch x (m x n); U: batch x (m x k); S: batch x k; Vt: batch x (k x n); k = min(m, n) <= 256. */
+/* M: batch x (m x n); U: batch x (m x k); S: batch x k; SVt: batch x (k x n);
+ * k = min(m, n) <= 256, m + n <= 4096. */
 int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* U,
-                     double* S, double* Vt);
+                     double* S, double* SVt);
 
 /* M: batch x (m x n); Q: batch x (m x k); R: batch x (k x n). */
 int yaqs_batched_qr(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* Q,

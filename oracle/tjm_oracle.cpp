@@ -182,9 +182,12 @@ void house_lq(int m, int n, const cd* M, vector<cd>& Lm, vector<cd>& Qm) {
 // ---------------------------------------------------------------------------
 // One-sided Jacobi SVD (restates the `svd` of Algorithms.jl:420,
 // Decompositions.jl:105, Dissipation.jl:281, StochasticProcess.jl:280).
-// M (m x n) = U (m x k) diag(S) Vt (k x n), k = min(m,n), S descending.
+// QR-preconditioned (Drmac-Veselic): side LEFT (orthonormal left vectors of
+// M, m x n) factors M^H = Q R and orthogonalises the columns of B = R^H
+// (m x k); side RIGHT factors M = Q R and orthogonalises B = R^H (n x k).
+// The columns of B converge to (requested singular vectors) x Sigma.
 // ---------------------------------------------------------------------------
-// Orthonormal completion: fills column `slot` of X (rows x cols) with the
+// Orthonormal completion: fills column `slot` of X (rows x *) with the
 // first unit vector e_c whose component orthogonal to columns `have` exceeds
 // 1/2 in norm (two Gram-Schmidt passes), normalised.
 void complete_column(int rows, vector<cd>& X, const vector<int>& have, int slot) {
@@ -207,111 +210,152 @@ void complete_column(int rows, vector<cd>& X, const vector<int>& have, int slot)
   }
 }
 
-void jacobi_svd(int m, int n, const cd* M, vector<cd>& U, vector<double>& S, vector<cd>& Vt) {
-  const bool tr = m < n;
-  const int q = tr ? n : m;  // rows of B
-  const int p = tr ? m : n;  // columns of B (the shorter side)
-  vector<cd> B((size_t)q * p);
-  if (!tr) {
-    std::copy(M, M + (size_t)m * n, B.begin());
-  } else {
-    for (int i = 0; i < m; ++i)
-      for (int j = 0; j < n; ++j) B[j + (size_t)q * i] = std::conj(M[i + (size_t)m * j]);
-  }
-  vector<cd> X((size_t)p * p, 0.0);
-  for (int i = 0; i < p; ++i) X[i + (size_t)p * i] = 1.0;
+// Block size of the block-cyclic Jacobi order (same rule as the GPU engine:
+// a pair of b-column blocks of B (q rows) fits 8192 complex values).
+int svd_block_size(int q, int p) {
+  int b = 8192 / (2 * q);
+  if (b > 32) b = 32;
+  if (b > p) b = p;
+  if (b < 1) b = 1;
+  return b;
+}
+
+enum { SVD_LEFT = 0, SVD_RIGHT = 1 };
+
+struct SvdOut {
+  int q = 0, p = 0, rank = 0;
+  vector<double> S;  // sorted descending, nulls zeroed (length p)
+  vector<cd> B;      // q x p after Jacobi
+  vector<int> ord;   // sorted column order
+};
+
+SvdOut svd_side(int m, int n, const cd* M, int side) {
+  SvdOut o;
+  const bool right = side == SVD_RIGHT;
+  const int mm = right ? m : n, nn = right ? n : m, k = std::min(m, n);
+  vector<cd> H((size_t)mm * nn);
+  for (int r = 0; r < mm; ++r)
+    for (int c = 0; c < nn; ++c)
+      H[r + (size_t)mm * c] = right ? M[r + (size_t)m * c] : std::conj(M[c + (size_t)m * r]);
+  vector<cd> Q, R;
+  house_qr(mm, nn, H.data(), Q, R);  // R (k x nn)
+  const int q = nn, p = k;
+  o.q = q;
+  o.p = p;
+  vector<cd>& B = o.B;
+  B.assign((size_t)q * p, 0.0);
+  for (int r = 0; r < q; ++r)
+    for (int c = 0; c <= std::min(r, p - 1); ++c) B[r + (size_t)q * c] = std::conj(R[c + (size_t)k * r]);
   const double tol = 2.220446049250313e-16 * q;
-  // Round-robin (tournament) ordering: p' = p rounded up to even, p'-1 rounds
-  // of p'/2 disjoint pairs.  The same order is used on the GPU.
-  const int pe = p + (p & 1);
-  vector<int> slots(pe);
+  auto rotate = [&](int i, int j, int& rotations) {
+    cd* bi = &B[(size_t)q * i];
+    cd* bj = &B[(size_t)q * j];
+    double al = 0, be = 0;
+    cd g = 0;
+    for (int r = 0; r < q; ++r) {
+      al += std::norm(bi[r]);
+      be += std::norm(bj[r]);
+      g += std::conj(bi[r]) * bj[r];
+    }
+    double ag = std::abs(g);
+    if (!(ag > tol * std::sqrt(al * be))) return;
+    ++rotations;
+    double zeta = (be - al) / (2.0 * ag);
+    double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+    double c = 1.0 / std::sqrt(1.0 + t * t);
+    double s = c * t;
+    cd e = g / ag;
+    cd se = s * e, sec = s * std::conj(e);
+    for (int r = 0; r < q; ++r) {
+      cd x = bi[r], y = bj[r];
+      bi[r] = c * x - sec * y;
+      bj[r] = se * x + c * y;
+    }
+  };
+  // Round-robin (tournament) slot of position t in round `round` of n players.
+  auto slot = [](int t, int round, int n) { return t == 0 ? 0 : ((t - 1 - round + 2 * (n - 1)) % (n - 1)) + 1; };
+  // Block-cyclic order: per sweep every diagonal block gets a round-robin
+  // pass, then every pair of blocks (round-robin over blocks) gets b rounds
+  // of disjoint cross pairs (k, (k + t) mod b).
+  const int b = svd_block_size(q, p);
+  const int nb = (p + b - 1) / b, nbe = nb + (nb & 1), be2 = b + (b & 1);
   for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
     int rotations = 0;
-    for (int i = 0; i < pe; ++i) slots[i] = i;
-    for (int round = 0; round < pe - 1; ++round) {
-      for (int pr = 0; pr < pe / 2; ++pr) {
-        int a = slots[pr], b = slots[pe - 1 - pr];
-        int i = std::min(a, b), j = std::max(a, b);
-        if (j >= p) continue;
-        cd* bi = &B[(size_t)q * i];
-        cd* bj = &B[(size_t)q * j];
-        double al = 0, be = 0;
-        cd g = 0;
-        for (int r = 0; r < q; ++r) {
-          al += std::norm(bi[r]);
-          be += std::norm(bj[r]);
-          g += std::conj(bi[r]) * bj[r];
+    for (int I = 0; I < nb; ++I) {
+      const int c0 = I * b, nc = std::min(b, p - c0);
+      for (int round = 0; round < be2 - 1; ++round)
+        for (int pr = 0; pr < be2 / 2; ++pr) {
+          int a = slot(pr, round, be2), cc = slot(be2 - 1 - pr, round, be2);
+          int i = std::min(a, cc), j = std::max(a, cc);
+          if (j >= nc) continue;
+          rotate(c0 + i, c0 + j, rotations);
         }
-        double ag = std::abs(g);
-        if (!(ag > tol * std::sqrt(al * be))) continue;
-        ++rotations;
-        double zeta = (be - al) / (2.0 * ag);
-        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
-        double c = 1.0 / std::sqrt(1.0 + t * t);
-        double s = c * t;
-        cd e = g / ag;
-        cd se = s * e, sec = s * std::conj(e);
-        for (int r = 0; r < q; ++r) {
-          cd x = bi[r], y = bj[r];
-          bi[r] = c * x - sec * y;
-          bj[r] = se * x + c * y;
-        }
-        cd* xi = &X[(size_t)p * i];
-        cd* xj = &X[(size_t)p * j];
-        for (int r = 0; r < p; ++r) {
-          cd x = xi[r], y = xj[r];
-          xi[r] = c * x - sec * y;
-          xj[r] = se * x + c * y;
-        }
-      }
-      // rotate slots 1..pe-1 (slot 0 fixed)
-      int last = slots[pe - 1];
-      for (int i = pe - 1; i > 1; --i) slots[i] = slots[i - 1];
-      slots[1] = last;
     }
+    for (int round = 0; round < nbe - 1; ++round)
+      for (int pr = 0; pr < nbe / 2; ++pr) {
+        int A = slot(pr, round, nbe), Bk = slot(nbe - 1 - pr, round, nbe);
+        int I = std::min(A, Bk), J = std::max(A, Bk);
+        if (J >= nb) continue;
+        const int c0 = I * b, n0 = std::min(b, p - c0), c1 = J * b, n1 = std::min(b, p - c1);
+        for (int t = 0; t < b; ++t)
+          for (int kk = 0; kk < b; ++kk) {
+            int jj = (kk + t) % b;
+            if (kk >= n0 || jj >= n1) continue;
+            rotate(c0 + kk, c1 + jj, rotations);
+          }
+      }
     if (rotations == 0) break;
   }
   vector<double> sig(p);
   for (int c = 0; c < p; ++c) sig[c] = nrm2(&B[(size_t)q * c], q);
-  vector<int> ord(p);
-  for (int i = 0; i < p; ++i) ord[i] = i;
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return sig[a] > sig[b]; });
-  const double smax = p > 0 ? sig[ord[0]] : 0.0;
-  // left vectors Y (q x p) = B / sigma, right vectors Z (p x p) = X (sorted)
-  vector<cd> Y((size_t)q * p, 0.0), Z((size_t)p * p, 0.0);
-  S.assign(p, 0.0);
-  vector<int> good;
-  vector<int> nulls;
-  for (int k = 0; k < p; ++k) {
-    int c = ord[k];
-    double s = sig[c];
-    if (smax > 0 && s > kSvdNullTol * smax) {
-      S[k] = s;
-      for (int r = 0; r < q; ++r) Y[(size_t)q * k + r] = B[(size_t)q * c + r] / s;
-      for (int r = 0; r < p; ++r) Z[(size_t)p * k + r] = X[(size_t)p * c + r];
-      good.push_back(k);
-    } else {
-      S[k] = 0.0;
-      nulls.push_back(k);
+  o.ord.resize(p);
+  for (int i = 0; i < p; ++i) o.ord[i] = i;
+  std::stable_sort(o.ord.begin(), o.ord.end(), [&](int a, int b2) { return sig[a] > sig[b2]; });
+  const double smax = p > 0 ? sig[o.ord[0]] : 0.0;
+  o.S.assign(p, 0.0);
+  o.rank = 0;
+  for (int kk = 0; kk < p; ++kk) {
+    double sv = sig[o.ord[kk]];
+    if (smax > 0 && sv > kSvdNullTol * smax) {
+      o.S[kk] = sv;
+      ++o.rank;
     }
   }
-  vector<int> haveY = good, haveZ = good;
-  for (int k : nulls) {
-    complete_column(q, Y, haveY, k);
-    haveY.push_back(k);
-    complete_column(p, Z, haveZ, k);
-    haveZ.push_back(k);
+  return o;
+}
+
+// Requested orthonormal vectors Y (q x need): B[:, ord[k]] / S[k], with
+// orthonormal completions for the null columns.
+vector<cd> svd_vectors(const SvdOut& o, int need) {
+  need = std::min(need, o.p);
+  vector<cd> Y((size_t)o.q * need, 0.0);
+  vector<int> have;
+  for (int kk = 0; kk < std::min(need, o.rank); ++kk) {
+    const cd* bc = &o.B[(size_t)o.q * o.ord[kk]];
+    for (int r = 0; r < o.q; ++r) Y[(size_t)o.q * kk + r] = bc[r] / o.S[kk];
+    have.push_back(kk);
   }
-  // M = U S V^H.  !tr: U = Y (m=q), V = Z (n=p).  tr: U = Z (m=p), V = Y (n=q).
-  const int k = p;
-  U.assign((size_t)m * k, 0.0);
-  Vt.assign((size_t)k * n, 0.0);
-  const vector<cd>& Uc = tr ? Z : Y;
-  const vector<cd>& Vc = tr ? Y : Z;
-  for (int j = 0; j < k; ++j) {
-    for (int i = 0; i < m; ++i) U[i + (size_t)m * j] = Uc[i + (size_t)m * j];
-    for (int i = 0; i < n; ++i) Vt[j + (size_t)k * i] = std::conj(Vc[i + (size_t)n * j]);
+  for (int kk = o.rank; kk < need; ++kk) {
+    complete_column(o.q, Y, have, kk);
+    have.push_back(kk);
   }
+  return Y;
+}
+
+// Component form used by the tests: U (m x k), S (k), SVt = U^H M (k x n).
+void jacobi_svd(int m, int n, const cd* M, vector<cd>& U, vector<double>& S, vector<cd>& SVt) {
+  SvdOut o = svd_side(m, n, M, SVD_LEFT);
+  const int k = o.p;
+  U = svd_vectors(o, k);
+  S = o.S;
+  SVt.assign((size_t)k * n, 0.0);
+  for (int c = 0; c < n; ++c)
+    for (int kk = 0; kk < k; ++kk) {
+      if (kk >= o.rank) continue;
+      cd sacc = 0;
+      for (int r = 0; r < m; ++r) sacc += std::conj(U[r + (size_t)m * kk]) * M[r + (size_t)m * c];
+      SVt[kk + (size_t)k * c] = sacc;
+    }
 }
 
 // Truncation rules (each restates one call site).
@@ -727,9 +771,12 @@ double tnorm2(const Ten& A) {
   return s;
 }
 
-// Split Theta (l, 4, r) by SVD; rule 0 = TDVP, 1 = relative.  Returns U (l,2,k), S, Vt (k,2,r).
-void split_theta(const Ten& Th, int rule, double thr, int max_bond, Ten& Uo, vector<double>& So, Ten& Vo,
-                 Counters& cnt) {
+// Split Theta (l, 4, r) by SVD into left (l,2,keep) and right (keep,2,r)
+// tensors; rule 0 = TDVP (absolute, min 2), 1 = relative.  With s_left the
+// singular values go left (U S | Vt, Vt orthonormal); otherwise right
+// (U | S Vt, U orthonormal).  The scaled factor is the product with M,
+// exactly zero for null singular values.
+void split_theta(const Ten& Th, int rule, double thr, int max_bond, bool s_left, Ten& Lo, Ten& Ro, Counters& cnt) {
   const int m = Th.l * 2, n = 2 * Th.r;
   vector<cd> M = Th.v;
   bool bad = false;
@@ -739,19 +786,34 @@ void split_theta(const Ten& Th, int rule, double thr, int max_bond, Ten& Uo, vec
       bad = true;
     }
   if (bad) cnt.nonfinite++;
-  vector<cd> U, Vt;
-  vector<double> S;
-  jacobi_svd(m, n, M.data(), U, S, Vt);
+  SvdOut o = svd_side(m, n, M.data(), s_left ? SVD_RIGHT : SVD_LEFT);
   cnt.svds++;
-  int keep = (rule == 0) ? keep_tdvp(S, thr, max_bond) : keep_relative(S, thr, max_bond);
-  const int k = (int)S.size();
-  Uo = Ten(Th.l, 2, keep);
-  for (int j = 0; j < keep; ++j)
-    for (int i = 0; i < m; ++i) Uo.v[i + (size_t)m * j] = U[i + (size_t)m * j];
-  Vo = Ten(keep, 2, Th.r);
-  for (int j = 0; j < n; ++j)
-    for (int i = 0; i < keep; ++i) Vo.v[i + (size_t)keep * j] = Vt[i + (size_t)k * j];
-  So.assign(S.begin(), S.begin() + keep);
+  const int keep = (rule == 0) ? keep_tdvp(o.S, thr, max_bond) : keep_relative(o.S, thr, max_bond);
+  vector<cd> Y = svd_vectors(o, keep);
+  Lo = Ten(Th.l, 2, keep);
+  Ro = Ten(keep, 2, Th.r);
+  if (!s_left) {  // U = Y (m x keep), S Vt = Y^H M
+    for (int j = 0; j < keep; ++j)
+      for (int i = 0; i < m; ++i) Lo.v[i + (size_t)m * j] = Y[i + (size_t)m * j];
+    for (int c = 0; c < n; ++c)
+      for (int kk = 0; kk < keep; ++kk) {
+        if (kk >= o.rank) continue;
+        cd sacc = 0;
+        for (int r = 0; r < m; ++r) sacc += std::conj(Y[r + (size_t)m * kk]) * M[r + (size_t)m * c];
+        Ro.v[kk + (size_t)keep * c] = sacc;
+      }
+  } else {  // Vt = Y^H (keep x n), U S = M Y
+    for (int c = 0; c < n; ++c)
+      for (int kk = 0; kk < keep; ++kk) Ro.v[kk + (size_t)keep * c] = std::conj(Y[c + (size_t)n * kk]);
+    for (int kk = 0; kk < keep; ++kk) {
+      if (kk >= o.rank) continue;
+      for (int i = 0; i < m; ++i) {
+        cd sacc = 0;
+        for (int c = 0; c < n; ++c) sacc += M[i + (size_t)m * c] * Y[c + (size_t)n * kk];
+        Lo.v[i + (size_t)m * kk] = sacc;
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -925,13 +987,9 @@ struct Sweeper {
     Ten Th = merge(s.t[i], s.t[i + 1]);
     Th.v = evolve(EL[i], ER[i + 2], P.W2[i], Th, dts);
     Ten U, V;
-    vector<double> S;
-    split_theta(Th, 0, P.thr, P.max_bond, U, S, V, cnt);
+    split_theta(Th, 0, P.thr, P.max_bond, false, U, V, cnt);
     s.t[i] = U;
     EL[i + 1] = update_left(s.t[i], P.W[i], EL[i]);
-    for (int b = 0; b < V.r; ++b)
-      for (int p = 0; p < 2; ++p)
-        for (int a = 0; a < V.l; ++a) V.at(a, p, b) *= S[a];
     V.v = evolve(EL[i + 1], ER[i + 2], P.W[i + 1], V, -dts);
     s.t[i + 1] = V;
   }
@@ -942,13 +1000,9 @@ struct Sweeper {
     Ten Th = merge(s.t[i], s.t[i + 1]);
     Th.v = evolve(EL[i], ER[i + 2], P.W2[i], Th, dts);
     Ten U, V;
-    vector<double> S;
-    split_theta(Th, 0, P.thr, P.max_bond, U, S, V, cnt);
+    split_theta(Th, 0, P.thr, P.max_bond, true, U, V, cnt);
     s.t[i + 1] = V;
     ER[i + 1] = update_right(s.t[i + 1], P.W[i + 1], ER[i + 2]);
-    for (int j = 0; j < U.r; ++j)
-      for (int p = 0; p < 2; ++p)
-        for (int a = 0; a < U.l; ++a) U.at(a, p, j) *= S[j];
     s.t[i] = U;
   }
 
@@ -998,11 +1052,7 @@ void apply_dissipation(const Problem& P, State& s, bool full_dt, double dt, Coun
             Ten Th = merge(s.t[i - 1], s.t[i]);
             apply_2site(Th, full_dt ? pr.diss_full : pr.diss_half);
             Ten U, V;
-            vector<double> S;
-            split_theta(Th, 1, P.thr, P.max_bond, U, S, V, cnt);
-            for (int b = 0; b < V.r; ++b)
-              for (int p = 0; p < 2; ++p)
-                for (int a = 0; a < V.l; ++a) V.at(a, p, b) *= S[a];
+            split_theta(Th, 1, P.thr, P.max_bond, false, U, V, cnt);
             s.t[i - 1] = U;
             s.t[i] = V;
           }
@@ -1088,11 +1138,7 @@ bool stochastic_process(const Problem& P, State& s, double dt, Draws& rng, Count
     Ten Th = merge(s.t[pr.s0], s.t[pr.s0 + 1]);
     apply_2site(Th, pr.mat);
     Ten U, V;
-    vector<double> S;
-    split_theta(Th, 1, P.thr, P.max_bond, U, S, V, cnt);
-    for (int b = 0; b < V.r; ++b)
-      for (int p = 0; p < 2; ++p)
-        for (int a = 0; a < V.l; ++a) V.at(a, p, b) *= S[a];
+    split_theta(Th, 1, P.thr, P.max_bond, false, U, V, cnt);
     s.t[pr.s0] = U;
     s.t[pr.s0 + 1] = V;
   }
@@ -1134,9 +1180,7 @@ double measure(const Obs& o, State& s) {
   // ENTROPY across the bond (s0, s0+1): Schmidt values of the center tensor.
   shift_oc(s, o.s0);
   const Ten& A = s.t[o.s0];
-  vector<cd> U, Vt;
-  vector<double> S;
-  jacobi_svd(A.l * A.d, A.r, A.v.data(), U, S, Vt);
+  const vector<double> S = svd_side(A.l * A.d, A.r, A.v.data(), SVD_LEFT).S;
   double nsq = 0;
   for (double x : S) nsq += x * x;
   double ent = 0;

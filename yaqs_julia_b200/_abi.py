@@ -79,7 +79,7 @@ class RunStats(C.Structure):
     _fields_ = [("matvecs", C.c_int64), ("krylov_solves", C.c_int64),
                 ("svds", C.c_int64), ("jumps", C.c_int64),
                 ("nonfinite_fixes", C.c_int64), ("flops", C.c_double),
-                ("device_ms", C.c_double)]
+                ("device_ms", C.c_double), ("svd_sweeps", C.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -477,6 +477,63 @@ def run_descriptors(desc: Descriptors, ctx=None) -> RunResult:
     return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
 
 
+class Session:
+    """A run held on the device (yaqs_analog_begin / advance / finish).
+
+    ``advance(n)`` evolves the next n recorded time indices of every
+    trajectory and returns their device time in ms."""
+
+    def __init__(self, desc: Descriptors, ctx=None):
+        from . import _lib
+        self.ctx = ctx or _lib.default_context()
+        self.desc = desc
+        h = C.c_void_p()
+        self.ctx.check(self.ctx._lib.yaqs_analog_begin(self.ctx.handle, C.byref(desc.mps), C.byref(desc.mpo),
+                                                       C.byref(desc.noise), desc.obs, desc.n_obs, C.byref(desc.cfg),
+                                                       C.byref(desc.rng), C.byref(h)))
+        self.handle = h
+
+    @property
+    def remaining(self) -> int:
+        return self.ctx._lib.yaqs_analog_remaining(self.handle)
+
+    def advance(self, n: int) -> float:
+        ms = C.c_double(0.0)
+        self.ctx.check(self.ctx._lib.yaqs_analog_advance(self.handle, n, C.byref(ms)))
+        return ms.value
+
+    PHASES = ("gemm", "mpo_apply", "lanczos_orth", "tridiag_exp", "svd_sweeps", "svd_vectors", "qr_factor",
+              "qr_formq", "norm_contraction", "env_update", "dissipation", "jump_step", "observables", "tdvp_sweep",
+              "step", "state_copy")
+
+    def profile(self) -> dict:
+        out = np.zeros(16)
+        self.ctx.check(self.ctx._lib.yaqs_analog_profile(self.handle, A.dptr(out)))
+        return dict(zip(self.PHASES, out.tolist()))
+
+    def finish(self) -> RunResult:
+        d = self.desc
+        nt, nobs, nout = d.num_traj, d.n_obs, d.n_out
+        traj = np.zeros((nt, max(nobs, 1), nout))
+        mean = np.zeros((max(nobs, 1), nout))
+        chi = np.zeros((nt, nout), dtype=np.int32)
+        st = A.RunStats()
+        h, self.handle = self.handle, None
+        self.ctx.check(self.ctx._lib.yaqs_analog_finish(h, A.dptr(traj), A.dptr(mean),
+                                                        chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st)))
+        return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
+
+
+def random_mps(length: int, chi: int, seed: int = 0) -> MPS:
+    """An MPS with every bond at min(2^b, 2^(L-b), chi) and Gaussian entries
+    (a saturated-bond-dimension start state; normalised by the engine)."""
+    rng = np.random.default_rng(seed)
+    dims = [min(2 ** min(b, length - b), chi) for b in range(length + 1)]
+    ts = [(rng.standard_normal((dims[i], 2, dims[i + 1])) + 1j * rng.standard_normal((dims[i], 2, dims[i + 1])))
+          for i in range(length)]
+    return MPS(length, tensors=ts)
+
+
 def run(initial_state: MPS, operator: MPO, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
         *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12, ctx=None) -> RunResult:
     """Simulator.run for an MPO (analog TJM).  Fills every observable's

@@ -12,6 +12,24 @@
 
 typedef double2 cplx;
 
+// Optional per-CTA phase timers (clock64 cycles), enabled when the host sets
+// g_prof to a [gridDim.x][PROF_N] buffer.  Thread 0 accumulates the CTA-level
+// elapsed time of each instrumented routine.
+#define PROF_N 16
+enum {
+  PF_GEMM = 0, PF_WAPPLY = 1, PF_ORTH = 2, PF_TRIDIAG = 3, PF_SVD = 4, PF_SVDVEC = 5, PF_QR = 6, PF_QRQ = 7,
+  PF_SCALAR = 8, PF_ENV = 9, PF_DISS = 10, PF_STOCH = 11, PF_EVAL = 12, PF_SWEEP = 13, PF_STEP = 14, PF_COPY = 15
+};
+__device__ unsigned long long* g_prof = nullptr;
+struct ProfScope {
+  long long t0;
+  int id;
+  __device__ __forceinline__ ProfScope(int i) : id(i) { t0 = (g_prof && threadIdx.x == 0) ? clock64() : 0; }
+  __device__ __forceinline__ ~ProfScope() {
+    if (g_prof && threadIdx.x == 0) g_prof[(long long)blockIdx.x * PROF_N + id] += (unsigned long long)(clock64() - t0);
+  }
+};
+
 __device__ __forceinline__ cplx cmk(double x, double y) { return make_double2(x, y); }
 __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ cplx csub(cplx a, cplx b) { return make_double2(a.x - b.x, a.y - b.y); }

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -25,6 +26,7 @@
 // Device program
 // ---------------------------------------------------------------------------
 __device__ void copy_state(Ctx& c, const DState& dst, const DState& src) {
+  ProfScope prof_scope_(PF_COPY);
   cta_copy(dst.a, src.a, c.P.mps_size);
   for (int b = threadIdx.x; b <= c.P.L; b += NT) dst.chi[b] = src.chi[b];
   if (threadIdx.x == 0) *dst.oc = *src.oc;
@@ -43,6 +45,7 @@ __device__ void sample(Ctx& c, const DState& phi, const DState& psi, int col) {
 }
 
 __device__ void run_step(Ctx& c, int j) {
+  ProfScope prof_scope_(PF_STEP);
   const DevParams& P = c.P;
   const int L = P.L;
   DState phi{P.phi + (long long)c.traj * P.mps_size, P.phi_chi + (long long)c.traj * (L + 1), P.phi_oc + c.traj};
@@ -116,7 +119,7 @@ struct CompSmem {
   LinalgSmem la;
 };
 
-__global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M, cplx* U, double* S, cplx* Vt,
+__global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M, cplx* U, double* S, cplx* SVt,
                                                     cplx* work, long long wstride, int* iwork) {
   extern __shared__ __align__(16) unsigned char smraw[];
   CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
@@ -132,9 +135,16 @@ __global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M,
   w.y = w0 + 4 * big;
   w.sig = reinterpret_cast<double*>(w0 + 4 * big + max(m, n));
   w.ord = iwork + (long long)b * SVD_MAX_COLS;
-  SvdResult r = dev_svd(M + (long long)m * n * b, m, n, w, sm.la, sm.e.r);
+  const cplx* Mb = M + (long long)m * n * b;
+  SvdResult r = dev_svd(Mb, m, n, SVD_LEFT, w, sm.la, sm.e.r, sm.e.u.svd);
   dev_svd_vectors(r, k, w, sm.e.r);
-  dev_svd_write(r, w, m, n, k, U + (long long)m * k * b, false, Vt + (long long)k * n * b, false);
+  cplx* Ub = U + (long long)m * k * b;
+  cplx* Sb = SVt + (long long)k * n * b;
+  cta_copy(Ub, w.Yo, (long long)m * k);
+  __syncthreads();
+  cta_gemm(gemm_args(k, n, m, w.Yo, m, 1, Mb, 1, m, Sb, 1, k, true, false), sm.e.u.gw.g);
+  for (long long e = threadIdx.x; e < (long long)k * n; e += NT)
+    if ((int)(e % k) >= r.rank) Sb[e] = make_double2(0.0, 0.0);
   for (int e = threadIdx.x; e < k; e += NT) S[(long long)k * b + e] = w.sig[e];
 }
 
@@ -359,7 +369,12 @@ struct yaqs_run {
   int* d_status = nullptr;
   unsigned long long* d_counters = nullptr;
   double* d_flops = nullptr;
+  unsigned long long* d_prof = nullptr;
   ~yaqs_run() {
+    if (d_prof) {
+      unsigned long long* z = nullptr;
+      cudaMemcpyToSymbol(g_prof, &z, sizeof(z));
+    }
     if (stream) cudaStreamSynchronize(stream);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -743,11 +758,28 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   run->d_flops = d_flops;
   run->launches.push_back(0);
   for (int j = (cfg->order == 2 ? 2 : 1); j < cfg->n_times; ++j) run->launches.push_back(j);
+  const char* pe = getenv("YAQS_PROFILE");
+  if (pe && pe[0] == '1') {
+    CUDA_TRY(ctx, dm.alloc(&run->d_prof, (size_t)slots * PROF_N));
+    CUDA_TRY(ctx, cudaMemset(run->d_prof, 0, (size_t)slots * PROF_N * sizeof(unsigned long long)));
+    CUDA_TRY(ctx, cudaMemcpyToSymbol(g_prof, &run->d_prof, sizeof(run->d_prof)));
+  }
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&run->e0));
   CUDA_TRY(ctx, cudaEventCreate(&run->e1));
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = guard.release();
+  return YAQS_OK;
+}
+
+int yaqs_analog_profile(yaqs_run* run, double* cycles) {
+  if (!run || !cycles) return set_err(nullptr, YAQS_E_ARG, "null argument");
+  for (int k = 0; k < PROF_N; ++k) cycles[k] = 0.0;
+  if (!run->d_prof) return YAQS_OK;
+  std::vector<unsigned long long> h((size_t)run->slots * PROF_N);
+  CUDA_TRY(run->ctx, cudaMemcpy(h.data(), run->d_prof, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  for (int sl = 0; sl < run->slots; ++sl)
+    for (int k = 0; k < PROF_N; ++k) cycles[k] += (double)h[(size_t)sl * PROF_N + k];
   return YAQS_OK;
 }
 
@@ -816,6 +848,7 @@ int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out, int32_
       stats->svds += cnt[s * 8 + 2];
       stats->jumps += cnt[s * 8 + 3];
       stats->nonfinite_fixes += cnt[s * 8 + 4];
+      stats->svd_sweeps += cnt[s * 8 + 5];
       stats->flops += fl[s];
     }
     stats->device_ms = run->device_ms;
@@ -850,6 +883,7 @@ int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const d
                      double* Vt) {
   if (!ctx || batch < 1 || m < 1 || n < 1 || std::min(m, n) > SVD_MAX_COLS || !M || !U || !S || !Vt)
     return set_err(ctx, YAQS_E_ARG, "bad svd arguments");
+  if (2 * (m + n) > SVD_SMEM_CPLX) return set_err(ctx, YAQS_E_UNSUPPORTED, "svd needs m + n <= 4096");
   std::lock_guard<std::mutex> lk(ctx->mu);
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int k = std::min(m, n);

@@ -69,6 +69,7 @@ __device__ __forceinline__ GemmArgs gemm_args(int M, int N, int K, const cplx* A
 
 // CTA-collective.  Ends with a __syncthreads() so C is visible to all.
 __device__ __noinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
+  ProfScope prof_scope_(PF_GEMM);
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
   const bool a_m_fast = (g.am == 1) || (g.ak != 1);

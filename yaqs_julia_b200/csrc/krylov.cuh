@@ -13,7 +13,7 @@
 #include "common.cuh"
 #include "gemm.cuh"
 
-#define WAPPLY_PT 64
+#define WAPPLY_PT 128
 #define WAPPLY_MAXI 32
 #define WAPPLY_MAXNNZ 1024
 #define KRYLOV_MAX 32
@@ -44,6 +44,7 @@ struct WApplySmem {
 // out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.
 __device__ __noinline__ void dev_wapply(const cplx* __restrict__ in, cplx* __restrict__ out, const WMat W,
                                         const WApplyGeom g, WApplySmem& ws) {
+  ProfScope prof_scope_(PF_WAPPLY);
   const int tid = threadIdx.x;
   for (int e = tid; e < W.nnz; e += NT) {
     ws.val[e] = W.val[e];
@@ -96,9 +97,17 @@ struct KrySmem {
   int m;
 };
 
+// Shared memory of one CTA.  The GEMM / MPO-apply staging and the SVD block
+// buffer are never live at the same time and share storage.
+#define SVD_SMEM_CPLX_K 8192
 struct EngineSmem {
-  GemmSmem g;
-  WApplySmem w;
+  union {
+    struct {
+      GemmSmem g;
+      WApplySmem w;
+    } gw;
+    cplx svd[SVD_SMEM_CPLX_K];
+  } u;
   RedScratch r;
   KrySmem k;
 };
@@ -108,7 +117,7 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   const int chil = h.chil, D = h.D, chir = h.chir, wl = h.wl, wr = h.wr;
   cta_gemm(gemm_args(chil * wl, D * chir, chil, h.L, 1, (long long)chil * wl, x, 1, chil, h.T1, 1,
                      (long long)chil * wl),
-           sm.g);
+           sm.u.gw.g);
   WApplyGeom g;
   g.n0 = chil;
   g.n1 = chir;
@@ -122,10 +131,10 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   g.no1 = D;
   g.oo1 = chil;
   g.oo2 = (long long)chil * D;
-  dev_wapply(h.T1, h.T2, h.W, g, sm.w);
+  dev_wapply(h.T1, h.T2, h.W, g, sm.u.gw.w);
   cta_gemm(gemm_args(chil * D, chir, wr * chir, h.T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
                      (long long)chil * D),
-           sm.g);
+           sm.u.gw.g);
 }
 
 __device__ __forceinline__ double heff_flops(int chil, int wl, int D, int chir, int wr) {
@@ -141,6 +150,7 @@ struct KrylovCfg {
 
 // Warp 0: y = exp(-i dt T) e_1 for the m x m Lanczos matrix in ks.
 __device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
+  ProfScope prof_scope_(PF_TRIDIAG);
   if (threadIdx.x >= 32) return;
   const int j = threadIdx.x;
   const bool on = j < m;
@@ -191,6 +201,7 @@ __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt,
     cplx* w = Q + qs * k;
     dev_heff(h, Q + qs * (k - 1), w, sm);
     ++mv;
+    ProfScope orth_scope_(PF_ORTH);
     double a_k = 0.0;
     for (int pass = 0; pass < 2; ++pass) {
       for (int j0 = 0; j0 < k; j0 += 8) {

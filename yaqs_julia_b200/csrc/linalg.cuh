@@ -27,6 +27,7 @@ struct LinalgSmem {
 // Factor H (m x n, col-major, ld m) in place: R in the upper triangle,
 // reflector vectors below, scalars in ls.tau.  CTA-collective.
 __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls, RedScratch& rs) {
+  ProfScope prof_scope_(PF_QR);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int kq = min(m, n);
   double fro2 = cta_norm2(H, (long long)m * n, rs);
@@ -74,6 +75,7 @@ __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls
 
 // Q (m x kq) of a factored H.  CTA-collective.
 __device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, LinalgSmem& ls) {
+  ProfScope prof_scope_(PF_QRQ);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int kq = min(m, n);
   for (long long e = tid; e < (long long)m * kq; e += NT) {
@@ -126,6 +128,7 @@ struct SvdWork {
 struct SvdResult {
   bool tr;
   int q, p, rank;  // rank = number of non-null singular values
+  int sweeps;
 };
 
 // Orthonormal completion of column k of Y (rows x *) against columns 0..k-1.
@@ -178,81 +181,196 @@ __device__ void dev_complete_column(cplx* Y, int rows, int k, cplx* y, RedScratc
   }
 }
 
-// SVD of M (m x n, col-major ld m), phase 1: Jacobi sweeps, sorting and
-// the sorted singular values in w.sig (null values set to 0).
-// CTA-collective.  Returns metadata (uniform in all threads).
-__device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, SvdWork& w, LinalgSmem& ls, RedScratch& rs) {
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+// Block size of the block-cyclic Jacobi ordering: blocks of b columns of B
+// (q rows) so that a pair of blocks fits the SVD_SMEM_CPLX shared buffer.
+// The CPU oracle uses the same rule.
+#define SVD_SMEM_CPLX 8192
+__host__ __device__ __forceinline__ int svd_block_size(int q, int p) {
+  int b = SVD_SMEM_CPLX / (2 * q);
+  if (b > 32) b = 32;
+  if (b > p) b = p;
+  if (b < 1) b = 1;
+  return b;
+}
+
+// Jacobi rotation parameters for columns with |b_i|^2 = al, |b_j|^2 = be,
+// b_i^H b_j = (gx, gy).  Same rotation as the oracle's
+//   zeta = (be-al)/(2|g|), t = sign(zeta)/(|zeta| + sqrt(1+zeta^2)),
+//   c = 1/sqrt(1+t^2), s = c t, e = g/|g|,
+// written with fewer dependent divisions/square roots:
+//   t = sign(d) 2|g| / (|d| + sqrt(d^2 + 4|g|^2)),  d = be - al.
+// Returns false when the pair is already orthogonal to tolerance.
+__device__ __forceinline__ bool jacobi_params(double al, double be, double gx, double gy, double tol, double& c,
+                                              cplx& se, cplx& sec) {
+  const double g2 = gx * gx + gy * gy;
+  if (!(g2 > tol * tol * (al * be))) return false;
+  const double rag = rsqrt(g2);
+  const double ag = g2 * rag;
+  const double d = be - al;
+  const double R = sqrt(fma(d, d, 4.0 * g2));
+  double t = 2.0 * ag / (fabs(d) + R);
+  if (d < 0.0) t = -t;
+  c = rsqrt(fma(t, t, 1.0));
+  const double f = c * t * rag;
+  se = make_double2(f * gx, f * gy);
+  sec = make_double2(f * gx, -f * gy);
+  return true;
+}
+
+// One Jacobi rotation pass over disjoint column pairs held in shared memory
+// (columns c of the stacked [B; X] block at sb + c*ld).  pairs(k) gives the
+// k-th pair as (i, j) local column indices, -1 to skip.  Each half-warp
+// takes one pair.
+template <class PairFn>
+__device__ __forceinline__ void smem_rotate_round(cplx* sb, int ld, int q, int rows, int npairs, PairFn pairs,
+                                                  double tol, int* rot) {
+  const int hl = threadIdx.x & 15, hw = threadIdx.x >> 4;
+  const unsigned mask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  for (int k = hw; k < npairs; k += NT / 16) {
+    int i, j;
+    pairs(k, i, j);
+    if (i < 0 || j < 0) continue;
+    cplx* bi = sb + (long long)ld * i;
+    cplx* bj = sb + (long long)ld * j;
+    double al = 0.0, be = 0.0, gx = 0.0, gy = 0.0;
+    for (int r = hl; r < q; r += 16) {
+      cplx x = bi[r], y = bj[r];
+      al += cabs2(x);
+      be += cabs2(y);
+      gx += x.x * y.x + x.y * y.y;
+      gy += x.x * y.y - x.y * y.x;
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      al += __shfl_xor_sync(mask, al, o);
+      be += __shfl_xor_sync(mask, be, o);
+      gx += __shfl_xor_sync(mask, gx, o);
+      gy += __shfl_xor_sync(mask, gy, o);
+    }
+    double c;
+    cplx se, sec;
+    if (!jacobi_params(al, be, gx, gy, tol, c, se, sec)) continue;
+    if (hl == 0) atomicAdd(rot, 1);
+    for (int r = hl; r < rows; r += 16) {
+      cplx x = bi[r], y = bj[r];
+      bi[r] = csub(cscale(x, c), cmul(sec, y));
+      bj[r] = cadd(cmul(se, x), cscale(y, c));
+    }
+  }
+  __syncthreads();
+}
+
+// Stage columns [c0, c0+nc0) and [c1, c1+nc1) of B into sb (ld = q), or
+// write them back.
+__device__ __forceinline__ void svd_stage(cplx* sb, int ld, const SvdWork& w, int q, int c0, int nc0, int c1, int nc1,
+                                          bool store) {
+  const int nc = nc0 + nc1;
+  for (long long e = threadIdx.x; e < (long long)nc * ld; e += NT) {
+    int r = (int)(e % ld), lc = (int)(e / ld);
+    int col = lc < nc0 ? c0 + lc : c1 + (lc - nc0);
+    cplx* g = w.B + (long long)q * col + r;
+    if (store) *g = sb[e];
+    else sb[e] = *g;
+  }
+  __syncthreads();
+}
+
+// SVD of M (m x n, col-major ld m), phase 1.  side LEFT asks for the left
+// singular vectors (orthonormal U, m-vectors), side RIGHT for the right ones
+// (orthonormal V, n-vectors).  QR-preconditioned one-sided Jacobi
+// (Drmac-Veselic): LEFT factors M^H = Q R and orthogonalises the columns of
+// B = R^H (m x k); RIGHT factors M = Q R and orthogonalises B = R^H
+// (n x k); k = min(m, n).  Either way B's columns converge to (vectors) x
+// Sigma.  Jacobi runs in the block-cyclic order (per sweep: every diagonal
+// block with a round-robin pass, then every pair of blocks in round-robin
+// order with b rounds of disjoint cross pairs) on blocks staged in the
+// shared buffer sb (SVD_SMEM_CPLX elements).  Leaves the sorted singular
+// values in w.sig (nulls set to 0).  CTA-collective; returns metadata.
+enum { SVD_LEFT = 0, SVD_RIGHT = 1 };
+__device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side, SvdWork& w, LinalgSmem& ls,
+                                          RedScratch& rs, cplx* sb) {
+  ProfScope prof_scope_(PF_SVD);
+  const int tid = threadIdx.x;
   SvdResult res;
-  res.tr = m < n;
-  const int q = res.tr ? n : m;
-  const int p = res.tr ? m : n;
+  res.tr = side == SVD_RIGHT;
+  const int mm = res.tr ? m : n;  // rows of the factored matrix H
+  const int nn = res.tr ? n : m;
+  const int k = min(m, n);
+  const int q = nn, p = k;
   res.q = q;
   res.p = p;
+  res.sweeps = 0;
+  cplx* H = w.X;
+  for (long long e = tid; e < (long long)mm * nn; e += NT) {
+    int r = (int)(e % mm), c = (int)(e / mm);
+    H[e] = res.tr ? M[e] : cconj(M[c + (long long)m * r]);
+  }
+  __syncthreads();
+  dev_qr_factor(H, mm, nn, ls, rs);
+  // B = R^H (nn x k): B[r, c] = conj(R[c, r]) for c <= r
   for (long long e = tid; e < (long long)q * p; e += NT) {
     int r = (int)(e % q), c = (int)(e / q);
-    w.B[e] = res.tr ? cconj(M[c + (long long)m * r]) : M[e];
-  }
-  for (long long e = tid; e < (long long)p * p; e += NT) {
-    int r = (int)(e % p), c = (int)(e / p);
-    w.X[e] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    w.B[e] = (c <= r) ? cconj(H[c + (long long)mm * r]) : make_double2(0.0, 0.0);
   }
   __syncthreads();
   const double tol = 2.220446049250313e-16 * q;
-  const int pe = p + (p & 1);
-  for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && pe > 1; ++sweep) {
+  const int ld = q;
+  const int b = svd_block_size(q, p);
+  const int nb = (p + b - 1) / b;
+  const int nbe = nb + (nb & 1);
+  const int be2 = b + (b & 1);
+  for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS; ++sweep) {
     if (tid == 0) ls.rot_count = 0;
     __syncthreads();
-    for (int round = 0; round < pe - 1; ++round) {
-      for (int pr = wid; pr < pe / 2; pr += NW) {
-        int ta = pr, tb = pe - 1 - pr;
-        int a = ta == 0 ? 0 : ((ta - 1 - round + 2 * (pe - 1)) % (pe - 1)) + 1;
-        int b = tb == 0 ? 0 : ((tb - 1 - round + 2 * (pe - 1)) % (pe - 1)) + 1;
-        int i = min(a, b), j = max(a, b);
-        if (j >= p) continue;
-        cplx* bi = w.B + (long long)q * i;
-        cplx* bj = w.B + (long long)q * j;
-        double al = 0.0, be = 0.0, gx = 0.0, gy = 0.0;
-        for (int r = lane; r < q; r += 32) {
-          cplx x = bi[r], y = bj[r];
-          al += cabs2(x);
-          be += cabs2(y);
-          gx += x.x * y.x + x.y * y.y;
-          gy += x.x * y.y - x.y * y.x;
-        }
-        al = warp_sum(al);
-        be = warp_sum(be);
-        gx = warp_sum(gx);
-        gy = warp_sum(gy);
-        double ag = sqrt(gx * gx + gy * gy);
-        if (!(ag > tol * sqrt(al * be))) continue;
-        if (lane == 0) atomicAdd(&ls.rot_count, 1);
-        double zeta = (be - al) / (2.0 * ag);
-        double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        double c = 1.0 / sqrt(1.0 + t * t);
-        double s = c * t;
-        cplx e = make_double2(gx / ag, gy / ag);
-        cplx se = cscale(e, s), sec = cscale(cconj(e), s);
-        for (int r = lane; r < q; r += 32) {
-          cplx x = bi[r], y = bj[r];
-          bi[r] = csub(cscale(x, c), cmul(sec, y));
-          bj[r] = cadd(cmul(se, x), cscale(y, c));
-        }
-        cplx* xi = w.X + (long long)p * i;
-        cplx* xj = w.X + (long long)p * j;
-        for (int r = lane; r < p; r += 32) {
-          cplx x = xi[r], y = xj[r];
-          xi[r] = csub(cscale(x, c), cmul(sec, y));
-          xj[r] = cadd(cmul(se, x), cscale(y, c));
-        }
+    for (int I = 0; I < nb; ++I) {
+      const int c0 = I * b, nc = min(b, p - c0);
+      svd_stage(sb, ld, w, q, c0, nc, 0, 0, false);
+      for (int round = 0; round < be2 - 1; ++round) {
+        smem_rotate_round(sb, ld, q, q, be2 / 2,
+                          [&](int pr, int& i, int& j) {
+                            int ta = pr, tb = be2 - 1 - pr;
+                            int a = ta == 0 ? 0 : ((ta - 1 - round + 2 * (be2 - 1)) % (be2 - 1)) + 1;
+                            int c = tb == 0 ? 0 : ((tb - 1 - round + 2 * (be2 - 1)) % (be2 - 1)) + 1;
+                            i = min(a, c);
+                            j = max(a, c);
+                            if (j >= nc) i = j = -1;
+                          },
+                          tol, &ls.rot_count);
       }
-      __syncthreads();
+      svd_stage(sb, ld, w, q, c0, nc, 0, 0, true);
+    }
+    for (int round = 0; round < nbe - 1; ++round) {
+      for (int pr = 0; pr < nbe / 2; ++pr) {
+        int ta = pr, tb = nbe - 1 - pr;
+        int A = ta == 0 ? 0 : ((ta - 1 - round + 2 * (nbe - 1)) % (nbe - 1)) + 1;
+        int Bk = tb == 0 ? 0 : ((tb - 1 - round + 2 * (nbe - 1)) % (nbe - 1)) + 1;
+        int I = min(A, Bk), J = max(A, Bk);
+        if (J >= nb) continue;
+        const int c0 = I * b, n0 = min(b, p - c0), c1 = J * b, n1 = min(b, p - c1);
+        svd_stage(sb, ld, w, q, c0, n0, c1, n1, false);
+        for (int t = 0; t < b; ++t) {
+          smem_rotate_round(sb, ld, q, q, b,
+                            [&](int kk, int& i, int& j) {
+                              int jj = (kk + t) % b;
+                              if (kk >= n0 || jj >= n1) {
+                                i = j = -1;
+                              } else {
+                                i = kk;
+                                j = n0 + jj;
+                              }
+                            },
+                            tol, &ls.rot_count);
+        }
+        svd_stage(sb, ld, w, q, c0, n0, c1, n1, true);
+      }
     }
     int rc = ls.rot_count;
     __syncthreads();
+    res.sweeps = sweep + 1;
     if (rc == 0) break;
   }
   // singular values
+  const int lane = tid & 31, wid = tid >> 5;
   for (int c = wid; c < p; c += NW) {
     const cplx* bc = w.B + (long long)q * c;
     double s = 0.0;
@@ -293,10 +411,11 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, SvdWork& 
   return res;
 }
 
-// Phase 2: sorted left/right vectors Yo (q x need), Zo (p x need):
-// Yo = B[:,ord[k]]/sigma_k, Zo = X[:,ord[k]] for non-null k, orthonormal
-// completions for null k < need.  CTA-collective.
+// Phase 2: the requested orthonormal vectors Yo (q x need): column k is
+// B[:, ord[k]] / sigma_k for non-null k and an orthonormal completion for
+// null k < need.  CTA-collective.
 __device__ __noinline__ void dev_svd_vectors(const SvdResult& res, int need, SvdWork& w, RedScratch& rs) {
+  ProfScope prof_scope_(PF_SVDVEC);
   const int tid = threadIdx.x, q = res.q, p = res.p;
   need = min(need, p);
   const int ng = min(need, res.rank);
@@ -304,15 +423,8 @@ __device__ __noinline__ void dev_svd_vectors(const SvdResult& res, int need, Svd
     int r = (int)(e % q), k = (int)(e / q);
     w.Yo[e] = cscale(w.B[r + (long long)q * w.ord[k]], 1.0 / w.sig[k]);
   }
-  for (long long e = tid; e < (long long)p * ng; e += NT) {
-    int r = (int)(e % p), k = (int)(e / p);
-    w.Zo[e] = w.X[r + (long long)p * w.ord[k]];
-  }
   __syncthreads();
-  for (int k = res.rank; k < need; ++k) {
-    dev_complete_column(w.Yo, q, k, w.y, rs);
-    dev_complete_column(w.Zo, p, k, w.y, rs);
-  }
+  for (int k = res.rank; k < need; ++k) dev_complete_column(w.Yo, q, k, w.y, rs);
 }
 
 // Truncation ranks (see the oracle for the reference lines they restate).
@@ -345,22 +457,3 @@ __device__ __forceinline__ int keep_relative(const double* S, int n, double thr,
   return max(1, min(rank, max_bond));
 }
 
-// Write the truncated factors of an SVD: U (m x keep, ld m) and
-// Vt (keep x n, ld keep).  scaleU / scaleV multiply the columns of U or
-// the rows of Vt by S.  CTA-collective.
-__device__ __forceinline__ void dev_svd_write(const SvdResult& r, const SvdWork& w, int m, int n, int keep,
-                                              cplx* U, bool scaleU, cplx* Vt, bool scaleV) {
-  for (long long e = threadIdx.x; e < (long long)m * keep; e += NT) {
-    int i = (int)(e % m), k = (int)(e / m);
-    cplx v = r.tr ? w.Zo[i + (long long)r.p * k] : w.Yo[i + (long long)r.q * k];
-    if (scaleU) v = cscale(v, w.sig[k]);
-    U[e] = v;
-  }
-  for (long long e = threadIdx.x; e < (long long)keep * n; e += NT) {
-    int k = (int)(e % keep), c = (int)(e / keep);
-    cplx v = r.tr ? cconj(w.Yo[c + (long long)r.q * k]) : cconj(w.Zo[c + (long long)r.p * k]);
-    if (scaleV) v = cscale(v, w.sig[k]);
-    Vt[e] = v;
-  }
-  __syncthreads();
-}

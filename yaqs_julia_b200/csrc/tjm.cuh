@@ -181,7 +181,7 @@ __device__ void qr_right(Ctx& c, const DState& s, int i) {
   dev_qr_factor(H, m, r, c.sm.la, c.sm.e.r);
   dev_qr_formq(H, m, r, A, c.sm.la);
   dev_qr_extract_r(H, m, r, Rb);
-  cta_gemm(gemm_args(rn, 2 * r2, r, Rb, 1, rn, An, 1, r, T, 1, rn), c.sm.e.g);
+  cta_gemm(gemm_args(rn, 2 * r2, r, Rb, 1, rn, An, 1, r, T, 1, rn), c.sm.e.u.gw.g);
   cta_copy(An, T, (long long)rn * 2 * r2);
   set_chi(c, s, i + 1, rn);
 }
@@ -208,7 +208,7 @@ __device__ void lq_left(Ctx& c, const DState& s, int i) {
     A[e] = cconj(Qh[cc + (long long)n2 * k]);
   }
   __syncthreads();
-  cta_gemm(gemm_args(2 * lp, rn, l, Ap, 1, 2 * lp, Rb, rn, 1, H, 1, 2 * lp, false, true), c.sm.e.g);
+  cta_gemm(gemm_args(2 * lp, rn, l, Ap, 1, 2 * lp, Rb, rn, 1, H, 1, 2 * lp, false, true), c.sm.e.u.gw.g);
   cta_copy(Ap, H, (long long)2 * lp * rn);
   set_chi(c, s, i, rn);
 }
@@ -240,6 +240,7 @@ __device__ void normalize_state(Ctx& c, const DState& s) {
 
 // Re <psi|psi> by full contraction (scalar_product, MPS.jl:528-585).
 __device__ double scalar_product(Ctx& c, const DState& s) {
+  ProfScope prof_scope_(PF_SCALAR);
   cplx* Ea = c.ws + c.P.lay.tA;
   cplx* Eb = c.ws + c.P.lay.tB;
   cplx* T = c.ws + c.P.lay.tC;
@@ -248,8 +249,8 @@ __device__ double scalar_product(Ctx& c, const DState& s) {
   for (int i = 0; i < c.P.L; ++i) {
     const int l = s.chi[i], r = s.chi[i + 1];
     const cplx* A = site_ptr(c, s, i);
-    cta_gemm(gemm_args(l, 2 * r, l, Ea, l, 1, A, 1, l, T, 1, l), c.sm.e.g);
-    cta_gemm(gemm_args(r, r, 2 * l, T, 2 * l, 1, A, 1, 2 * l, Eb, 1, r, false, true), c.sm.e.g);
+    cta_gemm(gemm_args(l, 2 * r, l, Ea, l, 1, A, 1, l, T, 1, l), c.sm.e.u.gw.g);
+    cta_gemm(gemm_args(r, r, 2 * l, T, 2 * l, 1, A, 1, 2 * l, Eb, 1, r, false, true), c.sm.e.u.gw.g);
     cplx* t = Ea;
     Ea = Eb;
     Eb = t;
@@ -276,12 +277,13 @@ __device__ void identity_env(Ctx& c, cplx* E, int dim, int w) {
 
 // EL[i+1] from EL[i], A_i, W_i  (update_left_environment)
 __device__ void update_left(Ctx& c, const DState& s, int i) {
+  ProfScope prof_scope_(PF_ENV);
   const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
   const cplx* A = site_ptr(c, s, i);
   cplx* T1 = c.ws + c.P.lay.T1;
   cplx* T2 = c.ws + c.P.lay.T2;
   cta_gemm(gemm_args(l * wl, 2 * r, l, envL(c, i), 1, (long long)l * wl, A, 1, l, T1, 1, (long long)l * wl),
-           c.sm.e.g);
+           c.sm.e.u.gw.g);
   WApplyGeom g;
   g.n0 = l;
   g.n1 = r;
@@ -295,17 +297,18 @@ __device__ void update_left(Ctx& c, const DState& s, int i) {
   g.no1 = 2;
   g.oo1 = l;
   g.oo2 = 2 * l;
-  dev_wapply(T1, T2, c.P.wm_envL[i], g, c.sm.e.w);
-  cta_gemm(gemm_args(r, wr * r, 2 * l, A, 2 * l, 1, T2, 1, 2 * l, envL(c, i + 1), 1, r, true, false), c.sm.e.g);
+  dev_wapply(T1, T2, c.P.wm_envL[i], g, c.sm.e.u.gw.w);
+  cta_gemm(gemm_args(r, wr * r, 2 * l, A, 2 * l, 1, T2, 1, 2 * l, envL(c, i + 1), 1, r, true, false), c.sm.e.u.gw.g);
 }
 
 // ER[i] from ER[i+1], A_i, W_i  (update_right_environment)
 __device__ void update_right(Ctx& c, const DState& s, int i) {
+  ProfScope prof_scope_(PF_ENV);
   const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
   const cplx* A = site_ptr(c, s, i);
   cplx* T1 = c.ws + c.P.lay.T1;
   cplx* T2 = c.ws + c.P.lay.T2;
-  cta_gemm(gemm_args(2 * l, r * wr, r, A, 1, 2 * l, envR(c, i + 1), (long long)r * wr, 1, T1, 1, 2 * l), c.sm.e.g);
+  cta_gemm(gemm_args(2 * l, r * wr, r, A, 1, 2 * l, envR(c, i + 1), (long long)r * wr, 1, T1, 1, 2 * l), c.sm.e.u.gw.g);
   WApplyGeom g;
   g.n0 = l;
   g.n1 = r;
@@ -319,8 +322,8 @@ __device__ void update_right(Ctx& c, const DState& s, int i) {
   g.no1 = 2;
   g.oo1 = 1;
   g.oo2 = 2 * r;
-  dev_wapply(T1, T2, c.P.wm_envR[i], g, c.sm.e.w);
-  cta_gemm(gemm_args(l, wl * l, 2 * r, A, 1, l, T2, 1, 2 * r, envR(c, i), 1, l, true, false), c.sm.e.g);
+  dev_wapply(T1, T2, c.P.wm_envR[i], g, c.sm.e.u.gw.w);
+  cta_gemm(gemm_args(l, wl * l, 2 * r, A, 1, l, T2, 1, 2 * r, envR(c, i), 1, l, true, false), c.sm.e.u.gw.g);
 }
 
 // ---------------------------------------------------------------------------
@@ -350,7 +353,7 @@ __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, con
 __device__ void merge(Ctx& c, const DState& s, int i, cplx* th) {
   const int l = s.chi[i], m = s.chi[i + 1], r = s.chi[i + 2];
   cta_gemm(gemm_args(2 * l, 2 * r, m, site_ptr(c, s, i), 1, 2 * l, site_ptr(c, s, i + 1), 1, m, th, 1, 2 * l),
-           c.sm.e.g);
+           c.sm.e.u.gw.g);
 }
 
 __device__ SvdWork svd_work(const Ctx& c) {
@@ -380,17 +383,22 @@ __device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
 }
 
 // SVD split of theta (2l x 2r) into sites i (l,2,keep) and i+1 (keep,2,r).
-// rule 0: TDVP (absolute, min 2); rule 1: relative.  S goes left if s_left.
+// rule 0: TDVP (absolute, min 2); rule 1: relative.  With s_left the
+// singular values go left (U S | Vt, Vt orthonormal, Algorithms.jl:701-708),
+// otherwise right (U | S Vt, U orthonormal, Algorithms.jl:656-663).  The
+// scaled factor is computed as a product with theta and is exactly zero for
+// null singular values.
 __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, int rule, bool s_left) {
   const int m = 2 * l, n = 2 * r;
   fix_nonfinite(c, th, (long long)m * n);
   SvdWork w = svd_work(c);
-  SvdResult res = dev_svd(th, m, n, w, c.sm.la, c.sm.e.r);
+  SvdResult res = dev_svd(th, m, n, s_left ? SVD_RIGHT : SVD_LEFT, w, c.sm.la, c.sm.e.r, c.sm.e.u.svd);
   if (threadIdx.x == 0) {
     int keep = rule == 0 ? keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond)
                          : keep_relative(w.sig, res.p, c.P.thr, c.P.max_bond);
     c.sm.bcast_i[0] = keep;
     c.cnt[2] += 1;
+    c.cnt[5] += res.sweeps;
   }
   __syncthreads();
   const int keep = c.sm.bcast_i[0];
@@ -401,11 +409,29 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
     return;
   }
   dev_svd_vectors(res, keep, w, c.sm.e.r);
-  dev_svd_write(res, w, m, n, keep, site_ptr(c, s, i), s_left, site_ptr(c, s, i + 1), !s_left);
+  cplx* Lt = site_ptr(c, s, i);
+  cplx* Rt = site_ptr(c, s, i + 1);
+  if (!s_left) {
+    cta_copy(Lt, w.Yo, (long long)m * keep);
+    __syncthreads();
+    cta_gemm(gemm_args(keep, n, m, w.Yo, m, 1, th, 1, m, Rt, 1, keep, true, false), c.sm.e.u.gw.g);
+    for (long long e = threadIdx.x; e < (long long)keep * n; e += NT)
+      if ((int)(e % keep) >= res.rank) Rt[e] = make_double2(0.0, 0.0);
+  } else {
+    for (long long e = threadIdx.x; e < (long long)keep * n; e += NT) {
+      int k = (int)(e % keep), cc = (int)(e / keep);
+      Rt[e] = cconj(w.Yo[cc + (long long)n * k]);
+    }
+    cta_gemm(gemm_args(m, keep, n, th, 1, m, w.Yo, 1, n, Lt, 1, m), c.sm.e.u.gw.g);
+    for (long long e = threadIdx.x; e < (long long)m * keep; e += NT)
+      if ((int)(e / m) >= res.rank) Lt[e] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
   set_chi(c, s, i + 1, keep);
 }
 
 __device__ void tdvp_sweep(Ctx& c, const DState& s) {
+  ProfScope prof_scope_(PF_SWEEP);
   const int L = c.P.L;
   const double dt = c.P.dt;
   shift_oc(c, s, 0);
@@ -496,6 +522,7 @@ __device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const
 // Dissipation (Dissipation.jl:37-159)
 // ---------------------------------------------------------------------------
 __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt) {
+  ProfScope prof_scope_(PF_DISS);
   const int L = c.P.L;
   if (!c.P.noise_present || c.P.all_zero) {
     for (int i = L - 1; i >= 1 && !c.sm.fail; --i) shift_oc(c, s, i - 1);
@@ -540,6 +567,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt)
 // Stochastic process (StochasticProcess.jl:219-330)
 // ---------------------------------------------------------------------------
 __device__ void stochastic_process(Ctx& c, const DState& s, double dt) {
+  ProfScope prof_scope_(PF_STOCH);
   const int L = c.P.L;
   const double dp = 1.0 - scalar_product(c, s);
   bool jump = false;
@@ -628,6 +656,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt) {
 // Observables
 // ---------------------------------------------------------------------------
 __device__ void evaluate(Ctx& c, const DState& s, int col) {
+  ProfScope prof_scope_(PF_EVAL);
   const int ncols = c.P.ncols;
   for (int k = 0; k < c.P.nobs && !c.sm.fail; ++k) {
     const DevObs& o = c.P.obs[k];
@@ -644,7 +673,7 @@ __device__ void evaluate(Ctx& c, const DState& s, int col) {
       shift_oc(c, s, o.s0);
       const int l = s.chi[o.s0], r = s.chi[o.s0 + 1];
       SvdWork w = svd_work(c);
-      SvdResult res = dev_svd(site_ptr(c, s, o.s0), 2 * l, r, w, c.sm.la, c.sm.e.r);
+      SvdResult res = dev_svd(site_ptr(c, s, o.s0), 2 * l, r, SVD_LEFT, w, c.sm.la, c.sm.e.r, c.sm.e.u.svd);
       if (threadIdx.x == 0) {
         double nsq = 0.0;
         for (int e = 0; e < res.p; ++e) nsq += w.sig[e] * w.sig[e];
