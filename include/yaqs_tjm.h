@@ -207,6 +207,8 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0,
                       yaqs_run** out);
 int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms);
 int yaqs_analog_remaining(const yaqs_run* run);
+/* Counters of the run so far (as returned by yaqs_analog_finish). */
+int yaqs_analog_stats(yaqs_run* run, yaqs_run_stats* stats);
 int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out,
                        int32_t* maxchi_out, yaqs_run_stats* stats);
 

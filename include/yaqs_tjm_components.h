@@ -48,6 +48,10 @@ int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D
                            const double* x, double dt, int32_t krylov_dim, double krylov_tol,
                            double krylov_exit_tol, double* out, int32_t* matvecs);
 
+/* Measured FP64 FMA throughput of the device (TFLOP/s, best of 5 runs of a
+ * DFMA loop over every SM): the denominator of the FP64 form's roofline. */
+int yaqs_fp64_peak(yaqs_ctx* ctx, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

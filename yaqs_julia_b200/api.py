@@ -506,6 +506,11 @@ class Session:
               "qr_formq", "norm_contraction", "env_update", "dissipation", "jump_step", "observables", "tdvp_sweep",
               "step", "state_copy")
 
+    def stats(self) -> dict:
+        st = A.RunStats()
+        self.ctx.check(self.ctx._lib.yaqs_analog_stats(self.handle, C.byref(st)))
+        return st.as_dict()
+
     def profile(self) -> dict:
         out = np.zeros(16)
         self.ctx.check(self.ctx._lib.yaqs_analog_profile(self.handle, A.dptr(out)))

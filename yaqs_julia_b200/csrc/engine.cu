@@ -192,6 +192,23 @@ __global__ void __launch_bounds__(NT, 1) expm_kernel(int chil, int D, int chir, 
   if (threadIdx.x == 0) matvecs[b] = mv;
 }
 
+// FP64 FMA throughput probe: 8 independent chains per thread.
+__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fma(x0, a, b);
+    x1 = fma(x1, a, b);
+    x2 = fma(x2, a, b);
+    x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b);
+    x5 = fma(x5, a, b);
+    x6 = fma(x6, a, b);
+    x7 = fma(x7, a, b);
+  }
+  double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 12345.678) out[0] = s;  // keep the chains live
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -772,6 +789,35 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   return YAQS_OK;
 }
 
+static int collect_stats(yaqs_run* run, yaqs_run_stats* stats) {
+  yaqs_ctx* ctx = run->ctx;
+  const int slots = run->slots;
+  std::vector<unsigned long long> cnt((size_t)slots * 8);
+  std::vector<double> fl(slots);
+  CUDA_TRY(ctx, cudaMemcpy(cnt.data(), run->d_counters, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(fl.data(), run->d_flops, fl.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  memset(stats, 0, sizeof(*stats));
+  for (int s = 0; s < slots; ++s) {
+    stats->matvecs += cnt[s * 8 + 0];
+    stats->krylov_solves += cnt[s * 8 + 1];
+    stats->svds += cnt[s * 8 + 2];
+    stats->jumps += cnt[s * 8 + 3];
+    stats->nonfinite_fixes += cnt[s * 8 + 4];
+    stats->svd_sweeps += cnt[s * 8 + 5];
+    stats->flops += fl[s];
+  }
+  stats->device_ms = run->device_ms;
+  return YAQS_OK;
+}
+
+int yaqs_analog_stats(yaqs_run* run, yaqs_run_stats* stats) {
+  if (!run || !stats) return set_err(nullptr, YAQS_E_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(run->ctx->mu);
+  CUDA_TRY(run->ctx, cudaSetDevice(run->ctx->device));
+  CUDA_TRY(run->ctx, cudaStreamSynchronize(run->stream));
+  return collect_stats(run, stats);
+}
+
 int yaqs_analog_profile(yaqs_run* run, double* cycles) {
   if (!run || !cycles) return set_err(nullptr, YAQS_E_ARG, "null argument");
   for (int k = 0; k < PROF_N; ++k) cycles[k] = 0.0;
@@ -837,21 +883,8 @@ int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out, int32_
       }
   }
   if (stats) {
-    std::vector<unsigned long long> cnt((size_t)slots * 8);
-    std::vector<double> fl(slots);
-    CUDA_TRY(ctx, cudaMemcpy(cnt.data(), run->d_counters, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-    CUDA_TRY(ctx, cudaMemcpy(fl.data(), run->d_flops, fl.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    memset(stats, 0, sizeof(*stats));
-    for (int s = 0; s < slots; ++s) {
-      stats->matvecs += cnt[s * 8 + 0];
-      stats->krylov_solves += cnt[s * 8 + 1];
-      stats->svds += cnt[s * 8 + 2];
-      stats->jumps += cnt[s * 8 + 3];
-      stats->nonfinite_fixes += cnt[s * 8 + 4];
-      stats->svd_sweeps += cnt[s * 8 + 5];
-      stats->flops += fl[s];
-    }
-    stats->device_ms = run->device_ms;
+    int st = collect_stats(run, stats);
+    if (st != YAQS_OK) return st;
   }
   for (int t = 0; t < num_traj; ++t) {
     if (status[t] != 0) {
@@ -908,6 +941,35 @@ int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const d
   CUDA_TRY(ctx, cudaMemcpy(U, dU, (size_t)batch * m * k * sizeof(cplx), cudaMemcpyDeviceToHost));
   CUDA_TRY(ctx, cudaMemcpy(Vt, dVt, (size_t)batch * k * n * sizeof(cplx), cudaMemcpyDeviceToHost));
   CUDA_TRY(ctx, cudaMemcpy(S, dS, (size_t)batch * k * sizeof(double), cudaMemcpyDeviceToHost));
+  return YAQS_OK;
+}
+
+int yaqs_fp64_peak(yaqs_ctx* ctx, double* tflops) {
+  if (!ctx || !tflops) return set_err(ctx, YAQS_E_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  DevMem dm;
+  double* d;
+  CUDA_TRY(ctx, dm.alloc(&d, 1));
+  const int blocks = ctx->sms * 8, iters = 1 << 16;
+  fp64_probe_kernel<<<blocks, 256>>>(d, 1024, 0.999999, 1e-7);  // warm-up
+  cudaEvent_t e0, e1;
+  CUDA_TRY(ctx, cudaEventCreate(&e0));
+  CUDA_TRY(ctx, cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 5; ++rep) {
+    cudaEventRecord(e0);
+    fp64_probe_kernel<<<blocks, 256>>>(d, iters, 0.999999, 1e-7);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CUDA_TRY(ctx, cudaGetLastError());
+  *tflops = 2.0 * 8.0 * iters * (double)blocks * 256 / (best * 1e-3) / 1e12;
   return YAQS_OK;
 }
 
