@@ -48,6 +48,28 @@ int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D
                            const double* x, double dt, int32_t krylov_dim, double krylov_tol,
                            double krylov_exit_tol, double* out, int32_t* matvecs);
 
+/*
+ * yaqs_batched_svd without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: a host whose device
+ * memory is owned by its own pool allocator (Julia's CUDA.jl, PyTorch), or
+ * a code path where an allocation would synchronise the device or could fail
+ * mid-run.  M, U, S and SVt are DEVICE pointers with the layouts of
+ * yaqs_batched_svd; the call enqueues one kernel on `stream` (a
+ * cudaStream_t, NULL for the default stream) and returns without waiting.
+ * Scratch comes from a fixed 8 MiB array compiled into the library (held by
+ * every GPU that loads it until exit): batch * (4 max(m,n)^2 + max(m,n) +
+ * 256) complex values plus 256 ints per problem must fit, otherwise the call
+ * returns YAQS_E_ARG before launching anything.  The first call on a device
+ * looks up the array's device address and sets the kernel's shared-memory
+ * limit; make that first call before any stream capture.  All calls share
+ * the one array and every call rewrites the scratch words it reads, so a
+ * call never depends on an earlier one; calls that overlap on the GPU (two
+ * streams, two threads) race on the array and must be serialised by the
+ * caller.
+ */
+int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M,
+                             double* U, double* S, double* SVt, void* stream);
+
 /* Measured FP64 FMA throughput of the device (TFLOP/s, best of 5 runs of a
  * DFMA loop over every SM): the denominator of the FP64 form's roofline. */
 int yaqs_fp64_peak(yaqs_ctx* ctx, double* tflops);

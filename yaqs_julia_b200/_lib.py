@@ -44,6 +44,8 @@ def lib():
         L.yaqs_analog_stats.argtypes = [C.c_void_p, P(A.RunStats)]
         L.yaqs_analog_finish.argtypes = [C.c_void_p, A.DPTR, A.DPTR, P(C.c_int32), P(A.RunStats)]
         L.yaqs_fp64_peak.argtypes = [C.c_void_p, P(C.c_double)]
+        L.yaqs_batched_svd_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4 + [
+            C.c_void_p]
         L.yaqs_batched_svd.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4
         L.yaqs_batched_qr.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 3
         L.yaqs_batched_project_site.argtypes = [C.c_void_p] + [C.c_int32] * 6 + [A.DPTR] * 5

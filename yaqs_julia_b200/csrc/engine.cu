@@ -866,7 +866,7 @@ int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out, int32_
   std::lock_guard<std::mutex> lk(ctx->mu);
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   CUDA_TRY(ctx, cudaStreamSynchronize(run->stream));
-  const int num_traj = run->num_traj, n_obs = run->n_obs, ncols = run->ncols, slots = run->slots;
+  const int num_traj = run->num_traj, n_obs = run->n_obs, ncols = run->ncols;
   std::vector<double> out((size_t)num_traj * std::max(n_obs, 1) * ncols);
   std::vector<int> status(num_traj);
   CUDA_TRY(ctx, cudaMemcpy(out.data(), run->d_traj_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -941,6 +941,63 @@ int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const d
   CUDA_TRY(ctx, cudaMemcpy(U, dU, (size_t)batch * m * k * sizeof(cplx), cudaMemcpyDeviceToHost));
   CUDA_TRY(ctx, cudaMemcpy(Vt, dVt, (size_t)batch * k * n * sizeof(cplx), cudaMemcpyDeviceToHost));
   CUDA_TRY(ctx, cudaMemcpy(S, dS, (size_t)batch * k * sizeof(double), cudaMemcpyDeviceToHost));
+  return YAQS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SVD without allocation
+// ---------------------------------------------------------------------------
+// yaqs_batched_svd_noalloc is for callers whose device memory is owned by
+// someone else (a Julia or PyTorch pool allocator that holds the whole
+// device, or a code path where a cudaMalloc would synchronise the device or
+// could fail mid-run): it takes device pointers and keeps its scratch in
+// this fixed array.  The array is part of the module image, so every GPU
+// that loads the library holds these 8 MiB until the process exits.  In host
+// code `g_noalloc_scratch` names a host-side stand-in, not device memory: the
+// kernel gets the device address from cudaGetSymbolAddress.
+#define YAQS_NOALLOC_SCRATCH_BYTES (8u << 20)
+static __device__ __align__(256) cplx g_noalloc_scratch[YAQS_NOALLOC_SCRATCH_BYTES / sizeof(cplx)];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_base[64] = {};  // device address of g_noalloc_scratch, per device ordinal
+}  // namespace
+
+int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* U,
+                             double* S, double* SVt, void* stream) {
+  if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
+  if (batch < 1 || m < 1 || n < 1 || std::min(m, n) > SVD_MAX_COLS || !M || !U || !S || !SVt)
+    return set_err(ctx, YAQS_E_ARG, "bad svd arguments");
+  if (2 * (m + n) > SVD_SMEM_CPLX) return set_err(ctx, YAQS_E_UNSUPPORTED, "svd needs m + n <= 4096");
+  if (ctx->device < 0 || ctx->device >= 64) return set_err(ctx, YAQS_E_UNSUPPORTED, "device ordinal above 63");
+  const long long big = (long long)std::max(m, n) * std::max(m, n);
+  const long long wstride = 4 * big + std::max(m, n) + SVD_MAX_COLS;
+  const unsigned long long need =
+      (unsigned long long)batch * wstride * sizeof(cplx) + (unsigned long long)batch * SVD_MAX_COLS * sizeof(int);
+  if (need > YAQS_NOALLOC_SCRATCH_BYTES)
+    return set_err(ctx, YAQS_E_ARG,
+                   "batch x (4 max(m,n)^2 + max(m,n) + 256) complex scratch exceeds the fixed 8 MiB of "
+                   "yaqs_batched_svd_noalloc; use fewer or smaller problems per call");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const size_t smem = sizeof(CompSmem);
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_base[ctx->device]) {  // once per device, with that device current
+      void* p = nullptr;
+      CUDA_TRY(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      CUDA_TRY(ctx, cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      g_noalloc_base[ctx->device] = p;
+    }
+    base = g_noalloc_base[ctx->device];
+  }
+  cplx* work = static_cast<cplx*>(base);
+  int* iwork = reinterpret_cast<int*>(work + (long long)batch * wstride);
+  svd_kernel<<<batch, NT, smem, static_cast<cudaStream_t>(stream)>>>(
+      m, n, reinterpret_cast<const cplx*>(M), reinterpret_cast<cplx*>(U), S, reinterpret_cast<cplx*>(SVt), work,
+      wstride, iwork);
+  CUDA_TRY(ctx, cudaGetLastError());
   return YAQS_OK;
 }
 
