@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 /* M: batch x (m x n); U: batch x (m x k); S: batch x k; SVt: batch x (k x n);
- * k = min(m, n) <= 256, m + n <= 4096. */
+ * k = min(m, n) <= 256, m + n <= 2048. */
 int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* U,
                      double* S, double* SVt);
 

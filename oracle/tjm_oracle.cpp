@@ -211,9 +211,9 @@ void complete_column(int rows, vector<cd>& X, const vector<int>& have, int slot)
 }
 
 // Block size of the block-cyclic Jacobi order (same rule as the GPU engine:
-// a pair of b-column blocks of B (q rows) fits 8192 complex values).
+// a pair of b-column blocks of B (q rows) fits 4096 complex values).
 int svd_block_size(int q, int p) {
-  int b = 8192 / (2 * q);
+  int b = 4096 / (2 * q);
   if (b > 32) b = 32;
   if (b > p) b = p;
   if (b < 1) b = 1;

@@ -88,7 +88,7 @@ __device__ void run_step(Ctx& c, int j) {
   }
 }
 
-__global__ void __launch_bounds__(NT, 1) tjm_step_kernel(const DevParams P, int j) {
+__global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int j) {
   extern __shared__ __align__(16) unsigned char smraw[];
   CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
   const int slot = blockIdx.x;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M,
   cta_copy(Ub, w.Yo, (long long)m * k);
   __syncthreads();
   cta_gemm(gemm_args(k, n, m, w.Yo, m, 1, Mb, 1, m, Sb, 1, k, true, false), sm.e.u.gw.g);
-  for (long long e = threadIdx.x; e < (long long)k * n; e += NT)
+  for (int e = threadIdx.x; e < k * n; e += NT)
     if ((int)(e % k) >= r.rank) Sb[e] = make_double2(0.0, 0.0);
   for (int e = threadIdx.x; e < k; e += NT) S[(long long)k * b + e] = w.sig[e];
 }
@@ -916,7 +916,7 @@ int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const d
                      double* Vt) {
   if (!ctx || batch < 1 || m < 1 || n < 1 || std::min(m, n) > SVD_MAX_COLS || !M || !U || !S || !Vt)
     return set_err(ctx, YAQS_E_ARG, "bad svd arguments");
-  if (2 * (m + n) > SVD_SMEM_CPLX) return set_err(ctx, YAQS_E_UNSUPPORTED, "svd needs m + n <= 4096");
+  if (2 * (m + n) > SVD_SMEM_CPLX) return set_err(ctx, YAQS_E_UNSUPPORTED, "svd needs m + n <= 2048");
   std::lock_guard<std::mutex> lk(ctx->mu);
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int k = std::min(m, n);
@@ -968,7 +968,7 @@ int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n,
   if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
   if (batch < 1 || m < 1 || n < 1 || std::min(m, n) > SVD_MAX_COLS || !M || !U || !S || !SVt)
     return set_err(ctx, YAQS_E_ARG, "bad svd arguments");
-  if (2 * (m + n) > SVD_SMEM_CPLX) return set_err(ctx, YAQS_E_UNSUPPORTED, "svd needs m + n <= 4096");
+  if (2 * (m + n) > SVD_SMEM_CPLX) return set_err(ctx, YAQS_E_UNSUPPORTED, "svd needs m + n <= 2048");
   if (ctx->device < 0 || ctx->device >= 64) return set_err(ctx, YAQS_E_UNSUPPORTED, "device ordinal above 63");
   const long long big = (long long)std::max(m, n) * std::max(m, n);
   const long long wstride = 4 * big + std::max(m, n) + SVD_MAX_COLS;

@@ -68,14 +68,16 @@ __device__ __forceinline__ GemmArgs gemm_args(int M, int N, int K, const cplx* A
 }
 
 // CTA-collective.  Ends with a __syncthreads() so C is visible to all.
-__device__ __noinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
+// Conjugation is a template parameter so the common unconjugated case has
+// no extra arithmetic in the inner loop.
+template <bool CA, bool CB>
+__device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   ProfScope prof_scope_(PF_GEMM);
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
   const bool a_m_fast = (g.am == 1) || (g.ak != 1);
   const bool b_n_fast = (g.bn == 1) || (g.bk != 1);
   const int nk = (g.K + GBK - 1) / GBK;
-  const double sa = g.conjA ? -1.0 : 1.0, sb = g.conjB ? -1.0 : 1.0;
   for (int tm = 0; tm < g.M; tm += GBM) {
     for (int tn = 0; tn < g.N; tn += GBN) {
       cplx acc[4][4];
@@ -125,19 +127,21 @@ __device__ __noinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
         for (int kk = 0; kk < GBK; ++kk) {
           cplx a[4], b[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            a[i] = sm.As[buf][kk][tx + 16 * i];
-            a[i].y *= sa;
-          }
+          for (int i = 0; i < 4; ++i) a[i] = sm.As[buf][kk][tx + 16 * i];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            b[j] = sm.Bs[buf][kk][ty + 16 * j];
-            b[j].y *= sb;
-          }
+          for (int j = 0; j < 4; ++j) b[j] = sm.Bs[buf][kk][ty + 16 * j];
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], b[j]);
+            for (int j = 0; j < 4; ++j) {
+              // acc += op(a) * op(b) with op = conj where requested
+              cplx& c = acc[i][j];
+              const double ay = CA ? -a[i].y : a[i].y, by = CB ? -b[j].y : b[j].y;
+              c.x = fma(a[i].x, b[j].x, c.x);
+              c.x = fma(-ay, by, c.x);
+              c.y = fma(a[i].x, by, c.y);
+              c.y = fma(ay, b[j].x, c.y);
+            }
         }
         __syncthreads();
       }
@@ -158,4 +162,14 @@ __device__ __noinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
     }
   }
   __syncthreads();
+}
+
+__device__ __forceinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
+  if (g.conjA) {
+    if (g.conjB) cta_gemm_t<true, true>(g, sm);
+    else cta_gemm_t<true, false>(g, sm);
+  } else {
+    if (g.conjB) cta_gemm_t<false, true>(g, sm);
+    else cta_gemm_t<false, false>(g, sm);
+  }
 }

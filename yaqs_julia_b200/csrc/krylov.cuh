@@ -13,9 +13,9 @@
 #include "common.cuh"
 #include "gemm.cuh"
 
-#define WAPPLY_PT 128
+#define WAPPLY_PT 64
 #define WAPPLY_MAXI 32
-#define WAPPLY_MAXNNZ 1024
+#define WAPPLY_MAXNNZ 512
 #define KRYLOV_MAX 32
 
 // Sparse MPO matrix M[o, i] in CSR form (rows are outputs).
@@ -39,9 +39,14 @@ struct WApplySmem {
   cplx val[WAPPLY_MAXNNZ];
   int col[WAPPLY_MAXNNZ];
   int rowp[WAPPLY_MAXI + 1];
+  int in_off[WAPPLY_MAXI];
+  int out_off[WAPPLY_MAXI];
 };
 
-// out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.
+// out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.  Each thread
+// owns pair slot tid % WAPPLY_PT of every tile and input/output rows
+// tid / WAPPLY_PT + k NT / WAPPLY_PT, so index arithmetic is per tile, not
+// per element.
 __device__ __noinline__ void dev_wapply(const cplx* __restrict__ in, cplx* __restrict__ out, const WMat W,
                                         const WApplyGeom g, WApplySmem& ws) {
   ProfScope prof_scope_(PF_WAPPLY);
@@ -51,30 +56,25 @@ __device__ __noinline__ void dev_wapply(const cplx* __restrict__ in, cplx* __res
     ws.col[e] = W.col[e];
   }
   for (int e = tid; e <= W.no; e += NT) ws.rowp[e] = W.rowp[e];
-  const long long npair = (long long)g.n0 * g.n1;
-  for (long long base = 0; base < npair; base += WAPPLY_PT) {
+  for (int i = tid; i < W.ni; i += NT) ws.in_off[i] = (int)((i % g.ni1) * g.ii1 + (i / g.ni1) * g.ii2);
+  for (int o = tid; o < W.no; o += NT) ws.out_off[o] = (int)((o % g.no1) * g.oo1 + (o / g.no1) * g.oo2);
+  const int npair = g.n0 * g.n1;
+  const int pl = tid % WAPPLY_PT, r0 = tid / WAPPLY_PT;
+  constexpr int RS = NT / WAPPLY_PT;
+  for (int base = 0; base < npair; base += WAPPLY_PT) {
+    const int pair = base + pl;
+    const bool live = pair < npair;
+    const int q0 = live ? pair % g.n0 : 0, q1 = live ? pair / g.n0 : 0;
+    const long long ib = q0 * g.is0 + q1 * g.is1, ob = q0 * g.os0 + q1 * g.os1;
     __syncthreads();
-    for (int e = tid; e < WAPPLY_PT * W.ni; e += NT) {
-      int pl = e % WAPPLY_PT, i = e / WAPPLY_PT;
-      long long pair = base + pl;
-      cplx v = make_double2(0.0, 0.0);
-      if (pair < npair) {
-        long long q0 = pair % g.n0, q1 = pair / g.n0;
-        int i1 = i % g.ni1, i2 = i / g.ni1;
-        v = in[q0 * g.is0 + q1 * g.is1 + i1 * g.ii1 + i2 * g.ii2];
+    for (int i = r0; i < W.ni; i += RS) ws.in[i][pl] = live ? in[ib + ws.in_off[i]] : make_double2(0.0, 0.0);
+    __syncthreads();
+    if (live) {
+      for (int o = r0; o < W.no; o += RS) {
+        cplx acc = make_double2(0.0, 0.0);
+        for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) cfma(acc, ws.val[z], ws.in[ws.col[z]][pl]);
+        out[ob + ws.out_off[o]] = acc;
       }
-      ws.in[i][pl] = v;
-    }
-    __syncthreads();
-    for (int e = tid; e < WAPPLY_PT * W.no; e += NT) {
-      int pl = e % WAPPLY_PT, o = e / WAPPLY_PT;
-      long long pair = base + pl;
-      if (pair >= npair) continue;
-      cplx acc = make_double2(0.0, 0.0);
-      for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) cfma(acc, ws.val[z], ws.in[ws.col[z]][pl]);
-      long long q0 = pair % g.n0, q1 = pair / g.n0;
-      int o1 = o % g.no1, o2 = o / g.no1;
-      out[q0 * g.os0 + q1 * g.os1 + o1 * g.oo1 + o2 * g.oo2] = acc;
     }
   }
   __syncthreads();
@@ -99,7 +99,7 @@ struct KrySmem {
 
 // Shared memory of one CTA.  The GEMM / MPO-apply staging and the SVD block
 // buffer are never live at the same time and share storage.
-#define SVD_SMEM_CPLX_K 8192
+#define SVD_SMEM_CPLX_K 4096
 struct EngineSmem {
   union {
     struct {

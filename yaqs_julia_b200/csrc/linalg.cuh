@@ -78,7 +78,7 @@ __device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, 
   ProfScope prof_scope_(PF_QRQ);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int kq = min(m, n);
-  for (long long e = tid; e < (long long)m * kq; e += NT) {
+  for (int e = tid; e < m * kq; e += NT) {
     int r = (int)(e % m), c = (int)(e / m);
     Q[e] = make_double2(r == c ? 1.0 : 0.0, 0.0);
   }
@@ -105,7 +105,7 @@ __device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, 
 // R (kq x n) of a factored H into Rout (ld kq), zero below the diagonal.
 __device__ __forceinline__ void dev_qr_extract_r(const cplx* H, int m, int n, cplx* Rout) {
   const int kq = min(m, n);
-  for (long long e = threadIdx.x; e < (long long)kq * n; e += NT) {
+  for (int e = threadIdx.x; e < kq * n; e += NT) {
     int r = (int)(e % kq), c = (int)(e / kq);
     Rout[e] = (r <= c) ? H[r + (long long)m * c] : make_double2(0.0, 0.0);
   }
@@ -184,7 +184,7 @@ __device__ void dev_complete_column(cplx* Y, int rows, int k, cplx* y, RedScratc
 // Block size of the block-cyclic Jacobi ordering: blocks of b columns of B
 // (q rows) so that a pair of blocks fits the SVD_SMEM_CPLX shared buffer.
 // The CPU oracle uses the same rule.
-#define SVD_SMEM_CPLX 8192
+#define SVD_SMEM_CPLX 4096
 __host__ __device__ __forceinline__ int svd_block_size(int q, int p) {
   int b = SVD_SMEM_CPLX / (2 * q);
   if (b > 32) b = 32;
@@ -265,7 +265,7 @@ __device__ __forceinline__ void smem_rotate_round(cplx* sb, int ld, int q, int r
 __device__ __forceinline__ void svd_stage(cplx* sb, int ld, const SvdWork& w, int q, int c0, int nc0, int c1, int nc1,
                                           bool store) {
   const int nc = nc0 + nc1;
-  for (long long e = threadIdx.x; e < (long long)nc * ld; e += NT) {
+  for (int e = threadIdx.x; e < nc * ld; e += NT) {
     int r = (int)(e % ld), lc = (int)(e / ld);
     int col = lc < nc0 ? c0 + lc : c1 + (lc - nc0);
     cplx* g = w.B + (long long)q * col + r;
@@ -301,14 +301,14 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
   res.p = p;
   res.sweeps = 0;
   cplx* H = w.X;
-  for (long long e = tid; e < (long long)mm * nn; e += NT) {
+  for (int e = tid; e < mm * nn; e += NT) {
     int r = (int)(e % mm), c = (int)(e / mm);
     H[e] = res.tr ? M[e] : cconj(M[c + (long long)m * r]);
   }
   __syncthreads();
   dev_qr_factor(H, mm, nn, ls, rs);
   // B = R^H (nn x k): B[r, c] = conj(R[c, r]) for c <= r
-  for (long long e = tid; e < (long long)q * p; e += NT) {
+  for (int e = tid; e < q * p; e += NT) {
     int r = (int)(e % q), c = (int)(e / q);
     w.B[e] = (c <= r) ? cconj(H[c + (long long)mm * r]) : make_double2(0.0, 0.0);
   }
@@ -419,7 +419,7 @@ __device__ __noinline__ void dev_svd_vectors(const SvdResult& res, int need, Svd
   const int tid = threadIdx.x, q = res.q, p = res.p;
   need = min(need, p);
   const int ng = min(need, res.rank);
-  for (long long e = tid; e < (long long)q * ng; e += NT) {
+  for (int e = tid; e < q * ng; e += NT) {
     int r = (int)(e % q), k = (int)(e / q);
     w.Yo[e] = cscale(w.B[r + (long long)q * w.ord[k]], 1.0 / w.sig[k]);
   }

@@ -195,7 +195,7 @@ __device__ void lq_left(Ctx& c, const DState& s, int i) {
   cplx* H = c.ws + c.P.lay.tA;
   cplx* Qh = c.ws + c.P.lay.tB;
   cplx* Rb = c.ws + c.P.lay.tC;
-  for (long long e = threadIdx.x; e < (long long)n2 * l; e += NT) {
+  for (int e = threadIdx.x; e < n2 * l; e += NT) {
     int cc = (int)(e % n2), ii = (int)(e / n2);
     H[e] = cconj(A[ii + (long long)l * cc]);
   }
@@ -203,7 +203,7 @@ __device__ void lq_left(Ctx& c, const DState& s, int i) {
   dev_qr_factor(H, n2, l, c.sm.la, c.sm.e.r);
   dev_qr_formq(H, n2, l, Qh, c.sm.la);
   dev_qr_extract_r(H, n2, l, Rb);
-  for (long long e = threadIdx.x; e < (long long)rn * n2; e += NT) {
+  for (int e = threadIdx.x; e < rn * n2; e += NT) {
     int k = (int)(e % rn), cc = (int)(e / rn);
     A[e] = cconj(Qh[cc + (long long)n2 * k]);
   }
@@ -267,7 +267,7 @@ __device__ __forceinline__ cplx* envL(const Ctx& c, int b) { return c.ws + c.P.l
 __device__ __forceinline__ cplx* envR(const Ctx& c, int b) { return c.ws + c.P.lay.ER + c.P.env_off[b]; }
 
 __device__ void identity_env(Ctx& c, cplx* E, int dim, int w) {
-  for (long long e = threadIdx.x; e < (long long)dim * w * dim; e += NT) {
+  for (int e = threadIdx.x; e < dim * w * dim; e += NT) {
     long long a = e % dim, rest = e / dim;
     long long m = rest % w, k = rest / w;
     E[e] = make_double2((m == 0 && a == k) ? 1.0 : 0.0, 0.0);
@@ -371,7 +371,7 @@ __device__ SvdWork svd_work(const Ctx& c) {
 // NaN/Inf -> 0 before the SVD (Algorithms.jl:414-417).
 __device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
   int bad = 0;
-  for (long long e = threadIdx.x; e < n; e += NT) {
+  for (int e = threadIdx.x; e < (int)n; e += NT) {
     cplx v = th[e];
     if (!isfinite(v.x) || !isfinite(v.y)) {
       th[e] = make_double2(0.0, 0.0);
@@ -415,15 +415,15 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
     cta_copy(Lt, w.Yo, (long long)m * keep);
     __syncthreads();
     cta_gemm(gemm_args(keep, n, m, w.Yo, m, 1, th, 1, m, Rt, 1, keep, true, false), c.sm.e.u.gw.g);
-    for (long long e = threadIdx.x; e < (long long)keep * n; e += NT)
+    for (int e = threadIdx.x; e < keep * n; e += NT)
       if ((int)(e % keep) >= res.rank) Rt[e] = make_double2(0.0, 0.0);
   } else {
-    for (long long e = threadIdx.x; e < (long long)keep * n; e += NT) {
+    for (int e = threadIdx.x; e < keep * n; e += NT) {
       int k = (int)(e % keep), cc = (int)(e / keep);
       Rt[e] = cconj(w.Yo[cc + (long long)n * k]);
     }
     cta_gemm(gemm_args(m, keep, n, th, 1, m, w.Yo, 1, n, Lt, 1, m), c.sm.e.u.gw.g);
-    for (long long e = threadIdx.x; e < (long long)m * keep; e += NT)
+    for (int e = threadIdx.x; e < m * keep; e += NT)
       if ((int)(e / m) >= res.rank) Lt[e] = make_double2(0.0, 0.0);
   }
   __syncthreads();
@@ -468,7 +468,7 @@ __device__ void tdvp_sweep(Ctx& c, const DState& s) {
 // ---------------------------------------------------------------------------
 // A[l,p,r] <- sum_k op[p,k] A[l,k,r] for a d x d op (d = 2 or 4), in place.
 __device__ void apply_local(cplx* A, int l, int d, int r, const cplx* op) {
-  for (long long e = threadIdx.x; e < (long long)l * r; e += NT) {
+  for (int e = threadIdx.x; e < l * r; e += NT) {
     long long a = e % l, b = e / l;
     cplx v[4], o[4];
     for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
@@ -485,7 +485,7 @@ __device__ void apply_local(cplx* A, int l, int d, int r, const cplx* op) {
 // sum |op . A|^2 (or sum |A|^2 when op == nullptr), d = 2 or 4.
 __device__ double local_norm2(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
   double sacc = 0.0;
-  for (long long e = threadIdx.x; e < (long long)l * r; e += NT) {
+  for (int e = threadIdx.x; e < l * r; e += NT) {
     long long a = e % l, b = e / l;
     cplx v[4];
     for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
@@ -505,7 +505,7 @@ __device__ double local_norm2(Ctx& c, const cplx* A, int l, int d, int r, const 
 // Re sum conj(A) (op A)
 __device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
   double sacc = 0.0;
-  for (long long e = threadIdx.x; e < (long long)l * r; e += NT) {
+  for (int e = threadIdx.x; e < l * r; e += NT) {
     long long a = e % l, b = e / l;
     cplx v[4];
     for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
