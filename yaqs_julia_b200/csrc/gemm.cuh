@@ -67,24 +67,41 @@ __device__ __forceinline__ GemmArgs gemm_args(int M, int N, int K, const cplx* A
   return g;
 }
 
+// FP64 tensor-core product: D (8x8) += A (8x4, row) * B (4x8, col).
+// Fragments (per lane, g = lane/4, t = lane%4): A[g][t], B[t][g],
+// D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // CTA-collective.  Ends with a __syncthreads() so C is visible to all.
-// Conjugation is a template parameter so the common unconjugated case has
-// no extra arithmetic in the inner loop.
+// Complex products run on the FP64 tensor cores (mma.sync m8n8k4): each of
+// the 8 warps owns a 32x16 complex sub-tile of the 64x64 CTA tile as 4x2
+// blocks of 8x8, each block accumulating re and im with four real MMAs.
+// Conjugation is a template parameter (a sign flip of the imaginary
+// fragment).
 template <bool CA, bool CB>
 __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   ProfScope prof_scope_(PF_GEMM);
   const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
+  const int lane = tid & 31, wid = tid >> 5;
+  const int wm = wid & 1, wn = wid >> 1;  // 2 x 4 warps
+  const int gq = lane >> 2, tq = lane & 3;
   const bool a_m_fast = (g.am == 1) || (g.ak != 1);
   const bool b_n_fast = (g.bn == 1) || (g.bk != 1);
   const int nk = (g.K + GBK - 1) / GBK;
   for (int tm = 0; tm < g.M; tm += GBM) {
     for (int tn = 0; tn < g.N; tn += GBN) {
-      cplx acc[4][4];
+      double cr[4][2][2], ci[4][2][2];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+        for (int j = 0; j < 2; ++j) {
+          cr[i][j][0] = cr[i][j][1] = 0.0;
+          ci[i][j][0] = ci[i][j][1] = 0.0;
+        }
       auto issue = [&](int kc, int buf) {
         const int k0 = kc * GBK;
 #pragma unroll
@@ -124,40 +141,47 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < GBK; ++kk) {
-          cplx a[4], b[4];
+        for (int k4 = 0; k4 < GBK; k4 += 4) {
+          double ar[4], ai[4], br[2], bi[2];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) a[i] = sm.As[buf][kk][tx + 16 * i];
+          for (int i = 0; i < 4; ++i) {
+            const cplx a = sm.As[buf][k4 + tq][wm * 32 + i * 8 + gq];
+            ar[i] = a.x;
+            ai[i] = CA ? -a.y : a.y;
+          }
 #pragma unroll
-          for (int j = 0; j < 4; ++j) b[j] = sm.Bs[buf][kk][ty + 16 * j];
+          for (int j = 0; j < 2; ++j) {
+            const cplx b = sm.Bs[buf][k4 + tq][wn * 16 + j * 8 + gq];
+            br[j] = b.x;
+            bi[j] = CB ? -b.y : b.y;
+          }
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              // acc += op(a) * op(b) with op = conj where requested
-              cplx& c = acc[i][j];
-              const double ay = CA ? -a[i].y : a[i].y, by = CB ? -b[j].y : b[j].y;
-              c.x = fma(a[i].x, b[j].x, c.x);
-              c.x = fma(-ay, by, c.x);
-              c.y = fma(a[i].x, by, c.y);
-              c.y = fma(ay, b[j].x, c.y);
+            for (int j = 0; j < 2; ++j) {
+              dmma884(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+              dmma884(cr[i][j][0], cr[i][j][1], -ai[i], bi[j]);
+              dmma884(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+              dmma884(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
             }
         }
         __syncthreads();
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int nn = tn + ty + 16 * j;
-        if (nn >= g.N) continue;
+      for (int i = 0; i < 4; ++i) {
+        const int mm = tm + wm * 32 + i * 8 + gq;
+        if (mm >= g.M) continue;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          int mm = tm + tx + 16 * i;
-          if (mm >= g.M) continue;
-          cplx* c = g.C + (long long)mm * g.cm + (long long)nn * g.cn;
-          cplx v = acc[i][j];
-          if (g.accumulate) v = cadd(v, *c);
-          *c = v;
-        }
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int nn = tn + wn * 16 + j * 8 + 2 * tq + h;
+            if (nn >= g.N) continue;
+            cplx* c = g.C + (long long)mm * g.cm + (long long)nn * g.cn;
+            cplx v = make_double2(cr[i][j][h], ci[i][j][h]);
+            if (g.accumulate) v = cadd(v, *c);
+            *c = v;
+          }
       }
     }
   }
