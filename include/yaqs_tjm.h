@@ -189,6 +189,56 @@ int yaqs_analog_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0,
                     yaqs_run_stats* stats);
 
 /*
+ * Digital TJM (DigitalTJM.jl).  A circuit is the flat gate list of a
+ * DigitalCircuit (DigitalTJM.jl:35-66): 1-qubit gates (2x2), 2-qubit gates
+ * (4x4, basis index p1 + 2*p2 with p1 on the smaller site, exactly as
+ * apply_local_gate_exact! reshapes it, DigitalTJM.jl:267-270) and barriers;
+ * a barrier with sample != 0 is a "SAMPLE_OBSERVABLES" barrier
+ * (DigitalTJM.jl:147-168).  Sites are 0-based, in the order given.
+ */
+enum { YAQS_GATE_BARRIER = 0, YAQS_GATE_1Q = 1, YAQS_GATE_2Q = 2 };
+typedef struct {
+  int32_t kind;
+  int32_t site[2];
+  double matrix[32];
+  int32_t sample;
+} yaqs_gate_desc;
+
+/* Circuit run settings (the TimeEvolutionConfig fields the digital path
+ * reads, plus the TJMOptions of DigitalTJM.jl:70-76). */
+enum { YAQS_METHOD_TEBD = 0 };
+typedef struct {
+  int32_t num_traj;
+  int32_t max_bond_dim;
+  double truncation_threshold;
+  int32_t local_method;       /* YAQS_METHOD_TEBD */
+  int32_t long_range_method;  /* YAQS_METHOD_TEBD (SWAP network) */
+  int32_t precision;
+  int32_t traj_offset;
+} yaqs_circuit_config;
+
+/*
+ * Layering of a circuit as process_circuit (DigitalTJM.jl:86-145) does it:
+ * number of layers and number of measurement columns of run_digital_tjm
+ * (DigitalTJM.jl:375-379: one per SAMPLE_OBSERVABLES barrier position, or 1).
+ */
+int yaqs_digital_plan(const yaqs_gate_desc* gates, int32_t n_gates, int32_t* n_layers, int32_t* n_samples);
+
+/*
+ * Digital TJM run: replaces the trajectory loop of Simulator._run_digital
+ * (Simulator.jl:71-125); each trajectory follows run_digital_tjm
+ * (DigitalTJM.jl:363-450) with TEBD gate application and SWAP chains for
+ * long-range gates (DigitalTJM.jl:251-330), local dissipation and a jump
+ * step after every 2-qubit gate (DigitalTJM.jl:405-420), and the
+ * observables at the sample barriers.  psi0 is normalised first
+ * (Simulator.jl:128).  Outputs as yaqs_analog_run with n_out = n_samples.
+ */
+int yaqs_digital_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
+                     const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                     const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, double* traj_out,
+                     double* mean_out, int32_t* maxchi_out, yaqs_run_stats* stats);
+
+/*
  * The same run in steps, for callers that interleave other work or time
  * individual time indices.  yaqs_analog_begin validates the descriptors,
  * copies every input to the device and sizes the workspaces; nothing is

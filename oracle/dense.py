@@ -76,3 +76,57 @@ def lindblad(Hm, psi0, jump_ops, dt, steps, observables, substeps=20):
             k4 = f(rho + h * k3)
             rho = rho + (h / 6.0) * (k1 + 2 * k2 + 2 * k3 + k4)
     return res
+
+
+def gate_op(op: np.ndarray, sites, L: int) -> np.ndarray:
+    """Dense 2^L matrix of a 1-qubit gate, or of a 4x4 gate whose basis index
+    is p1 + 2 p2 with p1 the smaller of the two (1-based) sites, as
+    apply_local_gate_exact! reads it (DigitalTJM.jl:266-269)."""
+    sites = sorted(sites)
+    if len(sites) == 1:
+        return site_op(op, sites[0], L)
+    a, b = sites[0] - 1, sites[1] - 1
+    n = 2 ** L
+    idx = np.arange(n)
+    ba, bb = (idx >> a) & 1, (idx >> b) & 1
+    col = ba + 2 * bb
+    M = np.zeros((n, n), dtype=np.complex128)
+    for row in range(4):
+        y = (idx & ~((1 << a) | (1 << b))) | ((row & 1) << a) | ((row >> 1) << b)
+        M[y, idx] += op[row, col]
+    return M
+
+
+def digital_pauli_density(L, layers, pauli_procs, observables, psi0=None):
+    """Exact ensemble of the digital TJM with Pauli noise.
+
+    ``layers`` is the output of process_circuit (gates with .op and 1-based
+    .sites); within a layer the 1-qubit gates act first, then every 2-qubit
+    gate followed by the noise of its local model.  For Pauli processes the
+    unravelled step (dissipation e^{-gamma/2}, jump with probability
+    1 - e^{-Gamma}, process k chosen with weight gamma_k) averages to the
+    channel rho -> e^{-Gamma} rho + (1 - e^{-Gamma}) sum_k gamma_k/Gamma P_k rho P_k.
+    ``pauli_procs`` is a list of (matrix, 1-based sites, gamma).
+    Returns <O> after every layer, shape (n_layers + 1, n_obs), row 0 the start."""
+    psi = product_state([[1, 0]] * L) if psi0 is None else psi0
+    rho = np.outer(psi, psi.conj())
+    out = [[np.trace(O @ rho).real for O in observables]]
+    for layer in layers:
+        for g in layer:
+            if len(g.sites) == 1:
+                U = gate_op(g.op, g.sites, L)
+                rho = U @ rho @ U.conj().T
+        for g in layer:
+            if len(g.sites) != 2:
+                continue
+            U = gate_op(g.op, g.sites, L)
+            rho = U @ rho @ U.conj().T
+            s = set(g.sites)
+            loc = [(gate_op(m, st, L), gm) for (m, st, gm) in pauli_procs
+                   if (len(st) == 1 and st[0] in s) or (len(st) == 2 and set(st) == s)]
+            G = sum(gm for _, gm in loc)
+            if G > 0:
+                jumped = sum((gm / G) * (P @ rho @ P.conj().T) for P, gm in loc)
+                rho = np.exp(-G) * rho + (1 - np.exp(-G)) * jumped
+        out.append([np.trace(O @ rho).real for O in observables])
+    return np.array(out)

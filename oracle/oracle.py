@@ -37,6 +37,10 @@ def lib():
         L.orc_analog_run.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.NoiseDesc), P(A.ObsDesc), C.c_int32,
                                      P(A.TevConfig), P(A.RngDesc), C.c_int32, C.c_int32, C.c_int32,
                                      A.DPTR, P(C.c_int32), P(A.RunStats)]
+        L.orc_digital_run.argtypes = [P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc), P(A.ObsDesc),
+                                      C.c_int32, P(A.CircuitConfig), P(A.RngDesc), C.c_int32, C.c_int32,
+                                      C.c_int32, A.DPTR, P(C.c_int32), P(A.RunStats)]
+        L.orc_digital_plan.argtypes = [P(A.GateDesc), C.c_int32, P(C.c_int32), P(C.c_int32)]
         L.orc_tdvp_evolve.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.ObsDesc), C.c_int32, P(A.TevConfig),
                                       C.c_int32, A.DPTR]
         L.orc_svd.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR, A.DPTR]
@@ -72,6 +76,28 @@ def analog_run(desc, t_begin=0, t_end=None, nthreads=None):
                             C.byref(desc.cfg), C.byref(desc.rng), t_begin, t_end, nth, A.dptr(traj),
                             chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st)))
     return traj[:, :desc.n_obs, :], chi, st.as_dict()
+
+
+def digital_run(desc, t_begin=0, t_end=None, nthreads=None):
+    """Digital trajectories of a packed circuit problem (api.CircuitDescriptors)."""
+    L = lib()
+    nt = desc.num_traj
+    t_end = nt if t_end is None else t_end
+    traj = np.zeros((nt, max(desc.n_obs, 1), desc.n_out))
+    chi = np.zeros((nt, desc.n_out), dtype=np.int32)
+    st = A.RunStats()
+    nth = nthreads or os.cpu_count() or 1
+    _check(L.orc_digital_run(C.byref(desc.mps), desc.gates, desc.n_gates, C.byref(desc.noise), desc.obs,
+                             desc.n_obs, C.byref(desc.cfg), C.byref(desc.rng), t_begin, t_end, nth, A.dptr(traj),
+                             chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st)))
+    return traj[:, :desc.n_obs, :], chi, st.as_dict()
+
+
+def digital_plan(gates, n_gates):
+    """(n_layers, n_samples) of a yaqs_gate_desc array (process_circuit / _sample_plan)."""
+    nl, ns = C.c_int32(0), C.c_int32(0)
+    _check(lib().orc_digital_plan(gates, n_gates, C.byref(nl), C.byref(ns)))
+    return nl.value, ns.value
 
 
 def tdvp_evolve(desc, n_steps):

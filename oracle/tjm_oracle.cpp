@@ -391,6 +391,20 @@ int keep_relative(const vector<double>& S, double thr, int max_bond) {
   return std::max(1, std::min(rank, max_bond));
 }
 
+// apply_local_gate_exact! (DigitalTJM.jl:282-292): absolute, drop while the
+// running sum plus s^2 stays <= thr, no minimum.
+int keep_tebd(const vector<double>& S, double thr, int max_bond) {
+  int n = (int)S.size();
+  double cur = 0;
+  int keep = n;
+  for (int k = n; k >= 1; --k) {
+    if (cur + S[k - 1] * S[k - 1] > thr) break;
+    cur += S[k - 1] * S[k - 1];
+    --keep;
+  }
+  return std::max(1, std::min(keep, max_bond));
+}
+
 // ---------------------------------------------------------------------------
 // Small symmetric eigensolver (cyclic Jacobi) for the Lanczos matrix.
 // ---------------------------------------------------------------------------
@@ -788,7 +802,9 @@ void split_theta(const Ten& Th, int rule, double thr, int max_bond, bool s_left,
   if (bad) cnt.nonfinite++;
   SvdOut o = svd_side(m, n, M.data(), s_left ? SVD_RIGHT : SVD_LEFT);
   cnt.svds++;
-  const int keep = (rule == 0) ? keep_tdvp(o.S, thr, max_bond) : keep_relative(o.S, thr, max_bond);
+  const int keep = rule == 0   ? keep_tdvp(o.S, thr, max_bond)
+                   : rule == 1 ? keep_relative(o.S, thr, max_bond)
+                               : keep_tebd(o.S, thr, max_bond);
   vector<cd> Y = svd_vectors(o, keep);
   Lo = Ten(Th.l, 2, keep);
   Ro = Ten(keep, 2, Th.r);
@@ -835,14 +851,18 @@ struct Obs {
   cd mat[16];
 };
 
+struct NoiseSet {  // a NoiseModel: `present` == false means `nothing`
+  bool present = false;
+  bool all_zero = true;
+  vector<NoiseProc> procs;
+};
+
 struct Problem {
   int L;
   vector<Wt> W;
   vector<Wt> W2;  // merged two-site W_group (Algorithms.jl:639-643), index i for sites (i, i+1)
   State psi0;
-  bool noise_present = false;
-  vector<NoiseProc> procs;
-  bool all_zero = true;
+  NoiseSet noise;
   vector<Obs> obs;
   double dt;
   int n_times, num_traj, max_bond, order;
@@ -1025,14 +1045,14 @@ struct Sweeper {
 // ---------------------------------------------------------------------------
 // Dissipation (Dissipation.jl:37-159), local processes
 // ---------------------------------------------------------------------------
-void apply_dissipation(const Problem& P, State& s, bool full_dt, double dt, Counters& cnt) {
+void apply_dissipation(const Problem& P, const NoiseSet& N, State& s, bool full_dt, double dt, Counters& cnt) {
   const int L = s.L;
-  if (!P.noise_present || P.all_zero) {  // :39-47
+  if (!N.present || N.all_zero) {  // :39-47
     for (int i = L - 1; i >= 1; --i) shift_oc(s, i - 1);
     return;
   }
   for (int i = L - 1; i >= 0; --i) {
-    for (const auto& pr : P.procs) {
+    for (const auto& pr : N.procs) {
       if (pr.nsites == 1 && pr.s0 == i) {
         if (pr.pauli_name) {
           double f = std::exp(-0.5 * dt * pr.gamma);
@@ -1043,7 +1063,7 @@ void apply_dissipation(const Problem& P, State& s, bool full_dt, double dt, Coun
       }
     }
     if (i > 0) {
-      for (const auto& pr : P.procs) {
+      for (const auto& pr : N.procs) {
         if (pr.nsites == 2 && pr.s1 == i) {
           if (pr.pauli_name) {
             double f = std::exp(-0.5 * dt * pr.gamma);
@@ -1071,10 +1091,10 @@ struct Cand {
   double dp;
 };
 
-bool stochastic_process(const Problem& P, State& s, double dt, Draws& rng, Counters& cnt) {
+bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt, Draws& rng, Counters& cnt) {
   const int L = s.L;
   double dp = 1.0 - scalar_product(s).real();
-  if (P.procs.empty() || rng.next() >= dp) {
+  if (N.procs.empty() || rng.next() >= dp) {
     shift_oc(s, 0);
     normalize_mps(s);
     return false;
@@ -1083,7 +1103,7 @@ bool stochastic_process(const Problem& P, State& s, double dt, Draws& rng, Count
   vector<Cand> cands;
   for (int site = 0; site < L; ++site) {
     shift_oc(s, site);
-    for (const auto& pr : P.procs) {
+    for (const auto& pr : N.procs) {
       if (pr.nsites == 1 && pr.s0 == site) {
         double nr;
         if (pr.pauli_proc) {
@@ -1097,7 +1117,7 @@ bool stochastic_process(const Problem& P, State& s, double dt, Draws& rng, Count
       }
     }
     if (site < L - 1) {
-      for (const auto& pr : P.procs) {
+      for (const auto& pr : N.procs) {
         if (pr.nsites == 2 && pr.s0 == site) {
           double nr;
           if (pr.pauli_proc) {
@@ -1216,29 +1236,29 @@ int run_trajectory(const Problem& P, long long traj, double* out, int* chi_out, 
   if (P.order == 2) {
     if (P.sample_timesteps) evaluate(P, s, out, 0, ncols, chi_out);
     // initialize (AnalogTJM.jl:21-33)
-    apply_dissipation(P, s, false, dt / 2, cnt);
-    if (P.noise_present) stochastic_process(P, s, dt, rng, cnt);
+    apply_dissipation(P, P.noise, s, false, dt / 2, cnt);
+    if (P.noise.present) stochastic_process(P, P.noise, s, dt, rng, cnt);
     auto sample = [&](int j) {  // AnalogTJM.jl:62-81
       State psi = s;
       sw.sweep(psi);
-      apply_dissipation(P, psi, false, dt / 2, cnt);
-      if (P.noise_present) stochastic_process(P, psi, dt, rng, cnt);
+      apply_dissipation(P, P.noise, psi, false, dt / 2, cnt);
+      if (P.noise.present) stochastic_process(P, P.noise, psi, dt, rng, cnt);
       evaluate(P, psi, out, P.sample_timesteps ? j : 0, ncols, chi_out);
     };
     if (P.sample_timesteps && P.n_times > 1) sample(1);
     for (int j = 2; j < P.n_times; ++j) {
       sw.sweep(s);  // step_through (AnalogTJM.jl:40-55)
-      apply_dissipation(P, s, true, dt, cnt);
-      if (P.noise_present) stochastic_process(P, s, dt, rng, cnt);
+      apply_dissipation(P, P.noise, s, true, dt, cnt);
+      if (P.noise.present) stochastic_process(P, P.noise, s, dt, rng, cnt);
       if (P.sample_timesteps || j == P.n_times - 1) sample(j);
     }
   } else {
     if (P.sample_timesteps) evaluate(P, s, out, 0, ncols, chi_out);
     for (int j = 1; j < P.n_times; ++j) {
       sw.sweep(s);
-      if (P.noise_present) {
-        apply_dissipation(P, s, true, dt, cnt);
-        stochastic_process(P, s, dt, rng, cnt);
+      if (P.noise.present) {
+        apply_dissipation(P, P.noise, s, true, dt, cnt);
+        stochastic_process(P, P.noise, s, dt, rng, cnt);
       }
       if (P.sample_timesteps)
         evaluate(P, s, out, j, ncols, chi_out);
@@ -1259,6 +1279,73 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+void load_state(Problem& P, const yaqs_mps_desc* psi0) {
+  const int L = psi0->L;
+  P.L = L;
+  P.psi0.L = L;
+  P.psi0.oc = 0;
+  P.psi0.t.resize(L);
+  for (int i = 0; i < L; ++i) {
+    int l = psi0->chi[i], r = psi0->chi[i + 1];
+    Ten T(l, 2, r);
+    const double* src = psi0->tensors[i];
+    for (size_t k = 0; k < T.v.size(); ++k) T.v[k] = cd(src[2 * k], src[2 * k + 1]);
+    P.psi0.t[i] = std::move(T);
+  }
+}
+
+// Noise processes; the dissipators exp(-0.5 dt_eff gamma L^dag L) are
+// precomputed for dt_eff = P.dt / 2 and P.dt (Dissipation.jl:62-69).
+bool load_noise(Problem& P, const yaqs_noise_desc* noise, std::string& err) {
+  P.noise.present = noise && noise->present;
+  P.noise.all_zero = true;
+  if (!P.noise.present) return true;
+  for (int k = 0; k < noise->n; ++k) {
+    const yaqs_noise_proc& q = noise->procs[k];
+    NoiseProc pr{};
+    pr.nsites = q.nsites;
+    pr.s0 = q.site[0];
+    pr.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
+    pr.gamma = q.strength;
+    pr.pauli_name = q.pauli_name != 0;
+    pr.pauli_proc = q.pauli_proc != 0;
+    if (q.nsites == 2 && pr.s1 != pr.s0 + 1) {
+      err = "only adjacent 2-site processes are supported";
+      return false;
+    }
+    int dd = q.nsites == 1 ? 2 : 4;
+    for (int e = 0; e < dd * dd; ++e) pr.mat[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);
+    cd LdL[16];
+    for (int i = 0; i < dd; ++i)
+      for (int j = 0; j < dd; ++j) {
+        cd sacc = 0;
+        for (int kk = 0; kk < dd; ++kk) sacc += std::conj(pr.mat[kk + dd * i]) * pr.mat[kk + dd * j];
+        LdL[i + dd * j] = sacc;
+      }
+    herm_expm(dd, LdL, -0.5 * (P.dt / 2) * pr.gamma, pr.diss_half);
+    herm_expm(dd, LdL, -0.5 * P.dt * pr.gamma, pr.diss_full);
+    if (pr.gamma != 0.0) P.noise.all_zero = false;
+    P.noise.procs.push_back(pr);
+  }
+  return true;
+}
+
+void load_obs_rng(Problem& P, const yaqs_obs_desc* obs, int n_obs, const yaqs_rng_desc* rng) {
+  for (int k = 0; k < n_obs; ++k) {
+    Obs o{};
+    o.kind = obs[k].kind;
+    o.s0 = obs[k].site[0];
+    o.s1 = obs[k].site[1];
+    int dd = o.kind == YAQS_OBS_LOCAL2 ? 4 : 2;
+    for (int e = 0; e < dd * dd; ++e) o.mat[e] = cd(obs[k].matrix[2 * e], obs[k].matrix[2 * e + 1]);
+    P.obs.push_back(o);
+  }
+  P.rng_mode = rng->mode;
+  P.seed = rng->seed;
+  P.uniforms = rng->uniforms;
+  P.stride = rng->stride;
+}
+
 bool load_problem(Problem& P, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
                   const yaqs_obs_desc* obs, int n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
                   std::string& err) {
@@ -1271,17 +1358,7 @@ bool load_problem(Problem& P, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
     err = "need L >= 2 and matching MPO length";
     return false;
   }
-  P.L = L;
-  P.psi0.L = L;
-  P.psi0.oc = 0;
-  P.psi0.t.resize(L);
-  for (int i = 0; i < L; ++i) {
-    int l = psi0->chi[i], r = psi0->chi[i + 1];
-    Ten T(l, 2, r);
-    const double* src = psi0->tensors[i];
-    for (size_t k = 0; k < T.v.size(); ++k) T.v[k] = cd(src[2 * k], src[2 * k + 1]);
-    P.psi0.t[i] = std::move(T);
-  }
+  load_state(P, psi0);
   P.W.resize(L);
   for (int i = 0; i < L; ++i) {
     Wt W(H->w[i], 2, H->w[i + 1]);
@@ -1320,50 +1397,161 @@ bool load_problem(Problem& P, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
     err = "bad config";
     return false;
   }
-  P.noise_present = noise && noise->present;
-  P.all_zero = true;
-  if (P.noise_present) {
-    for (int k = 0; k < noise->n; ++k) {
-      const yaqs_noise_proc& q = noise->procs[k];
-      NoiseProc pr{};
-      pr.nsites = q.nsites;
-      pr.s0 = q.site[0];
-      pr.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
-      pr.gamma = q.strength;
-      pr.pauli_name = q.pauli_name != 0;
-      pr.pauli_proc = q.pauli_proc != 0;
-      if (q.nsites == 2 && pr.s1 != pr.s0 + 1) {
-        err = "only adjacent 2-site processes are supported";
-        return false;
-      }
-      int dd = q.nsites == 1 ? 2 : 4;
-      for (int e = 0; e < dd * dd; ++e) pr.mat[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);
-      cd LdL[16];
-      for (int i = 0; i < dd; ++i)
-        for (int j = 0; j < dd; ++j) {
-          cd sacc = 0;
-          for (int k = 0; k < dd; ++k) sacc += std::conj(pr.mat[k + dd * i]) * pr.mat[k + dd * j];
-          LdL[i + dd * j] = sacc;
-        }
-      herm_expm(dd, LdL, -0.5 * (P.dt / 2) * pr.gamma, pr.diss_half);
-      herm_expm(dd, LdL, -0.5 * P.dt * pr.gamma, pr.diss_full);
-      if (pr.gamma != 0.0) P.all_zero = false;
-      P.procs.push_back(pr);
+  if (!load_noise(P, noise, err)) return false;
+  load_obs_rng(P, obs, n_obs, rng);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Digital TJM (DigitalTJM.jl:86-450), TEBD gate application
+// ---------------------------------------------------------------------------
+struct Gate {
+  int kind;  // 0 barrier, 1 one-qubit, 2 two-qubit
+  int a, b;  // sites as given
+  cd mat[16];
+  bool sample;
+};
+
+struct Circuit {
+  vector<vector<int>> layers;  // indices into gates
+  bool sample_at_start = false;
+  vector<bool> sample_after;   // per layer
+  int n_samples = 1;
+};
+
+// process_circuit (DigitalTJM.jl:86-145) and _sample_plan (:159-168).
+Circuit process_circuit(const vector<Gate>& gates) {
+  Circuit c;
+  vector<int> cur;
+  vector<char> busy;
+  std::vector<std::pair<int, bool>> barriers;  // (index, is_sample)
+  auto flush = [&]() {
+    c.layers.push_back(cur);
+    cur.clear();
+    std::fill(busy.begin(), busy.end(), 0);
+  };
+  for (size_t g = 0; g < gates.size(); ++g) {
+    const Gate& G = gates[g];
+    int mx = std::max(G.a, G.b);
+    if ((int)busy.size() <= mx) busy.resize(mx + 1, 0);
+    if (G.kind == 0) {
+      if (!cur.empty()) flush();
+      barriers.push_back({(int)c.layers.size(), G.sample});
+      continue;
+    }
+    bool overlap = busy[G.a] || (G.kind == 2 && busy[G.b]);
+    if (overlap) flush();
+    cur.push_back((int)g);
+    busy[G.a] = 1;
+    if (G.kind == 2) busy[G.b] = 1;
+  }
+  if (!cur.empty()) c.layers.push_back(cur);
+  c.sample_after.assign(c.layers.size(), false);
+  for (auto& bs : barriers) {
+    if (!bs.second) continue;
+    if (bs.first == 0) c.sample_at_start = true;
+    else if (bs.first <= (int)c.layers.size()) c.sample_after[bs.first - 1] = true;
+  }
+  int n = c.sample_at_start ? 1 : 0;
+  for (bool x : c.sample_after) n += x ? 1 : 0;
+  c.n_samples = n == 0 ? 1 : n;
+  return c;
+}
+
+const cd kSwap[16] = {1, 0, 0, 0, 0, 0, 1, 0, 0, 1, 0, 0, 0, 0, 0, 1};
+
+// apply_local_gate_exact! (DigitalTJM.jl:251-305)
+void tebd_apply(const Problem& P, State& s, const cd* op, int s1, Counters& cnt) {
+  shift_oc(s, s1);
+  Ten Th = merge(s.t[s1], s.t[s1 + 1]);
+  apply_2site(Th, op);
+  Ten U, V;
+  split_theta(Th, 2, P.thr, P.max_bond, false, U, V, cnt);
+  s.t[s1] = U;
+  s.t[s1 + 1] = V;
+  s.oc = s1 + 1;
+}
+
+// apply_window! with method :TEBD (DigitalTJM.jl:307-334)
+void apply_window_tebd(const Problem& P, State& s, const Gate& G, Counters& cnt) {
+  const int s1 = std::min(G.a, G.b), s2 = std::max(G.a, G.b);
+  if (s2 > s1 + 1) {
+    for (int k = s2 - 1; k >= s1 + 1; --k) tebd_apply(P, s, kSwap, k, cnt);
+    tebd_apply(P, s, G.mat, s1, cnt);
+    for (int k = s1 + 1; k <= s2 - 1; ++k) tebd_apply(P, s, kSwap, k, cnt);
+  } else {
+    tebd_apply(P, s, G.mat, s1, cnt);
+  }
+}
+
+// create_local_noise_model (DigitalTJM.jl:172-188)
+NoiseSet local_noise(const NoiseSet& N, int s1, int s2) {
+  NoiseSet out;
+  out.present = true;
+  out.all_zero = true;
+  for (const auto& pr : N.procs) {
+    bool take = pr.nsites == 1 ? (pr.s0 == s1 || pr.s0 == s2)
+                               : ((pr.s0 == s1 && pr.s1 == s2) || (pr.s0 == s2 && pr.s1 == s1));
+    if (take) {
+      out.procs.push_back(pr);
+      if (pr.gamma != 0.0) out.all_zero = false;
     }
   }
-  for (int k = 0; k < n_obs; ++k) {
-    Obs o{};
-    o.kind = obs[k].kind;
-    o.s0 = obs[k].site[0];
-    o.s1 = obs[k].site[1];
-    int dd = o.kind == YAQS_OBS_LOCAL2 ? 4 : 2;
-    for (int e = 0; e < dd * dd; ++e) o.mat[e] = cd(obs[k].matrix[2 * e], obs[k].matrix[2 * e + 1]);
-    P.obs.push_back(o);
+  return out;
+}
+
+// run_digital_tjm (DigitalTJM.jl:363-450)
+int run_digital(const Problem& P, const vector<Gate>& gates, const Circuit& C, long long traj, double* out,
+                int* chi_out, Counters& cnt) {
+  State s = P.psi0;
+  normalize_mps(s);  // Simulator.jl:128
+  Draws rng{&P, traj};
+  const int ncols = C.n_samples;
+  int col = 0;
+  if (C.sample_at_start) evaluate(P, s, out, col++, ncols, chi_out);
+  for (size_t l = 0; l < C.layers.size(); ++l) {
+    for (int g : C.layers[l])
+      if (gates[g].kind == 1) apply_1site(s.t[gates[g].a], gates[g].mat);  // apply_single_qubit_gate!
+    for (int g : C.layers[l]) {
+      const Gate& G = gates[g];
+      if (G.kind != 2) continue;
+      apply_window_tebd(P, s, G, cnt);
+      if (P.noise.present && !P.noise.procs.empty()) {
+        NoiseSet loc = local_noise(P.noise, std::min(G.a, G.b), std::max(G.a, G.b));
+        if (!loc.procs.empty()) {
+          apply_dissipation(P, loc, s, true, 1.0, cnt);
+          stochastic_process(P, loc, s, 1.0, rng, cnt);
+        } else {
+          normalize_mps(s);
+        }
+      } else {
+        normalize_mps(s);
+      }
+    }
+    if (C.sample_after[l]) evaluate(P, s, out, col++, ncols, chi_out);
   }
-  P.rng_mode = rng->mode;
-  P.seed = rng->seed;
-  P.uniforms = rng->uniforms;
-  P.stride = rng->stride;
+  if (!C.sample_at_start && col == 0 && !P.obs.empty()) evaluate(P, s, out, 0, ncols, chi_out);
+  return rng.exhausted ? YAQS_E_RNG : YAQS_OK;
+}
+
+bool load_circuit(const yaqs_gate_desc* gates, int n, int L, vector<Gate>& out, std::string& err) {
+  for (int g = 0; g < n; ++g) {
+    const yaqs_gate_desc& q = gates[g];
+    Gate G{};
+    G.kind = q.kind;
+    G.a = q.site[0];
+    G.b = q.kind == 2 ? q.site[1] : q.site[0];
+    G.sample = q.sample != 0;
+    if (q.kind < 0 || q.kind > 2 || (q.kind != 0 && (G.a < 0 || G.a >= L || G.b < 0 || G.b >= L)) ||
+        (q.kind == 2 && G.a == G.b)) {
+      err = "bad gate descriptor";
+      return false;
+    }
+    if (q.kind == 0) G.a = G.b = 0;
+    int dd = q.kind == 2 ? 4 : 2;
+    for (int e = 0; e < dd * dd && q.kind != 0; ++e) G.mat[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);
+    out.push_back(G);
+  }
   return true;
 }
 
@@ -1428,6 +1616,71 @@ int orc_analog_run(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs
   return YAQS_OK;
 }
 
+int orc_digital_plan(const yaqs_gate_desc* gates, int32_t n_gates, int32_t* n_layers, int32_t* n_samples) {
+  vector<Gate> G;
+  std::string err;
+  int L = 1;
+  for (int g = 0; g < n_gates; ++g) L = std::max(L, std::max(gates[g].site[0], gates[g].site[1]) + 1);
+  if (!load_circuit(gates, n_gates, L, G, err)) return fail(YAQS_E_ARG, err);
+  Circuit C = process_circuit(G);
+  *n_layers = (int32_t)C.layers.size();
+  *n_samples = C.n_samples;
+  return YAQS_OK;
+}
+
+// Digital TJM trajectories [t_begin, t_end) on nthreads host threads.
+int orc_digital_run(const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
+                    const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                    const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, int32_t t_begin, int32_t t_end,
+                    int32_t nthreads, double* traj_out, int32_t* maxchi_out, yaqs_run_stats* stats) {
+  if (!psi0 || !cfg || !rng || psi0->L < 2) return fail(YAQS_E_ARG, "bad descriptors");
+  Problem P;
+  std::string err;
+  load_state(P, psi0);
+  P.dt = 1.0;  // gate-level noise uses dt = 1 (DigitalTJM.jl:412-413)
+  P.num_traj = cfg->num_traj;
+  P.max_bond = cfg->max_bond_dim;
+  P.thr = cfg->truncation_threshold;
+  P.traj_offset = cfg->traj_offset;
+  if (!load_noise(P, noise, err)) return fail(YAQS_E_ARG, err);
+  load_obs_rng(P, obs, n_obs, rng);
+  vector<Gate> G;
+  if (!load_circuit(gates, n_gates, P.L, G, err)) return fail(YAQS_E_ARG, err);
+  Circuit C = process_circuit(G);
+  const int ncols = C.n_samples;
+  if (t_begin < 0 || t_end > P.num_traj || t_begin > t_end) return fail(YAQS_E_ARG, "bad trajectory range");
+  std::atomic<int> next(t_begin);
+  std::atomic<int> status(YAQS_OK);
+  std::mutex mu;
+  Counters total;
+  auto worker = [&]() {
+    Counters c;
+    for (;;) {
+      int t = next.fetch_add(1);
+      if (t >= t_end) break;
+      vector<double> out((size_t)n_obs * ncols, 0.0);
+      vector<int> chi(ncols, 0);
+      int st = run_digital(P, G, C, t, out.data(), chi.data(), c);
+      if (st != YAQS_OK) status.store(st);
+      if (traj_out) std::copy(out.begin(), out.end(), traj_out + (size_t)t * n_obs * ncols);
+      if (maxchi_out) std::copy(chi.begin(), chi.end(), maxchi_out + (size_t)t * ncols);
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    total.svds += c.svds;
+    total.jumps += c.jumps;
+  };
+  vector<std::thread> th;
+  for (int i = 0; i < std::max(1, (int)nthreads); ++i) th.emplace_back(worker);
+  for (auto& x : th) x.join();
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->svds = total.svds;
+    stats->jumps = total.jumps;
+  }
+  if (status.load() != YAQS_OK) return fail(status.load(), "injected uniform stream exhausted");
+  return YAQS_OK;
+}
+
 // Plain 2TDVP evolution without noise: n_steps sweeps of two_site_tdvp!, with
 // local_expect of the given 1-site observables after every sweep (the loop
 // of test/benchmark_tdvp.jl:195-212 and test/simulate_large_ising.jl:69-81).
@@ -1474,7 +1727,7 @@ int orc_qr(int32_t m, int32_t n, const double* M, double* Q, double* R) {
 
 int orc_truncation_rank(int32_t n, const double* S, double thr, int32_t max_bond, int32_t rule) {
   vector<double> s(S, S + n);
-  return rule == 0 ? keep_tdvp(s, thr, max_bond) : keep_relative(s, thr, max_bond);
+  return rule == 0 ? keep_tdvp(s, thr, max_bond) : rule == 1 ? keep_relative(s, thr, max_bond) : keep_tebd(s, thr, max_bond);
 }
 
 // exp(-i dt H_eff) x for H_eff = project_site(L, R, W) with (chil, D, chir) x.

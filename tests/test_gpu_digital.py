@@ -1,0 +1,149 @@
+"""Digital TJM on the GPU (yaqs_digital_run) against the oracle: every
+trajectory's observables within 1e-10 relative on the same draws, identical
+bond dimensions and jump counts, plus the reference's known answers."""
+import numpy as np
+import pytest
+
+from yaqs_julia_b200 import _abi as A
+from yaqs_julia_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+def _zs(L):
+    return [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+
+
+def _brickwork(L, depth, long_range=True, seed=0, ring=False):
+    rng = np.random.default_rng(seed)
+    c = api.DigitalCircuit(L)
+    c.add_gate(api.Barrier(), [])
+    for _ in range(depth):
+        for i in list(range(1, L, 2)) + list(range(2, L, 2)):
+            c.add_gate(api.Rzz(rng.uniform(0, 1)), [i, i + 1])
+        if ring:
+            c.add_gate(api.Rzz(rng.uniform(0, 1)), [L, 1])
+        for i in range(1, L + 1):
+            c.add_gate(api.Rx(rng.uniform(0, 1)), [i])
+        if long_range:
+            c.add_gate(api.Rxx(rng.uniform(0, 1)), [1, L])
+            c.add_gate(api.CX, [L - 1, 2])
+        c.add_gate(api.Barrier(), [])
+    return c
+
+
+def _compare(oracle, L, c, obs, nm=None, num_traj=1, chi=64, thr=1e-9, seed=1, uniforms=None, rtol=1e-10,
+             psi=None):
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=1.0, num_traj=num_traj, max_bond_dim=chi, truncation_threshold=thr)
+    mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
+    d = api.CircuitDescriptors(psi if psi is not None else api.MPS(L), c, cfg, nm, rng_mode=mode, seed=seed, uniforms=uniforms)
+    ref, chi_ref, st_ref = oracle.digital_run(d)
+    got = api.run_circuit_descriptors(d)
+    err = np.abs(got.trajectories - ref)
+    assert err.max() <= rtol * max(1.0, np.abs(ref).max()), err.max()
+    assert np.array_equal(got.max_bond, chi_ref)
+    assert got.stats["jumps"] == st_ref["jumps"]
+    return got, ref
+
+
+def test_bell_state_known_answer():
+    """test_DigitalTJM.jl:50-72."""
+    c = api.DigitalCircuit(2).add_gate(api.H, [1]).add_gate(api.Rzz(np.pi / 2), [1, 2])
+    cfg = api.TimeEvolutionConfig(_zs(2), 1.0, dt=1.0)
+    api.run(api.MPS(2), c, cfg)
+    assert abs(cfg.observables[0].results[0]) < 1e-10 and abs(cfg.observables[1].results[0] - 1) < 1e-10
+    assert cfg.num_traj == 1
+
+
+def test_noiseless_circuit_with_long_range_gates(oracle):
+    L = 7
+    _compare(oracle, L, _brickwork(L, 4), _zs(L), thr=0.0)
+
+
+@pytest.mark.parametrize("chi,thr", [(4, 1e-9), (8, 1e-4), (64, 1e-9)])
+def test_truncation_paths(oracle, chi, thr):
+    L = 8
+    _compare(oracle, L, _brickwork(L, 5, seed=3), _zs(L) + [api.Observable("S", None, 4, kind="entropy")],
+             chi=chi, thr=thr)
+
+
+def test_pauli_noise_injected_draws(oracle):
+    L = 8
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.05} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_y", "pauli_z")], L)
+    c = _brickwork(L, 4, seed=5)
+    u = np.random.default_rng(3).random((12, api.max_draws_digital(c)))
+    got, _ = _compare(oracle, L, c, _zs(L), nm=nm, num_traj=12, chi=16, uniforms=u)
+    assert got.stats["jumps"] > 0
+
+
+def test_relaxation_and_dephasing_philox(oracle):
+    L = 6
+    nm = api.NoiseModel([{"name": "lowering", "sites": [i], "strength": 0.1} for i in range(1, L + 1)] +
+                        [{"name": "pauli_z", "sites": [i], "strength": 0.1} for i in range(1, L + 1)], L)
+    c = _brickwork(L, 4, seed=6)
+    psi = api.MPS(L, state="x+")
+    got, _ = _compare(oracle, L, c, _zs(L), nm=nm, num_traj=10, chi=16, seed=0xBEEF, psi=psi)
+    assert got.stats["jumps"] > 0
+
+
+def test_two_site_processes_take_the_reference_sweeps(oracle):
+    """Two-site dissipators that split run the full reference sweeps."""
+    L = 5
+    nm = api.NoiseModel([{"name": "crosstalk_xz", "sites": [2, 3], "strength": 0.3},
+                         {"name": "lowering_two", "sites": [3, 4], "strength": 0.5},
+                         {"name": "raising", "sites": [1], "strength": 0.2}], L)
+    c = _brickwork(L, 3, seed=7, long_range=False)
+    u = np.random.default_rng(9).random((6, api.max_draws_digital(c)))
+    _compare(oracle, L, c, [api.Observable(f"X{i}", api.X, i) for i in range(1, L + 1)], nm=nm, num_traj=6,
+             chi=8, uniforms=u, psi=api.MPS(L, state="x+"))
+
+
+def test_ring_circuit_with_edge_gate(oracle):
+    """The (L, 1) edge of a ring runs as a SWAP chain of 2(L-2) gates."""
+    L = 10
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.02} for i in range(1, L + 1)], L)
+    _compare(oracle, L, _brickwork(L, 3, seed=8, ring=True, long_range=False), _zs(L), nm=nm, num_traj=6,
+             chi=16, seed=4)
+
+
+def test_untight_start_state(oracle):
+    """A start state with oversized bonds takes the sweeps that shrink them."""
+    L = 6
+    psi = api.random_mps(L, 8, seed=1)
+    ts = list(psi.tensors)
+    rng = np.random.default_rng(2)
+    ts[2] = rng.standard_normal((4, 2, 1)) + 0j  # bond 3 drops to 1: bond 2 (4) exceeds 2 x 1
+    ts[3] = rng.standard_normal((1, 2, 4)) + 0j
+    psi = api.MPS(L, tensors=ts)
+    nm = api.NoiseModel([{"name": "pauli_x", "sites": [i], "strength": 0.1} for i in range(1, L + 1)], L)
+    _compare(oracle, L, _brickwork(L, 2, seed=9), _zs(L), nm=nm, num_traj=4, chi=8, seed=5, psi=psi)
+
+
+def test_no_sampling_barrier_measures_at_the_end(oracle):
+    L = 4
+    c = api.DigitalCircuit(L)
+    for i in range(1, L):
+        c.add_gate(api.CX, [i, i + 1])
+    c.add_gate(api.Barrier("not a sample"), [])
+    c.add_gate(api.H, [2])
+    got, _ = _compare(oracle, L, c, _zs(L))
+    assert got.trajectories.shape == (1, L, 1)
+
+
+def test_injected_stream_exhaustion_reports_status():
+    L = 4
+    nm = api.NoiseModel([{"name": "pauli_x", "sites": [i], "strength": 0.5} for i in range(1, L + 1)], L)
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=2)
+    c = _brickwork(L, 2)
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED,
+                               uniforms=np.full((2, 1), 0.5))
+    from yaqs_julia_b200._lib import EngineError
+    with pytest.raises(EngineError, match="YAQS_E_RNG"):
+        api.run_circuit_descriptors(d)
+
+
+def test_library_plan_matches_host_plan():
+    c = _brickwork(6, 3, ring=True)
+    layers, _ = api.process_circuit(c)
+    assert api.digital_plan(c) == (len(layers), api.sample_plan(c)[2])

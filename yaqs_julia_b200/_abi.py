@@ -75,6 +75,23 @@ class TevConfig(C.Structure):
                 ("precision", C.c_int32), ("traj_offset", C.c_int32)]
 
 
+YAQS_GATE_BARRIER = 0
+YAQS_GATE_1Q = 1
+YAQS_GATE_2Q = 2
+
+
+class GateDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("site", C.c_int32 * 2), ("matrix", C.c_double * 32),
+                ("sample", C.c_int32)]
+
+
+class CircuitConfig(C.Structure):
+    _fields_ = [("num_traj", C.c_int32), ("max_bond_dim", C.c_int32),
+                ("truncation_threshold", C.c_double), ("local_method", C.c_int32),
+                ("long_range_method", C.c_int32), ("precision", C.c_int32),
+                ("traj_offset", C.c_int32)]
+
+
 class RunStats(C.Structure):
     _fields_ = [("matvecs", C.c_int64), ("krylov_solves", C.c_int64),
                 ("svds", C.c_int64), ("jumps", C.c_int64),

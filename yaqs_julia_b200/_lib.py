@@ -43,6 +43,10 @@ def lib():
         L.yaqs_analog_profile.argtypes = [C.c_void_p, A.DPTR]
         L.yaqs_analog_stats.argtypes = [C.c_void_p, P(A.RunStats)]
         L.yaqs_analog_finish.argtypes = [C.c_void_p, A.DPTR, A.DPTR, P(C.c_int32), P(A.RunStats)]
+        L.yaqs_digital_plan.argtypes = [P(A.GateDesc), C.c_int32, P(C.c_int32), P(C.c_int32)]
+        L.yaqs_digital_run.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),
+                                       P(A.ObsDesc), C.c_int32, P(A.CircuitConfig), P(A.RngDesc), A.DPTR, A.DPTR,
+                                       P(C.c_int32), P(A.RunStats)]
         L.yaqs_fp64_peak.argtypes = [C.c_void_p, P(C.c_double)]
         L.yaqs_batched_svd_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4 + [
             C.c_void_p]

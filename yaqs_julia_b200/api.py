@@ -56,6 +56,20 @@ def Rzz(theta):
 
 
 SWAP = np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, 1, 0, 0], [0, 0, 0, 1]], dtype=np.complex128)
+# CX as GateLibrary.jl:144-150 writes it (control on the second site under the
+# p1 + 2 p2 basis convention)
+CX = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=np.complex128)
+CZ = np.diag([1, 1, 1, -1]).astype(np.complex128)
+
+
+def Ry(theta):
+    c, s = math.cos(theta / 2), math.sin(theta / 2)
+    return np.array([[c, -s], [s, c]], dtype=np.complex128)
+
+
+def Rxx(theta):
+    c, s = math.cos(theta / 2), -1j * math.sin(theta / 2)
+    return np.array([[c, 0, 0, s], [0, c, s, 0], [0, s, c, 0], [s, 0, 0, c]], dtype=np.complex128)
 
 
 def kron2(a, b):
@@ -452,6 +466,137 @@ def max_draws(sim_params: TimeEvolutionConfig) -> int:
 
 
 # ---------------------------------------------------------------------------
+# Digital circuits (src/DigitalTJM.jl:35-168)
+# ---------------------------------------------------------------------------
+class Barrier:
+    """GateLibrary.Barrier (src/GateLibrary.jl:305-311)."""
+
+    def __init__(self, label: str = "SAMPLE_OBSERVABLES"):
+        self.label = label
+
+
+class DigitalGate:
+    def __init__(self, op, sites):
+        self.op = op if isinstance(op, Barrier) else np.asarray(op, dtype=np.complex128)
+        self.sites = list(sites)
+
+
+class DigitalCircuit:
+    """DigitalCircuit(num_qubits) with add_gate (add_gate!, DigitalTJM.jl:60-66).
+    Gates are 2x2 / 4x4 matrices (4x4 in the p1 + 2 p2 basis of the smaller
+    site first, as apply_local_gate_exact! reads them) or Barrier."""
+
+    def __init__(self, num_qubits: int):
+        self.num_qubits = int(num_qubits)
+        self.gates: list[DigitalGate] = []
+
+    def add_gate(self, op, sites):
+        if isinstance(sites, int):
+            sites = [sites]
+        self.gates.append(DigitalGate(op, sites))
+        return self
+
+
+def add_gate(circ: DigitalCircuit, op, sites):
+    return circ.add_gate(op, sites)
+
+
+def process_circuit(circ: DigitalCircuit):
+    """Greedy layering and barrier map (DigitalTJM.jl:86-145)."""
+    layers, barrier_map, cur, busy = [], {}, [], set()
+    for g in circ.gates:
+        if isinstance(g.op, Barrier):
+            if cur:
+                layers.append(cur)
+                cur, busy = [], set()
+            barrier_map.setdefault(len(layers), []).append(g.op.label)
+            continue
+        if any(q in busy for q in g.sites):
+            layers.append(cur)
+            cur, busy = [], set()
+        cur.append(g)
+        busy.update(g.sites)
+    if cur:
+        layers.append(cur)
+    return layers, barrier_map
+
+
+def sample_plan(circ: DigitalCircuit):
+    """(sample_at_start, sample_after, n_samples) of run_digital_tjm (DigitalTJM.jl:159-168, 375-379)."""
+    layers, bm = process_circuit(circ)
+    has = lambda i: any(lbl.upper() == "SAMPLE_OBSERVABLES" for lbl in bm.get(i, []))  # noqa: E731
+    start = has(0)
+    after = [l for l in range(1, len(layers) + 1) if has(l)]
+    n = (1 if start else 0) + len(after)
+    return start, after, max(n, 1)
+
+
+class CircuitDescriptors:
+    """Owns every buffer referenced by the C descriptors of a digital run."""
+
+    def __init__(self, psi0: MPS, circ: DigitalCircuit, sim_params: TimeEvolutionConfig,
+                 noise_model: NoiseModel | None, *, rng_mode: int = A.YAQS_RNG_PHILOX, seed: int = 0,
+                 uniforms: np.ndarray | None = None, traj_offset: int = 0, num_traj: int | None = None):
+        L = psi0.length
+        if circ.num_qubits != L:
+            raise ValueError("circuit and MPS sizes differ")
+        # reuse the analog packer for the state, noise, observables and rng
+        dummy = init_ising(L, 0.0, 0.0)
+        base = Descriptors(psi0, dummy, sim_params, noise_model, rng_mode=rng_mode, seed=seed,
+                           uniforms=uniforms, traj_offset=traj_offset, num_traj=num_traj)
+        self._base = base
+        self.mps, self.noise, self.obs, self.n_obs, self.rng = base.mps, base.noise, base.obs, base.n_obs, base.rng
+        self.num_traj = base.num_traj
+        self.gates = self.pack_gates(circ)
+        self.n_gates = len(circ.gates)
+        self.cfg = A.CircuitConfig(self.num_traj, sim_params.max_bond_dim, sim_params.truncation_threshold, 0, 0,
+                                   A.YAQS_PREC_FP64, traj_offset)
+        self.n_out = sample_plan(circ)[2]
+
+    @staticmethod
+    def pack_gates(circ: DigitalCircuit):
+        """yaqs_gate_desc array of the circuit (sites 0-based, matrices column-major)."""
+        gd = (A.GateDesc * max(1, len(circ.gates)))()
+        for k, g in enumerate(circ.gates):
+            d = gd[k]
+            if isinstance(g.op, Barrier):
+                d.kind = A.YAQS_GATE_BARRIER
+                d.sample = int(g.op.label.upper() == "SAMPLE_OBSERVABLES")
+                continue
+            if len(g.sites) == 1:
+                d.kind = A.YAQS_GATE_1Q
+                d.site[0] = d.site[1] = g.sites[0] - 1
+            elif len(g.sites) == 2:
+                d.kind = A.YAQS_GATE_2Q
+                d.site[0], d.site[1] = g.sites[0] - 1, g.sites[1] - 1
+            else:
+                raise ValueError("gates act on 1 or 2 qubits")
+            m = _c64(g.op)
+            for e in range(m.size):
+                d.matrix[e] = m[e]
+        return gd
+
+
+def create_local_noise_model(noise_model: NoiseModel, site1: int, site2: int) -> NoiseModel:
+    """Processes of a noise model that act after a gate on (site1, site2):
+    1-site processes on either site and 2-site processes on exactly that pair
+    (DigitalTJM.jl:172-188).  The engine applies the same selection on the
+    device (proc_on in the CUDA sources)."""
+    out = []
+    for p in noise_model.processes:
+        if len(p.sites) == 1 and p.sites[0] in (site1, site2):
+            out.append(p)
+        elif len(p.sites) == 2 and sorted(p.sites) == sorted((site1, site2)):
+            out.append(p)
+    return NoiseModel(out)
+
+
+def max_draws_digital(circ: DigitalCircuit) -> int:
+    """Upper bound on uniforms one digital trajectory consumes (2 per 2-qubit gate)."""
+    return 2 * max(1, sum(1 for g in circ.gates if not isinstance(g.op, Barrier) and len(g.sites) == 2))
+
+
+# ---------------------------------------------------------------------------
 # Simulator.run (src/Simulator.jl:22-69, 127-141) on the GPU engine
 # ---------------------------------------------------------------------------
 class RunResult:
@@ -475,6 +620,34 @@ def run_descriptors(desc: Descriptors, ctx=None) -> RunResult:
                                        desc.obs, nobs, C.byref(desc.cfg), C.byref(desc.rng), A.dptr(traj),
                                        A.dptr(mean), chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st)))
     return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
+
+
+def run_circuit_descriptors(desc: CircuitDescriptors, ctx=None) -> RunResult:
+    """Runs a packed circuit problem through yaqs_digital_run."""
+    from . import _lib
+    ctx = ctx or _lib.default_context()
+    nt, nobs, nout = desc.num_traj, desc.n_obs, desc.n_out
+    traj = np.zeros((nt, max(nobs, 1), nout))
+    mean = np.zeros((max(nobs, 1), nout))
+    chi = np.zeros((nt, nout), dtype=np.int32)
+    st = A.RunStats()
+    ctx.check(ctx._lib.yaqs_digital_run(ctx.handle, C.byref(desc.mps), desc.gates, desc.n_gates,
+                                        C.byref(desc.noise), desc.obs, nobs, C.byref(desc.cfg), C.byref(desc.rng),
+                                        A.dptr(traj), A.dptr(mean), chi.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        C.byref(st)))
+    return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
+
+
+def digital_plan(circ: DigitalCircuit) -> tuple[int, int]:
+    """(number of layers, number of measurement columns) as the library plans them."""
+    from . import _lib
+    L = _lib.lib()
+    gd = CircuitDescriptors.pack_gates(circ)
+    nl, ns = C.c_int32(0), C.c_int32(0)
+    st = L.yaqs_digital_plan(gd, len(circ.gates), C.byref(nl), C.byref(ns))
+    if st != 0:
+        raise _lib.EngineError(st, L.yaqs_last_error(None).decode())
+    return nl.value, ns.value
 
 
 class Session:
@@ -539,20 +712,36 @@ def random_mps(length: int, chi: int, seed: int = 0) -> MPS:
     return MPS(length, tensors=ts)
 
 
-def run(initial_state: MPS, operator: MPO, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
+def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
         *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12, ctx=None) -> RunResult:
-    """Simulator.run for an MPO (analog TJM).  Fills every observable's
-    ``trajectories`` [num_traj, n_out] and ``results`` [n_out] like
-    _run_analog.  As in the reference, a noiseless model runs one trajectory
-    and mutates ``sim_params.num_traj`` (Simulator.jl:27-29)."""
-    if not isinstance(operator, MPO):
-        raise TypeError("Simulation requires MPO (Analog).")
+    """Simulator.run (Simulator.jl:127-141) for an MPO (analog TJM) or a
+    DigitalCircuit (digital TJM, TEBD gate application).  Fills every
+    observable's ``trajectories`` and ``results`` like _run_analog /
+    _run_digital; the result's ``max_bond`` holds the per-trajectory bond
+    dimensions at each measurement.  As in the reference, a noiseless model
+    runs one trajectory and mutates ``sim_params.num_traj`` (Simulator.jl:27-29)."""
+    if not isinstance(operator, (MPO, DigitalCircuit)):
+        raise TypeError("Simulation requires MPO (Analog) or DigitalCircuit (Digital).")
     if noise_model is None or all(p.strength == 0 for p in noise_model.processes):
         sim_params.num_traj = 1
     mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
-    desc = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
-                       uniforms=uniforms, krylov_exit_tol=krylov_exit_tol)
-    res = run_descriptors(desc, ctx)
+    if isinstance(operator, DigitalCircuit):  # _run_digital, Simulator.jl:71-125
+        desc = CircuitDescriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
+                                  uniforms=uniforms)
+        res = run_circuit_descriptors(desc, ctx)
+    else:
+        desc = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
+                           uniforms=uniforms, krylov_exit_tol=krylov_exit_tol)
+        res = run_descriptors(desc, ctx)
+    if isinstance(operator, DigitalCircuit):
+        # obs buffers sized by sim_params.times; the first min(n_samples, columns) are filled (Simulator.jl:99-103)
+        ncol = len(sim_params.times) if sim_params.sample_timesteps else 1
+        n_copy = min(ncol, res.trajectories.shape[2])
+        for k, o in enumerate(sim_params.observables):
+            o.trajectories = np.zeros((sim_params.num_traj, ncol), dtype=np.complex128)
+            o.trajectories[:, :n_copy] = res.trajectories[:, k, :n_copy]
+            o.results = o.trajectories.real.sum(axis=0) / sim_params.num_traj
+        return res
     for k, o in enumerate(sim_params.observables):
         o.trajectories = res.trajectories[:, k, :].astype(np.complex128)
         o.results = res.mean[k].copy()

@@ -1,0 +1,263 @@
+// digital.cuh — per-trajectory digital TJM program executed by one CTA.
+//
+// Restates run_digital_tjm (DigitalTJM.jl:363-450) with TEBD gate
+// application (apply_local_gate_exact!, DigitalTJM.jl:251-305), SWAP chains
+// for long-range gates (DigitalTJM.jl:314-330) and the local noise step
+// after every 2-qubit gate (DigitalTJM.jl:405-420).
+//
+// The reference's noise step sweeps the whole chain (apply_dissipation walks
+// the orthogonality centre from site L to 1, stochastic_process! contracts
+// the full norm and normalize! re-canonicalises every site).  When every bond
+// of the chain is "tight" (no bond exceeds twice either neighbour), the thin
+// QR / LQ steps of those sweeps change no shape and are pure gauge moves:
+// every dissipator and jump touches only the gate's sites, each is applied
+// while the orthogonality centre sits on that site (as in the reference
+// sweep), the norm equals the norm of the centre tensor and normalisation
+// rescales it.  The device then performs the same operations at the gate's
+// sites only, which is equivalent up to rounding; on a chain that is not
+// tight, or with two-site dissipators that split, it runs the reference
+// sweeps, so bond dimensions always match the reference's.
+#pragma once
+#include "tjm.cuh"
+
+struct DevGate {
+  int kind;  // 1 one-qubit, 2 two-qubit
+  int a, b;  // sorted sites for 2-qubit gates (a < b)
+  cplx mat[16];
+};
+
+struct DigParams {
+  const DevGate* gates;
+  const int* layer_off;   // [n_layers + 1] into gates
+  const int* sample_col;  // [n_layers] measurement column after the layer, -1 for none
+  int n_layers;
+  int sample_at_start;
+  int any_sample;
+};
+
+__device__ __constant__ cplx c_swap[16] = {{1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}, {0, 0},
+                                           {0, 0}, {1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}};
+
+// Scale the orthogonality-centre tensor to unit norm (normalize!, MPS.jl:274-311).
+__device__ void normalize_center(Ctx& c, const DState& s) {
+  const int oc = *s.oc;
+  cplx* A = site_ptr(c, s, oc);
+  const long long n = (long long)s.chi[oc] * 2 * s.chi[oc + 1];
+  double nr = sqrt(cta_norm2(A, n, c.sm.e.r));
+  if (nr > 1e-13) cta_scale(A, n, 1.0 / nr);
+  __syncthreads();
+}
+
+// True when every bond satisfies chi[b] <= 2 chi[b-1] and chi[b] <= 2 chi[b+1]:
+// then the thin QR / LQ factorisations of a gauge sweep keep every shape, so
+// a sweep is a pure gauge move.  Uniform across the CTA.
+__device__ bool chain_tight(const Ctx& c, const DState& s) {
+  bool ok = true;
+  for (int b = 1; b < c.P.L; ++b) {
+    const int x = s.chi[b];
+    if (x > 2 * s.chi[b - 1] || x > 2 * s.chi[b + 1]) ok = false;
+  }
+  return ok;
+}
+
+// normalize! after a gate or a noise step: on a tight chain the full sweep
+// only rescales the centre tensor; otherwise run the sweep.
+__device__ void finish_normalize(Ctx& c, const DState& s) {
+  if (chain_tight(c, s))
+    normalize_center(c, s);
+  else
+    normalize_state(c, s);
+}
+
+// apply_local_gate_exact! on sites (s1, s1+1).
+__device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
+  shift_oc(c, s, s1);
+  if (c.sm.fail) return;
+  cplx* th = c.ws + c.P.lay.th;
+  const int l = s.chi[s1], r = s.chi[s1 + 2];
+  merge(c, s, s1, th);
+  apply_local(th, l, 4, r, op);
+  split(c, s, s1, th, l, r, 2, false);
+  __syncthreads();
+  if (threadIdx.x == 0) *s.oc = s1 + 1;
+  __syncthreads();
+}
+
+// apply_window! with method :TEBD (DigitalTJM.jl:307-334).
+__device__ void apply_window_tebd(Ctx& c, const DState& s, const DevGate& g) {
+  if (g.b > g.a + 1) {
+    for (int k = g.b - 1; k >= g.a + 1 && !c.sm.fail; --k) tebd_apply(c, s, c_swap, k);
+    if (!c.sm.fail) tebd_apply(c, s, g.mat, g.a);
+    for (int k = g.a + 1; k <= g.b - 1 && !c.sm.fail; ++k) tebd_apply(c, s, c_swap, k);
+  } else {
+    tebd_apply(c, s, g.mat, g.a);
+  }
+}
+
+// Local dissipation (dt = 1) and jump step after a 2-qubit gate on (s1, s2),
+// s1 < s2 (DigitalTJM.jl:405-420).  When the chain is tight and no
+// dissipator needs a two-site split, every operation of the reference sweeps
+// away from the gate's sites is a gauge move, and only the gate's sites are
+// visited; otherwise the reference sweeps run as they are.
+__device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
+  const DevParams& P = c.P;
+  int nloc = 0;
+  bool all_zero = true, split_diss = false;
+  for (int k = 0; k < P.nprocs; ++k) {
+    const DevProc& pr = P.procs[k];
+    if (!proc_on(pr, s1, s2)) continue;
+    ++nloc;
+    if (pr.gamma != 0.0) all_zero = false;
+    if (pr.nsites == 2 && !pr.pauli_name) split_diss = true;
+  }
+  if (!P.noise_present || nloc == 0) {
+    finish_normalize(c, s);
+    return;
+  }
+  if ((split_diss && !all_zero) || !chain_tight(c, s)) {
+    apply_dissipation(c, s, true, 1.0, s1, s2);
+    if (c.sm.fail) return;
+    stochastic_process(c, s, 1.0, s1, s2);
+    return;
+  }
+  cplx* th = c.ws + c.P.lay.th;
+  // apply_dissipation: the reference sweep reaches s2 before s1
+  if (!all_zero) {
+    const int sites[2] = {s2, s1};
+    for (int si = 0; si < 2 && !c.sm.fail; ++si) {
+      const int i = sites[si];
+      shift_oc(c, s, i);
+      for (int k = 0; k < P.nprocs; ++k) {
+        const DevProc& pr = P.procs[k];
+        if (!proc_on(pr, s1, s2) || pr.nsites != 1 || pr.s0 != i) continue;
+        cplx* A = site_ptr(c, s, i);
+        if (pr.pauli_name) {
+          cta_scale(A, (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * pr.gamma));
+          __syncthreads();
+        } else {
+          apply_local(A, s.chi[i], 2, s.chi[i + 1], pr.diss_full);
+        }
+      }
+      if (si == 0) {  // 2-site Pauli processes on (s1, s2) scale site s2
+        for (int k = 0; k < P.nprocs; ++k) {
+          const DevProc& pr = P.procs[k];
+          if (!proc_on(pr, s1, s2) || pr.nsites != 2 || pr.s1 != i) continue;
+          cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * pr.gamma));
+          __syncthreads();
+        }
+      }
+    }
+  }
+  if (c.sm.fail) return;
+  // stochastic_process!: the norm is the norm of the centre tensor
+  const int oc = *s.oc;
+  const double nrm = cta_norm2(site_ptr(c, s, oc), (long long)s.chi[oc] * 2 * s.chi[oc + 1], c.sm.e.r);
+  const double dp = 1.0 - nrm;
+  const double u1 = draw_uniform(c);
+  if (u1 >= dp) {
+    normalize_center(c, s);
+    return;
+  }
+  double* cand = reinterpret_cast<double*>(c.ws + c.P.lay.dbl) + SVD_MAX_COLS;
+  int* candp = c.wsi + c.P.lay.i_cand;
+  int nc = 0;
+  const int sites[2] = {s1, s2};
+  for (int si = 0; si < 2 && !c.sm.fail; ++si) {
+    const int site = sites[si];
+    shift_oc(c, s, site);
+    for (int k = 0; k < P.nprocs; ++k) {
+      const DevProc& pr = P.procs[k];
+      if (!proc_on(pr, s1, s2) || pr.nsites != 1 || pr.s0 != site) continue;
+      double nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1], pr.pauli_proc ? nullptr : pr.mat);
+      if (threadIdx.x == 0) {
+        cand[nc] = pr.gamma * nr;
+        candp[nc] = k;
+      }
+      ++nc;
+    }
+    if (site < P.L - 1) {
+      for (int k = 0; k < P.nprocs; ++k) {
+        const DevProc& pr = P.procs[k];
+        if (!proc_on(pr, s1, s2) || pr.nsites != 2 || pr.s0 != site) continue;
+        double nr;
+        if (pr.pauli_proc) {
+          nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1], nullptr);
+        } else {
+          merge(c, s, site, th);
+          nr = local_norm2(c, th, s.chi[site], 4, s.chi[site + 2], pr.mat);
+        }
+        if (threadIdx.x == 0) {
+          cand[nc] = pr.gamma * nr;
+          candp[nc] = k;
+        }
+        ++nc;
+      }
+    }
+  }
+  __syncthreads();
+  double total = 0.0;
+  for (int e = 0; e < nc; ++e) total += cand[e];
+  if (total == 0.0) {
+    normalize_center(c, s);
+    return;
+  }
+  const double r = draw_uniform(c);
+  double acc = 0.0;
+  int chosen = 0;
+  for (int e = 0; e < nc; ++e) {
+    acc += cand[e] / total;
+    if (r <= acc) {
+      chosen = e;
+      break;
+    }
+  }
+  const DevProc& pr = P.procs[candp[chosen]];
+  __syncthreads();
+  shift_oc(c, s, pr.s0);
+  if (pr.nsites == 1) {
+    apply_local(site_ptr(c, s, pr.s0), s.chi[pr.s0], 2, s.chi[pr.s0 + 1], pr.mat);
+  } else {
+    const int l = s.chi[pr.s0], rr = s.chi[pr.s0 + 2];
+    merge(c, s, pr.s0, th);
+    apply_local(th, l, 4, rr, pr.mat);
+    split(c, s, pr.s0, th, l, rr, 1, false);
+  }
+  if (threadIdx.x == 0) c.cnt[3] += 1;
+  finish_normalize(c, s);
+}
+
+// Launch 0: initial state, normalisation and the start sample; launch l >= 1:
+// layer l-1 (its 1-qubit gates first, then each 2-qubit gate followed by the
+// noise step) and the sample after it.
+__device__ void run_digital_step(Ctx& c, const DigParams& D, int launch) {
+  const DevParams& P = c.P;
+  const int L = P.L;
+  DState st{P.phi + (long long)c.traj * P.mps_size, P.phi_chi + (long long)c.traj * (L + 1), P.phi_oc + c.traj};
+  if (launch == 0) {
+    cta_copy(st.a, P.psi0, P.mps_size);
+    for (int b = threadIdx.x; b <= L; b += NT) st.chi[b] = P.chi0[b];
+    if (threadIdx.x == 0) *st.oc = 0;
+    __syncthreads();
+    normalize_state(c, st);  // Simulator.jl:128
+    if (D.sample_at_start) evaluate(c, st, 0);
+    if (D.n_layers == 0 && !D.any_sample && P.nobs > 0) evaluate(c, st, 0);
+    return;
+  }
+  const int l = launch - 1;
+  for (int g = D.layer_off[l]; g < D.layer_off[l + 1]; ++g) {
+    const DevGate& G = D.gates[g];
+    if (G.kind == 1) apply_local(site_ptr(c, st, G.a), st.chi[G.a], 2, st.chi[G.a + 1], G.mat);
+  }
+  for (int g = D.layer_off[l]; g < D.layer_off[l + 1] && !c.sm.fail; ++g) {
+    const DevGate& G = D.gates[g];
+    if (G.kind != 2) continue;
+    apply_window_tebd(c, st, G);
+    if (c.sm.fail) return;
+    digital_noise(c, st, G.a, G.b);
+    if (c.sm.fail) return;
+    if (threadIdx.x == 0) c.cnt[6] += 1;
+  }
+  if (c.sm.fail) return;
+  if (D.sample_col[l] >= 0) evaluate(c, st, D.sample_col[l]);
+  if (l == D.n_layers - 1 && !D.any_sample && P.nobs > 0) evaluate(c, st, 0);
+}

@@ -20,7 +20,7 @@
 
 #include "../../include/yaqs_tjm.h"
 #include "../../include/yaqs_tjm_components.h"
-#include "tjm.cuh"
+#include "digital.cuh"
 
 // ---------------------------------------------------------------------------
 // Device program
@@ -105,6 +105,31 @@ __global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int 
     __syncthreads();
     Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
     run_step(c, j);
+    __syncthreads();
+    if (threadIdx.x == 0 && sm.fail) P.status[t] = sm.fail;
+    __syncthreads();
+  }
+}
+
+// Digital TJM: launch 0 prepares every trajectory, launch l >= 1 applies
+// layer l-1 of the circuit (run_digital_tjm, DigitalTJM.jl:363-450).
+__global__ void __launch_bounds__(NT, 2) digital_step_kernel(const DevParams P, const DigParams D, int j) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+  const int slot = blockIdx.x;
+  cplx* ws = P.ws + (long long)slot * P.lay.total;
+  int* wsi = P.wsi + (long long)slot * P.lay.itotal;
+  for (;;) {
+    if (threadIdx.x == 0) sm.bcast_i[7] = atomicAdd(&P.queue[j], 1);
+    __syncthreads();
+    const int t = sm.bcast_i[7];
+    __syncthreads();
+    if (t >= P.num_traj) break;
+    if (P.status[t] != 0) continue;
+    if (threadIdx.x == 0) sm.fail = 0;
+    __syncthreads();
+    Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
+    run_digital_step(c, D, j);
     __syncthreads();
     if (threadIdx.x == 0 && sm.fail) P.status[t] = sm.fail;
     __syncthreads();
@@ -365,6 +390,65 @@ int upload_wmats(yaqs_ctx* ctx, DevMem& dm, const std::vector<HostWMat>& all, st
 
 inline hcd cload(const double* p, size_t k) { return hcd(p[2 * k], p[2 * k + 1]); }
 
+// Noise processes for the device: jump operator and the dissipators
+// exp(-0.5 dt_eff gamma L^dag L) for dt_eff = dt/2 and dt (Dissipation.jl:62-69).
+int pack_noise(yaqs_ctx* ctx, const yaqs_noise_desc* noise, int nprocs, int L, double dt, std::vector<DevProc>& hp,
+               bool& all_zero) {
+  hp.assign(std::max(nprocs, 1), DevProc());
+  all_zero = true;
+  for (int k = 0; k < nprocs; ++k) {
+    const yaqs_noise_proc& q = noise->procs[k];
+    DevProc& d = hp[k];
+    memset(&d, 0, sizeof(d));
+    d.nsites = q.nsites;
+    d.s0 = q.site[0];
+    d.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
+    if (q.nsites < 1 || q.nsites > 2 || d.s0 < 0 || d.s1 >= L || (q.nsites == 2 && d.s1 != d.s0 + 1))
+      return set_err(ctx, q.nsites == 2 ? YAQS_E_UNSUPPORTED : YAQS_E_ARG,
+                     "noise processes must be 1-site or adjacent 2-site with sites in range");
+    d.gamma = q.strength;
+    d.pauli_name = q.pauli_name;
+    d.pauli_proc = q.pauli_proc;
+    if (q.strength != 0.0) all_zero = false;
+    const int dd = q.nsites == 1 ? 2 : 4;
+    hcd M[16], LdL[16], e1[16], e2[16];
+    for (int e = 0; e < dd * dd; ++e) M[e] = cload(q.matrix, e);
+    for (int i = 0; i < dd; ++i)
+      for (int j = 0; j < dd; ++j) {
+        hcd sacc = 0;
+        for (int kk = 0; kk < dd; ++kk) sacc += std::conj(M[kk + dd * i]) * M[kk + dd * j];
+        LdL[i + dd * j] = sacc;
+      }
+    herm_expm(dd, LdL, -0.5 * (dt / 2) * q.strength, e1);
+    herm_expm(dd, LdL, -0.5 * dt * q.strength, e2);
+    for (int e = 0; e < dd * dd; ++e) {
+      d.mat[e] = make_double2(M[e].real(), M[e].imag());
+      d.diss_half[e] = make_double2(e1[e].real(), e1[e].imag());
+      d.diss_full[e] = make_double2(e2[e].real(), e2[e].imag());
+    }
+  }
+  return YAQS_OK;
+}
+
+int pack_obs(yaqs_ctx* ctx, const yaqs_obs_desc* obs, int n_obs, int L, std::vector<DevObs>& ho) {
+  ho.assign(std::max(n_obs, 1), DevObs());
+  for (int k = 0; k < n_obs; ++k) {
+    const yaqs_obs_desc& o = obs[k];
+    DevObs& d = ho[k];
+    memset(&d, 0, sizeof(d));
+    d.kind = o.kind;
+    d.s0 = o.site[0];
+    d.s1 = o.site[1];
+    bool ok = (o.kind == YAQS_OBS_LOCAL1 && d.s0 >= 0 && d.s0 < L) ||
+              (o.kind == YAQS_OBS_LOCAL2 && d.s0 >= 0 && d.s0 + 1 < L && d.s1 == d.s0 + 1) ||
+              (o.kind == YAQS_OBS_ENTROPY && d.s0 >= 0 && d.s0 + 1 < L);
+    if (!ok) return set_err(ctx, YAQS_E_ARG, "bad observable descriptor");
+    const int dd = o.kind == YAQS_OBS_LOCAL2 ? 4 : 2;
+    for (int e = 0; e < dd * dd; ++e) d.mat[e] = make_double2(o.matrix[2 * e], o.matrix[2 * e + 1]);
+  }
+  return YAQS_OK;
+}
+
 }  // namespace
 
 // One analog run held on the device between yaqs_analog_begin and
@@ -373,6 +457,8 @@ struct yaqs_run {
   yaqs_ctx* ctx = nullptr;
   DevMem dm;
   DevParams P;
+  int digital = 0;  // 0 analog TJM program, 1 digital (circuit) program
+  DigParams D;
   int slots = 0;
   size_t smem = 0;
   int num_traj = 0, n_obs = 0, ncols = 0;
@@ -398,6 +484,120 @@ struct yaqs_run {
     if (stream) cudaStreamDestroy(stream);
   }
 };
+
+// Uploads what the analog and digital programs share (site capacities and
+// offsets, noise processes, observables, the initial state) and allocates
+// the trajectory states, per-slot workspaces and outputs.  Expects P.L,
+// P.num_traj, P.mps_size, P.lay, run->slots, run->n_obs and run->ncols set.
+static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, const std::vector<int>& chi0,
+              const std::vector<int>& w, const std::vector<long long>& mps_off, const std::vector<long long>& env_off,
+              const yaqs_mps_desc* psi0, const std::vector<DevProc>& hp, const std::vector<DevObs>& ho,
+              const yaqs_rng_desc* rng, int nqueue) {
+  DevMem& dm = run->dm;
+  DevParams& P = run->P;
+  const int L = P.L, num_traj = P.num_traj, slots = run->slots, n_obs = run->n_obs, ncols = run->ncols;
+  const long long mps_size = P.mps_size;
+  const WsLayout& lay = P.lay;
+  int *d_cap, *d_w, *d_chi0;
+  long long *d_mps_off, *d_env_off;
+  CUDA_TRY(ctx, dm.alloc(&d_cap, L + 1));
+  CUDA_TRY(ctx, dm.alloc(&d_w, L + 1));
+  CUDA_TRY(ctx, dm.alloc(&d_chi0, L + 1));
+  CUDA_TRY(ctx, dm.alloc(&d_mps_off, L));
+  CUDA_TRY(ctx, dm.alloc(&d_env_off, L + 1));
+  CUDA_TRY(ctx, cudaMemcpy(d_cap, cap.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_w, w.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_chi0, chi0.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_mps_off, mps_off.data(), L * sizeof(long long), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_env_off, env_off.data(), (L + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+  P.cap = d_cap;
+  P.w = d_w;
+  P.chi0 = d_chi0;
+  P.mps_off = d_mps_off;
+  P.env_off = d_env_off;
+
+  DevProc* d_procs;
+  DevObs* d_obs;
+  CUDA_TRY(ctx, dm.alloc(&d_procs, hp.size()));
+  CUDA_TRY(ctx, dm.alloc(&d_obs, ho.size()));
+  CUDA_TRY(ctx, cudaMemcpy(d_procs, hp.data(), hp.size() * sizeof(DevProc), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_obs, ho.data(), ho.size() * sizeof(DevObs), cudaMemcpyHostToDevice));
+  P.procs = d_procs;
+  P.obs = d_obs;
+
+  // initial state arena (compact tensors at the site slots)
+  std::vector<hcd> arena((size_t)mps_size, 0.0);
+  for (int i = 0; i < L; ++i) {
+    const size_t n = (size_t)chi0[i] * 2 * chi0[i + 1];
+    if (!psi0->tensors[i]) return set_err(ctx, YAQS_E_ARG, "null MPS tensor");
+    for (size_t e = 0; e < n; ++e) arena[mps_off[i] + e] = cload(psi0->tensors[i], e);
+  }
+  cplx* d_psi0;
+  CUDA_TRY(ctx, dm.alloc(&d_psi0, mps_size));
+  CUDA_TRY(ctx, cudaMemcpy(d_psi0, arena.data(), mps_size * sizeof(cplx), cudaMemcpyHostToDevice));
+  P.psi0 = d_psi0;
+
+  cplx* d_phi;
+  int *d_phi_chi, *d_phi_oc, *d_status, *d_queue, *d_chi_out, *d_wsi;
+  long long* d_rng_pos;
+  double *d_traj_out, *d_flops, *d_uniforms = nullptr;
+  unsigned long long* d_counters;
+  cplx* d_ws;
+  CUDA_TRY(ctx, dm.alloc(&d_phi, (size_t)num_traj * mps_size));
+  CUDA_TRY(ctx, dm.alloc(&d_phi_chi, (size_t)num_traj * (L + 1)));
+  CUDA_TRY(ctx, dm.alloc(&d_phi_oc, num_traj));
+  CUDA_TRY(ctx, dm.alloc(&d_status, num_traj));
+  CUDA_TRY(ctx, dm.alloc(&d_queue, nqueue));
+  CUDA_TRY(ctx, dm.alloc(&d_chi_out, (size_t)num_traj * ncols));
+  CUDA_TRY(ctx, dm.alloc(&d_rng_pos, num_traj));
+  CUDA_TRY(ctx, dm.alloc(&d_traj_out, (size_t)num_traj * std::max(n_obs, 1) * ncols));
+  CUDA_TRY(ctx, dm.alloc(&d_flops, slots));
+  CUDA_TRY(ctx, dm.alloc(&d_counters, (size_t)slots * 8));
+  CUDA_TRY(ctx, dm.alloc(&d_ws, (size_t)slots * lay.total));
+  CUDA_TRY(ctx, dm.alloc(&d_wsi, (size_t)slots * lay.itotal));
+  CUDA_TRY(ctx, cudaMemset(d_status, 0, num_traj * sizeof(int)));
+  CUDA_TRY(ctx, cudaMemset(d_queue, 0, nqueue * sizeof(int)));
+  CUDA_TRY(ctx, cudaMemset(d_rng_pos, 0, num_traj * sizeof(long long)));
+  CUDA_TRY(ctx, cudaMemset(d_traj_out, 0, (size_t)num_traj * std::max(n_obs, 1) * ncols * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(d_chi_out, 0, (size_t)num_traj * ncols * sizeof(int)));
+  CUDA_TRY(ctx, cudaMemset(d_flops, 0, slots * sizeof(double)));
+  CUDA_TRY(ctx, cudaMemset(d_counters, 0, (size_t)slots * 8 * sizeof(unsigned long long)));
+  if (rng->mode == YAQS_RNG_INJECTED) {
+    CUDA_TRY(ctx, dm.alloc(&d_uniforms, (size_t)num_traj * rng->stride));
+    CUDA_TRY(ctx, cudaMemcpy(d_uniforms, rng->uniforms, (size_t)num_traj * rng->stride * sizeof(double),
+                             cudaMemcpyHostToDevice));
+  }
+  P.phi = d_phi;
+  P.phi_chi = d_phi_chi;
+  P.phi_oc = d_phi_oc;
+  P.status = d_status;
+  P.queue = d_queue;
+  P.chi_out = d_chi_out;
+  P.rng_pos = d_rng_pos;
+  P.traj_out = d_traj_out;
+  P.flops = d_flops;
+  P.counters = d_counters;
+  P.ws = d_ws;
+  P.wsi = d_wsi;
+  P.uniforms = d_uniforms;
+
+  run->num_traj = num_traj;
+  run->d_traj_out = d_traj_out;
+  run->d_chi_out = d_chi_out;
+  run->d_status = d_status;
+  run->d_counters = d_counters;
+  run->d_flops = d_flops;
+  const char* pe = getenv("YAQS_PROFILE");
+  if (pe && pe[0] == '1') {
+    CUDA_TRY(ctx, dm.alloc(&run->d_prof, (size_t)slots * PROF_N));
+    CUDA_TRY(ctx, cudaMemset(run->d_prof, 0, (size_t)slots * PROF_N * sizeof(unsigned long long)));
+    CUDA_TRY(ctx, cudaMemcpyToSymbol(g_prof, &run->d_prof, sizeof(run->d_prof)));
+  }
+  CUDA_TRY(ctx, cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking));
+  CUDA_TRY(ctx, cudaEventCreate(&run->e0));
+  CUDA_TRY(ctx, cudaEventCreate(&run->e1));
+  return YAQS_OK;
+}
 
 extern "C" {
 
@@ -570,53 +770,14 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
       return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO too wide for the sparse MPO apply");
 
   // ---- noise and observables ----
-  std::vector<DevProc> hp(std::max(nprocs, 1));
+  std::vector<DevProc> hp;
+  std::vector<DevObs> ho;
   bool all_zero = true;
-  for (int k = 0; k < nprocs; ++k) {
-    const yaqs_noise_proc& q = noise->procs[k];
-    DevProc& d = hp[k];
-    memset(&d, 0, sizeof(d));
-    d.nsites = q.nsites;
-    d.s0 = q.site[0];
-    d.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
-    if (q.nsites < 1 || q.nsites > 2 || d.s0 < 0 || d.s1 >= L || (q.nsites == 2 && d.s1 != d.s0 + 1))
-      return set_err(ctx, q.nsites == 2 ? YAQS_E_UNSUPPORTED : YAQS_E_ARG,
-                     "noise processes must be 1-site or adjacent 2-site with sites in range");
-    d.gamma = q.strength;
-    d.pauli_name = q.pauli_name;
-    d.pauli_proc = q.pauli_proc;
-    if (q.strength != 0.0) all_zero = false;
-    const int dd = q.nsites == 1 ? 2 : 4;
-    hcd M[16], LdL[16], e1[16], e2[16];
-    for (int e = 0; e < dd * dd; ++e) M[e] = cload(q.matrix, e);
-    for (int i = 0; i < dd; ++i)
-      for (int j = 0; j < dd; ++j) {
-        hcd s = 0;
-        for (int kk = 0; kk < dd; ++kk) s += std::conj(M[kk + dd * i]) * M[kk + dd * j];
-        LdL[i + dd * j] = s;
-      }
-    herm_expm(dd, LdL, -0.5 * (cfg->dt / 2) * q.strength, e1);
-    herm_expm(dd, LdL, -0.5 * cfg->dt * q.strength, e2);
-    for (int e = 0; e < dd * dd; ++e) {
-      d.mat[e] = make_double2(M[e].real(), M[e].imag());
-      d.diss_half[e] = make_double2(e1[e].real(), e1[e].imag());
-      d.diss_full[e] = make_double2(e2[e].real(), e2[e].imag());
-    }
-  }
-  std::vector<DevObs> ho(std::max(n_obs, 1));
-  for (int k = 0; k < n_obs; ++k) {
-    const yaqs_obs_desc& o = obs[k];
-    DevObs& d = ho[k];
-    memset(&d, 0, sizeof(d));
-    d.kind = o.kind;
-    d.s0 = o.site[0];
-    d.s1 = o.site[1];
-    bool ok = (o.kind == YAQS_OBS_LOCAL1 && d.s0 >= 0 && d.s0 < L) ||
-              (o.kind == YAQS_OBS_LOCAL2 && d.s0 >= 0 && d.s0 + 1 < L && d.s1 == d.s0 + 1) ||
-              (o.kind == YAQS_OBS_ENTROPY && d.s0 >= 0 && d.s0 + 1 < L);
-    if (!ok) return set_err(ctx, YAQS_E_ARG, "bad observable descriptor");
-    const int dd = o.kind == YAQS_OBS_LOCAL2 ? 4 : 2;
-    for (int e = 0; e < dd * dd; ++e) d.mat[e] = make_double2(o.matrix[2 * e], o.matrix[2 * e + 1]);
+  {
+    int st = pack_noise(ctx, noise, nprocs, L, cfg->dt, hp, all_zero);
+    if (st != YAQS_OK) return st;
+    st = pack_obs(ctx, obs, n_obs, L, ho);
+    if (st != YAQS_OK) return st;
   }
 
   // ---- slots and memory admission ----
@@ -669,26 +830,14 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   P.kry_n = kry_n;
   P.lay = lay;
 
-  int *d_cap, *d_w, *d_chi0;
-  long long *d_mps_off, *d_env_off;
-  CUDA_TRY(ctx, dm.alloc(&d_cap, L + 1));
-  CUDA_TRY(ctx, dm.alloc(&d_w, L + 1));
-  CUDA_TRY(ctx, dm.alloc(&d_chi0, L + 1));
-  CUDA_TRY(ctx, dm.alloc(&d_mps_off, L));
-  CUDA_TRY(ctx, dm.alloc(&d_env_off, L + 1));
-  CUDA_TRY(ctx, cudaMemcpy(d_cap, cap.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(d_w, w.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(d_chi0, chi0.data(), (L + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(d_mps_off, mps_off.data(), L * sizeof(long long), cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(d_env_off, env_off.data(), (L + 1) * sizeof(long long), cudaMemcpyHostToDevice));
-  P.cap = d_cap;
-  P.w = d_w;
-  P.chi0 = d_chi0;
-  P.mps_off = d_mps_off;
-  P.env_off = d_env_off;
-
+  run->slots = slots;
+  run->smem = smem;
+  run->n_obs = n_obs;
+  run->ncols = ncols;
+  int st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, cfg->n_times);
+  if (st != YAQS_OK) return st;
   std::vector<WMat> views;
-  int st = upload_wmats(ctx, dm, all, views);
+  st = upload_wmats(ctx, dm, all, views);
   if (st != YAQS_OK) return st;
   WMat* d_views;
   CUDA_TRY(ctx, dm.alloc(&d_views, views.size()));
@@ -698,92 +847,8 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   P.wm_envL = d_views + L + (L - 1);
   P.wm_envR = d_views + L + (L - 1) + L;
 
-  DevProc* d_procs;
-  DevObs* d_obs;
-  CUDA_TRY(ctx, dm.alloc(&d_procs, hp.size()));
-  CUDA_TRY(ctx, dm.alloc(&d_obs, ho.size()));
-  CUDA_TRY(ctx, cudaMemcpy(d_procs, hp.data(), hp.size() * sizeof(DevProc), cudaMemcpyHostToDevice));
-  CUDA_TRY(ctx, cudaMemcpy(d_obs, ho.data(), ho.size() * sizeof(DevObs), cudaMemcpyHostToDevice));
-  P.procs = d_procs;
-  P.obs = d_obs;
-
-  // initial state arena (compact tensors at the site slots)
-  std::vector<hcd> arena((size_t)mps_size, 0.0);
-  for (int i = 0; i < L; ++i) {
-    const size_t n = (size_t)chi0[i] * 2 * chi0[i + 1];
-    if (!psi0->tensors[i]) return set_err(ctx, YAQS_E_ARG, "null MPS tensor");
-    for (size_t e = 0; e < n; ++e) arena[mps_off[i] + e] = cload(psi0->tensors[i], e);
-  }
-  cplx* d_psi0;
-  CUDA_TRY(ctx, dm.alloc(&d_psi0, mps_size));
-  CUDA_TRY(ctx, cudaMemcpy(d_psi0, arena.data(), mps_size * sizeof(cplx), cudaMemcpyHostToDevice));
-  P.psi0 = d_psi0;
-
-  cplx* d_phi;
-  int *d_phi_chi, *d_phi_oc, *d_status, *d_queue, *d_chi_out, *d_wsi;
-  long long* d_rng_pos;
-  double *d_traj_out, *d_flops, *d_uniforms = nullptr;
-  unsigned long long* d_counters;
-  cplx* d_ws;
-  CUDA_TRY(ctx, dm.alloc(&d_phi, (size_t)num_traj * mps_size));
-  CUDA_TRY(ctx, dm.alloc(&d_phi_chi, (size_t)num_traj * (L + 1)));
-  CUDA_TRY(ctx, dm.alloc(&d_phi_oc, num_traj));
-  CUDA_TRY(ctx, dm.alloc(&d_status, num_traj));
-  CUDA_TRY(ctx, dm.alloc(&d_queue, cfg->n_times));
-  CUDA_TRY(ctx, dm.alloc(&d_chi_out, (size_t)num_traj * ncols));
-  CUDA_TRY(ctx, dm.alloc(&d_rng_pos, num_traj));
-  CUDA_TRY(ctx, dm.alloc(&d_traj_out, (size_t)num_traj * std::max(n_obs, 1) * ncols));
-  CUDA_TRY(ctx, dm.alloc(&d_flops, slots));
-  CUDA_TRY(ctx, dm.alloc(&d_counters, (size_t)slots * 8));
-  CUDA_TRY(ctx, dm.alloc(&d_ws, (size_t)slots * lay.total));
-  CUDA_TRY(ctx, dm.alloc(&d_wsi, (size_t)slots * lay.itotal));
-  CUDA_TRY(ctx, cudaMemset(d_status, 0, num_traj * sizeof(int)));
-  CUDA_TRY(ctx, cudaMemset(d_queue, 0, cfg->n_times * sizeof(int)));
-  CUDA_TRY(ctx, cudaMemset(d_rng_pos, 0, num_traj * sizeof(long long)));
-  CUDA_TRY(ctx, cudaMemset(d_traj_out, 0, (size_t)num_traj * std::max(n_obs, 1) * ncols * sizeof(double)));
-  CUDA_TRY(ctx, cudaMemset(d_chi_out, 0, (size_t)num_traj * ncols * sizeof(int)));
-  CUDA_TRY(ctx, cudaMemset(d_flops, 0, slots * sizeof(double)));
-  CUDA_TRY(ctx, cudaMemset(d_counters, 0, (size_t)slots * 8 * sizeof(unsigned long long)));
-  if (rng->mode == YAQS_RNG_INJECTED) {
-    CUDA_TRY(ctx, dm.alloc(&d_uniforms, (size_t)num_traj * rng->stride));
-    CUDA_TRY(ctx, cudaMemcpy(d_uniforms, rng->uniforms, (size_t)num_traj * rng->stride * sizeof(double),
-                             cudaMemcpyHostToDevice));
-  }
-  P.phi = d_phi;
-  P.phi_chi = d_phi_chi;
-  P.phi_oc = d_phi_oc;
-  P.status = d_status;
-  P.queue = d_queue;
-  P.chi_out = d_chi_out;
-  P.rng_pos = d_rng_pos;
-  P.traj_out = d_traj_out;
-  P.flops = d_flops;
-  P.counters = d_counters;
-  P.ws = d_ws;
-  P.wsi = d_wsi;
-  P.uniforms = d_uniforms;
-
-  run->slots = slots;
-  run->smem = smem;
-  run->num_traj = num_traj;
-  run->n_obs = n_obs;
-  run->ncols = ncols;
-  run->d_traj_out = d_traj_out;
-  run->d_chi_out = d_chi_out;
-  run->d_status = d_status;
-  run->d_counters = d_counters;
-  run->d_flops = d_flops;
   run->launches.push_back(0);
   for (int j = (cfg->order == 2 ? 2 : 1); j < cfg->n_times; ++j) run->launches.push_back(j);
-  const char* pe = getenv("YAQS_PROFILE");
-  if (pe && pe[0] == '1') {
-    CUDA_TRY(ctx, dm.alloc(&run->d_prof, (size_t)slots * PROF_N));
-    CUDA_TRY(ctx, cudaMemset(run->d_prof, 0, (size_t)slots * PROF_N * sizeof(unsigned long long)));
-    CUDA_TRY(ctx, cudaMemcpyToSymbol(g_prof, &run->d_prof, sizeof(run->d_prof)));
-  }
-  CUDA_TRY(ctx, cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking));
-  CUDA_TRY(ctx, cudaEventCreate(&run->e0));
-  CUDA_TRY(ctx, cudaEventCreate(&run->e1));
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = guard.release();
   return YAQS_OK;
@@ -844,7 +909,10 @@ int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms) {
   CUDA_TRY(ctx, cudaEventRecord(run->e0, run->stream));
   for (int k = 0; k < n; ++k) {
     const int j = run->launches[run->next++];
-    tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, j);
+    if (run->digital)
+      digital_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, run->D, j);
+    else
+      tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, j);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return set_err(ctx, YAQS_E_CUDA, std::string("launch: ") + cudaGetErrorString(le));
   }
@@ -902,6 +970,274 @@ int yaqs_analog_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_des
                     double* traj_out, double* mean_out, int32_t* maxchi_out, yaqs_run_stats* stats) {
   yaqs_run* run = nullptr;
   int st = yaqs_analog_begin(ctx, psi0, H, noise, obs, n_obs, cfg, rng, &run);
+  if (st != YAQS_OK) return st;
+  st = yaqs_analog_advance(run, yaqs_analog_remaining(run), nullptr);
+  if (st != YAQS_OK) {
+    yaqs_analog_finish(run, nullptr, nullptr, nullptr, nullptr);
+    return st;
+  }
+  return yaqs_analog_finish(run, traj_out, mean_out, maxchi_out, stats);
+}
+
+// ---- digital TJM ----
+namespace {
+struct HostCircuit {
+  std::vector<std::vector<int>> layers;  // gate indices per layer
+  bool sample_at_start = false;
+  std::vector<char> sample_after;  // per layer
+  int n_samples = 1;
+};
+
+// process_circuit (DigitalTJM.jl:86-145) and _sample_plan (:159-168): gates
+// are packed greedily in program order, a new layer starting whenever a gate
+// touches a site the current layer already uses; a barrier closes the current
+// layer, and a sampling barrier requests a measurement after the layers
+// completed so far (before the first layer when none is).
+int plan_circuit(yaqs_ctx* ctx, const yaqs_gate_desc* gates, int n, int L, HostCircuit& c) {
+  std::vector<int> cur;
+  std::vector<char> busy(L, 0);
+  std::vector<std::pair<int, bool>> barriers;
+  for (int g = 0; g < n; ++g) {
+    const yaqs_gate_desc& q = gates[g];
+    if (q.kind == YAQS_GATE_BARRIER) {
+      if (!cur.empty()) {
+        c.layers.push_back(cur);
+        cur.clear();
+        std::fill(busy.begin(), busy.end(), 0);
+      }
+      barriers.push_back({(int)c.layers.size(), q.sample != 0});
+      continue;
+    }
+    const int a = q.site[0], b = q.kind == YAQS_GATE_2Q ? q.site[1] : q.site[0];
+    if ((q.kind != YAQS_GATE_1Q && q.kind != YAQS_GATE_2Q) || a < 0 || a >= L || b < 0 || b >= L ||
+        (q.kind == YAQS_GATE_2Q && a == b))
+      return set_err(ctx, YAQS_E_ARG, "bad gate descriptor (gate " + std::to_string(g) + ")");
+    if (busy[a] || busy[b]) {
+      c.layers.push_back(cur);
+      cur.clear();
+      std::fill(busy.begin(), busy.end(), 0);
+    }
+    cur.push_back(g);
+    busy[a] = busy[b] = 1;
+  }
+  if (!cur.empty()) c.layers.push_back(cur);
+  c.sample_after.assign(c.layers.size(), 0);
+  for (auto& bs : barriers) {
+    if (!bs.second) continue;
+    if (bs.first == 0)
+      c.sample_at_start = true;
+    else
+      c.sample_after[bs.first - 1] = 1;
+  }
+  int ns = c.sample_at_start ? 1 : 0;
+  for (char x : c.sample_after) ns += x ? 1 : 0;
+  c.n_samples = ns == 0 ? 1 : ns;
+  return YAQS_OK;
+}
+
+int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
+                  const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                  const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out) {
+  if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!psi0 || !cfg || !rng || (n_obs > 0 && !obs) || n_gates < 0 || (n_gates > 0 && !gates))
+    return set_err(ctx, YAQS_E_ARG, "null descriptor");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int L = psi0->L;
+  if (L < 2 || L > MAX_L) return set_err(ctx, YAQS_E_ARG, "need 2 <= L <= 256");
+  if (!psi0->chi || !psi0->tensors) return set_err(ctx, YAQS_E_ARG, "null tensor arrays");
+  if (psi0->chi[0] != 1 || psi0->chi[L] != 1) return set_err(ctx, YAQS_E_ARG, "boundary bond dimensions must be 1");
+  for (int b = 0; b <= L; ++b)
+    if (psi0->chi[b] < 1) return set_err(ctx, YAQS_E_ARG, "bond dimension < 1");
+  if (cfg->num_traj < 1 || cfg->max_bond_dim < 1) return set_err(ctx, YAQS_E_ARG, "bad config (num_traj, max_bond_dim)");
+  if (cfg->local_method != YAQS_METHOD_TEBD || cfg->long_range_method != YAQS_METHOD_TEBD)
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "only TEBD gate application is served by this build");
+  if (cfg->precision != YAQS_PREC_FP64)
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "only the ComplexF64 form is served by this build");
+  if (n_obs < 0 || n_obs > MAX_OBS) return set_err(ctx, YAQS_E_ARG, "n_obs out of range");
+  if (rng->mode != YAQS_RNG_PHILOX && rng->mode != YAQS_RNG_INJECTED) return set_err(ctx, YAQS_E_ARG, "bad rng mode");
+  if (rng->mode == YAQS_RNG_INJECTED && (!rng->uniforms || rng->stride < 1))
+    return set_err(ctx, YAQS_E_ARG, "injected uniforms need a buffer and stride >= 1");
+  const int nprocs = (noise && noise->present) ? noise->n : 0;
+  if (nprocs < 0 || nprocs > MAX_PROCS || (nprocs > 0 && !noise->procs)) return set_err(ctx, YAQS_E_ARG, "bad noise descriptor");
+  HostCircuit C;
+  int st = plan_circuit(ctx, gates, n_gates, L, C);
+  if (st != YAQS_OK) return st;
+
+  // ---- capacities and layout (no environments or Krylov basis) ----
+  std::vector<int> cap(L + 1), chi0(psi0->chi, psi0->chi + L + 1), w(L + 1, 1);
+  for (int b = 0; b <= L; ++b) {
+    long long sz = 1;
+    int e = std::min(b, L - b);
+    for (int k = 0; k < e && sz < (1 << 20); ++k) sz *= 2;
+    cap[b] = (int)std::max<long long>(std::min<long long>(sz, cfg->max_bond_dim), chi0[b]);
+    if (2 * cap[b] > SVD_MAX_COLS) return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
+  }
+  const int capmax = *std::max_element(cap.begin(), cap.end());
+  std::vector<long long> mps_off(L), env_off(L + 1, 0);
+  long long mps_size = 0, kry_n = 0;
+  for (int i = 0; i < L; ++i) {
+    mps_off[i] = mps_size;
+    mps_size += (long long)cap[i] * 2 * cap[i + 1];
+    kry_n = std::max(kry_n, (long long)cap[i] * 2 * cap[i + 1]);
+    if (i + 2 <= L) kry_n = std::max(kry_n, (long long)cap[i] * 4 * cap[i + 2]);
+  }
+  const long long tmp = 4LL * capmax * capmax + 16;
+  WsLayout lay;
+  long long off = 0;
+  auto take = [&](long long n) {
+    long long o = off;
+    off += (n + 1) & ~1LL;
+    return o;
+  };
+  lay.psi = lay.EL = lay.ER = lay.Q = lay.T1 = lay.T2 = take(0);
+  lay.tA = take(tmp);
+  lay.tB = take(tmp);
+  lay.tC = take(tmp);
+  lay.th = take(kry_n);
+  lay.B = take(tmp);
+  lay.X = take(tmp);
+  lay.Yo = take(tmp);
+  lay.Zo = take(tmp);
+  lay.y = take(2 * capmax + 16);
+  lay.dbl = take((SVD_MAX_COLS + MAX_PROCS) / 2 + 8);
+  lay.total = off;
+  long long ioff = 0;
+  lay.i_chi = ioff;
+  ioff += L + 1;
+  lay.i_oc = ioff;
+  ioff += 1;
+  lay.i_ord = ioff;
+  ioff += SVD_MAX_COLS;
+  lay.i_cand = ioff;
+  ioff += MAX_PROCS;
+  lay.itotal = (ioff + 31) & ~31LL;
+
+  // gate noise uses dt = 1 (DigitalTJM.jl:412-413)
+  std::vector<DevProc> hp;
+  std::vector<DevObs> ho;
+  bool all_zero = true;
+  st = pack_noise(ctx, noise, nprocs, L, 1.0, hp, all_zero);
+  if (st != YAQS_OK) return st;
+  st = pack_obs(ctx, obs, n_obs, L, ho);
+  if (st != YAQS_OK) return st;
+
+  // ---- slots and memory admission ----
+  const int num_traj = cfg->num_traj;
+  const int ncols = C.n_samples;
+  const int n_layers = (int)C.layers.size();
+  const size_t smem = sizeof(CtaSmem);
+  CUDA_TRY(ctx, cudaFuncSetAttribute(digital_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, digital_step_kernel, NT, smem));
+  if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
+  size_t free_b = 0, total_b = 0;
+  CUDA_TRY(ctx, cudaMemGetInfo(&free_b, &total_b));
+  const size_t per_traj = (size_t)mps_size * sizeof(cplx) + (L + 2) * sizeof(int) + 64 +
+                          (size_t)n_obs * ncols * sizeof(double) + ncols * sizeof(int);
+  const size_t per_slot = (size_t)lay.total * sizeof(cplx) + lay.itotal * sizeof(int) + 8 * 8 + 8;
+  const size_t fixed = (size_t)mps_size * sizeof(cplx) + (size_t)(n_gates + 1) * sizeof(DevGate) + (64u << 20);
+  const size_t budget = free_b > (size_t)(1u << 30) ? free_b - (size_t)(1u << 30) : 0;
+  if (fixed + (size_t)num_traj * per_traj + per_slot > budget)
+    return set_err(ctx, YAQS_E_OOM, "trajectory states do not fit in device memory");
+  int slots = std::min(num_traj, ctx->sms * per_sm);
+  while (slots > 1 && fixed + (size_t)num_traj * per_traj + (size_t)slots * per_slot > budget) --slots;
+
+  yaqs_run* run = new yaqs_run();
+  std::unique_ptr<yaqs_run> guard(run);
+  run->ctx = ctx;
+  run->digital = 1;
+  DevParams& P = run->P;
+  memset(&P, 0, sizeof(P));
+  P.L = L;
+  P.n_times = n_layers + 1;
+  P.max_bond = cfg->max_bond_dim;
+  P.nobs = n_obs;
+  P.nprocs = nprocs;
+  P.noise_present = (noise && noise->present) ? 1 : 0;
+  P.all_zero = all_zero ? 1 : 0;
+  P.rng_mode = rng->mode;
+  P.num_traj = num_traj;
+  P.traj_offset = cfg->traj_offset;
+  P.ncols = ncols;
+  P.dt = 1.0;
+  P.thr = cfg->truncation_threshold;
+  P.seed = rng->seed;
+  P.stride = rng->stride;
+  P.mps_size = mps_size;
+  P.kry_n = kry_n;
+  P.lay = lay;
+  run->slots = slots;
+  run->smem = smem;
+  run->n_obs = n_obs;
+  run->ncols = ncols;
+  st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, n_layers + 1);
+  if (st != YAQS_OK) return st;
+
+  // ---- gates in layer order ----
+  std::vector<DevGate> hg;
+  std::vector<int> layer_off(1, 0), sample_col(std::max(n_layers, 1), -1);
+  int col = C.sample_at_start ? 1 : 0;
+  for (int l = 0; l < n_layers; ++l) {
+    for (int g : C.layers[l]) {
+      const yaqs_gate_desc& q = gates[g];
+      DevGate d;
+      memset(&d, 0, sizeof(d));
+      d.kind = q.kind;
+      d.a = q.kind == YAQS_GATE_2Q ? std::min(q.site[0], q.site[1]) : q.site[0];
+      d.b = q.kind == YAQS_GATE_2Q ? std::max(q.site[0], q.site[1]) : q.site[0];
+      const int dd = q.kind == YAQS_GATE_2Q ? 4 : 2;
+      for (int e = 0; e < dd * dd; ++e) d.mat[e] = make_double2(q.matrix[2 * e], q.matrix[2 * e + 1]);
+      hg.push_back(d);
+    }
+    layer_off.push_back((int)hg.size());
+    if (C.sample_after[l]) sample_col[l] = col++;
+  }
+  if (hg.empty()) hg.resize(1);
+  DevGate* d_gates;
+  int *d_layer_off, *d_sample_col;
+  CUDA_TRY(ctx, run->dm.alloc(&d_gates, hg.size()));
+  CUDA_TRY(ctx, run->dm.alloc(&d_layer_off, layer_off.size()));
+  CUDA_TRY(ctx, run->dm.alloc(&d_sample_col, sample_col.size()));
+  CUDA_TRY(ctx, cudaMemcpy(d_gates, hg.data(), hg.size() * sizeof(DevGate), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_layer_off, layer_off.data(), layer_off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(d_sample_col, sample_col.data(), sample_col.size() * sizeof(int), cudaMemcpyHostToDevice));
+  DigParams& D = run->D;
+  D.gates = d_gates;
+  D.layer_off = d_layer_off;
+  D.sample_col = d_sample_col;
+  D.n_layers = n_layers;
+  D.sample_at_start = C.sample_at_start ? 1 : 0;
+  D.any_sample = (col > 0) ? 1 : 0;
+  for (int j = 0; j <= n_layers; ++j) run->launches.push_back(j);
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  *out = guard.release();
+  return YAQS_OK;
+}
+}  // namespace
+
+int yaqs_digital_plan(const yaqs_gate_desc* gates, int32_t n_gates, int32_t* n_layers, int32_t* n_samples) {
+  if (n_gates < 0 || (n_gates > 0 && !gates) || !n_layers || !n_samples)
+    return set_err(nullptr, YAQS_E_ARG, "null argument");
+  int L = 1;
+  for (int g = 0; g < n_gates; ++g)
+    if (gates[g].kind != YAQS_GATE_BARRIER)
+      L = std::max(L, std::max(gates[g].site[0], gates[g].kind == YAQS_GATE_2Q ? gates[g].site[1] : 0) + 1);
+  HostCircuit C;
+  int st = plan_circuit(nullptr, gates, n_gates, L, C);
+  if (st != YAQS_OK) return st;
+  *n_layers = (int32_t)C.layers.size();
+  *n_samples = C.n_samples;
+  return YAQS_OK;
+}
+
+int yaqs_digital_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
+                     const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                     const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, double* traj_out, double* mean_out,
+                     int32_t* maxchi_out, yaqs_run_stats* stats) {
+  yaqs_run* run = nullptr;
+  int st = digital_begin(ctx, psi0, gates, n_gates, noise, obs, n_obs, cfg, rng, &run);
   if (st != YAQS_OK) return st;
   st = yaqs_analog_advance(run, yaqs_analog_remaining(run), nullptr);
   if (st != YAQS_OK) {

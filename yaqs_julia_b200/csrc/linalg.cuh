@@ -457,3 +457,15 @@ __device__ __forceinline__ int keep_relative(const double* S, int n, double thr,
   return max(1, min(rank, max_bond));
 }
 
+// apply_local_gate_exact! (DigitalTJM.jl:282-292): absolute, drop while the
+// running sum plus s^2 stays <= thr, no minimum.
+__device__ __forceinline__ int keep_tebd(const double* S, int n, double thr, int max_bond) {
+  double cur = 0.0;
+  int keep = n;
+  for (int k = n; k >= 1; --k) {
+    if (cur + S[k - 1] * S[k - 1] > thr) break;
+    cur += S[k - 1] * S[k - 1];
+    --keep;
+  }
+  return max(1, min(keep, max_bond));
+}

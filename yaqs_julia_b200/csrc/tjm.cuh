@@ -383,7 +383,7 @@ __device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
 }
 
 // SVD split of theta (2l x 2r) into sites i (l,2,keep) and i+1 (keep,2,r).
-// rule 0: TDVP (absolute, min 2); rule 1: relative.  With s_left the
+// rule 0: TDVP (absolute, min 2); 1: relative; 2: TEBD.  With s_left the
 // singular values go left (U S | Vt, Vt orthonormal, Algorithms.jl:701-708),
 // otherwise right (U | S Vt, U orthonormal, Algorithms.jl:656-663).  The
 // scaled factor is computed as a product with theta and is exactly zero for
@@ -394,8 +394,9 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
   SvdWork w = svd_work(c);
   SvdResult res = dev_svd(th, m, n, s_left ? SVD_RIGHT : SVD_LEFT, w, c.sm.la, c.sm.e.r, c.sm.e.u.svd);
   if (threadIdx.x == 0) {
-    int keep = rule == 0 ? keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond)
-                         : keep_relative(w.sig, res.p, c.P.thr, c.P.max_bond);
+    int keep = rule == 0   ? keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond)
+               : rule == 1 ? keep_relative(w.sig, res.p, c.P.thr, c.P.max_bond)
+                           : keep_tebd(w.sig, res.p, c.P.thr, c.P.max_bond);
     c.sm.bcast_i[0] = keep;
     c.cnt[2] += 1;
     c.cnt[5] += res.sweeps;
@@ -521,10 +522,25 @@ __device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const
 // ---------------------------------------------------------------------------
 // Dissipation (Dissipation.jl:37-159)
 // ---------------------------------------------------------------------------
-__device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt) {
+// Processes taken by a noise step: all of them (f1 < 0), or the local noise
+// model of a gate on sites (f1, f2) (create_local_noise_model,
+// DigitalTJM.jl:172-188): 1-site processes on either site and 2-site
+// processes on exactly that pair.
+__device__ __forceinline__ bool proc_on(const DevProc& pr, int f1, int f2) {
+  if (f1 < 0) return true;
+  return pr.nsites == 1 ? (pr.s0 == f1 || pr.s0 == f2) : ((pr.s0 == f1 && pr.s1 == f2) || (pr.s0 == f2 && pr.s1 == f1));
+}
+
+__device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt, int f1 = -1, int f2 = -1) {
   ProfScope prof_scope_(PF_DISS);
   const int L = c.P.L;
-  if (!c.P.noise_present || c.P.all_zero) {
+  bool all_zero = c.P.all_zero != 0;
+  if (f1 >= 0) {
+    all_zero = true;
+    for (int k = 0; k < c.P.nprocs; ++k)
+      if (proc_on(c.P.procs[k], f1, f2) && c.P.procs[k].gamma != 0.0) all_zero = false;
+  }
+  if (!c.P.noise_present || all_zero) {
     for (int i = L - 1; i >= 1 && !c.sm.fail; --i) shift_oc(c, s, i - 1);
     return;
   }
@@ -532,7 +548,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt)
   for (int i = L - 1; i >= 0 && !c.sm.fail; --i) {
     for (int k = 0; k < c.P.nprocs; ++k) {
       const DevProc& pr = c.P.procs[k];
-      if (pr.nsites == 1 && pr.s0 == i) {
+      if (pr.nsites == 1 && pr.s0 == i && proc_on(pr, f1, f2)) {
         cplx* A = site_ptr(c, s, i);
         const long long n = (long long)s.chi[i] * 2 * s.chi[i + 1];
         if (pr.pauli_name) {
@@ -546,7 +562,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt)
     if (i > 0) {
       for (int k = 0; k < c.P.nprocs && !c.sm.fail; ++k) {
         const DevProc& pr = c.P.procs[k];
-        if (pr.nsites == 2 && pr.s1 == i) {
+        if (pr.nsites == 2 && pr.s1 == i && proc_on(pr, f1, f2)) {
           if (pr.pauli_name) {
             cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * dt * pr.gamma));
             __syncthreads();
@@ -566,12 +582,14 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt)
 // ---------------------------------------------------------------------------
 // Stochastic process (StochasticProcess.jl:219-330)
 // ---------------------------------------------------------------------------
-__device__ void stochastic_process(Ctx& c, const DState& s, double dt) {
+__device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = -1, int f2 = -1) {
   ProfScope prof_scope_(PF_STOCH);
   const int L = c.P.L;
   const double dp = 1.0 - scalar_product(c, s);
   bool jump = false;
-  if (c.P.nprocs > 0) {
+  int ntake = 0;
+  for (int k = 0; k < c.P.nprocs; ++k) ntake += proc_on(c.P.procs[k], f1, f2) ? 1 : 0;
+  if (ntake > 0) {
     double u1 = draw_uniform(c);
     jump = u1 < dp;
   }
@@ -588,7 +606,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt) {
     shift_oc(c, s, site);
     for (int k = 0; k < c.P.nprocs; ++k) {
       const DevProc& pr = c.P.procs[k];
-      if (pr.nsites == 1 && pr.s0 == site) {
+      if (pr.nsites == 1 && pr.s0 == site && proc_on(pr, f1, f2)) {
         double nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1],
                                 pr.pauli_proc ? nullptr : pr.mat);
         if (threadIdx.x == 0) {
@@ -601,7 +619,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt) {
     if (site < L - 1) {
       for (int k = 0; k < c.P.nprocs; ++k) {
         const DevProc& pr = c.P.procs[k];
-        if (pr.nsites == 2 && pr.s0 == site) {
+        if (pr.nsites == 2 && pr.s0 == site && proc_on(pr, f1, f2)) {
           double nr;
           if (pr.pauli_proc) {
             nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1], nullptr);
