@@ -18,6 +18,14 @@ than L2.  Multi-GPU runs are independent replicas (one process per GPU,
 launched by torchrun); the value is the sum of every rank's trajectory-steps
 over the slowest rank's time.
 
+--workload digital times the digital TJM instead: a Trotterised Ising
+circuit on L=40 qubits (per Trotter layer RZZ(2 J dt) on odd then even
+bonds, RX(2 g dt) on every qubit, a SAMPLE_OBSERVABLES barrier; J = g = 1,
+dt = 0.05, 60 layers), Pauli X/Y/Z noise 0.01 per qubit after every 2-qubit
+gate, TEBD with chi_max = 128 and threshold 1e-9, 512 trajectories, <Z_i> on
+every qubit after every layer.  A step is one Trotter layer of every
+trajectory (three launches of the processed circuit).
+
 --impl reference times the CPU restatement of the reference algorithm
 (the reference itself is Julia, not runnable here) on all host cores, on
 bounded samples of the same workload.
@@ -56,6 +64,30 @@ def workload(L, chi, n_times, num_traj, start):
     nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
     psi = api.random_mps(L, chi, seed=1) if start == "sat" else api.MPS(L, state="Neel")
     return psi, H, cfg, nm
+
+
+DIG_METRIC = "digital TJM trajectory-layers/s (L=40 Ising Trotter circuit, chi=128, 512 trajectories)"
+DIG_UNIT = "trajectory-layers/s"
+DIG_SEED = 0xC0FFEE03
+DIG_DEPTH = 60
+
+
+def digital_workload(L, depth, num_traj, chi=128):
+    J = g = 1.0
+    dt = 0.05
+    c = api.DigitalCircuit(L)
+    for _ in range(depth):
+        for i in list(range(1, L, 2)) + list(range(2, L, 2)):
+            c.add_gate(api.Rzz(2 * J * dt), [i, i + 1])
+        for i in range(1, L + 1):
+            c.add_gate(api.Rx(2 * g * dt), [i])
+        c.add_gate(api.Barrier(), [])
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.01} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_y", "pauli_z")], L)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=1.0, num_traj=num_traj, max_bond_dim=chi,
+                                  truncation_threshold=1e-9)
+    return api.MPS(L), c, cfg, nm
 
 
 class ClockSampler:
@@ -165,9 +197,38 @@ def cpu_sample(L, chi, start):
     return steps / dt, cores, f"{cores} trajectories x 2 time indices (t=0..0.1) of the same workload, {dt:.1f} s"
 
 
+def cpu_sample_digital(L, depth):
+    """Oracle on all host cores: 2 full-circuit trajectories per core.
+    Returns (trajectory-layers/s, cores, sample text)."""
+    from oracle import oracle as O
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    psi, c, cfg, nm = digital_workload(L, depth, 2 * cores)
+    d = api.CircuitDescriptors(psi, c, cfg, nm, seed=DIG_SEED)
+    t0 = time.perf_counter()
+    O.digital_run(d, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return 2 * cores * depth / dt, cores, f"{2 * cores} trajectories x {depth} layers of the same circuit, {dt:.1f} s"
+
+
 def run_reference(args):
     ws, rank, local, dist = dist_setup()
     if rank != 0:
+        return
+    if args.workload == "digital":
+        vals = []
+        for k in range(args.warmup + args.steps):
+            v, cores, sample = cpu_sample_digital(40, DIG_DEPTH)
+            if k >= args.warmup:
+                vals.append(v)
+        value = float(np.mean(vals))
+        line = {"impl": "reference", "metric": DIG_METRIC, "value": value, "unit": DIG_UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "config": {"workload": "digital TJM, L=40 Ising Trotter circuit, 60 layers, chi=128"},
+                "cpu_baseline": {"value": value, "unit": DIG_UNIT, "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": DIG_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "reference Julia (Yaqs.jl) cannot run here; CPU restatement (oracle/tjm_oracle.cpp)"}
+        print(json.dumps(line), flush=True)
         return
     vals = []
     for k in range(args.warmup + args.steps):
@@ -203,6 +264,81 @@ def C_sizeof(desc):
     return C.sizeof(desc.noise) + C.sizeof(desc.obs) + C.sizeof(desc.cfg) + C.sizeof(desc.rng)
 
 
+def run_digital(args):
+    """The digital TJM workload: W untimed Trotter layers, then the timed ones."""
+    ws, rank, local, dist = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from yaqs_julia_b200 import _lib
+    ctx = _lib.Context(local)
+    L, nt, depth = 40, args.traj or 512, DIG_DEPTH
+    K = args.steps if args.steps_given else depth - args.warmup
+    if args.warmup + K > depth:
+        raise SystemExit(f"--warmup + --steps must be <= {depth}")
+    psi, c, cfg, nm = digital_workload(L, depth, nt)
+    n_layers, n_samples = api.digital_plan(c)
+    per = n_layers // depth
+    assert per * depth == n_layers and n_samples == depth
+    desc = api.CircuitDescriptors(psi, c, cfg, nm, seed=DIG_SEED, traj_offset=rank * nt)
+    sess = api.Session(desc, ctx)
+    sess.advance(1 + per * args.warmup)
+    st0 = sess.stats()
+    clocks = ClockSampler(local)
+    barrier_sync(dist)
+    clocks.start()
+    dev_ms = sess.advance(per * K)
+    barrier_sync(dist)
+    ck = clocks.stop()
+    st1 = sess.stats()
+    res = sess.finish()
+    t_max = reduce_max(dist, dev_ms / 1e3)
+    value = reduce_sum(dist, nt * K) / t_max
+    import ctypes as C
+    pk = C.c_double(0.0)
+    ctx.check(ctx._lib.yaqs_fp64_peak(ctx.handle, C.byref(pk)))
+    achieved = (st1["flops"] - st0["flops"]) / (dev_ms / 1e3) / 1e12
+    barrier_sync(dist)
+    t0 = time.perf_counter()
+    e2e_psi = digital_workload(L, depth, nt)
+    e2e_desc = api.CircuitDescriptors(*e2e_psi, seed=DIG_SEED, traj_offset=rank * nt)
+    api.run_circuit_descriptors(e2e_desc, ctx)
+    barrier_sync(dist)
+    e2e_s = reduce_max(dist, time.perf_counter() - t0)
+    e2e_value = reduce_sum(dist, nt * depth) / e2e_s
+    h2d = (sum(t.nbytes for t in e2e_psi[0].tensors) + 4 * (L + 1) + C.sizeof(e2e_desc.gates) +
+           C_sizeof(e2e_desc))
+    d2h = nt * L * depth * 8 + L * depth * 8 + nt * depth * 4 + nt * 4
+    cpu = None
+    if rank == 0 and not args.no_cpu and ws == 1:
+        v, cores, sample = cpu_sample_digital(L, depth)
+        cpu = {"value": v, "unit": DIG_UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        line = {"metric": DIG_METRIC, "value": value, "unit": DIG_UNIT, "n_gpus": ws, "steps": K,
+                "warmup": args.warmup, "ms_per_step": dev_ms / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "config": {"workload": f"digital TJM, L={L} Ising Trotter circuit (RZZ odd/even, RX all; J=g=1, "
+                                       f"dt=0.05), {depth} layers, Pauli XYZ noise 0.01 after every 2-qubit gate, "
+                                       f"TEBD chi_max=128 thr=1e-9, {nt} trajectories per GPU",
+                           "L": L, "chi": 128, "num_traj": nt, "layers": depth, "parallelism": f"replicas x{ws}",
+                           "l2": "working set below L2 (bond dimensions stay small); every layer rereads the "
+                                 "trajectory states, no flush"},
+                "gpu_launches": per * K,
+                "roofline": {"bound": "fp64", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
+                             "frac": achieved / pk.value if pk.value else None, "traffic": None,
+                             "kernel": "digital_step_kernel",
+                             "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run",
+                             "achieved_counts": "nominal TEBD work: theta merge GEMM + 4x4 gate + SVD as "
+                                                "4 m n min(m,n) complex MACs (8 flops each)"},
+                "e2e": {"value": e2e_value, "unit": DIG_UNIT, "h2d_bytes_per_step": h2d / depth,
+                        "d2h_bytes_per_step": d2h / depth, "seconds": e2e_s},
+                "cpu_baseline": cpu, "clocks": ck,
+                "stats": {"jumps": res.stats["jumps"], "svds": res.stats["svds"],
+                          "max_bond": int(res.max_bond.max())}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def run_ours(args):
     ws, rank, local, dist = dist_setup()
     import torch
@@ -235,8 +371,10 @@ def run_ours(args):
     pk = C.c_double(0.0)
     ctx.check(ctx._lib.yaqs_fp64_peak(ctx.handle, C.byref(pk)))
     achieved = flops_timed / (dev_ms / 1e3) / 1e12
-    # end to end: the public C-ABI call on host buffers, K time indices
-    e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm = workload(L, chi, args.steps + 1, nt, args.start)
+    # end to end: the public C-ABI call on host buffers, a complete run of 2K
+    # time indices from t = 0 (its first index costs one sweep, the others two)
+    e2e_steps = 2 * args.steps
+    e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm = workload(L, chi, e2e_steps + 1, nt, args.start)
     barrier_sync(dist)
     t0 = time.perf_counter()
     e2e_desc = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt)
@@ -244,7 +382,7 @@ def run_ours(args):
     barrier_sync(dist)
     e2e_s = reduce_max(dist, time.perf_counter() - t0)
     h2d, d2h = desc_bytes(e2e_desc, e2e_desc.n_obs, e2e_desc.n_out, nt, L)
-    e2e_value = reduce_sum(dist, nt * args.steps) / e2e_s
+    e2e_value = reduce_sum(dist, nt * e2e_steps) / e2e_s
     cpu = None
     if rank == 0 and not args.no_cpu and ws == 1:
         v, cores, sample = cpu_sample(L, chi, args.start)
@@ -267,8 +405,8 @@ def run_ours(args):
                              "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run; "
                                             "MEASURED_PEAKS.json has no FP64 entry",
                              "achieved_counts": "H_eff product flops only (8 flops per complex MAC)"},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-                        "d2h_bytes_per_step": d2h / args.steps, "seconds": e2e_s},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                        "d2h_bytes_per_step": d2h / e2e_steps, "seconds": e2e_s, "steps": e2e_steps},
                 "cpu_baseline": cpu, "clocks": ck,
                 "stats": {"matvecs_timed": matvecs_timed, "flops_timed": flops_timed,
                           "jumps": res.stats["jumps"], "svd_sweeps": res.stats["svd_sweeps"],
@@ -284,10 +422,11 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--workload", default="analog", choices=["analog", "digital"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--traj", type=int, default=1024)
+    ap.add_argument("--traj", type=int, default=None)
     ap.add_argument("--chi", type=int, default=64)
     ap.add_argument("--L", type=int, default=30)
     ap.add_argument("--start", default="sat", choices=["sat", "neel"])
@@ -295,12 +434,19 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="enable the engine's per-phase device timers and report them (not for timing runs)")
     args = ap.parse_args()
+    args.steps_given = args.steps is not None
+    if args.steps is None:
+        args.steps = 2
+    if args.traj is None and args.workload == "analog":
+        args.traj = 1024
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     if args.profile:
         os.environ["YAQS_PROFILE"] = "1"
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "digital":
+        run_digital(args)
     else:
         run_ours(args)
 

@@ -274,6 +274,17 @@ int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out,
  */
 int yaqs_analog_profile(yaqs_run* run, double* cycles);
 
+/*
+ * A digital run in steps: as yaqs_digital_run, but returns a run handle
+ * that yaqs_analog_advance / _remaining / _stats / _profile / _finish
+ * drive.  One advance step is one launch: the first prepares and normalises
+ * every trajectory (and takes the start sample), each further one applies
+ * one layer of the processed circuit (DigitalTJM.jl:380-430).
+ */
+int yaqs_digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
+                       const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                       const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out);
+
 #ifdef __cplusplus
 }
 #endif

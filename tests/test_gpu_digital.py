@@ -147,3 +147,21 @@ def test_library_plan_matches_host_plan():
     c = _brickwork(6, 3, ring=True)
     layers, _ = api.process_circuit(c)
     assert api.digital_plan(c) == (len(layers), api.sample_plan(c)[2])
+
+
+def test_session_steps_match_one_call(oracle):
+    """yaqs_digital_begin + advance per layer gives the one-call result."""
+    L = 6
+    nm = api.NoiseModel([{"name": "pauli_y", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    c = _brickwork(L, 3, seed=11)
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=5, max_bond_dim=16)
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, seed=21)
+    one = api.run_circuit_descriptors(d)
+    sess = api.Session(d)
+    n_layers, _ = api.digital_plan(c)
+    assert sess.remaining == n_layers + 1
+    while sess.remaining:
+        sess.advance(2)
+    res = sess.finish()
+    assert np.array_equal(res.trajectories, one.trajectories)
+    assert res.stats["flops"] > 0

@@ -47,6 +47,8 @@ def lib():
         L.yaqs_digital_run.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),
                                        P(A.ObsDesc), C.c_int32, P(A.CircuitConfig), P(A.RngDesc), A.DPTR, A.DPTR,
                                        P(C.c_int32), P(A.RunStats)]
+        L.yaqs_digital_begin.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),
+                                         P(A.ObsDesc), C.c_int32, P(A.CircuitConfig), P(A.RngDesc), P(C.c_void_p)]
         L.yaqs_fp64_peak.argtypes = [C.c_void_p, P(C.c_double)]
         L.yaqs_batched_svd_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4 + [
             C.c_void_p]

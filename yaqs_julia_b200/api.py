@@ -651,19 +651,26 @@ def digital_plan(circ: DigitalCircuit) -> tuple[int, int]:
 
 
 class Session:
-    """A run held on the device (yaqs_analog_begin / advance / finish).
+    """A run held on the device (yaqs_analog_begin or yaqs_digital_begin,
+    then advance / finish).
 
-    ``advance(n)`` evolves the next n recorded time indices of every
+    ``advance(n)`` evolves the next n recorded time indices (analog) or
+    circuit layers (digital; the first step prepares the states) of every
     trajectory and returns their device time in ms."""
 
-    def __init__(self, desc: Descriptors, ctx=None):
+    def __init__(self, desc, ctx=None):
         from . import _lib
         self.ctx = ctx or _lib.default_context()
         self.desc = desc
         h = C.c_void_p()
-        self.ctx.check(self.ctx._lib.yaqs_analog_begin(self.ctx.handle, C.byref(desc.mps), C.byref(desc.mpo),
-                                                       C.byref(desc.noise), desc.obs, desc.n_obs, C.byref(desc.cfg),
-                                                       C.byref(desc.rng), C.byref(h)))
+        if isinstance(desc, CircuitDescriptors):  # one advance step = one circuit layer (launch 0 prepares)
+            self.ctx.check(self.ctx._lib.yaqs_digital_begin(self.ctx.handle, C.byref(desc.mps), desc.gates,
+                                                            desc.n_gates, C.byref(desc.noise), desc.obs, desc.n_obs,
+                                                            C.byref(desc.cfg), C.byref(desc.rng), C.byref(h)))
+        else:
+            self.ctx.check(self.ctx._lib.yaqs_analog_begin(self.ctx.handle, C.byref(desc.mps), C.byref(desc.mpo),
+                                                           C.byref(desc.noise), desc.obs, desc.n_obs,
+                                                           C.byref(desc.cfg), C.byref(desc.rng), C.byref(h)))
         self.handle = h
 
     @property

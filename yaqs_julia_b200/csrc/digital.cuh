@@ -75,11 +75,17 @@ __device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
   if (c.sm.fail) return;
   cplx* th = c.ws + c.P.lay.th;
   const int l = s.chi[s1], r = s.chi[s1 + 2];
+  const int k = s.chi[s1 + 1];
   merge(c, s, s1, th);
   apply_local(th, l, 4, r, op);
   split(c, s, s1, th, l, r, 2, false);
   __syncthreads();
-  if (threadIdx.x == 0) *s.oc = s1 + 1;
+  if (threadIdx.x == 0) {
+    *s.oc = s1 + 1;
+    // nominal work: theta merge GEMM, 4x4 gate, SVD counted as 4 m n min(m, n) complex MACs
+    const double m = 2.0 * l, n = 2.0 * r;
+    *c.fl += 8.0 * (m * n * k + 4.0 * m * n + 4.0 * m * n * fmin(m, n));
+  }
   __syncthreads();
 }
 

@@ -1232,6 +1232,13 @@ int yaqs_digital_plan(const yaqs_gate_desc* gates, int32_t n_gates, int32_t* n_l
   return YAQS_OK;
 }
 
+int yaqs_digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
+                       const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                       const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out) {
+  if (!out) return set_err(ctx, YAQS_E_ARG, "null run handle");
+  return digital_begin(ctx, psi0, gates, n_gates, noise, obs, n_obs, cfg, rng, out);
+}
+
 int yaqs_digital_run(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
                      const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
                      const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, double* traj_out, double* mean_out,
