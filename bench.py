@@ -290,6 +290,7 @@ def run_digital(args):
     barrier_sync(dist)
     ck = clocks.stop()
     st1 = sess.stats()
+    phases = sess.profile() if args.profile else None
     res = sess.finish()
     t_max = reduce_max(dist, dev_ms / 1e3)
     value = reduce_sum(dist, nt * K) / t_max
@@ -334,6 +335,10 @@ def run_digital(args):
                 "cpu_baseline": cpu, "clocks": ck,
                 "stats": {"jumps": res.stats["jumps"], "svds": res.stats["svds"],
                           "max_bond": int(res.max_bond.max())}}
+        if phases:
+            tot = phases["step"] or 1.0
+            line["phases_pct_of_step"] = {k: round(100 * v / tot, 2) for k, v in phases.items()}
+            line["phases_note"] = "tdvp_sweep = TEBD gate application, jump_step = gate noise step"
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -71,6 +71,7 @@ __device__ void finish_normalize(Ctx& c, const DState& s) {
 
 // apply_local_gate_exact! on sites (s1, s1+1).
 __device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
+  ProfScope prof_scope_(PF_SWEEP);
   shift_oc(c, s, s1);
   if (c.sm.fail) return;
   cplx* th = c.ws + c.P.lay.th;
@@ -106,24 +107,72 @@ __device__ void apply_window_tebd(Ctx& c, const DState& s, const DevGate& g) {
 // away from the gate's sites is a gauge move, and only the gate's sites are
 // visited; otherwise the reference sweeps run as they are.
 __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
+  ProfScope prof_scope_(PF_STOCH);
   const DevParams& P = c.P;
   int nloc = 0;
-  bool all_zero = true, split_diss = false;
+  bool all_zero = true, split_diss = false, scalar_only = true;
+  double fdiss = 1.0;
   for (int k = 0; k < P.nprocs; ++k) {
     const DevProc& pr = P.procs[k];
     if (!proc_on(pr, s1, s2)) continue;
     ++nloc;
     if (pr.gamma != 0.0) all_zero = false;
     if (pr.nsites == 2 && !pr.pauli_name) split_diss = true;
+    if (pr.nsites != 1 || !pr.pauli_name || !pr.pauli_proc || !pr.unitary) scalar_only = false;
+    fdiss *= exp(-0.5 * pr.gamma);
   }
   if (!P.noise_present || nloc == 0) {
     finish_normalize(c, s);
     return;
   }
-  if ((split_diss && !all_zero) || !chain_tight(c, s)) {
+  const bool tight = chain_tight(c, s);
+  if ((split_diss && !all_zero) || !tight) {
     apply_dissipation(c, s, true, 1.0, s1, s2);
     if (c.sm.fail) return;
     stochastic_process(c, s, 1.0, s1, s2);
+    return;
+  }
+  if (scalar_only) {
+    // Pauli processes on single sites: every dissipator is a scalar, every
+    // candidate weight is gamma times the state norm, and a unitary jump on
+    // any site keeps the gauge, so nothing needs the centre moved.
+    const int oc = *s.oc;
+    cplx* A = site_ptr(c, s, oc);
+    const long long n = (long long)s.chi[oc] * 2 * s.chi[oc + 1];
+    if (!all_zero) {
+      cta_scale(A, n, fdiss);
+      __syncthreads();
+    }
+    const double nrm = cta_norm2(A, n, c.sm.e.r);
+    const double u1 = draw_uniform(c);
+    if (u1 >= 1.0 - nrm) {
+      normalize_center(c, s);
+      return;
+    }
+    double total = 0.0;
+    for (int k = 0; k < P.nprocs; ++k)
+      if (proc_on(P.procs[k], s1, s2)) total += P.procs[k].gamma * nrm;
+    if (total == 0.0) {
+      normalize_center(c, s);
+      return;
+    }
+    const double r = draw_uniform(c);
+    double acc = 0.0;
+    int chosen = -1, first = -1;
+    const int sites[2] = {s1, s2};
+    for (int si = 0; si < 2 && chosen < 0; ++si)
+      for (int k = 0; k < P.nprocs && chosen < 0; ++k) {
+        const DevProc& pr = P.procs[k];
+        if (!proc_on(pr, s1, s2) || pr.s0 != sites[si]) continue;
+        if (first < 0) first = k;
+        acc += pr.gamma * nrm / total;
+        if (r <= acc) chosen = k;
+      }
+    if (chosen < 0) chosen = first;  // rounding left the cumulative sum below r: the first candidate
+    const DevProc& pr = P.procs[chosen];
+    apply_local(site_ptr(c, s, pr.s0), s.chi[pr.s0], 2, s.chi[pr.s0 + 1], pr.mat);
+    if (threadIdx.x == 0) c.cnt[3] += 1;
+    normalize_center(c, s);
     return;
   }
   cplx* th = c.ws + c.P.lay.th;
@@ -236,6 +285,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
 // layer l-1 (its 1-qubit gates first, then each 2-qubit gate followed by the
 // noise step) and the sample after it.
 __device__ void run_digital_step(Ctx& c, const DigParams& D, int launch) {
+  ProfScope prof_scope_(PF_STEP);
   const DevParams& P = c.P;
   const int L = P.L;
   DState st{P.phi + (long long)c.traj * P.mps_size, P.phi_chi + (long long)c.traj * (L + 1), P.phi_oc + c.traj};

@@ -419,6 +419,10 @@ int pack_noise(yaqs_ctx* ctx, const yaqs_noise_desc* noise, int nprocs, int L, d
         for (int kk = 0; kk < dd; ++kk) sacc += std::conj(M[kk + dd * i]) * M[kk + dd * j];
         LdL[i + dd * j] = sacc;
       }
+    double dev = 0.0;
+    for (int i = 0; i < dd; ++i)
+      for (int j = 0; j < dd; ++j) dev = std::max(dev, std::abs(LdL[i + dd * j] - (i == j ? 1.0 : 0.0)));
+    d.unitary = dev < 1e-13 ? 1 : 0;
     herm_expm(dd, LdL, -0.5 * (dt / 2) * q.strength, e1);
     herm_expm(dd, LdL, -0.5 * dt * q.strength, e2);
     for (int e = 0; e < dd * dd; ++e) {

@@ -22,6 +22,7 @@ enum { ST_OK = 0, ST_ARG = 1, ST_NONFINITE = 3, ST_RNG = 7, ST_UNSUPPORTED = 8 }
 struct DevProc {
   int nsites, s0, s1;
   int pauli_name, pauli_proc;
+  int unitary;  // matrix^dag matrix = 1 (a jump then keeps every tensor's gauge)
   double gamma;
   cplx mat[16];
   cplx diss_half[16];
