@@ -1,10 +1,11 @@
 // engine.cu — kernels and C-ABI of the B200 TJM trajectory engine.
 //
-// One persistent kernel launch per recorded time index.  Each CTA (256
-// threads) owns a workspace slot and pulls trajectories from an atomic queue;
-// for each it runs that trajectory's share of analog_tjm_2 / analog_tjm_1
-// (AnalogTJM.jl:21-176) entirely on the device, with the MPS of every
-// trajectory resident in HBM between launches.
+// One persistent kernel launch per advance call, covering any number of
+// recorded time indices (or circuit layers).  Each CTA (256 threads) owns a
+// workspace slot and pulls (time index, trajectory) units from an atomic
+// queue; for each it runs that trajectory's share of analog_tjm_2 /
+// analog_tjm_1 (AnalogTJM.jl:21-176) or of run_digital_tjm entirely on the
+// device, with the MPS of every trajectory resident in HBM throughout.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -88,52 +89,80 @@ __device__ void run_step(Ctx& c, int j) {
   }
 }
 
-__global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int j) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+// Work units of a launch are (position, trajectory) pairs in position-major
+// order, where the positions first .. first+count-1 index P.jlist.  Each CTA
+// pulls the next unit from an atomic counter, so work is balanced at the
+// granularity of one time index (or circuit layer) of one trajectory, not of
+// whole trajectories.  A unit runs only after the same trajectory's previous
+// position has finished: that unit was pulled earlier by a CTA that is
+// executing it, so the wait always ends; it is still bounded (about 100 s)
+// and gives up with ST_TIMEOUT.
+#define DONE_WAIT_POLLS 100000000LL
+__device__ bool wait_done(const DevParams& P, int t, int need, CtaSmem& sm) {
+  if (threadIdx.x == 0) {
+    volatile int* d = P.done + t;
+    int ok = 0;
+    for (long long it = 0; it < DONE_WAIT_POLLS; ++it) {
+      if (*d >= need) {
+        ok = 1;
+        break;
+      }
+      __nanosleep(1000);
+    }
+    __threadfence();
+    sm.bcast_i[6] = ok;
+  }
+  __syncthreads();
+  const int ok = sm.bcast_i[6];
+  __syncthreads();
+  return ok != 0;
+}
+
+template <class StepFn>
+__device__ void run_units(const DevParams& P, CtaSmem& sm, int first, int count, StepFn step) {
   const int slot = blockIdx.x;
   cplx* ws = P.ws + (long long)slot * P.lay.total;
   int* wsi = P.wsi + (long long)slot * P.lay.itotal;
+  const int nt = P.num_traj;
+  const int total = count * nt;
   for (;;) {
-    if (threadIdx.x == 0) sm.bcast_i[7] = atomicAdd(&P.queue[j], 1);
+    if (threadIdx.x == 0) sm.bcast_i[7] = atomicAdd(&P.queue[first], 1);
     __syncthreads();
-    const int t = sm.bcast_i[7];
+    const int u = sm.bcast_i[7];
     __syncthreads();
-    if (t >= P.num_traj) break;
-    if (P.status[t] != 0) continue;
-    if (threadIdx.x == 0) sm.fail = 0;
+    if (u >= total) break;
+    const int k = u / nt, t = u - k * nt, pos = first + k;
+    bool ready = true;
+    if (k > 0) ready = wait_done(P, t, pos - 1, sm);
+    if (threadIdx.x == 0) sm.fail = ready ? 0 : ST_TIMEOUT;
     __syncthreads();
-    Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
-    run_step(c, j);
+    if (ready && P.status[t] == 0) {
+      Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
+      step(c, P.jlist[pos]);
+    }
     __syncthreads();
-    if (threadIdx.x == 0 && sm.fail) P.status[t] = sm.fail;
+    if (threadIdx.x == 0) {
+      if (sm.fail && P.status[t] == 0) P.status[t] = sm.fail;
+      __threadfence();
+      atomicExch(P.done + t, pos);
+    }
     __syncthreads();
   }
 }
 
-// Digital TJM: launch 0 prepares every trajectory, launch l >= 1 applies
-// layer l-1 of the circuit (run_digital_tjm, DigitalTJM.jl:363-450).
-__global__ void __launch_bounds__(NT, 2) digital_step_kernel(const DevParams P, const DigParams D, int j) {
+__global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int first, int count) {
   extern __shared__ __align__(16) unsigned char smraw[];
   CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
-  const int slot = blockIdx.x;
-  cplx* ws = P.ws + (long long)slot * P.lay.total;
-  int* wsi = P.wsi + (long long)slot * P.lay.itotal;
-  for (;;) {
-    if (threadIdx.x == 0) sm.bcast_i[7] = atomicAdd(&P.queue[j], 1);
-    __syncthreads();
-    const int t = sm.bcast_i[7];
-    __syncthreads();
-    if (t >= P.num_traj) break;
-    if (P.status[t] != 0) continue;
-    if (threadIdx.x == 0) sm.fail = 0;
-    __syncthreads();
-    Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
-    run_digital_step(c, D, j);
-    __syncthreads();
-    if (threadIdx.x == 0 && sm.fail) P.status[t] = sm.fail;
-    __syncthreads();
-  }
+  run_units(P, sm, first, count, [](Ctx& c, int j) { run_step(c, j); });
+}
+
+// Digital TJM: position 0 prepares every trajectory, position l >= 1 applies
+// layer l-1 of the circuit (run_digital_tjm, DigitalTJM.jl:363-450).
+__global__ void __launch_bounds__(NT, 2) digital_step_kernel(const DevParams P, const DigParams D, int first,
+                                                             int count) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+  run_units(P, sm, first, count, [&D](Ctx& c, int j) { run_digital_step(c, D, j); });
 }
 
 // ---------------------------------------------------------------------------
@@ -603,6 +632,20 @@ static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, 
   return YAQS_OK;
 }
 
+// Uploads the launch list (time index or layer per position) and marks no
+// position done for any trajectory.
+static int upload_positions(yaqs_ctx* ctx, yaqs_run* run) {
+  int *d_jlist, *d_done;
+  const size_t np = run->launches.size();
+  CUDA_TRY(ctx, run->dm.alloc(&d_jlist, std::max<size_t>(np, 1)));
+  CUDA_TRY(ctx, run->dm.alloc(&d_done, run->P.num_traj));
+  CUDA_TRY(ctx, cudaMemcpy(d_jlist, run->launches.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemset(d_done, 0xff, run->P.num_traj * sizeof(int)));  // -1
+  run->P.jlist = d_jlist;
+  run->P.done = d_done;
+  return YAQS_OK;
+}
+
 extern "C" {
 
 const char* yaqs_version(void) { return "yaqs-b200 0.1.0 (sm_100a, FP64 trajectory engine)"; }
@@ -853,6 +896,8 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
 
   run->launches.push_back(0);
   for (int j = (cfg->order == 2 ? 2 : 1); j < cfg->n_times; ++j) run->launches.push_back(j);
+  st = upload_positions(ctx, run);
+  if (st != YAQS_OK) return st;
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = guard.release();
   return YAQS_OK;
@@ -911,12 +956,17 @@ int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms) {
   const int avail = (int)(run->launches.size() - run->next);
   n = std::min(n, avail);
   CUDA_TRY(ctx, cudaEventRecord(run->e0, run->stream));
-  for (int k = 0; k < n; ++k) {
-    const int j = run->launches[run->next++];
+  // one launch for all n positions (several when position x trajectory
+  // units would overflow the 32-bit unit counter)
+  const int per_launch = (int)std::max<long long>(1, (1LL << 30) / std::max(1, run->P.num_traj));
+  while (n > 0) {
+    const int first = (int)run->next, cnt = std::min(n, per_launch);
+    run->next += cnt;
+    n -= cnt;
     if (run->digital)
-      digital_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, run->D, j);
+      digital_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, run->D, first, cnt);
     else
-      tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, j);
+      tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, first, cnt);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return set_err(ctx, YAQS_E_CUDA, std::string("launch: ") + cudaGetErrorString(le));
   }
@@ -960,8 +1010,9 @@ int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out, int32_
   }
   for (int t = 0; t < num_traj; ++t) {
     if (status[t] != 0) {
-      const char* why = status[t] == ST_RNG ? "injected uniform stream exhausted"
+      const char* why = status[t] == ST_RNG           ? "injected uniform stream exhausted"
                         : status[t] == ST_UNSUPPORTED ? "bond dimension exceeded its planned capacity"
+                        : status[t] == ST_TIMEOUT     ? "a bounded device wait gave up"
                                                       : "trajectory failed";
       return set_err(ctx, status[t], std::string(why) + " (trajectory " + std::to_string(t) + ")");
     }
@@ -1215,6 +1266,8 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   D.sample_at_start = C.sample_at_start ? 1 : 0;
   D.any_sample = (col > 0) ? 1 : 0;
   for (int j = 0; j <= n_layers; ++j) run->launches.push_back(j);
+  st = upload_positions(ctx, run);
+  if (st != YAQS_OK) return st;
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = guard.release();
   return YAQS_OK;

@@ -17,7 +17,7 @@
 #define MAX_OBS 512
 
 enum { OBS_LOCAL1 = 1, OBS_LOCAL2 = 2, OBS_ENTROPY = 3 };
-enum { ST_OK = 0, ST_ARG = 1, ST_NONFINITE = 3, ST_RNG = 7, ST_UNSUPPORTED = 8 };
+enum { ST_OK = 0, ST_ARG = 1, ST_NONFINITE = 3, ST_TIMEOUT = 5, ST_RNG = 7, ST_UNSUPPORTED = 8 };
 
 struct DevProc {
   int nsites, s0, s1;
@@ -76,7 +76,9 @@ struct DevParams {
   int* status;         // [num_traj]
   unsigned long long* counters;  // [num_slots][8]
   double* flops;                 // [num_slots]
-  int* queue;                    // [n_times]
+  int* queue;                    // [n_times] unit counter of the launch starting at each position
+  int* done;                     // [num_traj] last launch-list position completed by each trajectory
+  const int* jlist;              // [n_positions] time index (or layer) run at each launch-list position
 };
 
 struct CtaSmem {
