@@ -353,7 +353,8 @@ def run_ours(args):
     L, chi, nt = args.L, args.chi, args.traj
     n_times = args.warmup + args.steps + 1
     psi, H, cfg, nm = workload(L, chi, n_times, nt, args.start)
-    desc = api.Descriptors(psi, H, cfg, nm, seed=SEED, traj_offset=rank * nt)
+    prec = A.YAQS_PREC_MIXED if args.precision == "mixed" else A.YAQS_PREC_FP64
+    desc = api.Descriptors(psi, H, cfg, nm, seed=SEED, traj_offset=rank * nt, precision=prec)
     sess = api.Session(desc, ctx)
     for _ in range(args.warmup):
         sess.advance(1)
@@ -382,10 +383,23 @@ def run_ours(args):
     e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm = workload(L, chi, e2e_steps + 1, nt, args.start)
     barrier_sync(dist)
     t0 = time.perf_counter()
-    e2e_desc = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt)
+    e2e_desc = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt,
+                               precision=prec)
     e2e_res = api.run_descriptors(e2e_desc, ctx)
     barrier_sync(dist)
     e2e_s = reduce_max(dist, time.perf_counter() - t0)
+    err = None
+    if args.precision == "mixed":
+        # the same run (same draws) in the FP64 form: error of every observable
+        d64 = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt)
+        r64 = api.run_descriptors(d64, ctx)
+        dz = np.abs(e2e_res.trajectories[:, :L] - r64.trajectories[:, :L])
+        ds = np.abs(e2e_res.trajectories[:, L] - r64.trajectories[:, L])
+        same = np.all(np.abs(e2e_res.trajectories - r64.trajectories).reshape(nt, -1).max(1) < 1e-3)
+        err = {"z_max_abs": float(dz.max()), "z_mean_abs": float(dz.mean()), "s_half_max_abs": float(ds.max()),
+               "z_ensemble_mean_max_abs": float(np.abs(e2e_res.mean[:L] - r64.mean[:L]).max()),
+               "trajectories_compared": nt, "all_jump_records_equal": bool(same),
+               "run": f"{e2e_steps} time indices from t=0, same Philox draws"}
     h2d, d2h = desc_bytes(e2e_desc, e2e_desc.n_obs, e2e_desc.n_out, nt, L)
     e2e_value = reduce_sum(dist, nt * e2e_steps) / e2e_s
     cpu = None
@@ -395,11 +409,14 @@ def run_ours(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "c64 contractions (3xTF32 tensor cores) + c128 Lanczos/SVD/QR/norms"
+                if args.precision == "mixed" else "c128", "data": "synthetic",
                 "config": {"workload": f"analog TJM, L={L} Heisenberg XXX h=0.3, dephasing gamma=0.05, dt=0.05, "
                                        f"2-site TDVP chi_max={chi}, thr=1e-9, {nt} trajectories per GPU, "
                                        f"start={'saturated chi MPS' if args.start == 'sat' else 'Neel'}",
                            "L": L, "chi": chi, "num_traj": nt, "dt": 0.05, "parallelism": f"replicas x{ws}",
+                           "precision": args.precision,
                            "l2": "inputs larger than L2: %d trajectory states of up to %.1f MB each" % (
                                nt, sum(min(2 ** min(b, L - b), chi) * 2 * min(2 ** min(b + 1, L - b - 1), chi)
                                        for b in range(L)) * 16 / 1e6)},
@@ -416,6 +433,8 @@ def run_ours(args):
                 "stats": {"matvecs_timed": matvecs_timed, "flops_timed": flops_timed,
                           "jumps": res.stats["jumps"], "svd_sweeps": res.stats["svd_sweeps"],
                           "svds": res.stats["svds"], "max_bond": int(res.max_bond.max())}}
+        if err is not None:
+            line["err_vs_fp64"] = err
         if phases:
             tot = phases["step"] or 1.0
             line["phases_pct_of_step"] = {k: round(100 * v / tot, 2) for k, v in phases.items()}
@@ -429,6 +448,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--workload", default="analog", choices=["analog", "digital"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="analog contraction precision: fp64, or mixed (complex FP32 on the tensor cores)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--traj", type=int, default=None)

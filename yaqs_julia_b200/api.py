@@ -720,13 +720,18 @@ def random_mps(length: int, chi: int, seed: int = 0) -> MPS:
 
 
 def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
-        *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12, ctx=None) -> RunResult:
+        *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12,
+        precision: str = "fp64", ctx=None) -> RunResult:
     """Simulator.run (Simulator.jl:127-141) for an MPO (analog TJM) or a
     DigitalCircuit (digital TJM, TEBD gate application).  Fills every
     observable's ``trajectories`` and ``results`` like _run_analog /
     _run_digital; the result's ``max_bond`` holds the per-trajectory bond
     dimensions at each measurement.  As in the reference, a noiseless model
-    runs one trajectory and mutates ``sim_params.num_traj`` (Simulator.jl:27-29)."""
+    runs one trajectory and mutates ``sim_params.num_traj`` (Simulator.jl:27-29).
+    ``precision="mixed"`` runs the analog H_eff and environment contractions
+    in complex FP32 on the tensor cores (Lanczos orthogonalisation, SVD/QR,
+    norms and jump probabilities stay FP64)."""
+    prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
     if not isinstance(operator, (MPO, DigitalCircuit)):
         raise TypeError("Simulation requires MPO (Analog) or DigitalCircuit (Digital).")
     if noise_model is None or all(p.strength == 0 for p in noise_model.processes):
@@ -738,7 +743,7 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
         res = run_circuit_descriptors(desc, ctx)
     else:
         desc = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
-                           uniforms=uniforms, krylov_exit_tol=krylov_exit_tol)
+                           uniforms=uniforms, krylov_exit_tol=krylov_exit_tol, precision=prec)
         res = run_descriptors(desc, ctx)
     if isinstance(operator, DigitalCircuit):
         # obs buffers sized by sim_params.times; the first min(n_samples, columns) are filled (Simulator.jl:99-103)

@@ -693,8 +693,8 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
     return set_err(ctx, YAQS_E_ARG, "bad config (n_times, num_traj, max_bond_dim, dt)");
   if (cfg->krylov_dim < 1 || cfg->krylov_dim > KRYLOV_MAX) return set_err(ctx, YAQS_E_ARG, "krylov_dim must be in [1, 32]");
   if (cfg->order != 1 && cfg->order != 2) return set_err(ctx, YAQS_E_ARG, "order must be 1 or 2");
-  if (cfg->precision != YAQS_PREC_FP64)
-    return set_err(ctx, YAQS_E_UNSUPPORTED, "only the ComplexF64 form is served by this build");
+  if (cfg->precision != YAQS_PREC_FP64 && cfg->precision != YAQS_PREC_MIXED)
+    return set_err(ctx, YAQS_E_ARG, "precision must be YAQS_PREC_FP64 or YAQS_PREC_MIXED");
   if (n_obs < 0 || n_obs > MAX_OBS) return set_err(ctx, YAQS_E_ARG, "n_obs out of range");
   if (rng->mode != YAQS_RNG_PHILOX && rng->mode != YAQS_RNG_INJECTED) return set_err(ctx, YAQS_E_ARG, "bad rng mode");
   if (rng->mode == YAQS_RNG_INJECTED && (!rng->uniforms || rng->stride < 1))
@@ -756,6 +756,21 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   lay.Zo = take(tmp);
   lay.y = take(2 * capmax + 16);
   lay.dbl = take((SVD_MAX_COLS + MAX_PROCS) / 2 + 8);
+  const bool mixed = cfg->precision == YAQS_PREC_MIXED;
+  {
+    // mixed form: FP32 copies of one left and one right environment, of a site
+    // tensor and of a Krylov vector, and FP32 contraction intermediates
+    long long emax = 0, amax = 0;
+    for (int b = 0; b <= L; ++b) emax = std::max(emax, (long long)cap[b] * cap[b] * w[b]);
+    for (int i = 0; i < L; ++i) amax = std::max(amax, 2LL * cap[i] * cap[i + 1]);
+    auto takef = [&](long long nf) { return take(mixed ? (nf + 1) / 2 : 0); };
+    lay.Lf = takef(emax);
+    lay.Rf = takef(emax);
+    lay.xf = takef(kry_n);
+    lay.T1f = takef(t_size);
+    lay.T2f = takef(t_size);
+    lay.Af = takef(amax);
+  }
   lay.total = off;
   long long ioff = 0;
   lay.i_chi = ioff;
@@ -856,6 +871,7 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   P.L = L;
   P.n_times = cfg->n_times;
   P.order = cfg->order;
+  P.mixed = mixed ? 1 : 0;
   P.sample_ts = cfg->sample_timesteps != 0;
   P.max_bond = cfg->max_bond_dim;
   P.nobs = n_obs;
@@ -1109,7 +1125,8 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   if (cfg->local_method != YAQS_METHOD_TEBD || cfg->long_range_method != YAQS_METHOD_TEBD)
     return set_err(ctx, YAQS_E_UNSUPPORTED, "only TEBD gate application is served by this build");
   if (cfg->precision != YAQS_PREC_FP64)
-    return set_err(ctx, YAQS_E_UNSUPPORTED, "only the ComplexF64 form is served by this build");
+    return set_err(ctx, YAQS_E_UNSUPPORTED,
+                   "digital runs are served in ComplexF64 only (their work is SVD/QR, which stays FP64)");
   if (n_obs < 0 || n_obs > MAX_OBS) return set_err(ctx, YAQS_E_ARG, "n_obs out of range");
   if (rng->mode != YAQS_RNG_PHILOX && rng->mode != YAQS_RNG_INJECTED) return set_err(ctx, YAQS_E_ARG, "bad rng mode");
   if (rng->mode == YAQS_RNG_INJECTED && (!rng->uniforms || rng->stride < 1))
@@ -1147,6 +1164,7 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
     return o;
   };
   lay.psi = lay.EL = lay.ER = lay.Q = lay.T1 = lay.T2 = take(0);
+  lay.Lf = lay.Rf = lay.xf = lay.T1f = lay.T2f = lay.Af = take(0);
   lay.tA = take(tmp);
   lay.tB = take(tmp);
   lay.tC = take(tmp);

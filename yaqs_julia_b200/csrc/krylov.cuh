@@ -11,7 +11,7 @@
 // is taken on one warp by Taylor series over substeps of norm <= 1/2.
 #pragma once
 #include "common.cuh"
-#include "gemm.cuh"
+#include "gemm_tf32.cuh"
 
 #define WAPPLY_PT 64
 #define WAPPLY_MAXI 32
@@ -46,10 +46,21 @@ struct WApplySmem {
 // out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.  Each thread
 // owns pair slot tid % WAPPLY_PT of every tile and input/output rows
 // tid / WAPPLY_PT + k NT / WAPPLY_PT, so index arithmetic is per tile, not
-// per element.
-__device__ __noinline__ void dev_wapply(const cplx* __restrict__ in, cplx* __restrict__ out, const WMat W,
+// per element.  T is cplx (FP64 form) or float2 (mixed form, FP32 products).
+__device__ __forceinline__ void wfma(cplx& acc, cplx v, cplx x) { cfma(acc, v, x); }
+__device__ __forceinline__ void wfma(float2& acc, cplx v, float2 x) {
+  const float vr = (float)v.x, vi = (float)v.y;
+  acc.x = fmaf(vr, x.x, fmaf(-vi, x.y, acc.x));
+  acc.y = fmaf(vr, x.y, fmaf(vi, x.x, acc.y));
+}
+__device__ __forceinline__ void wzero(cplx& z) { z = make_double2(0.0, 0.0); }
+__device__ __forceinline__ void wzero(float2& z) { z = make_float2(0.f, 0.f); }
+
+template <class T>
+__device__ __noinline__ void dev_wapply(const T* __restrict__ in, T* __restrict__ out, const WMat W,
                                         const WApplyGeom g, WApplySmem& ws) {
   ProfScope prof_scope_(PF_WAPPLY);
+  T(*sin)[WAPPLY_PT] = reinterpret_cast<T(*)[WAPPLY_PT]>(&ws.in[0][0]);
   const int tid = threadIdx.x;
   for (int e = tid; e < W.nnz; e += NT) {
     ws.val[e] = W.val[e];
@@ -61,18 +72,20 @@ __device__ __noinline__ void dev_wapply(const cplx* __restrict__ in, cplx* __res
   const int npair = g.n0 * g.n1;
   const int pl = tid % WAPPLY_PT, r0 = tid / WAPPLY_PT;
   constexpr int RS = NT / WAPPLY_PT;
+  T zero;
+  wzero(zero);
   for (int base = 0; base < npair; base += WAPPLY_PT) {
     const int pair = base + pl;
     const bool live = pair < npair;
     const int q0 = live ? pair % g.n0 : 0, q1 = live ? pair / g.n0 : 0;
     const long long ib = q0 * g.is0 + q1 * g.is1, ob = q0 * g.os0 + q1 * g.os1;
     __syncthreads();
-    for (int i = r0; i < W.ni; i += RS) ws.in[i][pl] = live ? in[ib + ws.in_off[i]] : make_double2(0.0, 0.0);
+    for (int i = r0; i < W.ni; i += RS) sin[i][pl] = live ? in[ib + ws.in_off[i]] : zero;
     __syncthreads();
     if (live) {
       for (int o = r0; o < W.no; o += RS) {
-        cplx acc = make_double2(0.0, 0.0);
-        for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) cfma(acc, ws.val[z], ws.in[ws.col[z]][pl]);
+        T acc = zero;
+        for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) wfma(acc, ws.val[z], sin[ws.col[z]][pl]);
         out[ob + ws.out_off[o]] = acc;
       }
     }
@@ -87,6 +100,13 @@ struct HeffOp {
   int chil, D, chir, wl, wr;
   cplx* T1;
   cplx* T2;
+  // mixed form: FP32 copies of the environments and FP32 intermediates
+  int mixed = 0;
+  const cflt* Lf = nullptr;
+  const cflt* Rf = nullptr;
+  cflt* xf = nullptr;
+  cflt* T1f = nullptr;
+  cflt* T2f = nullptr;
 };
 
 struct KrySmem {
@@ -112,12 +132,22 @@ struct EngineSmem {
   KrySmem k;
 };
 
-// y = H_eff x.  CTA-collective.
+// y = H_eff x.  CTA-collective.  In the mixed form x is rounded to FP32, the
+// three contractions run in FP32 (tensor cores for the two GEMMs) and y is
+// written back in FP64.
 __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, EngineSmem& sm) {
   const int chil = h.chil, D = h.D, chir = h.chir, wl = h.wl, wr = h.wr;
-  cta_gemm(gemm_args(chil * wl, D * chir, chil, h.L, 1, (long long)chil * wl, x, 1, chil, h.T1, 1,
-                     (long long)chil * wl),
-           sm.u.gw.g);
+  if (h.mixed) {
+    GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(sm.u.gw.g);
+    cta_to_f32(h.xf, x, (long long)chil * D * chir);
+    cta_gemm_tf32<cflt>(gemm_args_f(chil * wl, D * chir, chil, h.Lf, 1, (long long)chil * wl, h.xf, 1, chil, h.T1f,
+                                    1, (long long)chil * wl),
+                        gf);
+  } else {
+    cta_gemm(gemm_args(chil * wl, D * chir, chil, h.L, 1, (long long)chil * wl, x, 1, chil, h.T1, 1,
+                       (long long)chil * wl),
+             sm.u.gw.g);
+  }
   WApplyGeom g;
   g.n0 = chil;
   g.n1 = chir;
@@ -131,10 +161,18 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   g.no1 = D;
   g.oo1 = chil;
   g.oo2 = (long long)chil * D;
-  dev_wapply(h.T1, h.T2, h.W, g, sm.u.gw.w);
-  cta_gemm(gemm_args(chil * D, chir, wr * chir, h.T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
-                     (long long)chil * D),
-           sm.u.gw.g);
+  if (h.mixed) {
+    GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(sm.u.gw.g);
+    dev_wapply<cflt>(h.T1f, h.T2f, h.W, g, sm.u.gw.w);
+    cta_gemm_tf32<cplx>(gemm_args_f(chil * D, chir, wr * chir, h.T2f, 1, (long long)chil * D, h.Rf, chir, 1, y, 1,
+                                    (long long)chil * D),
+                        gf);
+  } else {
+    dev_wapply<cplx>(h.T1, h.T2, h.W, g, sm.u.gw.w);
+    cta_gemm(gemm_args(chil * D, chir, wr * chir, h.T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
+                       (long long)chil * D),
+             sm.u.gw.g);
+  }
 }
 
 __device__ __forceinline__ double heff_flops(int chil, int wl, int D, int chir, int wr) {

@@ -37,6 +37,8 @@ struct DevObs {
 // Offsets (in cplx elements) of the parts of one slot's workspace.
 struct WsLayout {
   long long psi, EL, ER, Q, T1, T2, tA, tB, tC, th, B, X, Yo, Zo, y, dbl;
+  // mixed form (FP32 buffers, offsets in complex-double units)
+  long long Lf, Rf, xf, T1f, T2f, Af;
   long long total;
   // int workspace (per slot)
   long long i_chi, i_oc, i_ord, i_cand, itotal;
@@ -45,6 +47,7 @@ struct WsLayout {
 struct DevParams {
   int L, n_times, order, sample_ts, max_bond, nobs, nprocs, noise_present, all_zero, rng_mode, num_traj,
       traj_offset, ncols;
+  int mixed;  // H_eff and environment contractions in complex FP32 on the tensor cores
   double dt, thr;
   KrylovCfg kc;
   unsigned long long seed;
@@ -285,8 +288,20 @@ __device__ void update_left(Ctx& c, const DState& s, int i) {
   const cplx* A = site_ptr(c, s, i);
   cplx* T1 = c.ws + c.P.lay.T1;
   cplx* T2 = c.ws + c.P.lay.T2;
-  cta_gemm(gemm_args(l * wl, 2 * r, l, envL(c, i), 1, (long long)l * wl, A, 1, l, T1, 1, (long long)l * wl),
-           c.sm.e.u.gw.g);
+  cflt* Af = reinterpret_cast<cflt*>(c.ws + c.P.lay.Af);
+  cflt* Ef = reinterpret_cast<cflt*>(c.ws + c.P.lay.Lf);
+  cflt* T1f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T1f);
+  cflt* T2f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T2f);
+  GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(c.sm.e.u.gw.g);
+  if (c.P.mixed) {
+    cta_to_f32(Af, A, (long long)l * 2 * r);
+    cta_to_f32(Ef, envL(c, i), (long long)l * wl * l);
+    cta_gemm_tf32<cflt>(gemm_args_f(l * wl, 2 * r, l, Ef, 1, (long long)l * wl, Af, 1, l, T1f, 1, (long long)l * wl),
+                        gf);
+  } else {
+    cta_gemm(gemm_args(l * wl, 2 * r, l, envL(c, i), 1, (long long)l * wl, A, 1, l, T1, 1, (long long)l * wl),
+             c.sm.e.u.gw.g);
+  }
   WApplyGeom g;
   g.n0 = l;
   g.n1 = r;
@@ -300,8 +315,15 @@ __device__ void update_left(Ctx& c, const DState& s, int i) {
   g.no1 = 2;
   g.oo1 = l;
   g.oo2 = 2 * l;
-  dev_wapply(T1, T2, c.P.wm_envL[i], g, c.sm.e.u.gw.w);
-  cta_gemm(gemm_args(r, wr * r, 2 * l, A, 2 * l, 1, T2, 1, 2 * l, envL(c, i + 1), 1, r, true, false), c.sm.e.u.gw.g);
+  if (c.P.mixed) {
+    dev_wapply<cflt>(T1f, T2f, c.P.wm_envL[i], g, c.sm.e.u.gw.w);
+    cta_gemm_tf32<cplx>(gemm_args_f(r, wr * r, 2 * l, Af, 2 * l, 1, T2f, 1, 2 * l, envL(c, i + 1), 1, r, true, false),
+                        gf);
+  } else {
+    dev_wapply<cplx>(T1, T2, c.P.wm_envL[i], g, c.sm.e.u.gw.w);
+    cta_gemm(gemm_args(r, wr * r, 2 * l, A, 2 * l, 1, T2, 1, 2 * l, envL(c, i + 1), 1, r, true, false),
+             c.sm.e.u.gw.g);
+  }
 }
 
 // ER[i] from ER[i+1], A_i, W_i  (update_right_environment)
@@ -311,7 +333,19 @@ __device__ void update_right(Ctx& c, const DState& s, int i) {
   const cplx* A = site_ptr(c, s, i);
   cplx* T1 = c.ws + c.P.lay.T1;
   cplx* T2 = c.ws + c.P.lay.T2;
-  cta_gemm(gemm_args(2 * l, r * wr, r, A, 1, 2 * l, envR(c, i + 1), (long long)r * wr, 1, T1, 1, 2 * l), c.sm.e.u.gw.g);
+  cflt* Af = reinterpret_cast<cflt*>(c.ws + c.P.lay.Af);
+  cflt* Ef = reinterpret_cast<cflt*>(c.ws + c.P.lay.Rf);
+  cflt* T1f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T1f);
+  cflt* T2f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T2f);
+  GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(c.sm.e.u.gw.g);
+  if (c.P.mixed) {
+    cta_to_f32(Af, A, (long long)l * 2 * r);
+    cta_to_f32(Ef, envR(c, i + 1), (long long)r * wr * r);
+    cta_gemm_tf32<cflt>(gemm_args_f(2 * l, r * wr, r, Af, 1, 2 * l, Ef, (long long)r * wr, 1, T1f, 1, 2 * l), gf);
+  } else {
+    cta_gemm(gemm_args(2 * l, r * wr, r, A, 1, 2 * l, envR(c, i + 1), (long long)r * wr, 1, T1, 1, 2 * l),
+             c.sm.e.u.gw.g);
+  }
   WApplyGeom g;
   g.n0 = l;
   g.n1 = r;
@@ -325,8 +359,13 @@ __device__ void update_right(Ctx& c, const DState& s, int i) {
   g.no1 = 2;
   g.oo1 = 1;
   g.oo2 = 2 * r;
-  dev_wapply(T1, T2, c.P.wm_envR[i], g, c.sm.e.u.gw.w);
-  cta_gemm(gemm_args(l, wl * l, 2 * r, A, 1, l, T2, 1, 2 * r, envR(c, i), 1, l, true, false), c.sm.e.u.gw.g);
+  if (c.P.mixed) {
+    dev_wapply<cflt>(T1f, T2f, c.P.wm_envR[i], g, c.sm.e.u.gw.w);
+    cta_gemm_tf32<cplx>(gemm_args_f(l, wl * l, 2 * r, Af, 1, l, T2f, 1, 2 * r, envR(c, i), 1, l, true, false), gf);
+  } else {
+    dev_wapply<cplx>(T1, T2, c.P.wm_envR[i], g, c.sm.e.u.gw.w);
+    cta_gemm(gemm_args(l, wl * l, 2 * r, A, 1, l, T2, 1, 2 * r, envR(c, i), 1, l, true, false), c.sm.e.u.gw.g);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -344,6 +383,18 @@ __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, con
   h.wr = c.P.w[br];
   h.T1 = c.ws + c.P.lay.T1;
   h.T2 = c.ws + c.P.lay.T2;
+  h.mixed = c.P.mixed;
+  if (c.P.mixed) {  // FP32 environments for the whole Krylov solve
+    cflt* Lf = reinterpret_cast<cflt*>(c.ws + c.P.lay.Lf);
+    cflt* Rf = reinterpret_cast<cflt*>(c.ws + c.P.lay.Rf);
+    cta_to_f32(Lf, h.L, (long long)l * h.wl * l);
+    cta_to_f32(Rf, h.R, (long long)r * h.wr * r);
+    h.Lf = Lf;
+    h.Rf = Rf;
+    h.xf = reinterpret_cast<cflt*>(c.ws + c.P.lay.xf);
+    h.T1f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T1f);
+    h.T2f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T2f);
+  }
   int mv = dev_expm_krylov(h, x, dt, c.P.kc, c.ws + c.P.lay.Q, c.P.kry_n, c.sm.e);
   if (threadIdx.x == 0) {
     c.cnt[0] += mv;
