@@ -285,6 +285,73 @@ int yaqs_digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate
                        const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
                        const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out);
 
+/*
+ * Serving.  A request loop that runs many simulations at once on one GPU:
+ * analog and digital requests of different L, bond dimension, MPO width and
+ * trajectory count (the Simulator.run calls of many users, Simulator.jl:
+ * 127-141).  Requests are admitted in arrival order while their trajectory
+ * states and outputs fit in hbm_budget; every admitted run advances by
+ * `chunk` recorded time indices (analog) or circuit layers (digital) per
+ * launch, and all of them share ONE persistent kernel launch whose CTAs pull
+ * (run, position, trajectory) work units and share one pool of slot
+ * workspaces sized for the largest request the server accepts.  A request
+ * that arrives while others run joins at the next launch; a finished run
+ * leaves and frees its memory.  Each request's results equal those of the
+ * same yaqs_analog_run / yaqs_digital_run call: a trajectory's arithmetic
+ * does not depend on which slot or launch runs it.  All functions are safe
+ * to call from several host threads.
+ */
+typedef struct yaqs_server yaqs_server;
+typedef struct {
+  int32_t max_L;          /* longest chain served */
+  int32_t max_bond_dim;   /* largest max_bond_dim served (<= 128) */
+  int32_t max_mpo_width;  /* widest MPO bond served (analog, <= 8) */
+  int32_t krylov_dim;     /* largest krylov_dim served */
+  int32_t mixed;          /* 1: also size the slots for YAQS_PREC_MIXED requests */
+  int32_t chunk;          /* positions every run advances per launch (>= 1) */
+  int64_t hbm_budget;     /* bytes for admitted runs (0: 90% of the free memory left after the slot pool) */
+} yaqs_server_config;
+
+enum { YAQS_REQ_QUEUED = 0, YAQS_REQ_RUNNING = 1, YAQS_REQ_DONE = 2, YAQS_REQ_FAILED = 3 };
+
+typedef struct {
+  int64_t submitted, completed, failed, launches;
+  int64_t queued_now, running_now;
+  int64_t bytes_in_use, hbm_budget;
+  int32_t slots;               /* CTAs of every served launch */
+  double latency_p50_s;        /* submit -> done over completed requests */
+  double latency_p99_s;
+  double queue_p50_s;          /* submit -> admitted */
+  double queue_p99_s;
+  double busy_s;               /* device time of all served launches */
+} yaqs_server_stats;
+
+int yaqs_server_create(yaqs_ctx* ctx, const yaqs_server_config* cfg, yaqs_server** out);
+/* Copies every descriptor and buffer; the caller may free them on return. */
+int yaqs_server_submit_analog(yaqs_server* srv, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
+                              const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                              const yaqs_tev_config* cfg, const yaqs_rng_desc* rng, int64_t* id);
+int yaqs_server_submit_digital(yaqs_server* srv, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates,
+                               int32_t n_gates, const yaqs_noise_desc* noise, const yaqs_obs_desc* obs,
+                               int32_t n_obs, const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng,
+                               int64_t* id);
+/* *state receives YAQS_REQ_*. */
+int yaqs_server_poll(yaqs_server* srv, int64_t id, int32_t* state);
+/* Waits until the request is done or failed; YAQS_E_TIMEOUT after timeout_s (< 0: no limit). */
+int yaqs_server_wait(yaqs_server* srv, int64_t id, double timeout_s);
+/*
+ * Outputs of a finished request (as yaqs_analog_run / yaqs_digital_run;
+ * any pointer may be NULL) and times_s[3] = {queued, running, total}
+ * seconds; releases the request.  A failed request returns its status and
+ * message (yaqs_server_last_error).
+ */
+int yaqs_server_take(yaqs_server* srv, int64_t id, double* traj_out, double* mean_out, int32_t* maxchi_out,
+                     yaqs_run_stats* stats, double* times_s);
+const char* yaqs_server_last_error(yaqs_server* srv);
+int yaqs_server_stats_get(yaqs_server* srv, yaqs_server_stats* out);
+/* Fails whatever is still queued or running and frees the server. */
+int yaqs_server_destroy(yaqs_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,7 +41,9 @@ def test_abi_struct_layouts_match_header(tmp_path):
         pytest.skip("no C compiler")
     structs = {"yaqs_mps_desc": A.MpsDesc, "yaqs_mpo_desc": A.MpoDesc, "yaqs_noise_proc": A.NoiseProc,
                "yaqs_noise_desc": A.NoiseDesc, "yaqs_obs_desc": A.ObsDesc, "yaqs_rng_desc": A.RngDesc,
-               "yaqs_tev_config": A.TevConfig, "yaqs_run_stats": A.RunStats}
+               "yaqs_tev_config": A.TevConfig, "yaqs_run_stats": A.RunStats, "yaqs_gate_desc": A.GateDesc,
+               "yaqs_circuit_config": A.CircuitConfig, "yaqs_server_config": A.ServerConfig,
+               "yaqs_server_stats": A.ServerStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "yaqs_tjm.h"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -105,3 +105,22 @@ class RunStats(C.Structure):
 def dptr(a):
     """double* of a C-contiguous float64/complex128 numpy buffer."""
     return a.ctypes.data_as(DPTR)
+
+
+YAQS_REQ_QUEUED, YAQS_REQ_RUNNING, YAQS_REQ_DONE, YAQS_REQ_FAILED = 0, 1, 2, 3
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_L", C.c_int32), ("max_bond_dim", C.c_int32), ("max_mpo_width", C.c_int32),
+                ("krylov_dim", C.c_int32), ("mixed", C.c_int32), ("chunk", C.c_int32), ("hbm_budget", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("launches", C.c_int64),
+                ("queued_now", C.c_int64), ("running_now", C.c_int64), ("bytes_in_use", C.c_int64),
+                ("hbm_budget", C.c_int64), ("slots", C.c_int32), ("latency_p50_s", C.c_double),
+                ("latency_p99_s", C.c_double), ("queue_p50_s", C.c_double), ("queue_p99_s", C.c_double),
+                ("busy_s", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}

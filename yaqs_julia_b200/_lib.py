@@ -49,6 +49,21 @@ def lib():
                                        P(C.c_int32), P(A.RunStats)]
         L.yaqs_digital_begin.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),
                                          P(A.ObsDesc), C.c_int32, P(A.CircuitConfig), P(A.RngDesc), P(C.c_void_p)]
+        L.yaqs_server_create.argtypes = [C.c_void_p, P(A.ServerConfig), P(C.c_void_p)]
+        L.yaqs_server_submit_analog.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.MpoDesc), P(A.NoiseDesc),
+                                                P(A.ObsDesc), C.c_int32, P(A.TevConfig), P(A.RngDesc),
+                                                P(C.c_int64)]
+        L.yaqs_server_submit_digital.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32,
+                                                 P(A.NoiseDesc), P(A.ObsDesc), C.c_int32, P(A.CircuitConfig),
+                                                 P(A.RngDesc), P(C.c_int64)]
+        L.yaqs_server_poll.argtypes = [C.c_void_p, C.c_int64, P(C.c_int32)]
+        L.yaqs_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_double]
+        L.yaqs_server_take.argtypes = [C.c_void_p, C.c_int64, A.DPTR, A.DPTR, P(C.c_int32), P(A.RunStats),
+                                       A.DPTR]
+        L.yaqs_server_last_error.argtypes = [C.c_void_p]
+        L.yaqs_server_last_error.restype = C.c_char_p
+        L.yaqs_server_stats_get.argtypes = [C.c_void_p, P(A.ServerStats)]
+        L.yaqs_server_destroy.argtypes = [C.c_void_p]
         L.yaqs_fp64_peak.argtypes = [C.c_void_p, P(C.c_double)]
         L.yaqs_batched_svd_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4 + [
             C.c_void_p]

@@ -709,6 +709,96 @@ class Session:
         return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
 
 
+class Server:
+    """Request loop serving many simulations at once on one GPU
+    (yaqs_server_*): requests of any size are admitted as device memory
+    frees up, all admitted runs advance together in one persistent kernel
+    launch per step, and each request's results equal those of running it
+    alone.  ``submit`` copies the request and returns an id at once."""
+
+    def __init__(self, max_L: int = 64, max_bond_dim: int = 128, max_mpo_width: int = 5, krylov_dim: int = 25,
+                 mixed: bool = True, chunk: int = 1, hbm_budget: int = 0, ctx=None):
+        from . import _lib
+        self.ctx = ctx or _lib.default_context()
+        self._lib = self.ctx._lib
+        cfg = A.ServerConfig(max_L, max_bond_dim, max_mpo_width, krylov_dim, int(mixed), chunk, hbm_budget)
+        h = C.c_void_p()
+        self.ctx.check(self._lib.yaqs_server_create(self.ctx.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self._meta = {}
+
+    def _check_static(self, st):
+        if st != A.YAQS_OK:
+            from . import _lib
+            raise _lib.EngineError(st, self._lib.yaqs_last_error(None).decode())
+
+    def submit(self, initial_state: MPS, operator, sim_params: TimeEvolutionConfig,
+               noise_model: NoiseModel | None = None, *, seed: int = 0, uniforms: np.ndarray | None = None,
+               precision: str = "fp64", traj_offset: int = 0) -> int:
+        mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
+        rid = C.c_int64(0)
+        if isinstance(operator, DigitalCircuit):
+            d = CircuitDescriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
+                                   uniforms=uniforms, traj_offset=traj_offset)
+            st = self._lib.yaqs_server_submit_digital(self.handle, C.byref(d.mps), d.gates, d.n_gates,
+                                                      C.byref(d.noise), d.obs, d.n_obs, C.byref(d.cfg),
+                                                      C.byref(d.rng), C.byref(rid))
+        else:
+            prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
+            d = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
+                            uniforms=uniforms, precision=prec, traj_offset=traj_offset)
+            st = self._lib.yaqs_server_submit_analog(self.handle, C.byref(d.mps), C.byref(d.mpo), C.byref(d.noise),
+                                                     d.obs, d.n_obs, C.byref(d.cfg), C.byref(d.rng), C.byref(rid))
+        self._check_static(st)
+        self._meta[rid.value] = (d.num_traj, d.n_obs, d.n_out)
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        s = C.c_int32(0)
+        self._check_static(self._lib.yaqs_server_poll(self.handle, rid, C.byref(s)))
+        return s.value
+
+    def wait(self, rid: int, timeout: float | None = None):
+        self._check_static(self._lib.yaqs_server_wait(self.handle, rid, -1.0 if timeout is None else timeout))
+
+    def result(self, rid: int, timeout: float | None = None) -> RunResult:
+        """Waits for the request and returns its RunResult (``times`` = queued, running, total seconds)."""
+        self.wait(rid, timeout)
+        nt, nobs, nout = self._meta.pop(rid)
+        traj = np.zeros((nt, max(nobs, 1), nout))
+        mean = np.zeros((max(nobs, 1), nout))
+        chi = np.zeros((nt, nout), dtype=np.int32)
+        st = A.RunStats()
+        times = np.zeros(3)
+        code = self._lib.yaqs_server_take(self.handle, rid, A.dptr(traj), A.dptr(mean),
+                                          chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(st), A.dptr(times))
+        if code != A.YAQS_OK:
+            from . import _lib
+            raise _lib.EngineError(code, self._lib.yaqs_server_last_error(self.handle).decode())
+        res = RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
+        res.times = times
+        return res
+
+    def stats(self) -> dict:
+        s = A.ServerStats()
+        self._check_static(self._lib.yaqs_server_stats_get(self.handle, C.byref(s)))
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.yaqs_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+
 def random_mps(length: int, chi: int, seed: int = 0) -> MPS:
     """An MPS with every bond at min(2^b, 2^(L-b), chi) and Gaussian entries
     (a saturated-bond-dimension start state; normalised by the engine)."""

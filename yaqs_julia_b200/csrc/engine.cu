@@ -482,6 +482,111 @@ int pack_obs(yaqs_ctx* ctx, const yaqs_obs_desc* obs, int n_obs, int L, std::vec
   return YAQS_OK;
 }
 
+// Structural capacities cap(b) = max(min(2^min(b, L-b), chi_max), chi0(b)) of
+// every bond and the sizes that follow from them.
+struct Caps {
+  std::vector<int> cap;
+  std::vector<long long> mps_off, env_off;
+  long long mps_size = 0, env_size = 0, kry_n = 0, t_size = 0;
+  int capmax = 1;
+};
+
+bool plan_caps(int L, const int* chi0, const int* w, int max_bond, Caps& c) {
+  c.cap.assign(L + 1, 1);
+  for (int b = 0; b <= L; ++b) {
+    long long sz = 1;
+    const int e = std::min(b, L - b);
+    for (int k = 0; k < e && sz < (1 << 20); ++k) sz *= 2;
+    c.cap[b] = (int)std::max<long long>(std::min<long long>(sz, max_bond), chi0 ? chi0[b] : 1);
+    if (2 * c.cap[b] > SVD_MAX_COLS) return false;
+  }
+  c.capmax = *std::max_element(c.cap.begin(), c.cap.end());
+  c.mps_off.assign(L, 0);
+  c.env_off.assign(L + 1, 0);
+  c.mps_size = c.env_size = c.kry_n = c.t_size = 0;
+  for (int i = 0; i < L; ++i) {
+    c.mps_off[i] = c.mps_size;
+    c.mps_size += (long long)c.cap[i] * 2 * c.cap[i + 1];
+  }
+  for (int b = 0; b <= L; ++b) {
+    c.env_off[b] = c.env_size;
+    c.env_size += (long long)c.cap[b] * c.cap[b] * w[b];
+  }
+  for (int i = 0; i < L; ++i) {
+    c.kry_n = std::max(c.kry_n, (long long)c.cap[i] * 2 * c.cap[i + 1]);
+    c.t_size = std::max(c.t_size, (long long)c.cap[i] * c.cap[i + 1] * 2 * std::max(w[i], w[i + 1]));
+    if (i + 2 <= L) {
+      c.kry_n = std::max(c.kry_n, (long long)c.cap[i] * 4 * c.cap[i + 2]);
+      c.t_size = std::max(c.t_size, (long long)c.cap[i] * c.cap[i + 2] * 4 * std::max(w[i], w[i + 2]));
+    }
+  }
+  return true;
+}
+
+// Per-slot workspace of one trajectory's program (offsets in complex-double
+// units, each buffer 32-byte aligned).  analog = false leaves out what the
+// digital program does not use (the sampled copy, environments, Krylov basis,
+// contraction intermediates).
+WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, bool mixed) {
+  const long long tmp = 4LL * c.capmax * c.capmax + 16;
+  WsLayout lay;
+  long long off = 0;
+  auto take = [&](long long n) {
+    long long o = off;
+    off += (n + 1) & ~1LL;
+    return o;
+  };
+  lay.psi = take(analog ? c.mps_size : 0);
+  lay.EL = take(analog ? c.env_size : 0);
+  lay.ER = take(analog ? c.env_size : 0);
+  lay.Q = take(analog ? (long long)(kdim + 1) * c.kry_n : 0);
+  lay.T1 = take(analog ? c.t_size : 0);
+  lay.T2 = take(analog ? c.t_size : 0);
+  lay.tA = take(tmp);
+  lay.tB = take(tmp);
+  lay.tC = take(tmp);
+  lay.th = take(c.kry_n);
+  lay.B = take(tmp);
+  lay.X = take(tmp);
+  lay.Yo = take(tmp);
+  lay.Zo = take(tmp);
+  lay.y = take(2 * c.capmax + 16);
+  lay.dbl = take((SVD_MAX_COLS + MAX_PROCS) / 2 + 8);
+  // mixed form: FP32 copies of one left and one right environment, of a site
+  // tensor and of a Krylov vector, and FP32 contraction intermediates
+  long long emax = 0, amax = 0;
+  for (int b = 0; b <= L; ++b) emax = std::max(emax, (long long)c.cap[b] * c.cap[b] * w[b]);
+  for (int i = 0; i < L; ++i) amax = std::max(amax, 2LL * c.cap[i] * c.cap[i + 1]);
+  const bool mf = analog && mixed;
+  auto takef = [&](long long nf) { return take(mf ? (nf + 1) / 2 : 0); };
+  lay.Lf = takef(emax);
+  lay.Rf = takef(emax);
+  lay.xf = takef(c.kry_n);
+  lay.T1f = takef(c.t_size);
+  lay.T2f = takef(c.t_size);
+  lay.Af = takef(amax);
+  lay.total = off;
+  long long ioff = 0;
+  lay.i_chi = ioff;
+  ioff += L + 1;
+  lay.i_oc = ioff;
+  ioff += 1;
+  lay.i_ord = ioff;
+  ioff += SVD_MAX_COLS;
+  lay.i_cand = ioff;
+  ioff += MAX_PROCS;
+  lay.itotal = (ioff + 31) & ~31LL;
+  return lay;
+}
+
+// Slot workspaces owned by a server and shared by every run it admits.
+struct ServePool {
+  int slots = 0;
+  long long ws_stride = 0, wsi_stride = 0;
+  cplx* ws = nullptr;
+  int* wsi = nullptr;
+};
+
 }  // namespace
 
 // One analog run held on the device between yaqs_analog_begin and
@@ -525,7 +630,7 @@ struct yaqs_run {
 static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, const std::vector<int>& chi0,
               const std::vector<int>& w, const std::vector<long long>& mps_off, const std::vector<long long>& env_off,
               const yaqs_mps_desc* psi0, const std::vector<DevProc>& hp, const std::vector<DevObs>& ho,
-              const yaqs_rng_desc* rng, int nqueue) {
+              const yaqs_rng_desc* rng, int nqueue, const ServePool* pool) {
   DevMem& dm = run->dm;
   DevParams& P = run->P;
   const int L = P.L, num_traj = P.num_traj, slots = run->slots, n_obs = run->n_obs, ncols = run->ncols;
@@ -586,8 +691,15 @@ static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, 
   CUDA_TRY(ctx, dm.alloc(&d_traj_out, (size_t)num_traj * std::max(n_obs, 1) * ncols));
   CUDA_TRY(ctx, dm.alloc(&d_flops, slots));
   CUDA_TRY(ctx, dm.alloc(&d_counters, (size_t)slots * 8));
-  CUDA_TRY(ctx, dm.alloc(&d_ws, (size_t)slots * lay.total));
-  CUDA_TRY(ctx, dm.alloc(&d_wsi, (size_t)slots * lay.itotal));
+  if (pool) {
+    d_ws = pool->ws;
+    d_wsi = pool->wsi;
+    P.lay.total = pool->ws_stride;
+    P.lay.itotal = pool->wsi_stride;
+  } else {
+    CUDA_TRY(ctx, dm.alloc(&d_ws, (size_t)slots * lay.total));
+    CUDA_TRY(ctx, dm.alloc(&d_wsi, (size_t)slots * lay.itotal));
+  }
   CUDA_TRY(ctx, cudaMemset(d_status, 0, num_traj * sizeof(int)));
   CUDA_TRY(ctx, cudaMemset(d_queue, 0, nqueue * sizeof(int)));
   CUDA_TRY(ctx, cudaMemset(d_rng_pos, 0, num_traj * sizeof(long long)));
@@ -671,9 +783,10 @@ int yaqs_ctx_destroy(yaqs_ctx* ctx) {
 
 const char* yaqs_last_error(const yaqs_ctx* ctx) { return ctx ? ctx->err.c_str() : g_static_err.c_str(); }
 
-int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
-                      const yaqs_obs_desc* obs, int32_t n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
-                      yaqs_run** out) {
+static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
+                             const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
+                             const yaqs_tev_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out,
+                             const ServePool* pool) {
   if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
   if (!out) return set_err(ctx, YAQS_E_ARG, "null run handle");
   *out = nullptr;
@@ -703,85 +816,16 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   if (nprocs < 0 || nprocs > MAX_PROCS || (nprocs > 0 && !noise->procs)) return set_err(ctx, YAQS_E_ARG, "bad noise descriptor");
 
   // ---- capacities and layouts ----
-  std::vector<int> cap(L + 1), chi0(psi0->chi, psi0->chi + L + 1), w(H->w, H->w + L + 1);
-  for (int b = 0; b <= L; ++b) {
-    long long s = 1;
-    int e = std::min(b, L - b);
-    for (int k = 0; k < e && s < (1 << 20); ++k) s *= 2;
-    long long structural = std::min<long long>(s, cfg->max_bond_dim);
-    cap[b] = (int)std::max<long long>(structural, chi0[b]);
-    if (2 * cap[b] > SVD_MAX_COLS) return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
-  }
-  int capmax = *std::max_element(cap.begin(), cap.end());
-  int wmax = *std::max_element(w.begin(), w.end());
-  std::vector<long long> mps_off(L), env_off(L + 1);
-  long long mps_size = 0, env_size = 0, kry_n = 0, t_size = 0;
-  for (int i = 0; i < L; ++i) {
-    mps_off[i] = mps_size;
-    mps_size += (long long)cap[i] * 2 * cap[i + 1];
-  }
-  for (int b = 0; b <= L; ++b) {
-    env_off[b] = env_size;
-    env_size += (long long)cap[b] * cap[b] * w[b];
-  }
-  for (int i = 0; i < L; ++i) {
-    kry_n = std::max(kry_n, (long long)cap[i] * 2 * cap[i + 1]);
-    t_size = std::max(t_size, (long long)cap[i] * cap[i + 1] * 2 * std::max(w[i], w[i + 1]));
-    if (i + 2 <= L) {
-      kry_n = std::max(kry_n, (long long)cap[i] * 4 * cap[i + 2]);
-      t_size = std::max(t_size, (long long)cap[i] * cap[i + 2] * 4 * std::max(w[i], w[i + 2]));
-    }
-  }
-  const long long tmp = 4LL * capmax * capmax + 16;
-  WsLayout lay;
-  long long off = 0;
-  auto take = [&](long long n) {
-    long long o = off;
-    off += (n + 1) & ~1LL;  // keep 32-byte alignment
-    return o;
-  };
-  lay.psi = take(mps_size);
-  lay.EL = take(env_size);
-  lay.ER = take(env_size);
-  lay.Q = take((long long)(cfg->krylov_dim + 1) * kry_n);
-  lay.T1 = take(t_size);
-  lay.T2 = take(t_size);
-  lay.tA = take(tmp);
-  lay.tB = take(tmp);
-  lay.tC = take(tmp);
-  lay.th = take(kry_n);
-  lay.B = take(tmp);
-  lay.X = take(tmp);
-  lay.Yo = take(tmp);
-  lay.Zo = take(tmp);
-  lay.y = take(2 * capmax + 16);
-  lay.dbl = take((SVD_MAX_COLS + MAX_PROCS) / 2 + 8);
+  std::vector<int> chi0(psi0->chi, psi0->chi + L + 1), w(H->w, H->w + L + 1);
+  Caps caps;
+  if (!plan_caps(L, chi0.data(), w.data(), cfg->max_bond_dim, caps))
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
   const bool mixed = cfg->precision == YAQS_PREC_MIXED;
-  {
-    // mixed form: FP32 copies of one left and one right environment, of a site
-    // tensor and of a Krylov vector, and FP32 contraction intermediates
-    long long emax = 0, amax = 0;
-    for (int b = 0; b <= L; ++b) emax = std::max(emax, (long long)cap[b] * cap[b] * w[b]);
-    for (int i = 0; i < L; ++i) amax = std::max(amax, 2LL * cap[i] * cap[i + 1]);
-    auto takef = [&](long long nf) { return take(mixed ? (nf + 1) / 2 : 0); };
-    lay.Lf = takef(emax);
-    lay.Rf = takef(emax);
-    lay.xf = takef(kry_n);
-    lay.T1f = takef(t_size);
-    lay.T2f = takef(t_size);
-    lay.Af = takef(amax);
-  }
-  lay.total = off;
-  long long ioff = 0;
-  lay.i_chi = ioff;
-  ioff += L + 1;
-  lay.i_oc = ioff;
-  ioff += 1;
-  lay.i_ord = ioff;
-  ioff += SVD_MAX_COLS;
-  lay.i_cand = ioff;
-  ioff += MAX_PROCS;
-  lay.itotal = (ioff + 31) & ~31LL;
+  const WsLayout lay = plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed);
+  const std::vector<int>& cap = caps.cap;
+  const std::vector<long long>& mps_off = caps.mps_off;
+  const std::vector<long long>& env_off = caps.env_off;
+  const long long mps_size = caps.mps_size, kry_n = caps.kry_n;
 
   // ---- MPO sparse matrices (merged two-site W of Algorithms.jl:639-643) ----
   auto Wat = [&](int i, int m, int po, int pi, int mr) {
@@ -850,6 +894,8 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tjm_step_kernel, NT, smem));
   if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
+  if (pool && (lay.total > pool->ws_stride || lay.itotal > pool->wsi_stride))
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "the request's workspace exceeds the server's slot shape");
   size_t free_b = 0, total_b = 0;
   CUDA_TRY(ctx, cudaMemGetInfo(&free_b, &total_b));
   const size_t per_traj = (size_t)mps_size * sizeof(cplx) + (L + 2) * sizeof(int) + 64 +
@@ -857,10 +903,11 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   const size_t per_slot = (size_t)lay.total * sizeof(cplx) + lay.itotal * sizeof(int) + 8 * 8 + 8;
   const size_t fixed = (size_t)mps_size * sizeof(cplx) + (64u << 20);
   const size_t budget = free_b > (size_t)(1u << 30) ? free_b - (size_t)(1u << 30) : 0;
-  if (fixed + (size_t)num_traj * per_traj + per_slot > budget)
+  if (fixed + (size_t)num_traj * per_traj + (pool ? 0 : per_slot) > budget)
     return set_err(ctx, YAQS_E_OOM, "trajectory states do not fit in device memory");
   int slots = std::min(num_traj, ctx->sms * per_sm);
   while (slots > 1 && fixed + (size_t)num_traj * per_traj + (size_t)slots * per_slot > budget) --slots;
+  if (pool) slots = pool->slots;
 
   yaqs_run* run = new yaqs_run();
   std::unique_ptr<yaqs_run> guard(run);
@@ -897,7 +944,7 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   run->smem = smem;
   run->n_obs = n_obs;
   run->ncols = ncols;
-  int st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, cfg->n_times);
+  int st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, cfg->n_times, pool);
   if (st != YAQS_OK) return st;
   std::vector<WMat> views;
   st = upload_wmats(ctx, dm, all, views);
@@ -917,6 +964,12 @@ int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_d
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   *out = guard.release();
   return YAQS_OK;
+}
+
+int yaqs_analog_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                      const yaqs_obs_desc* obs, int32_t n_obs, const yaqs_tev_config* cfg, const yaqs_rng_desc* rng,
+                      yaqs_run** out) {
+  return analog_begin_impl(ctx, psi0, H, noise, obs, n_obs, cfg, rng, out, nullptr);
 }
 
 static int collect_stats(yaqs_run* run, yaqs_run_stats* stats) {
@@ -1108,7 +1161,8 @@ int plan_circuit(yaqs_ctx* ctx, const yaqs_gate_desc* gates, int n, int L, HostC
 
 int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int32_t n_gates,
                   const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
-                  const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out) {
+                  const yaqs_circuit_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out,
+                  const ServePool* pool = nullptr) {
   if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
   *out = nullptr;
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1138,54 +1192,15 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   if (st != YAQS_OK) return st;
 
   // ---- capacities and layout (no environments or Krylov basis) ----
-  std::vector<int> cap(L + 1), chi0(psi0->chi, psi0->chi + L + 1), w(L + 1, 1);
-  for (int b = 0; b <= L; ++b) {
-    long long sz = 1;
-    int e = std::min(b, L - b);
-    for (int k = 0; k < e && sz < (1 << 20); ++k) sz *= 2;
-    cap[b] = (int)std::max<long long>(std::min<long long>(sz, cfg->max_bond_dim), chi0[b]);
-    if (2 * cap[b] > SVD_MAX_COLS) return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
-  }
-  const int capmax = *std::max_element(cap.begin(), cap.end());
-  std::vector<long long> mps_off(L), env_off(L + 1, 0);
-  long long mps_size = 0, kry_n = 0;
-  for (int i = 0; i < L; ++i) {
-    mps_off[i] = mps_size;
-    mps_size += (long long)cap[i] * 2 * cap[i + 1];
-    kry_n = std::max(kry_n, (long long)cap[i] * 2 * cap[i + 1]);
-    if (i + 2 <= L) kry_n = std::max(kry_n, (long long)cap[i] * 4 * cap[i + 2]);
-  }
-  const long long tmp = 4LL * capmax * capmax + 16;
-  WsLayout lay;
-  long long off = 0;
-  auto take = [&](long long n) {
-    long long o = off;
-    off += (n + 1) & ~1LL;
-    return o;
-  };
-  lay.psi = lay.EL = lay.ER = lay.Q = lay.T1 = lay.T2 = take(0);
-  lay.Lf = lay.Rf = lay.xf = lay.T1f = lay.T2f = lay.Af = take(0);
-  lay.tA = take(tmp);
-  lay.tB = take(tmp);
-  lay.tC = take(tmp);
-  lay.th = take(kry_n);
-  lay.B = take(tmp);
-  lay.X = take(tmp);
-  lay.Yo = take(tmp);
-  lay.Zo = take(tmp);
-  lay.y = take(2 * capmax + 16);
-  lay.dbl = take((SVD_MAX_COLS + MAX_PROCS) / 2 + 8);
-  lay.total = off;
-  long long ioff = 0;
-  lay.i_chi = ioff;
-  ioff += L + 1;
-  lay.i_oc = ioff;
-  ioff += 1;
-  lay.i_ord = ioff;
-  ioff += SVD_MAX_COLS;
-  lay.i_cand = ioff;
-  ioff += MAX_PROCS;
-  lay.itotal = (ioff + 31) & ~31LL;
+  std::vector<int> chi0(psi0->chi, psi0->chi + L + 1), w(L + 1, 1);
+  Caps caps;
+  if (!plan_caps(L, chi0.data(), w.data(), cfg->max_bond_dim, caps))
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
+  const WsLayout lay = plan_layout(L, caps, w.data(), false, 0, false);
+  const std::vector<int>& cap = caps.cap;
+  const std::vector<long long>& mps_off = caps.mps_off;
+  const std::vector<long long>& env_off = caps.env_off;
+  const long long mps_size = caps.mps_size, kry_n = caps.kry_n;
 
   // gate noise uses dt = 1 (DigitalTJM.jl:412-413)
   std::vector<DevProc> hp;
@@ -1205,6 +1220,8 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, digital_step_kernel, NT, smem));
   if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
+  if (pool && (lay.total > pool->ws_stride || lay.itotal > pool->wsi_stride))
+    return set_err(ctx, YAQS_E_UNSUPPORTED, "the request's workspace exceeds the server's slot shape");
   size_t free_b = 0, total_b = 0;
   CUDA_TRY(ctx, cudaMemGetInfo(&free_b, &total_b));
   const size_t per_traj = (size_t)mps_size * sizeof(cplx) + (L + 2) * sizeof(int) + 64 +
@@ -1212,10 +1229,11 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   const size_t per_slot = (size_t)lay.total * sizeof(cplx) + lay.itotal * sizeof(int) + 8 * 8 + 8;
   const size_t fixed = (size_t)mps_size * sizeof(cplx) + (size_t)(n_gates + 1) * sizeof(DevGate) + (64u << 20);
   const size_t budget = free_b > (size_t)(1u << 30) ? free_b - (size_t)(1u << 30) : 0;
-  if (fixed + (size_t)num_traj * per_traj + per_slot > budget)
+  if (fixed + (size_t)num_traj * per_traj + (pool ? 0 : per_slot) > budget)
     return set_err(ctx, YAQS_E_OOM, "trajectory states do not fit in device memory");
   int slots = std::min(num_traj, ctx->sms * per_sm);
   while (slots > 1 && fixed + (size_t)num_traj * per_traj + (size_t)slots * per_slot > budget) --slots;
+  if (pool) slots = pool->slots;
 
   yaqs_run* run = new yaqs_run();
   std::unique_ptr<yaqs_run> guard(run);
@@ -1245,7 +1263,7 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   run->smem = smem;
   run->n_obs = n_obs;
   run->ncols = ncols;
-  st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, n_layers + 1);
+  st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, n_layers + 1, pool);
   if (st != YAQS_OK) return st;
 
   // ---- gates in layer order ----
@@ -1532,3 +1550,8 @@ int yaqs_batched_project_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving (yaqs_server_*)
+// ---------------------------------------------------------------------------
+#include "server.cuh"
