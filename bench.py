@@ -90,6 +90,67 @@ def digital_workload(L, depth, num_traj, chi=128):
     return api.MPS(L), c, cfg, nm
 
 
+BATCH_SEED = 0xC0FFEE04
+SERVE_SEED = 0xC0FFEE05
+
+
+def batch_requests(n=64, steps=40, seed=BATCH_SEED):
+    """64 independent analog simulations with seeded parameters: model in
+    {Ising g~U[0.2,1.5], XY init_general_hamiltonian(L,1+a,1-a,0,0,0,0)
+    a~U[0,1], Heisenberg (1,1,1,0,0,h) h~U[0,1]}, L in {8,...,64}, chi_max in
+    {16,...,128}, 64..512 trajectories, lowering and pauli_z noise with
+    gamma~U[0.01,0.2], dt = 0.05, `steps` steps, <Z_i> on every site.  Ising
+    starts from |0...0>, XY and Heisenberg from the Neel state."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        model = int(rng.integers(3))
+        L = int(rng.choice([8, 16, 24, 32, 48, 64]))
+        chi = int(rng.choice([16, 32, 64, 128]))
+        nt = int(rng.integers(64, 513))
+        g1, g2 = rng.uniform(0.01, 0.2, 2)
+        if model == 0:
+            par = float(rng.uniform(0.2, 1.5))
+            H, name, state = api.init_ising(L, 1.0, par), "ising", "zeros"
+        elif model == 1:
+            par = float(rng.uniform(0, 1))
+            H, name, state = api.init_general_hamiltonian(L, 1 + par, 1 - par, 0, 0, 0, 0), "xy", "Neel"
+        else:
+            par = float(rng.uniform(0, 1))
+            H, name, state = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, par), "heisenberg", "Neel"
+        obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+        cfg = api.TimeEvolutionConfig(obs, steps * 0.05, dt=0.05, num_traj=nt, max_bond_dim=chi)
+        nm = api.NoiseModel([{"name": "lowering", "sites": [i], "strength": g1} for i in range(1, L + 1)] +
+                            [{"name": "pauli_z", "sites": [i], "strength": g2} for i in range(1, L + 1)], L)
+        out.append({"name": name, "par": par, "L": L, "chi": chi, "nt": nt, "w": max(H.bond_dims),
+                    "problem": (api.MPS(L, state=state), H, cfg, nm), "seed": 1000 + k})
+    return out
+
+
+def ring_request(rng):
+    """A QAOA ring request: n in {12,20,32,48}, p in {1,2,4} layers of RZZ on
+    every ring edge (odd bonds, even bonds, then the (n,1) edge through the
+    SWAP chain) then RX, angles
+    ~U[0,pi], Pauli X/Y/Z noise 0.005/3 each per gate, chi_max = 64,
+    128..1024 trajectories, <Z_i Z_i+1> on the adjacent pairs."""
+    n = int(rng.choice([12, 20, 32, 48]))
+    p = int(rng.choice([1, 2, 4]))
+    nt = int(rng.integers(128, 1025))
+    c = api.DigitalCircuit(n)
+    for _ in range(p):
+        g, b = rng.uniform(0, np.pi, 2)
+        for i in list(range(1, n, 2)) + list(range(2, n, 2)):  # odd then even bonds
+            c.add_gate(api.Rzz(g), [i, i + 1])
+        c.add_gate(api.Rzz(g), [n, 1])
+        for i in range(1, n + 1):
+            c.add_gate(api.Rx(b), [i])
+    nm = api.NoiseModel([{"name": nme, "sites": [i], "strength": 0.005 / 3} for i in range(1, n + 1)
+                         for nme in ("pauli_x", "pauli_y", "pauli_z")], n)
+    obs = [api.Observable(f"ZZ{i}", np.kron(api.Z, api.Z), [i, i + 1]) for i in range(1, n)]
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=1.0, num_traj=nt, max_bond_dim=64)
+    return {"n": n, "p": p, "nt": nt, "problem": (api.MPS(n), c, cfg, nm)}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -344,6 +405,108 @@ def run_digital(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """64 uneven analog simulations through one server (all admitted runs share
+    each persistent launch); value = total trajectory-steps / wall time."""
+    import torch
+    torch.cuda.set_device(0)
+    from yaqs_julia_b200 import _lib
+    ctx = _lib.Context(0)
+    steps = args.steps if args.steps_given else 40
+    reqs = batch_requests(steps=steps)
+    # bucket order: (chi, MPO width), so similar runs sit next to each other in every launch
+    reqs.sort(key=lambda r: (r["chi"], r["w"], r["L"]))
+    prec = args.precision
+    clocks = ClockSampler(0)
+    with api.Server(max_L=64, max_bond_dim=128, max_mpo_width=5, mixed=True, chunk=args.chunk, ctx=ctx) as srv:
+        clocks.start()
+        t0 = time.perf_counter()
+        ids = [srv.submit(*r["problem"], seed=r["seed"], precision=prec) for r in reqs]
+        res = [srv.result(i) for i in ids]
+        wall = time.perf_counter() - t0
+        ck = clocks.stop()
+        st = srv.stats()
+    total = sum(r["nt"] * steps for r in reqs)
+    line = {"metric": "TJM trajectory-steps/s, 64 uneven analog simulations served together", "value": total / wall,
+            "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 contractions + c128 Lanczos/SVD/QR" if prec == "mixed" else "c128",
+            "data": "synthetic",
+            "config": {"workload": f"64 analog TJM simulations (seed 0x{BATCH_SEED:X}): Ising/XY/Heisenberg, "
+                                   f"L in 8..64, chi_max in 16..128, 64..512 trajectories, lowering+dephasing, "
+                                   f"dt=0.05, {steps} steps; one server, chunk={args.chunk}",
+                       "precision": prec, "trajectory_steps": total},
+            "wall_s": wall, "device_busy_s": st["busy_s"], "launches": st["launches"], "slots": st["slots"],
+            "latency_p50_s": st["latency_p50_s"], "latency_p99_s": st["latency_p99_s"],
+            "queue_p50_s": st["queue_p50_s"], "queue_p99_s": st["queue_p99_s"], "clocks": ck,
+            "max_bond_reached": {f"chi{c}": int(max([r.max_bond.max() for q, r in zip(reqs, res) if q["chi"] == c],
+                                                    default=0)) for c in (16, 32, 64, 128)},
+            "jumps": int(sum(r.stats["jumps"] for r in res))}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Poisson arrivals of QAOA ring requests at 0.8 x the measured capacity."""
+    import torch
+    torch.cuda.set_device(0)
+    from yaqs_julia_b200 import _lib
+    ctx = _lib.Context(0)
+    rng = np.random.default_rng(SERVE_SEED)
+
+    def work(r):  # trajectory-layers of a request
+        return r["nt"] * api.digital_plan(r["problem"][1])[0]
+
+    # mean work per request of the arrival distribution
+    wrng = np.random.default_rng(SERVE_SEED + 1)
+    mean_work = float(np.mean([work(ring_request(wrng)) for _ in range(400)]))
+    with api.Server(max_L=48, max_bond_dim=64, max_mpo_width=1, mixed=False, chunk=args.chunk, ctx=ctx) as srv:
+        # capacity: trajectory-layers/s of a calibration set submitted at once,
+        # turned into requests/s with the distribution's mean work per request
+        calib = [ring_request(rng) for _ in range(48)]
+        t0 = time.perf_counter()
+        ids = [srv.submit(*r["problem"], seed=SERVE_SEED + k) for k, r in enumerate(calib)]
+        for i in ids:
+            srv.result(i)
+        cap_work = sum(work(r) for r in calib) / (time.perf_counter() - t0)
+        cap = cap_work / mean_work
+        lam = 0.8 * cap
+        n_req = max(8, int(round(lam * args.duration)))
+        reqs = [ring_request(rng) for _ in range(n_req)]
+        gaps = rng.exponential(1.0 / lam, n_req)
+        clocks = ClockSampler(0)
+        base = srv.stats()
+        clocks.start()
+        t0 = time.perf_counter()
+        ids = []
+        t_next = t0
+        for k, r in enumerate(reqs):
+            t_next += gaps[k]
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(*r["problem"], seed=SERVE_SEED + 100 + k))
+        res = [srv.result(i) for i in ids]
+        wall = time.perf_counter() - t0
+        ck = clocks.stop()
+        st = srv.stats()
+    lat = np.array([r.times[2] for r in res])
+    qd = np.array([r.times[0] for r in res])
+    layers = sum(q["nt"] * q["p"] for q in reqs)
+    line = {"metric": "served digital TJM requests: p50/p99 latency at 0.8 x capacity", "value": float(np.percentile(lat, 50)),
+            "unit": "s (p50 latency)", "n_gpus": 1, "steps": n_req, "warmup": len(calib), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"QAOA ring requests (seed 0x{SERVE_SEED:X}): n in {{12,20,32,48}}, p in {{1,2,4}}, "
+                                   "Pauli XYZ 0.005/3 per gate, chi_max=64, 128..1024 trajectories, Poisson arrivals "
+                                   f"at 0.8 x measured capacity ({cap:.2f} req/s) for {args.duration:.0f} s",
+                       "chunk": args.chunk},
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+            "queue_p50_s": float(np.percentile(qd, 50)), "queue_p99_s": float(np.percentile(qd, 99)),
+            "capacity_req_s": cap, "capacity_traj_layers_s": cap_work, "mean_traj_layers_per_req": mean_work,
+            "offered_req_s": lam, "completed": len(res), "wall_s": wall,
+            "trajectory_layers_per_s": layers / wall, "device_busy_s": st["busy_s"] - base["busy_s"],
+            "launches": st["launches"] - base["launches"], "clocks": ck}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args):
     ws, rank, local, dist = dist_setup()
     import torch
@@ -447,7 +610,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
-    ap.add_argument("--workload", default="analog", choices=["analog", "digital"])
+    ap.add_argument("--workload", default="analog", choices=["analog", "digital", "batch", "serve"])
+    ap.add_argument("--chunk", type=int, default=2, help="batch/serve: positions each run advances per launch")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of Poisson arrivals")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="analog contraction precision: fp64, or mixed (complex FP32 on the tensor cores)")
     ap.add_argument("--warmup", type=int, default=3)
@@ -473,6 +638,10 @@ def main():
         run_reference(args)
     elif args.workload == "digital":
         run_digital(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 
