@@ -3,7 +3,9 @@
 
 Workload (default): the L=30 Heisenberg chain H = sum(XX+YY+ZZ) + 0.3 sum Z
 (init_general_hamiltonian(30,1,1,1,0,0,0.3)), dephasing (pauli_z, gamma=0.05)
-on every site, dt=0.05, 2-site TDVP, max bond dimension 64, threshold 1e-9,
+on every site, dt=0.05, 1-site TDVP with 2-site growth up to bond dimension
+64 (the local dynamic TDVP of the Python lineage; --tdvp 2site runs the Julia
+reference's two_site_tdvp! instead), threshold 1e-9,
 second-order TJM with sampling at every time index, <Z_i> on all 30 sites
 plus the half-chain entropy, 1024 trajectories per GPU, Philox draws.  The
 start state is an MPS with every bulk bond already at 64 (Gaussian
@@ -50,6 +52,10 @@ from yaqs_julia_b200 import _abi as A  # noqa: E402
 from yaqs_julia_b200 import api  # noqa: E402
 
 METRIC = "TJM trajectory-steps/s (L=30 Heisenberg, chi=64, 1024 trajectories)"
+TDVP_NAMES = {"dynamic": A.YAQS_TDVP_DYNAMIC, "2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE}
+TDVP = [A.YAQS_TDVP_DYNAMIC]  # set from --tdvp
+TDVP_DESC = {"dynamic": "1-site TDVP with 2-site growth (local dynamic TDVP)", "2site": "2-site TDVP",
+             "1site": "1-site TDVP"}
 UNIT = "trajectory-steps/s"
 SEED = 0xC0FFEE02
 
@@ -250,7 +256,7 @@ def cpu_sample(L, chi, start):
     from oracle import oracle as O
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     psi, H, cfg, nm = workload(L, chi, 3, cores, start)
-    d = api.Descriptors(psi, H, cfg, nm, seed=SEED)
+    d = api.Descriptors(psi, H, cfg, nm, seed=SEED, tdvp_mode=TDVP[0])
     t0 = time.perf_counter()
     O.analog_run(d, nthreads=cores)
     dt = time.perf_counter() - t0
@@ -301,6 +307,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": f"L={args.L} Heisenberg h=0.3, chi={args.chi}, dephasing 0.05, dt=0.05, "
+                                   f"{TDVP_DESC[args.tdvp]}, "
                                    f"start={args.start}", "L": args.L, "chi": args.chi},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -517,7 +524,7 @@ def run_ours(args):
     n_times = args.warmup + args.steps + 1
     psi, H, cfg, nm = workload(L, chi, n_times, nt, args.start)
     prec = A.YAQS_PREC_MIXED if args.precision == "mixed" else A.YAQS_PREC_FP64
-    desc = api.Descriptors(psi, H, cfg, nm, seed=SEED, traj_offset=rank * nt, precision=prec)
+    desc = api.Descriptors(psi, H, cfg, nm, seed=SEED, traj_offset=rank * nt, precision=prec, tdvp_mode=TDVP[0])
     sess = api.Session(desc, ctx)
     for _ in range(args.warmup):
         sess.advance(1)
@@ -547,14 +554,15 @@ def run_ours(args):
     barrier_sync(dist)
     t0 = time.perf_counter()
     e2e_desc = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt,
-                               precision=prec)
+                               precision=prec, tdvp_mode=TDVP[0])
     e2e_res = api.run_descriptors(e2e_desc, ctx)
     barrier_sync(dist)
     e2e_s = reduce_max(dist, time.perf_counter() - t0)
     err = None
     if args.precision == "mixed":
         # the same run (same draws) in the FP64 form: error of every observable
-        d64 = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt)
+        d64 = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt,
+                              tdvp_mode=TDVP[0])
         r64 = api.run_descriptors(d64, ctx)
         dz = np.abs(e2e_res.trajectories[:, :L] - r64.trajectories[:, :L])
         ds = np.abs(e2e_res.trajectories[:, L] - r64.trajectories[:, L])
@@ -576,10 +584,10 @@ def run_ours(args):
                 "dtype": "c64 contractions (3xTF32 tensor cores) + c128 Lanczos/SVD/QR/norms"
                 if args.precision == "mixed" else "c128", "data": "synthetic",
                 "config": {"workload": f"analog TJM, L={L} Heisenberg XXX h=0.3, dephasing gamma=0.05, dt=0.05, "
-                                       f"2-site TDVP chi_max={chi}, thr=1e-9, {nt} trajectories per GPU, "
+                                       f"{TDVP_DESC[args.tdvp]} chi_max={chi}, thr=1e-9, {nt} trajectories per GPU, "
                                        f"start={'saturated chi MPS' if args.start == 'sat' else 'Neel'}",
                            "L": L, "chi": chi, "num_traj": nt, "dt": 0.05, "parallelism": f"replicas x{ws}",
-                           "precision": args.precision,
+                           "precision": args.precision, "tdvp": args.tdvp,
                            "l2": "inputs larger than L2: %d trajectory states of up to %.1f MB each" % (
                                nt, sum(min(2 ** min(b, L - b), chi) * 2 * min(2 ** min(b + 1, L - b - 1), chi)
                                        for b in range(L)) * 16 / 1e6)},
@@ -611,6 +619,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--workload", default="analog", choices=["analog", "digital", "batch", "serve"])
+    ap.add_argument("--tdvp", default="dynamic", choices=list(TDVP_NAMES),
+                    help="analog sweep: dynamic (1-site TDVP with 2-site growth up to chi, the configuration's "
+                         "mode), 2site (the Julia reference's two_site_tdvp!) or 1site")
     ap.add_argument("--chunk", type=int, default=2, help="batch/serve: positions each run advances per launch")
     ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of Poisson arrivals")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
@@ -625,6 +636,7 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="enable the engine's per-phase device timers and report them (not for timing runs)")
     args = ap.parse_args()
+    TDVP[0] = TDVP_NAMES[args.tdvp]
     args.steps_given = args.steps is not None
     if args.steps is None:
         args.steps = 2

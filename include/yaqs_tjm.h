@@ -147,7 +147,21 @@ typedef struct {
   double krylov_exit_tol;
   int32_t precision;
   int32_t traj_offset;
+  int32_t tdvp_mode;      /* YAQS_TDVP_* */
 } yaqs_tev_config;
+
+/*
+ * TDVP sweep of every time step.
+ * 2SITE:   two_site_tdvp! (Algorithms.jl:580-760), the reference's analog path.
+ * 1SITE:   single_site_tdvp! (Algorithms.jl:472-533): bond dimensions stay
+ *          those of the start state.
+ * DYNAMIC: the Python lineage's local_dynamic_tdvp
+ *          (mqt-yaqs/src/mqt/yaqs/core/methods/tdvp.py:667-855): per bond a
+ *          2-site update while the bond is below max_bond_dim (its split keeps
+ *          min(rank, max_bond_dim) values, no threshold), a 1-site update with
+ *          bond back-evolution once it has reached it.
+ */
+enum { YAQS_TDVP_2SITE = 0, YAQS_TDVP_1SITE = 1, YAQS_TDVP_DYNAMIC = 2 };
 
 /* Counters of one run (summed over trajectories). */
 typedef struct {

@@ -804,7 +804,8 @@ void split_theta(const Ten& Th, int rule, double thr, int max_bond, bool s_left,
   cnt.svds++;
   const int keep = rule == 0   ? keep_tdvp(o.S, thr, max_bond)
                    : rule == 1 ? keep_relative(o.S, thr, max_bond)
-                               : keep_tebd(o.S, thr, max_bond);
+                   : rule == 2 ? keep_tebd(o.S, thr, max_bond)
+                               : std::max(1, std::min((int)o.S.size(), max_bond));  // dynamic TDVP split
   vector<cd> Y = svd_vectors(o, keep);
   Lo = Ten(Th.l, 2, keep);
   Ro = Ten(keep, 2, Th.r);
@@ -874,6 +875,7 @@ struct Problem {
   const double* uniforms;
   long long stride;
   int traj_offset;
+  int tdvp_mode = YAQS_TDVP_2SITE;
 };
 
 // Hermitian matrix exponential exp(c * H) for small H (n<=4) via Jacobi on
@@ -1031,7 +1033,16 @@ struct Sweeper {
     split_left(s, i, dts);
   }
 
-  void sweep(State& s) {  // _tdvp_sweep_hamiltonian_2site!, Algorithms.jl:580-603
+  void sweep(State& s) {
+    if (P.tdvp_mode == YAQS_TDVP_1SITE)
+      sweep_1site(s);
+    else if (P.tdvp_mode == YAQS_TDVP_DYNAMIC)
+      sweep_dynamic(s);
+    else
+      sweep_2site(s);
+  }
+
+  void sweep_2site(State& s) {  // _tdvp_sweep_hamiltonian_2site!, Algorithms.jl:580-603
     shift_oc(s, 0);
     const int L = s.L;
     const double dt = P.dt;
@@ -1039,6 +1050,141 @@ struct Sweeper {
     for (int i = 0; i <= L - 3; ++i) forward(s, i, dt / 2);
     if (L >= 2) split_left(s, L - 2, dt);
     for (int i = L - 3; i >= 0; --i) backward(s, i, dt / 2);
+  }
+
+  // exp(-i dt H_bond) C for the bond matrix C (k x r) between EL and ER
+  // (project_bond, Algorithms.jl:222-226).
+  vector<cd> evolve_bond(const Env& Le, const Env& Re, int k, int r, const vector<cd>& C, double dt) {
+    auto op = [&](const vector<cd>& in, vector<cd>& out) {
+      const int w = Le.w;
+      // T1[a, m, kr] = sum_k L[a, m, k] C[k, kr];  out[a, b] = sum_{m, kr} T1[a, m, kr] R[b, m, kr]
+      vector<cd> T1((size_t)Le.b * w * r);
+      matmul(Le.b * w, r, k, Le.v.data(), in.data(), T1.data());
+      out.assign((size_t)Le.b * Re.b, 0.0);
+      for (int b = 0; b < Re.b; ++b)
+        for (int kr = 0; kr < r; ++kr)
+          for (int m = 0; m < w; ++m) {
+            const cd rv = Re.at(b, m, kr);
+            if (rv == cd(0)) continue;
+            const cd* t = &T1[(size_t)Le.b * (m + (size_t)w * kr)];
+            cd* o = &out[(size_t)Le.b * b];
+            for (int a = 0; a < Le.b; ++a) o[a] += t[a] * rv;
+          }
+      cnt.flops += 8.0 * ((double)Le.b * w * k * r + (double)Le.b * w * r * Re.b);
+    };
+    return expm_krylov(op, C, dt, P.kp, cnt);
+  }
+
+  // site i = Q R (thin QR), Q -> site i, EL[i+1], R evolved by dtb and
+  // absorbed into site i+1.
+  void qr_bond_forward(State& s, int i, double dtb) {
+    Ten& A = s.t[i];
+    vector<cd> Q, R;
+    house_qr(A.l * A.d, A.r, A.v.data(), Q, R);
+    const int rn = std::min(A.l * A.d, A.r), r = A.r;
+    Ten An(A.l, A.d, rn);
+    An.v = Q;
+    A = std::move(An);
+    EL[i + 1] = update_left(s.t[i], P.W[i], EL[i]);
+    R = evolve_bond(EL[i + 1], ER[i + 1], rn, r, R, dtb);
+    Ten& N = s.t[i + 1];
+    Ten Nn(rn, N.d, N.r);
+    matmul(rn, N.d * N.r, r, R.data(), N.v.data(), Nn.v.data());
+    N = std::move(Nn);
+  }
+
+  // site i = L Q (thin LQ), Q -> site i, ER[i], L evolved by dtb and
+  // absorbed into site i-1.
+  void lq_bond_backward(State& s, int i, double dtb) {
+    Ten& A = s.t[i];
+    vector<cd> Lm, Qm;
+    house_lq(A.l, A.d * A.r, A.v.data(), Lm, Qm);
+    const int rn = std::min(A.l, A.d * A.r), l = A.l;
+    Ten An(rn, A.d, A.r);
+    An.v = Qm;
+    A = std::move(An);
+    ER[i] = update_right(s.t[i], P.W[i], ER[i + 1]);
+    Lm = evolve_bond(EL[i], ER[i], l, rn, Lm, dtb);
+    Ten& Pv = s.t[i - 1];
+    Ten Pn(Pv.l, Pv.d, rn);
+    matmul(Pv.l * Pv.d, rn, l, Pv.v.data(), Lm.data(), Pn.v.data());
+    Pv = std::move(Pn);
+  }
+
+  void evolve_site(State& s, int i, double dts) {
+    s.t[i].v = evolve(EL[i], ER[i + 1], P.W[i], s.t[i], dts);
+  }
+
+  // _tdvp_sweep_hamiltonian_1site!, Algorithms.jl:472-533
+  void sweep_1site(State& s) {
+    shift_oc(s, 0);
+    const int L = s.L;
+    const double dt = P.dt;
+    init_envs(s);
+    for (int i = 0; i < L; ++i) {
+      evolve_site(s, i, dt / 2);
+      if (i < L - 1) qr_bond_forward(s, i, -dt / 2);
+    }
+    for (int i = L - 1; i >= 0; --i) {
+      evolve_site(s, i, dt / 2);
+      if (i > 0) lq_bond_backward(s, i, -dt / 2);
+    }
+    s.oc = 0;
+  }
+
+  // local_dynamic_tdvp (mqt-yaqs/src/mqt/yaqs/core/methods/tdvp.py:667-855),
+  // in the Julia tensor layout: a 2-site update (split keeping
+  // min(rank, max_bond) values) while the bond is below max_bond, else a
+  // 1-site update with bond back-evolution; the last site (first site on
+  // the way back) takes a 1-site update once a 1-site step reached it.
+  void sweep_dynamic(State& s) {
+    shift_oc(s, 0);
+    const int L = s.L;
+    const double dt = P.dt;
+    init_envs(s);
+    bool lock = false;
+    for (int i = 0; i < L; ++i) {  // left to right (tdvp.py:706-781)
+      const int bond = s.t[i].r;
+      if (bond >= P.max_bond || lock) {
+        evolve_site(s, i, dt / 2);
+        if (i != L - 1) qr_bond_forward(s, i, -dt / 2);
+        if (i == L - 2) lock = true;
+      } else if (i == L - 1) {
+        continue;
+      } else {
+        Ten Th = merge(s.t[i], s.t[i + 1]);
+        Th.v = evolve(EL[i], ER[i + 2], P.W2[i], Th, dt / 2);
+        Ten U, V;
+        split_theta(Th, 3, P.thr, P.max_bond, false, U, V, cnt);
+        s.t[i] = U;
+        s.t[i + 1] = V;
+        EL[i + 1] = update_left(s.t[i], P.W[i], EL[i]);
+        if (i != L - 2) s.t[i + 1].v = evolve(EL[i + 1], ER[i + 2], P.W[i + 1], s.t[i + 1], -dt / 2);
+      }
+    }
+    lock = false;
+    for (int i = L - 1; i >= 0; --i) {  // right to left (tdvp.py:786-855)
+      const int bond = s.t[i].l;
+      if (bond >= P.max_bond || lock) {
+        evolve_site(s, i, dt / 2);
+        if (i != 0) {
+          lq_bond_backward(s, i, -dt / 2);
+          if (i == 1) lock = true;
+        }
+      } else if (i == 0) {
+        continue;
+      } else {
+        Ten Th = merge(s.t[i - 1], s.t[i]);
+        Th.v = evolve(EL[i - 1], ER[i + 1], P.W2[i - 1], Th, dt / 2);
+        Ten U, V;
+        split_theta(Th, 3, P.thr, P.max_bond, true, U, V, cnt);
+        s.t[i - 1] = U;
+        s.t[i] = V;
+        ER[i] = update_right(s.t[i], P.W[i], ER[i + 1]);
+        if (i != 1) s.t[i - 1].v = evolve(EL[i - 1], ER[i], P.W[i - 1], s.t[i - 1], -dt / 2);
+      }
+    }
+    s.oc = 0;
   }
 };
 
@@ -1393,6 +1539,11 @@ bool load_problem(Problem& P, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
   P.kp.tol = cfg->krylov_tol;
   P.kp.exit_tol = cfg->krylov_exit_tol;
   P.traj_offset = cfg->traj_offset;
+  P.tdvp_mode = cfg->tdvp_mode;
+  if (P.tdvp_mode < YAQS_TDVP_2SITE || P.tdvp_mode > YAQS_TDVP_DYNAMIC) {
+    err = "bad tdvp_mode";
+    return false;
+  }
   if (P.n_times < 1 || P.num_traj < 1 || P.max_bond < 1 || P.kp.kdim < 1) {
     err = "bad config";
     return false;

@@ -4,7 +4,7 @@ The fixtures are outputs the reference itself committed (it cannot be run
 here: Julia is not installed).  This script only copies and subsets them:
 
 * tdvp_benchmark.csv   <- tdvp_benchmark_results.csv (test/benchmark_tdvp.jl:94-216):
-                          L=6, dt=0.05, T=2, <Z> at sites 1,3,6; Exact and 2TDVP rows.
+                          L=6, dt=0.05, T=2, <Z> at sites 1,3,6; Exact, 1TDVP and 2TDVP rows.
 * large_ising.csv      <- large_ising_results.csv (test/simulate_large_ising.jl:31-98):
                           L=30 Ising 2TDVP, chi<=32, <Z> at sites 1,16,30.
 * tjm_vs_qutip_a.csv,
@@ -30,7 +30,7 @@ def main():
         w = csv.writer(g)
         w.writerow(next(r))
         for row in r:
-            if row[1] in ("Exact", "2TDVP"):
+            if row[1] in ("Exact", "1TDVP", "2TDVP"):
                 w.writerow(row)
     shutil.copyfile(os.path.join(REF, "large_ising_results.csv"), os.path.join(HERE, "large_ising.csv"))
     base = os.path.join(REF, "00_safety_checks_full_algorithms", "analogTJM_check")

@@ -180,3 +180,57 @@ def test_run_fills_observables_like_reference():
         assert o.trajectories.shape == (4, len(cfg.times))
         assert np.allclose(o.results, res.trajectories[:, k, :].mean(0))
     assert np.allclose(cfg.observables[0].trajectories[:, 0], 1.0)
+
+
+def _compare_mode(oracle, psi, H, cfg, nm, mode, uniforms, rtol):
+    d = api.Descriptors(psi, H, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=uniforms, tdvp_mode=mode)
+    ref, chi_ref, st_ref = oracle.analog_run(d)
+    got = api.run_descriptors(d)
+    err = np.abs(got.trajectories - ref)
+    assert err.max() <= rtol, err.max()
+    assert np.array_equal(got.max_bond, chi_ref)
+    assert got.stats["jumps"] == st_ref["jumps"]
+    return got
+
+
+def test_single_site_tdvp_trajectories_match_oracle(oracle):
+    """single_site_tdvp! (Algorithms.jl:472-533) inside the TJM step."""
+    L = 8
+    H = api.init_ising(L, 1.0, 0.7)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.5, dt=0.05, num_traj=6, max_bond_dim=8)
+    nm = api.NoiseModel([{"name": "lowering", "sites": [i], "strength": 0.1} for i in range(1, L + 1)] +
+                        [{"name": "pauli_z", "sites": [i], "strength": 0.1} for i in range(1, L + 1)], L)
+    u = np.random.default_rng(21).random((6, api.max_draws(cfg)))
+    psi = api.MPS(L).pad_bond_dimension(4, 1e-3, seed=2)
+    got = _compare_mode(oracle, psi, H, cfg, nm, A.YAQS_TDVP_1SITE, u, 1e-10)
+    assert got.max_bond.max() <= 4
+
+
+@pytest.mark.parametrize("chi", [4, 16])
+def test_dynamic_tdvp_trajectories_match_oracle(oracle, chi):
+    """local_dynamic_tdvp (mqt-yaqs tdvp.py:667-855) inside the TJM step: 2-site
+    growth below chi_max, 1-site updates at it."""
+    L = 10
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = ([api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)] +
+           [api.Observable("S", None, L // 2, kind="entropy")])
+    cfg = api.TimeEvolutionConfig(obs, 0.5, dt=0.05, num_traj=6, max_bond_dim=chi)
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    u = np.random.default_rng(22).random((6, api.max_draws(cfg)))
+    got = _compare_mode(oracle, api.MPS(L, state="Neel"), H, cfg, nm, A.YAQS_TDVP_DYNAMIC, u, 1e-10)
+    assert got.max_bond.max() == min(chi, 2 ** (L // 2))
+
+
+def test_dynamic_tdvp_mixed_precision(oracle):
+    L = 10
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.5, dt=0.05, num_traj=4, max_bond_dim=8)
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    u = np.random.default_rng(23).random((4, api.max_draws(cfg)))
+    d = api.Descriptors(api.MPS(L, state="Neel"), H, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=u,
+                        tdvp_mode=A.YAQS_TDVP_DYNAMIC, precision=A.YAQS_PREC_MIXED)
+    ref, _, _ = oracle.analog_run(d)
+    got = api.run_descriptors(d)
+    assert np.abs(got.trajectories - ref).max() < 1e-5

@@ -25,6 +25,7 @@ YAQS_RNG_INJECTED = 1
 
 YAQS_PREC_FP64 = 0
 YAQS_PREC_MIXED = 1
+YAQS_TDVP_2SITE, YAQS_TDVP_1SITE, YAQS_TDVP_DYNAMIC = 0, 1, 2
 
 STATUS_NAMES = {
     0: "YAQS_OK", 1: "YAQS_E_ARG", 2: "YAQS_E_OOM", 3: "YAQS_E_NONFINITE",
@@ -72,7 +73,7 @@ class TevConfig(C.Structure):
                 ("truncation_threshold", C.c_double), ("order", C.c_int32),
                 ("sample_timesteps", C.c_int32), ("krylov_dim", C.c_int32),
                 ("krylov_tol", C.c_double), ("krylov_exit_tol", C.c_double),
-                ("precision", C.c_int32), ("traj_offset", C.c_int32)]
+                ("precision", C.c_int32), ("traj_offset", C.c_int32), ("tdvp_mode", C.c_int32)]
 
 
 YAQS_GATE_BARRIER = 0

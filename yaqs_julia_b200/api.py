@@ -178,6 +178,29 @@ class MPS:
     def bond_dims(self):
         return [1] + [t.shape[2] for t in self.tensors]
 
+    def pad_bond_dimension(self, target_dim: int, noise_scale: float = 1e-8, seed: int = 0):
+        """pad_bond_dimension! (MPS.jl:453-494): grow every bond below
+        target_dim to target_dim, filling the new slices with complex noise of
+        amplitude noise_scale (seeded here; the reference draws from the global
+        RNG).  The engine normalises the state before it evolves it."""
+        rng = np.random.default_rng(seed)
+        for i in range(self.length - 1):
+            A, B = self.tensors[i], self.tensors[i + 1]
+            r = A.shape[2]
+            if r >= target_dim:
+                continue
+            nA = np.zeros((A.shape[0], A.shape[1], target_dim), dtype=np.complex128)
+            nA[:, :, :r] = A
+            nA[:, :, r:] = noise_scale * (rng.standard_normal((A.shape[0], A.shape[1], target_dim - r)) +
+                                          1j * rng.standard_normal((A.shape[0], A.shape[1], target_dim - r)))
+            nB = np.zeros((target_dim, B.shape[1], B.shape[2]), dtype=np.complex128)
+            nB[:r] = B
+            nB[r:] = noise_scale * (rng.standard_normal((target_dim - r, B.shape[1], B.shape[2])) +
+                                    1j * rng.standard_normal((target_dim - r, B.shape[1], B.shape[2])))
+            self.tensors[i] = np.asfortranarray(nA)
+            self.tensors[i + 1] = np.asfortranarray(nB)
+        return self
+
     def to_vec(self) -> np.ndarray:
         """MPS.to_vec (src/MPS.jl:766-775): site 1 is the fastest index."""
         v = self.tensors[0]
@@ -376,7 +399,8 @@ class Descriptors:
     def __init__(self, psi0: MPS, H: MPO, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None,
                  *, rng_mode: int = A.YAQS_RNG_PHILOX, seed: int = 0, uniforms: np.ndarray | None = None,
                  krylov_dim: int = 25, krylov_tol: float = 1e-10, krylov_exit_tol: float = 1e-12,
-                 precision: int = A.YAQS_PREC_FP64, traj_offset: int = 0, num_traj: int | None = None):
+                 precision: int = A.YAQS_PREC_FP64, traj_offset: int = 0, num_traj: int | None = None,
+                 tdvp_mode: int = A.YAQS_TDVP_2SITE):
         L = psi0.length
         if H.length != L:
             raise ValueError("MPO and MPS lengths differ")
@@ -444,7 +468,7 @@ class Descriptors:
         self.cfg = A.TevConfig(sim_params.dt, len(sim_params.times), nt, sim_params.max_bond_dim,
                                sim_params.truncation_threshold, sim_params.order,
                                int(sim_params.sample_timesteps), krylov_dim, krylov_tol, krylov_exit_tol,
-                               precision, traj_offset)
+                               precision, traj_offset, tdvp_mode)
         self.n_out = len(sim_params.times) if sim_params.sample_timesteps else 1
         # rng
         if rng_mode == A.YAQS_RNG_INJECTED:

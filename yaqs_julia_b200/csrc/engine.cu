@@ -806,6 +806,8 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
     return set_err(ctx, YAQS_E_ARG, "bad config (n_times, num_traj, max_bond_dim, dt)");
   if (cfg->krylov_dim < 1 || cfg->krylov_dim > KRYLOV_MAX) return set_err(ctx, YAQS_E_ARG, "krylov_dim must be in [1, 32]");
   if (cfg->order != 1 && cfg->order != 2) return set_err(ctx, YAQS_E_ARG, "order must be 1 or 2");
+  if (cfg->tdvp_mode < YAQS_TDVP_2SITE || cfg->tdvp_mode > YAQS_TDVP_DYNAMIC)
+    return set_err(ctx, YAQS_E_ARG, "tdvp_mode must be YAQS_TDVP_2SITE, _1SITE or _DYNAMIC");
   if (cfg->precision != YAQS_PREC_FP64 && cfg->precision != YAQS_PREC_MIXED)
     return set_err(ctx, YAQS_E_ARG, "precision must be YAQS_PREC_FP64 or YAQS_PREC_MIXED");
   if (n_obs < 0 || n_obs > MAX_OBS) return set_err(ctx, YAQS_E_ARG, "n_obs out of range");
@@ -871,6 +873,8 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
       return Wat(i, ml, po, pi, mr);
     }));
   }
+  for (int b = 0; b <= L; ++b)  // bond: identity on the MPO bond, physical dimension 1
+    all.push_back(build_wmat(w[b], w[b], [&](int o, int in) { return hcd(o == in ? 1.0 : 0.0, 0.0); }));
   for (auto& m : all)
     if (m.ni > WAPPLY_MAXI || m.no > WAPPLY_MAXI || (int)m.val.size() > WAPPLY_MAXNNZ)
       return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO too wide for the sparse MPO apply");
@@ -919,6 +923,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   P.n_times = cfg->n_times;
   P.order = cfg->order;
   P.mixed = mixed ? 1 : 0;
+  P.tdvp_mode = cfg->tdvp_mode;
   P.sample_ts = cfg->sample_timesteps != 0;
   P.max_bond = cfg->max_bond_dim;
   P.nobs = n_obs;
@@ -956,6 +961,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   P.wm_heff2 = d_views + L;
   P.wm_envL = d_views + L + (L - 1);
   P.wm_envR = d_views + L + (L - 1) + L;
+  P.wm_bond = d_views + L + (L - 1) + L + L;
 
   run->launches.push_back(0);
   for (int j = (cfg->order == 2 ? 2 : 1); j < cfg->n_times; ++j) run->launches.push_back(j);

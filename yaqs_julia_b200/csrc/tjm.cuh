@@ -48,6 +48,7 @@ struct DevParams {
   int L, n_times, order, sample_ts, max_bond, nobs, nprocs, noise_present, all_zero, rng_mode, num_traj,
       traj_offset, ncols;
   int mixed;  // H_eff and environment contractions in complex FP32 on the tensor cores
+  int tdvp_mode;  // YAQS_TDVP_2SITE / _1SITE / _DYNAMIC
   double dt, thr;
   KrylovCfg kc;
   unsigned long long seed;
@@ -60,6 +61,7 @@ struct DevParams {
   const WMat* wm_heff2;      // [L-1]
   const WMat* wm_envL;       // [L]
   const WMat* wm_envR;       // [L]
+  const WMat* wm_bond;       // [L+1] identity on the MPO bond (project_bond as a D = 1 H_eff)
   const long long* env_off;  // [L+1]
   long long kry_n;
   const DevProc* procs;
@@ -450,7 +452,8 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
   if (threadIdx.x == 0) {
     int keep = rule == 0   ? keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond)
                : rule == 1 ? keep_relative(w.sig, res.p, c.P.thr, c.P.max_bond)
-                           : keep_tebd(w.sig, res.p, c.P.thr, c.P.max_bond);
+               : rule == 2 ? keep_tebd(w.sig, res.p, c.P.thr, c.P.max_bond)
+                           : max(1, min(res.p, c.P.max_bond));  // dynamic TDVP split (tdvp.py:144-152)
     c.sm.bcast_i[0] = keep;
     c.cnt[2] += 1;
     c.cnt[5] += res.sweeps;
@@ -485,15 +488,161 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
   set_chi(c, s, i + 1, keep);
 }
 
-__device__ void tdvp_sweep(Ctx& c, const DState& s) {
-  ProfScope prof_scope_(PF_SWEEP);
+// _init_envs (Algorithms.jl:802-819) after moving the centre to site 0.
+__device__ void init_envs(Ctx& c, const DState& s) {
   const int L = c.P.L;
-  const double dt = c.P.dt;
   shift_oc(c, s, 0);
-  cplx* th = c.ws + c.P.lay.th;
   identity_env(c, envR(c, L), s.chi[L], c.P.w[L]);
   for (int i = L - 1; i >= 1; --i) update_right(c, s, i);
   identity_env(c, envL(c, 0), s.chi[0], c.P.w[0]);
+}
+
+// exp(-i dtb H_bond) C on bond b (project_bond, Algorithms.jl:222-226), C (k x r).
+__device__ void evolve_bond(Ctx& c, cplx* C, int k, int r, int b, double dtb) {
+  evolve(c, C, k, 1, r, b, b, c.P.wm_bond[b], dtb);
+}
+
+// Site i = Q R (thin QR): Q -> site i, EL[i+1] from it, R evolved by dtb on
+// bond i+1 and absorbed into site i+1 (Algorithms.jl:491-505).
+__device__ void qr_bond_forward(Ctx& c, const DState& s, int i, double dtb) {
+  const int l = s.chi[i], r = s.chi[i + 1], m = 2 * l, rn = min(m, r);
+  const int r2 = s.chi[i + 2];
+  cplx* A = site_ptr(c, s, i);
+  cplx* An = site_ptr(c, s, i + 1);
+  cplx* H = c.ws + c.P.lay.tA;
+  cplx* Rb = c.ws + c.P.lay.tB;
+  cplx* T = c.ws + c.P.lay.tC;
+  cta_copy(H, A, (long long)m * r);
+  __syncthreads();
+  dev_qr_factor(H, m, r, c.sm.la, c.sm.e.r);
+  dev_qr_formq(H, m, r, A, c.sm.la);
+  dev_qr_extract_r(H, m, r, Rb);
+  set_chi(c, s, i + 1, rn);
+  if (c.sm.fail) return;
+  update_left(c, s, i);
+  evolve_bond(c, Rb, rn, r, i + 1, dtb);
+  cta_gemm(gemm_args(rn, 2 * r2, r, Rb, 1, rn, An, 1, r, T, 1, rn), c.sm.e.u.gw.g);
+  cta_copy(An, T, (long long)rn * 2 * r2);
+  __syncthreads();
+}
+
+// Site i = L Q (thin LQ): Q -> site i, ER[i] from it, L evolved by dtb on
+// bond i and absorbed into site i-1 (Algorithms.jl:515-529).
+__device__ void lq_bond_backward(Ctx& c, const DState& s, int i, double dtb) {
+  const int l = s.chi[i], r = s.chi[i + 1], n2 = 2 * r, rn = min(l, n2);
+  const int lp = s.chi[i - 1];
+  cplx* A = site_ptr(c, s, i);
+  cplx* Ap = site_ptr(c, s, i - 1);
+  cplx* H = c.ws + c.P.lay.tA;
+  cplx* Qh = c.ws + c.P.lay.tB;
+  cplx* Rb = c.ws + c.P.lay.tC;
+  for (int e = threadIdx.x; e < n2 * l; e += NT) {
+    int cc = (int)(e % n2), ii = (int)(e / n2);
+    H[e] = cconj(A[ii + (long long)l * cc]);
+  }
+  __syncthreads();
+  dev_qr_factor(H, n2, l, c.sm.la, c.sm.e.r);
+  dev_qr_formq(H, n2, l, Qh, c.sm.la);
+  dev_qr_extract_r(H, n2, l, Rb);
+  for (int e = threadIdx.x; e < rn * n2; e += NT) {
+    int k = (int)(e % rn), cc = (int)(e / rn);
+    A[e] = cconj(Qh[cc + (long long)n2 * k]);
+  }
+  cplx* Lm = H;  // L = R^H (l x rn)
+  for (int e = threadIdx.x; e < l * rn; e += NT) {
+    int a = (int)(e % l), k = (int)(e / l);
+    Lm[e] = cconj(Rb[k + (long long)rn * a]);
+  }
+  set_chi(c, s, i, rn);
+  if (c.sm.fail) return;
+  update_right(c, s, i);
+  evolve_bond(c, Lm, l, rn, i, dtb);
+  cta_gemm(gemm_args(2 * lp, rn, l, Ap, 1, 2 * lp, Lm, 1, l, Rb, 1, 2 * lp), c.sm.e.u.gw.g);
+  cta_copy(Ap, Rb, (long long)2 * lp * rn);
+  __syncthreads();
+}
+
+__device__ void evolve_site1(Ctx& c, const DState& s, int i, double dts) {
+  evolve(c, site_ptr(c, s, i), s.chi[i], 2, s.chi[i + 1], i, i + 1, c.P.wm_heff1[i], dts);
+}
+
+// _tdvp_sweep_hamiltonian_1site! (Algorithms.jl:472-533).
+__device__ void tdvp_sweep_1site(Ctx& c, const DState& s) {
+  const int L = c.P.L;
+  const double dt = c.P.dt;
+  init_envs(c, s);
+  for (int i = 0; i < L && !c.sm.fail; ++i) {
+    evolve_site1(c, s, i, dt / 2);
+    if (i < L - 1) qr_bond_forward(c, s, i, -dt / 2);
+  }
+  for (int i = L - 1; i >= 0 && !c.sm.fail; --i) {
+    evolve_site1(c, s, i, dt / 2);
+    if (i > 0) lq_bond_backward(c, s, i, -dt / 2);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *s.oc = 0;
+  __syncthreads();
+}
+
+// local_dynamic_tdvp (mqt-yaqs/src/mqt/yaqs/core/methods/tdvp.py:667-855):
+// per bond a 2-site update while the bond is below max_bond_dim (split
+// keeping min(rank, max_bond_dim) values), a 1-site update with bond
+// back-evolution once it has reached it; once a 1-site step reaches the
+// last bond the last site (first site on the way back) is updated alone.
+__device__ void tdvp_sweep_dynamic(Ctx& c, const DState& s) {
+  const int L = c.P.L;
+  const double dt = c.P.dt;
+  cplx* th = c.ws + c.P.lay.th;
+  init_envs(c, s);
+  bool lock = false;
+  for (int i = 0; i < L && !c.sm.fail; ++i) {
+    if (s.chi[i + 1] >= c.P.max_bond || lock) {
+      evolve_site1(c, s, i, dt / 2);
+      if (i != L - 1) qr_bond_forward(c, s, i, -dt / 2);
+      if (i == L - 2) lock = true;
+    } else if (i == L - 1) {
+      continue;
+    } else {
+      const int l = s.chi[i], r = s.chi[i + 2];
+      merge(c, s, i, th);
+      evolve(c, th, l, 4, r, i, i + 2, c.P.wm_heff2[i], dt / 2);
+      split(c, s, i, th, l, r, 3, false);
+      if (c.sm.fail) break;
+      update_left(c, s, i);
+      if (i != L - 2)
+        evolve(c, site_ptr(c, s, i + 1), s.chi[i + 1], 2, r, i + 1, i + 2, c.P.wm_heff1[i + 1], -dt / 2);
+    }
+  }
+  lock = false;
+  for (int i = L - 1; i >= 0 && !c.sm.fail; --i) {
+    if (s.chi[i] >= c.P.max_bond || lock) {
+      evolve_site1(c, s, i, dt / 2);
+      if (i != 0) {
+        lq_bond_backward(c, s, i, -dt / 2);
+        if (i == 1) lock = true;
+      }
+    } else if (i == 0) {
+      continue;
+    } else {
+      const int l = s.chi[i - 1], r = s.chi[i + 1];
+      merge(c, s, i - 1, th);
+      evolve(c, th, l, 4, r, i - 1, i + 1, c.P.wm_heff2[i - 1], dt / 2);
+      split(c, s, i - 1, th, l, r, 3, true);
+      if (c.sm.fail) break;
+      update_right(c, s, i);
+      if (i != 1) evolve(c, site_ptr(c, s, i - 1), s.chi[i - 1], 2, s.chi[i], i - 1, i, c.P.wm_heff1[i - 1], -dt / 2);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *s.oc = 0;
+  __syncthreads();
+}
+
+__device__ void tdvp_sweep_2site(Ctx& c, const DState& s) {
+  const int L = c.P.L;
+  const double dt = c.P.dt;
+  cplx* th = c.ws + c.P.lay.th;
+  init_envs(c, s);
   // forward (Algorithms.jl:631-672)
   for (int i = 0; i <= L - 3 && !c.sm.fail; ++i) {
     const int l = s.chi[i], r = s.chi[i + 2];
@@ -516,6 +665,16 @@ __device__ void tdvp_sweep(Ctx& c, const DState& s) {
     if (c.sm.fail) break;
     update_right(c, s, i + 1);
   }
+}
+
+__device__ void tdvp_sweep(Ctx& c, const DState& s) {
+  ProfScope prof_scope_(PF_SWEEP);
+  if (c.P.tdvp_mode == 1)
+    tdvp_sweep_1site(c, s);
+  else if (c.P.tdvp_mode == 2)
+    tdvp_sweep_dynamic(c, s);
+  else
+    tdvp_sweep_2site(c, s);
 }
 
 // ---------------------------------------------------------------------------
