@@ -428,7 +428,7 @@ def run_batch(args):
     with api.Server(max_L=64, max_bond_dim=128, max_mpo_width=5, mixed=True, chunk=args.chunk, ctx=ctx) as srv:
         clocks.start()
         t0 = time.perf_counter()
-        ids = [srv.submit(*r["problem"], seed=r["seed"], precision=prec) for r in reqs]
+        ids = [srv.submit(*r["problem"], seed=r["seed"], precision=prec, tdvp=args.tdvp) for r in reqs]
         res = [srv.result(i) for i in ids]
         wall = time.perf_counter() - t0
         ck = clocks.stop()
@@ -440,8 +440,8 @@ def run_batch(args):
             "data": "synthetic",
             "config": {"workload": f"64 analog TJM simulations (seed 0x{BATCH_SEED:X}): Ising/XY/Heisenberg, "
                                    f"L in 8..64, chi_max in 16..128, 64..512 trajectories, lowering+dephasing, "
-                                   f"dt=0.05, {steps} steps; one server, chunk={args.chunk}",
-                       "precision": prec, "trajectory_steps": total},
+                                   f"dt=0.05, {steps} steps, {TDVP_DESC[args.tdvp]}; one server, chunk={args.chunk}",
+                       "precision": prec, "tdvp": args.tdvp, "trajectory_steps": total},
             "wall_s": wall, "device_busy_s": st["busy_s"], "launches": st["launches"], "slots": st["slots"],
             "latency_p50_s": st["latency_p50_s"], "latency_p99_s": st["latency_p99_s"],
             "queue_p50_s": st["queue_p50_s"], "queue_p99_s": st["queue_p99_s"], "clocks": ck,

@@ -758,7 +758,7 @@ class Server:
 
     def submit(self, initial_state: MPS, operator, sim_params: TimeEvolutionConfig,
                noise_model: NoiseModel | None = None, *, seed: int = 0, uniforms: np.ndarray | None = None,
-               precision: str = "fp64", traj_offset: int = 0) -> int:
+               precision: str = "fp64", traj_offset: int = 0, tdvp: str = "2site") -> int:
         mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
         rid = C.c_int64(0)
         if isinstance(operator, DigitalCircuit):
@@ -770,7 +770,7 @@ class Server:
         else:
             prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
             d = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
-                            uniforms=uniforms, precision=prec, traj_offset=traj_offset)
+                            uniforms=uniforms, precision=prec, traj_offset=traj_offset, tdvp_mode=TDVP_MODES[tdvp])
             st = self._lib.yaqs_server_submit_analog(self.handle, C.byref(d.mps), C.byref(d.mpo), C.byref(d.noise),
                                                      d.obs, d.n_obs, C.byref(d.cfg), C.byref(d.rng), C.byref(rid))
         self._check_static(st)
@@ -833,9 +833,12 @@ def random_mps(length: int, chi: int, seed: int = 0) -> MPS:
     return MPS(length, tensors=ts)
 
 
+TDVP_MODES = {"2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE, "dynamic": A.YAQS_TDVP_DYNAMIC}
+
+
 def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
         *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12,
-        precision: str = "fp64", ctx=None) -> RunResult:
+        precision: str = "fp64", tdvp: str = "2site", ctx=None) -> RunResult:
     """Simulator.run (Simulator.jl:127-141) for an MPO (analog TJM) or a
     DigitalCircuit (digital TJM, TEBD gate application).  Fills every
     observable's ``trajectories`` and ``results`` like _run_analog /
@@ -844,7 +847,10 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
     runs one trajectory and mutates ``sim_params.num_traj`` (Simulator.jl:27-29).
     ``precision="mixed"`` runs the analog H_eff and environment contractions
     in complex FP32 on the tensor cores (Lanczos orthogonalisation, SVD/QR,
-    norms and jump probabilities stay FP64)."""
+    norms and jump probabilities stay FP64).  ``tdvp`` selects the sweep:
+    "2site" (two_site_tdvp!, the reference's analog path), "1site"
+    (single_site_tdvp!) or "dynamic" (1-site TDVP with 2-site growth up to
+    max_bond_dim, the Python lineage's local_dynamic_tdvp)."""
     prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
     if not isinstance(operator, (MPO, DigitalCircuit)):
         raise TypeError("Simulation requires MPO (Analog) or DigitalCircuit (Digital).")
@@ -857,7 +863,8 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
         res = run_circuit_descriptors(desc, ctx)
     else:
         desc = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
-                           uniforms=uniforms, krylov_exit_tol=krylov_exit_tol, precision=prec)
+                           uniforms=uniforms, krylov_exit_tol=krylov_exit_tol, precision=prec,
+                           tdvp_mode=TDVP_MODES[tdvp])
         res = run_descriptors(desc, ctx)
     if isinstance(operator, DigitalCircuit):
         # obs buffers sized by sim_params.times; the first min(n_samples, columns) are filled (Simulator.jl:99-103)
