@@ -38,37 +38,6 @@ struct DigParams {
 __device__ __constant__ cplx c_swap[16] = {{1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}, {0, 0},
                                            {0, 0}, {1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}};
 
-// Scale the orthogonality-centre tensor to unit norm (normalize!, MPS.jl:274-311).
-__device__ void normalize_center(Ctx& c, const DState& s) {
-  const int oc = *s.oc;
-  cplx* A = site_ptr(c, s, oc);
-  const long long n = (long long)s.chi[oc] * 2 * s.chi[oc + 1];
-  double nr = sqrt(cta_norm2(A, n, c.sm.e.r));
-  if (nr > 1e-13) cta_scale(A, n, 1.0 / nr);
-  __syncthreads();
-}
-
-// True when every bond satisfies chi[b] <= 2 chi[b-1] and chi[b] <= 2 chi[b+1]:
-// then the thin QR / LQ factorisations of a gauge sweep keep every shape, so
-// a sweep is a pure gauge move.  Uniform across the CTA.
-__device__ bool chain_tight(const Ctx& c, const DState& s) {
-  bool ok = true;
-  for (int b = 1; b < c.P.L; ++b) {
-    const int x = s.chi[b];
-    if (x > 2 * s.chi[b - 1] || x > 2 * s.chi[b + 1]) ok = false;
-  }
-  return ok;
-}
-
-// normalize! after a gate or a noise step: on a tight chain the full sweep
-// only rescales the centre tensor; otherwise run the sweep.
-__device__ void finish_normalize(Ctx& c, const DState& s) {
-  if (chain_tight(c, s))
-    normalize_center(c, s);
-  else
-    normalize_state(c, s);
-}
-
 // apply_local_gate_exact! on sites (s1, s1+1).
 __device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
   ProfScope prof_scope_(PF_SWEEP);

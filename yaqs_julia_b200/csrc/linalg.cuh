@@ -14,6 +14,7 @@
 #define SVD_NULL_TOL 1e-14
 #define JACOBI_MAX_SWEEPS 60
 #define SVD_MAX_COLS 256
+#define QR_REG_ROWS 4  // Householder rows per lane kept in registers (m - j - 1 <= 128)
 
 struct LinalgSmem {
   cplx tau[SVD_MAX_COLS];
@@ -58,16 +59,67 @@ __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls
       ls.tau[j] = t;
     }
     const cplx ct = cconj(t);
-    for (int c = j + 1 + wid; c < n; c += NW) {
-      cplx* x = H + (long long)m * c;
-      cplx acc = make_double2(0.0, 0.0);
-      if (lane == 0) acc = x[j];
-      for (int i = j + 1 + lane; i < m; i += 32) cfmac(acc, col[i], x[i]);
-      acc.x = warp_sum(acc.x);
-      acc.y = warp_sum(acc.y);
-      acc = cmul(acc, ct);
-      for (int i = j + 1 + lane; i < m; i += 32) x[i] = csub(x[i], cmul(acc, col[i]));
-      if (lane == 0) x[j] = csub(x[j], acc);
+    if (m - j - 1 <= 32 * QR_REG_ROWS) {
+      // reflector rows held in registers; two trailing columns per warp pass
+      cplx v[QR_REG_ROWS];
+#pragma unroll
+      for (int q = 0; q < QR_REG_ROWS; ++q) {
+        const int i = j + 1 + lane + 32 * q;
+        v[q] = i < m ? col[i] : make_double2(0.0, 0.0);
+      }
+      for (int c0 = j + 1 + wid; c0 < n; c0 += 2 * NW) {
+        const int c1 = c0 + NW;
+        const bool two = c1 < n;
+        cplx* x0 = H + (long long)m * c0;
+        cplx* x1 = H + (long long)m * (two ? c1 : c0);
+        cplx a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+        if (lane == 0) {
+          a0 = x0[j];
+          a1 = x1[j];
+        }
+        cplx y0[QR_REG_ROWS], y1[QR_REG_ROWS];
+#pragma unroll
+        for (int q = 0; q < QR_REG_ROWS; ++q) {
+          const int i = j + 1 + lane + 32 * q;
+          y0[q] = i < m ? x0[i] : make_double2(0.0, 0.0);
+          y1[q] = i < m ? x1[i] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < QR_REG_ROWS; ++q) {
+          cfmac(a0, v[q], y0[q]);
+          cfmac(a1, v[q], y1[q]);
+        }
+        a0.x = warp_sum(a0.x);
+        a0.y = warp_sum(a0.y);
+        a1.x = warp_sum(a1.x);
+        a1.y = warp_sum(a1.y);
+        a0 = cmul(a0, ct);
+        a1 = cmul(a1, ct);
+#pragma unroll
+        for (int q = 0; q < QR_REG_ROWS; ++q) {
+          const int i = j + 1 + lane + 32 * q;
+          if (i < m) {
+            x0[i] = csub(y0[q], cmul(a0, v[q]));
+            if (two) x1[i] = csub(y1[q], cmul(a1, v[q]));
+          }
+        }
+        if (lane == 0) {
+          x0[j] = csub(x0[j], a0);
+          if (two) x1[j] = csub(x1[j], a1);
+        }
+      }
+    } else {
+      for (int c = j + 1 + wid; c < n; c += NW) {
+        cplx* x = H + (long long)m * c;
+        cplx acc = make_double2(0.0, 0.0);
+        if (lane == 0) acc = x[j];
+        for (int i = j + 1 + lane; i < m; i += 32) cfmac(acc, col[i], x[i]);
+        acc.x = warp_sum(acc.x);
+        acc.y = warp_sum(acc.y);
+        acc = cmul(acc, ct);
+        for (int i = j + 1 + lane; i < m; i += 32) x[i] = csub(x[i], cmul(acc, col[i]));
+        if (lane == 0) x[j] = csub(x[j], acc);
+      }
     }
     __syncthreads();
   }
@@ -87,16 +139,66 @@ __device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, 
     const cplx t = ls.tau[j];
     if (t.x == 0.0 && t.y == 0.0) continue;
     const cplx* v = H + (long long)m * j;
-    for (int c = j + wid; c < kq; c += NW) {
-      cplx* q = Q + (long long)m * c;
-      cplx acc = make_double2(0.0, 0.0);
-      if (lane == 0) acc = q[j];
-      for (int i = j + 1 + lane; i < m; i += 32) cfmac(acc, v[i], q[i]);
-      acc.x = warp_sum(acc.x);
-      acc.y = warp_sum(acc.y);
-      acc = cmul(acc, t);
-      for (int i = j + 1 + lane; i < m; i += 32) q[i] = csub(q[i], cmul(acc, v[i]));
-      if (lane == 0) q[j] = csub(q[j], acc);
+    if (m - j - 1 <= 32 * QR_REG_ROWS) {
+      cplx vr[QR_REG_ROWS];
+#pragma unroll
+      for (int qq = 0; qq < QR_REG_ROWS; ++qq) {
+        const int i = j + 1 + lane + 32 * qq;
+        vr[qq] = i < m ? v[i] : make_double2(0.0, 0.0);
+      }
+      for (int c0 = j + wid; c0 < kq; c0 += 2 * NW) {
+        const int c1 = c0 + NW;
+        const bool two = c1 < kq;
+        cplx* q0 = Q + (long long)m * c0;
+        cplx* q1 = Q + (long long)m * (two ? c1 : c0);
+        cplx a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+        if (lane == 0) {
+          a0 = q0[j];
+          a1 = q1[j];
+        }
+        cplx y0[QR_REG_ROWS], y1[QR_REG_ROWS];
+#pragma unroll
+        for (int qq = 0; qq < QR_REG_ROWS; ++qq) {
+          const int i = j + 1 + lane + 32 * qq;
+          y0[qq] = i < m ? q0[i] : make_double2(0.0, 0.0);
+          y1[qq] = i < m ? q1[i] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int qq = 0; qq < QR_REG_ROWS; ++qq) {
+          cfmac(a0, vr[qq], y0[qq]);
+          cfmac(a1, vr[qq], y1[qq]);
+        }
+        a0.x = warp_sum(a0.x);
+        a0.y = warp_sum(a0.y);
+        a1.x = warp_sum(a1.x);
+        a1.y = warp_sum(a1.y);
+        a0 = cmul(a0, t);
+        a1 = cmul(a1, t);
+#pragma unroll
+        for (int qq = 0; qq < QR_REG_ROWS; ++qq) {
+          const int i = j + 1 + lane + 32 * qq;
+          if (i < m) {
+            q0[i] = csub(y0[qq], cmul(a0, vr[qq]));
+            if (two) q1[i] = csub(y1[qq], cmul(a1, vr[qq]));
+          }
+        }
+        if (lane == 0) {
+          q0[j] = csub(q0[j], a0);
+          if (two) q1[j] = csub(q1[j], a1);
+        }
+      }
+    } else {
+      for (int c = j + wid; c < kq; c += NW) {
+        cplx* q = Q + (long long)m * c;
+        cplx acc = make_double2(0.0, 0.0);
+        if (lane == 0) acc = q[j];
+        for (int i = j + 1 + lane; i < m; i += 32) cfmac(acc, v[i], q[i]);
+        acc.x = warp_sum(acc.x);
+        acc.y = warp_sum(acc.y);
+        acc = cmul(acc, t);
+        for (int i = j + 1 + lane; i < m; i += 32) q[i] = csub(q[i], cmul(acc, v[i]));
+        if (lane == 0) q[j] = csub(q[j], acc);
+      }
     }
     __syncthreads();
   }

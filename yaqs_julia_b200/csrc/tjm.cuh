@@ -92,6 +92,7 @@ struct CtaSmem {
   int bcast_i[8];
   double bcast_d[8];
   int fail;
+  int canon;  // the state is in mixed canonical form around its centre
 };
 
 struct Ctx {  // per-CTA view
@@ -244,6 +245,38 @@ __device__ void normalize_state(Ctx& c, const DState& s) {
   __syncthreads();
   if (threadIdx.x == 0) *s.oc = 0;
   __syncthreads();
+}
+
+// Scale the orthogonality-centre tensor to unit norm (normalize!, MPS.jl:274-311).
+__device__ void normalize_center(Ctx& c, const DState& s) {
+  const int oc = *s.oc;
+  cplx* A = site_ptr(c, s, oc);
+  const long long n = (long long)s.chi[oc] * 2 * s.chi[oc + 1];
+  double nr = sqrt(cta_norm2(A, n, c.sm.e.r));
+  if (nr > 1e-13) cta_scale(A, n, 1.0 / nr);
+  __syncthreads();
+}
+
+// True when every bond satisfies chi[b] <= 2 chi[b-1] and chi[b] <= 2 chi[b+1]:
+// then the thin QR / LQ factorisations of a gauge sweep keep every shape, so
+// a sweep is a pure gauge move.  Uniform across the CTA.
+__device__ bool chain_tight(const Ctx& c, const DState& s) {
+  bool ok = true;
+  for (int b = 1; b < c.P.L; ++b) {
+    const int x = s.chi[b];
+    if (x > 2 * s.chi[b - 1] || x > 2 * s.chi[b + 1]) ok = false;
+  }
+  return ok;
+}
+
+// normalize! of a state in mixed canonical form around its centre: on a
+// tight chain the full sweep only rescales the centre tensor; otherwise run
+// the sweep.
+__device__ void finish_normalize(Ctx& c, const DState& s) {
+  if (chain_tight(c, s))
+    normalize_center(c, s);
+  else
+    normalize_state(c, s);
 }
 
 // Re <psi|psi> by full contraction (scalar_product, MPS.jl:528-585).
@@ -486,6 +519,8 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
   }
   __syncthreads();
   set_chi(c, s, i + 1, keep);
+  if (threadIdx.x == 0) *s.oc = s_left ? i : i + 1;  // the scaled factor holds the centre
+  __syncthreads();
 }
 
 // _init_envs (Algorithms.jl:802-819) after moving the centre to site 0.
@@ -753,6 +788,32 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
     for (int k = 0; k < c.P.nprocs; ++k)
       if (proc_on(c.P.procs[k], f1, f2) && c.P.procs[k].gamma != 0.0) all_zero = false;
   }
+  // Every dissipator a scalar (Pauli names, Dissipation.jl:14-21, 57-60, 88-91)
+  // on a tight chain: the sweep only multiplies the state by their product
+  // and moves the centre to site 0 by shape-preserving gauge steps.
+  bool scalar_only = true;
+  double fscal = 1.0;
+  for (int k = 0; k < c.P.nprocs; ++k) {
+    const DevProc& pr = c.P.procs[k];
+    if (!proc_on(pr, f1, f2)) continue;
+    if (!pr.pauli_name) scalar_only = false;
+    fscal *= exp(-0.5 * dt * pr.gamma);
+  }
+  if ((!c.P.noise_present || all_zero || scalar_only) && chain_tight(c, s)) {
+    shift_oc(c, s, 0);
+    if (c.P.noise_present && !all_zero) {
+      cplx* A = site_ptr(c, s, 0);
+      cta_scale(A, (long long)s.chi[0] * 2 * s.chi[1], fscal);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) c.sm.canon = 1;
+    __syncthreads();
+    return;
+  }
+  // The reference sweep applies its first dissipators to site L while the
+  // centre sits elsewhere, so the chain is not canonical afterwards.
+  if (threadIdx.x == 0) c.sm.canon = 0;
+  __syncthreads();
   if (!c.P.noise_present || all_zero) {
     for (int i = L - 1; i >= 1 && !c.sm.fail; --i) shift_oc(c, s, i - 1);
     return;
@@ -807,8 +868,10 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
     jump = u1 < dp;
   }
   if (!jump) {
-    shift_oc(c, s, 0);
-    normalize_state(c, s);
+    if (c.sm.canon)
+      finish_normalize(c, s);
+    else
+      normalize_state(c, s);
     return;
   }
   double* cand = reinterpret_cast<double*>(c.ws + c.P.lay.dbl) + SVD_MAX_COLS;
@@ -853,8 +916,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
   double total = 0.0;
   for (int e = 0; e < nc; ++e) total += cand[e];
   if (total == 0.0) {
-    shift_oc(c, s, 0);
-    normalize_state(c, s);
+    finish_normalize(c, s);  // the candidate scan moved the centre through every site
     return;
   }
   const double r = draw_uniform(c);
@@ -880,7 +942,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
     split(c, s, pr.s0, th, l, rr, 1, false);
   }
   if (threadIdx.x == 0) c.cnt[3] += 1;
-  normalize_state(c, s);
+  finish_normalize(c, s);
 }
 
 // ---------------------------------------------------------------------------
