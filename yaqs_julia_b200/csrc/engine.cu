@@ -312,6 +312,7 @@ struct DevMem {
 // Sparse M[o, i] built from a dense lambda, in CSR.
 struct HostWMat {
   int no = 0, ni = 0;
+  int ident = 0;
   std::vector<int> rowp, col;
   std::vector<hcd> val;
 };
@@ -404,6 +405,7 @@ int upload_wmats(yaqs_ctx* ctx, DevMem& dm, const std::vector<HostWMat>& all, st
     w.no = m.no;
     w.ni = m.ni;
     w.nnz = (int)m.val.size();
+    w.ident = m.ident;
     w.rowp = di + hi.size();
     hi.insert(hi.end(), m.rowp.begin(), m.rowp.end());
     w.col = di + hi.size();
@@ -873,8 +875,10 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
       return Wat(i, ml, po, pi, mr);
     }));
   }
-  for (int b = 0; b <= L; ++b)  // bond: identity on the MPO bond, physical dimension 1
+  for (int b = 0; b <= L; ++b) {  // bond: identity on the MPO bond, physical dimension 1
     all.push_back(build_wmat(w[b], w[b], [&](int o, int in) { return hcd(o == in ? 1.0 : 0.0, 0.0); }));
+    all.back().ident = 1;
+  }
   for (auto& m : all)
     if (m.ni > WAPPLY_MAXI || m.no > WAPPLY_MAXI || (int)m.val.size() > WAPPLY_MAXNNZ)
       return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO too wide for the sparse MPO apply");

@@ -21,6 +21,7 @@
 // Sparse MPO matrix M[o, i] in CSR form (rows are outputs).
 struct WMat {
   int no, ni, nnz;
+  int ident;  // identity map with a physical dimension of 1 (bond): T2 is T1
   const int* rowp;  // no+1
   const int* col;   // nnz
   const cplx* val;  // nnz
@@ -161,15 +162,24 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   g.no1 = D;
   g.oo1 = chil;
   g.oo2 = (long long)chil * D;
+  // an identity W with D = 1 (the bond operator) leaves T1 in T2's layout
   if (h.mixed) {
     GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(sm.u.gw.g);
-    dev_wapply<cflt>(h.T1f, h.T2f, h.W, g, sm.u.gw.w);
-    cta_gemm_tf32<cplx>(gemm_args_f(chil * D, chir, wr * chir, h.T2f, 1, (long long)chil * D, h.Rf, chir, 1, y, 1,
+    const cflt* T2 = h.T1f;
+    if (!h.W.ident) {
+      dev_wapply<cflt>(h.T1f, h.T2f, h.W, g, sm.u.gw.w);
+      T2 = h.T2f;
+    }
+    cta_gemm_tf32<cplx>(gemm_args_f(chil * D, chir, wr * chir, T2, 1, (long long)chil * D, h.Rf, chir, 1, y, 1,
                                     (long long)chil * D),
                         gf);
   } else {
-    dev_wapply<cplx>(h.T1, h.T2, h.W, g, sm.u.gw.w);
-    cta_gemm(gemm_args(chil * D, chir, wr * chir, h.T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
+    const cplx* T2 = h.T1;
+    if (!h.W.ident) {
+      dev_wapply<cplx>(h.T1, h.T2, h.W, g, sm.u.gw.w);
+      T2 = h.T2;
+    }
+    cta_gemm(gemm_args(chil * D, chir, wr * chir, T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
                        (long long)chil * D),
              sm.u.gw.g);
   }
