@@ -216,17 +216,34 @@ typedef struct {
   int32_t site[2];
   double matrix[32];
   int32_t sample;
+  /*
+   * 2-qubit gates applied by TDVP only: the gate is exp(-i coeff g1 (x) g2)
+   * with g1 acting on site[0] and g2 on site[1] (2x2 column-major complex),
+   * GateLibrary.generator / hamiltonian_coeff (GateLibrary.jl:24-36).
+   */
+  int32_t has_generator;
+  double coeff;
+  double gen1[8];
+  double gen2[8];
 } yaqs_gate_desc;
 
 /* Circuit run settings (the TimeEvolutionConfig fields the digital path
  * reads, plus the TJMOptions of DigitalTJM.jl:70-76). */
-enum { YAQS_METHOD_TEBD = 0 };
+/*
+ * TEBD: apply_local_gate_exact! (merge, 4x4, SVD) with SWAP chains for
+ * long-range gates (DigitalTJM.jl:251-334).  TDVP: the reference's default
+ * (TJMOptions(), DigitalTJM.jl:76): the window s1..s2 evolves under the
+ * product MPO coeff g1 (x) 1 ... 1 (x) g2 (construct_window_mpo,
+ * DigitalTJM.jl:192-236) by one forward circuit 2-site TDVP sweep
+ * (_tdvp_sweep_circuit_2site!, Algorithms.jl:606-627, 762-800).
+ */
+enum { YAQS_METHOD_TEBD = 0, YAQS_METHOD_TDVP = 1 };
 typedef struct {
   int32_t num_traj;
   int32_t max_bond_dim;
   double truncation_threshold;
-  int32_t local_method;       /* YAQS_METHOD_TEBD */
-  int32_t long_range_method;  /* YAQS_METHOD_TEBD (SWAP network) */
+  int32_t local_method;       /* YAQS_METHOD_* for nearest-neighbour gates */
+  int32_t long_range_method;  /* YAQS_METHOD_* for gates on sites further apart */
   int32_t precision;
   int32_t traj_offset;
 } yaqs_circuit_config;
@@ -242,7 +259,8 @@ int yaqs_digital_plan(const yaqs_gate_desc* gates, int32_t n_gates, int32_t* n_l
  * Digital TJM run: replaces the trajectory loop of Simulator._run_digital
  * (Simulator.jl:71-125); each trajectory follows run_digital_tjm
  * (DigitalTJM.jl:363-450) with TEBD gate application and SWAP chains for
- * long-range gates (DigitalTJM.jl:251-330), local dissipation and a jump
+ * long-range gates (DigitalTJM.jl:251-330) or TDVP windows, local
+ * dissipation and a jump
  * step after every 2-qubit gate (DigitalTJM.jl:405-420), and the
  * observables at the sample barriers.  psi0 is normalised first
  * (Simulator.jl:128).  Outputs as yaqs_analog_run with n_out = n_samples.

@@ -858,6 +858,22 @@ struct NoiseSet {  // a NoiseModel: `present` == false means `nothing`
   vector<NoiseProc> procs;
 };
 
+// W_group of two neighbouring MPO tensors (Algorithms.jl:639-643).
+Wt merge_wt(const Wt& W1, const Wt& Wn) {
+  Wt G(W1.wl, 4, Wn.wr);
+  for (int l = 0; l < W1.wl; ++l)
+    for (int r = 0; r < Wn.wr; ++r)
+      for (int p1o = 0; p1o < 2; ++p1o)
+        for (int p2o = 0; p2o < 2; ++p2o)
+          for (int p1i = 0; p1i < 2; ++p1i)
+            for (int p2i = 0; p2i < 2; ++p2i) {
+              cd sacc = 0;
+              for (int k = 0; k < W1.wr; ++k) sacc += W1.at(l, p1o, p1i, k) * Wn.at(k, p2o, p2i, r);
+              G.at(l, p1o + 2 * p2o, p1i + 2 * p2i, r) = sacc;
+            }
+  return G;
+}
+
 struct Problem {
   int L;
   vector<Wt> W;
@@ -876,6 +892,7 @@ struct Problem {
   long long stride;
   int traj_offset;
   int tdvp_mode = YAQS_TDVP_2SITE;
+  int local_method = YAQS_METHOD_TEBD, long_range_method = YAQS_METHOD_TEBD;  // digital
 };
 
 // Hermitian matrix exponential exp(c * H) for small H (n<=4) via Jacobi on
@@ -1513,21 +1530,7 @@ bool load_problem(Problem& P, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
     P.W[i] = std::move(W);
   }
   P.W2.resize(L - 1);
-  for (int i = 0; i + 1 < L; ++i) {  // W_group, Algorithms.jl:639-643
-    const Wt &W1 = P.W[i], &Wn = P.W[i + 1];
-    Wt G(W1.wl, 4, Wn.wr);
-    for (int l = 0; l < W1.wl; ++l)
-      for (int r = 0; r < Wn.wr; ++r)
-        for (int p1o = 0; p1o < 2; ++p1o)
-          for (int p2o = 0; p2o < 2; ++p2o)
-            for (int p1i = 0; p1i < 2; ++p1i)
-              for (int p2i = 0; p2i < 2; ++p2i) {
-                cd sacc = 0;
-                for (int k = 0; k < W1.wr; ++k) sacc += W1.at(l, p1o, p1i, k) * Wn.at(k, p2o, p2i, r);
-                G.at(l, p1o + 2 * p2o, p1i + 2 * p2i, r) = sacc;
-              }
-    P.W2[i] = std::move(G);
-  }
+  for (int i = 0; i + 1 < L; ++i) P.W2[i] = merge_wt(P.W[i], P.W[i + 1]);
   P.dt = cfg->dt;
   P.n_times = cfg->n_times;
   P.num_traj = cfg->num_traj;
@@ -1561,6 +1564,9 @@ struct Gate {
   int a, b;  // sites as given
   cd mat[16];
   bool sample;
+  bool has_gen;  // exp(-i coeff g1 (x) g2), g1 on a, g2 on b
+  double coeff;
+  cd g1[4], g2[4];
 };
 
 struct Circuit {
@@ -1635,6 +1641,54 @@ void apply_window_tebd(const Problem& P, State& s, const Gate& G, Counters& cnt)
   }
 }
 
+// apply_window! with method :TDVP (DigitalTJM.jl:335-358): the window
+// s1..s2 (padding 0) evolves under construct_window_mpo (DigitalTJM.jl:
+// 192-236) by one _tdvp_sweep_circuit_2site! (Algorithms.jl:606-627):
+// forward 2-site updates by +1 with back-evolution by -1 (:631-672), then the
+// edge pair by +1 split to the right (:762-800); the centre ends on s2.
+void apply_window_tdvp(const Problem& P, State& s, const Gate& G, Counters& cnt) {
+  const int s1 = std::min(G.a, G.b), s2 = std::max(G.a, G.b), n = s2 - s1 + 1;
+  shift_oc(s, s1);
+  const cd* gs1 = G.a == s1 ? G.g1 : G.g2;  // the generator of the smaller site
+  const cd* gs2 = G.a == s1 ? G.g2 : G.g1;
+  vector<Wt> W(n, Wt(1, 2, 1));
+  for (int j = 0; j < n; ++j)
+    for (int po = 0; po < 2; ++po)
+      for (int pi = 0; pi < 2; ++pi) {
+        cd v = po == pi ? 1.0 : 0.0;
+        if (j == 0) v = G.coeff * gs1[po + 2 * pi];
+        else if (j == n - 1) v = gs2[po + 2 * pi];
+        W[j].v[po + 2 * pi] = v;
+      }
+  vector<Wt> W2(n - 1);
+  for (int j = 0; j + 1 < n; ++j) W2[j] = merge_wt(W[j], W[j + 1]);
+  vector<Env> EL(n + 1), ER(n + 1);
+  EL[0] = identity_env(s.t[s1].l, 1);
+  ER[n] = identity_env(s.t[s2].r, 1);
+  for (int j = n - 1; j >= 1; --j) ER[j] = update_right(s.t[s1 + j], W[j], ER[j + 1]);
+  Sweeper sw(P, cnt);
+  for (int j = 0; j + 2 < n; ++j) {  // forward (Algorithms.jl:617-620)
+    Ten Th = merge(s.t[s1 + j], s.t[s1 + j + 1]);
+    Th.v = sw.evolve(EL[j], ER[j + 2], W2[j], Th, 1.0);
+    Ten U, V;
+    split_theta(Th, 0, P.thr, P.max_bond, false, U, V, cnt);
+    s.t[s1 + j] = U;
+    EL[j + 1] = update_left(s.t[s1 + j], W[j], EL[j]);
+    V.v = sw.evolve(EL[j + 1], ER[j + 2], W[j + 1], V, -1.0);
+    s.t[s1 + j + 1] = V;
+  }
+  {  // edge (Algorithms.jl:762-800)
+    const int j = n - 2;
+    Ten Th = merge(s.t[s1 + j], s.t[s1 + j + 1]);
+    Th.v = sw.evolve(EL[j], ER[j + 2], W2[j], Th, 1.0);
+    Ten U, V;
+    split_theta(Th, 0, P.thr, P.max_bond, false, U, V, cnt);
+    s.t[s1 + j] = U;
+    s.t[s1 + j + 1] = V;
+  }
+  s.oc = s2;
+}
+
 // create_local_noise_model (DigitalTJM.jl:172-188)
 NoiseSet local_noise(const NoiseSet& N, int s1, int s2) {
   NoiseSet out;
@@ -1666,7 +1720,11 @@ int run_digital(const Problem& P, const vector<Gate>& gates, const Circuit& C, l
     for (int g : C.layers[l]) {
       const Gate& G = gates[g];
       if (G.kind != 2) continue;
-      apply_window_tebd(P, s, G, cnt);
+      const bool lr = std::abs(G.a - G.b) > 1;
+      if ((lr ? P.long_range_method : P.local_method) == YAQS_METHOD_TDVP)
+        apply_window_tdvp(P, s, G, cnt);
+      else
+        apply_window_tebd(P, s, G, cnt);
       if (P.noise.present && !P.noise.procs.empty()) {
         NoiseSet loc = local_noise(P.noise, std::min(G.a, G.b), std::max(G.a, G.b));
         if (!loc.procs.empty()) {
@@ -1701,6 +1759,12 @@ bool load_circuit(const yaqs_gate_desc* gates, int n, int L, vector<Gate>& out, 
     if (q.kind == 0) G.a = G.b = 0;
     int dd = q.kind == 2 ? 4 : 2;
     for (int e = 0; e < dd * dd && q.kind != 0; ++e) G.mat[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);
+    G.has_gen = q.kind == 2 && q.has_generator;
+    G.coeff = q.coeff;
+    for (int e = 0; e < 4; ++e) {
+      G.g1[e] = cd(q.gen1[2 * e], q.gen1[2 * e + 1]);
+      G.g2[e] = cd(q.gen2[2 * e], q.gen2[2 * e + 1]);
+    }
     out.push_back(G);
   }
   return true;
@@ -1797,6 +1861,16 @@ int orc_digital_run(const yaqs_mps_desc* psi0, const yaqs_gate_desc* gates, int3
   load_obs_rng(P, obs, n_obs, rng);
   vector<Gate> G;
   if (!load_circuit(gates, n_gates, P.L, G, err)) return fail(YAQS_E_ARG, err);
+  P.local_method = cfg->local_method;
+  P.long_range_method = cfg->long_range_method;
+  P.kp.kdim = 25;  // expm_krylov(..., 25) in the circuit sweeps (Algorithms.jl:185)
+  P.kp.tol = 1e-10;
+  P.kp.exit_tol = 1e-12;
+  for (const Gate& g : G) {
+    const bool lr = std::abs(g.a - g.b) > 1;
+    if (g.kind == 2 && (lr ? P.long_range_method : P.local_method) == YAQS_METHOD_TDVP && !g.has_gen)
+      return fail(YAQS_E_ARG, "a gate applied by TDVP needs its generator (GateLibrary.generator)");
+  }
   Circuit C = process_circuit(G);
   const int ncols = C.n_samples;
   if (t_begin < 0 || t_end > P.num_traj || t_begin > t_end) return fail(YAQS_E_ARG, "bad trajectory range");

@@ -165,3 +165,51 @@ def test_session_steps_match_one_call(oracle):
     res = sess.finish()
     assert np.array_equal(res.trajectories, one.trajectories)
     assert res.stats["flops"] > 0
+
+
+def _tdvp_circuit(L, depth, seed, long_range=True):
+    rng = np.random.default_rng(seed)
+    c = api.DigitalCircuit(L)
+    c.add_gate(api.Barrier(), [])
+    for _ in range(depth):
+        for i in range(1, L + 1):
+            c.add_gate(api.Rx(rng.uniform(0, 1)), [i])
+        for i in list(range(1, L, 2)) + list(range(2, L, 2)):
+            g = [api.RzzGate, api.RxxGate, api.RyyGate][rng.integers(3)](rng.uniform(0, 1.5))
+            c.add_gate(g, [i, i + 1])
+        c.add_gate(api.CXGate(), [2, 3])
+        if long_range:
+            c.add_gate(api.RzzGate(rng.uniform(0, 1)), [1, L])
+            c.add_gate(api.CPhaseGate(rng.uniform(0, 1)), [L - 1, 2])
+        c.add_gate(api.Barrier(), [])
+    return c
+
+
+@pytest.mark.parametrize("chi", [4, 32])
+def test_tdvp_window_gates_match_oracle(oracle, chi):
+    """apply_window! with :TDVP, the reference's default TJMOptions (window
+    MPO + forward circuit 2-site sweep), with Pauli noise after every gate."""
+    L = 7
+    c = _tdvp_circuit(L, 3, seed=12)
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.03} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_z")], L)
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=6, max_bond_dim=chi)
+    u = np.random.default_rng(13).random((6, api.max_draws_digital(c)))
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=u,
+                               local_method="tdvp", long_range_method="tdvp")
+    ref, chi_ref, st_ref = oracle.digital_run(d)
+    got = api.run_circuit_descriptors(d)
+    assert np.abs(got.trajectories - ref).max() < 1e-10
+    assert np.array_equal(got.max_bond, chi_ref)
+    assert got.stats["jumps"] == st_ref["jumps"]
+
+
+def test_tdvp_local_tebd_long_range_mix(oracle):
+    L = 6
+    c = _tdvp_circuit(L, 2, seed=14)
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=1, max_bond_dim=16)
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, None, local_method="tdvp", long_range_method="tebd")
+    ref, chi_ref, _ = oracle.digital_run(d)
+    got = api.run_circuit_descriptors(d)
+    assert np.abs(got.trajectories - ref).max() < 1e-10
+    assert np.array_equal(got.max_bond, chi_ref)

@@ -139,3 +139,75 @@ def test_truncated_bond_dimensions_respect_caps(oracle, chi, thr):
     tr, mx, _ = _run(oracle, L, c, _zs(L), chi=chi, thr=thr)
     assert mx.max() <= chi
     assert np.all(np.abs(tr) <= 1 + 1e-9)
+
+
+def _run_m(oracle, L, c, obs, method, nm=None, num_traj=1, chi=64, thr=0.0, seed=1, uniforms=None, psi=None):
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=1.0, num_traj=num_traj, max_bond_dim=chi, truncation_threshold=thr)
+    mode = api.A.YAQS_RNG_INJECTED if uniforms is not None else api.A.YAQS_RNG_PHILOX
+    d = api.CircuitDescriptors(psi or api.MPS(L), c, cfg, nm, rng_mode=mode, seed=seed, uniforms=uniforms,
+                               local_method=method, long_range_method=method)
+    return oracle.digital_run(d)
+
+
+def test_generators_reproduce_gate_matrices():
+    """exp(-i coeff g1 (x) g2) in the p1 + 2 p2 basis (g1 on the first site)
+    is the gate for the symmetric gates; CX's generator puts the control on
+    its first site while its matrix constant (GateLibrary.jl:144-150) has it
+    on the second."""
+    import scipy.linalg as sl
+    for g in [api.RzzGate(0.7), api.RxxGate(-1.1), api.RyyGate(0.4), api.CZGate(), api.CPhaseGate(0.9)]:
+        U = sl.expm(-1j * g.coeff * np.kron(g.generator[1], g.generator[0]))
+        assert np.allclose(U, g.matrix, atol=1e-12), g.name
+    cx = api.CXGate()
+    U = sl.expm(-1j * cx.coeff * np.kron(cx.generator[1], cx.generator[0]))
+    swap = api.SWAP
+    assert np.allclose(U, swap @ cx.matrix @ swap, atol=1e-12)
+
+
+def test_tdvp_window_adjacent_gates_are_exact(oracle):
+    """A 2-site window is one Krylov exponential of coeff g1 (x) g2 between
+    identity environments: the gate itself (DigitalTJM.jl:335-358)."""
+    L = 5
+    rng = np.random.default_rng(3)
+    c = api.DigitalCircuit(L)
+    c.add_gate(api.Barrier(), [])
+    for _ in range(3):
+        for i in range(1, L + 1):
+            c.add_gate(api.Rx(rng.uniform(0, 1)), [i])
+        for i in list(range(1, L, 2)) + list(range(2, L, 2)):
+            g = [api.RzzGate, api.RxxGate, api.RyyGate][rng.integers(3)](rng.uniform(0, 1.5))
+            c.add_gate(g, [i, i + 1])
+        c.add_gate(api.CZGate(), [2, 3])
+        c.add_gate(api.CPhaseGate(0.8), [4, 5])
+        c.add_gate(api.Barrier(), [])
+    tr_tdvp, chi_tdvp, _ = _run_m(oracle, L, c, _zs(L), "tdvp")
+    tr_tebd, _, _ = _run_m(oracle, L, c, _zs(L), "tebd")
+    assert np.abs(tr_tdvp - tr_tebd).max() < 1e-9
+
+
+def test_tdvp_window_long_range_gate_matches_dense_with_full_bonds(oracle):
+    """A long-range Rzz by the TDVP window against the exact gate: with bonds
+    already at full rank the projected sweep reproduces it."""
+    L = 4
+    c = api.DigitalCircuit(L)
+    for i in range(1, L + 1):
+        c.add_gate(api.H, [i])
+    for i in range(1, L):
+        c.add_gate(api.CZGate(), [i, i + 1])
+    c.add_gate(api.Barrier(), [])
+    c.add_gate(api.RzzGate(0.6), [1, 4])
+    c.add_gate(api.Barrier(), [])
+    layers, _ = api.process_circuit(c)
+    ref = D.digital_pauli_density(L, layers, [], [D.site_op(api.Z, i, L) for i in range(1, L + 1)] +
+                                  [D.site_op(api.X, i, L) for i in range(1, L + 1)])
+    obs = _zs(L) + [api.Observable(f"X{i}", api.X, i) for i in range(1, L + 1)]
+    psi = api.MPS(L).pad_bond_dimension(4, 1e-9, seed=1)
+    tr, _, _ = _run_m(oracle, L, c, obs, "tdvp", psi=psi, chi=4)
+    _, after, _ = api.sample_plan(c)
+    assert np.abs(tr[0].T - ref[after]).max() < 1e-8
+
+
+def test_tdvp_method_needs_generators(oracle):
+    c = api.DigitalCircuit(2).add_gate(api.SWAP, [1, 2])
+    with pytest.raises(RuntimeError, match="generator"):
+        _run_m(oracle, 2, c, _zs(2), "tdvp")

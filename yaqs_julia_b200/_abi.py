@@ -83,7 +83,8 @@ YAQS_GATE_2Q = 2
 
 class GateDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("site", C.c_int32 * 2), ("matrix", C.c_double * 32),
-                ("sample", C.c_int32)]
+                ("sample", C.c_int32), ("has_generator", C.c_int32), ("coeff", C.c_double),
+                ("gen1", C.c_double * 8), ("gen2", C.c_double * 8)]
 
 
 class CircuitConfig(C.Structure):
@@ -125,3 +126,5 @@ class ServerStats(C.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+YAQS_METHOD_TEBD, YAQS_METHOD_TDVP = 0, 1

@@ -72,6 +72,60 @@ def Rxx(theta):
     return np.array([[c, 0, 0, s], [0, c, s, 0], [0, s, c, 0], [s, 0, 0, c]], dtype=np.complex128)
 
 
+def Ryy(theta):
+    c, s = math.cos(theta / 2), -1j * math.sin(theta / 2)
+    return np.array([[c, 0, 0, -s], [0, c, s, 0], [0, s, c, 0], [-s, 0, 0, c]], dtype=np.complex128)
+
+
+def CPhase(theta):
+    return np.diag([1, 1, 1, np.exp(1j * theta)]).astype(np.complex128)
+
+
+class GateOp:
+    """A gate as GateLibrary defines it: its matrix and, for the 2-qubit
+    gates TDVP can apply, the generator pair and coefficient with
+    gate = exp(-i coeff g1 (x) g2), g1 on the gate's first site
+    (generator / hamiltonian_coeff, GateLibrary.jl:24-36).  Usable wherever a
+    matrix is (np.asarray gives the matrix)."""
+
+    def __init__(self, matrix, generator=None, coeff=1.0, name=""):
+        self.matrix = np.asarray(matrix, dtype=np.complex128)
+        self.generator = None if generator is None else tuple(np.asarray(g, dtype=np.complex128) for g in generator)
+        self.coeff = float(coeff)
+        self.name = name
+
+    def __array__(self, dtype=None, copy=None):
+        return self.matrix if dtype is None else self.matrix.astype(dtype)
+
+
+_I_MINUS_Z = np.array([[0, 0], [0, 2]], dtype=np.complex128)
+_I_MINUS_X = np.array([[1, -1], [-1, 1]], dtype=np.complex128)
+
+
+def RxxGate(theta):  # GateLibrary.jl:258-272
+    return GateOp(Rxx(theta), (X, X), theta / 2, "rxx")
+
+
+def RyyGate(theta):  # GateLibrary.jl:274-288
+    return GateOp(Ryy(theta), (Y, Y), theta / 2, "ryy")
+
+
+def RzzGate(theta):  # GateLibrary.jl:290-302
+    return GateOp(Rzz(theta), (Z, Z), theta / 2, "rzz")
+
+
+def CXGate():  # GateLibrary.jl:142-157
+    return GateOp(CX, (_I_MINUS_Z, _I_MINUS_X), math.pi / 4, "cx")
+
+
+def CZGate():  # GateLibrary.jl:167-187
+    return GateOp(CZ, (_I_MINUS_Z, _I_MINUS_Z), math.pi / 4, "cz")
+
+
+def CPhaseGate(theta):  # GateLibrary.jl:197-233
+    return GateOp(CPhase(theta), (_I_MINUS_Z, _I_MINUS_Z), -theta / 4, "cphase")
+
+
 def kron2(a, b):
     """Julia's kron(a, b) reshaped to the (p1_out, p2_out, p1_in, p2_in)
     convention: kron(A, B) acts with B on the FIRST site (Noise.jl:47-57)."""
@@ -500,7 +554,12 @@ class Barrier:
 
 
 class DigitalGate:
-    def __init__(self, op, sites):
+    def __init__(self, op, sites, generator=None):
+        self.generator, self.coeff = None, 1.0
+        if isinstance(op, GateOp):
+            self.generator, self.coeff = op.generator, op.coeff
+        if generator is not None:  # add_gate!(...; generator=...) (DigitalTJM.jl:64-66): exp(-i g1 (x) g2)
+            self.generator, self.coeff = tuple(np.asarray(g, dtype=np.complex128) for g in generator), 1.0
         self.op = op if isinstance(op, Barrier) else np.asarray(op, dtype=np.complex128)
         self.sites = list(sites)
 
@@ -514,15 +573,15 @@ class DigitalCircuit:
         self.num_qubits = int(num_qubits)
         self.gates: list[DigitalGate] = []
 
-    def add_gate(self, op, sites):
+    def add_gate(self, op, sites, generator=None):
         if isinstance(sites, int):
             sites = [sites]
-        self.gates.append(DigitalGate(op, sites))
+        self.gates.append(DigitalGate(op, sites, generator))
         return self
 
 
-def add_gate(circ: DigitalCircuit, op, sites):
-    return circ.add_gate(op, sites)
+def add_gate(circ: DigitalCircuit, op, sites, generator=None):
+    return circ.add_gate(op, sites, generator)
 
 
 def process_circuit(circ: DigitalCircuit):
@@ -560,7 +619,8 @@ class CircuitDescriptors:
 
     def __init__(self, psi0: MPS, circ: DigitalCircuit, sim_params: TimeEvolutionConfig,
                  noise_model: NoiseModel | None, *, rng_mode: int = A.YAQS_RNG_PHILOX, seed: int = 0,
-                 uniforms: np.ndarray | None = None, traj_offset: int = 0, num_traj: int | None = None):
+                 uniforms: np.ndarray | None = None, traj_offset: int = 0, num_traj: int | None = None,
+                 local_method: str = "tebd", long_range_method: str = "tebd"):
         L = psi0.length
         if circ.num_qubits != L:
             raise ValueError("circuit and MPS sizes differ")
@@ -573,8 +633,9 @@ class CircuitDescriptors:
         self.num_traj = base.num_traj
         self.gates = self.pack_gates(circ)
         self.n_gates = len(circ.gates)
-        self.cfg = A.CircuitConfig(self.num_traj, sim_params.max_bond_dim, sim_params.truncation_threshold, 0, 0,
-                                   A.YAQS_PREC_FP64, traj_offset)
+        meth = {"tebd": A.YAQS_METHOD_TEBD, "tdvp": A.YAQS_METHOD_TDVP}
+        self.cfg = A.CircuitConfig(self.num_traj, sim_params.max_bond_dim, sim_params.truncation_threshold,
+                                   meth[local_method], meth[long_range_method], A.YAQS_PREC_FP64, traj_offset)
         self.n_out = sample_plan(circ)[2]
 
     @staticmethod
@@ -598,6 +659,13 @@ class CircuitDescriptors:
             m = _c64(g.op)
             for e in range(m.size):
                 d.matrix[e] = m[e]
+            if g.generator is not None and len(g.sites) == 2:
+                d.has_generator = 1
+                d.coeff = g.coeff
+                g1, g2 = _c64(g.generator[0]), _c64(g.generator[1])
+                for e in range(8):
+                    d.gen1[e] = g1[e]
+                    d.gen2[e] = g2[e]
         return gd
 
 

@@ -23,10 +23,12 @@
 struct DevGate {
   int kind;  // 1 one-qubit, 2 two-qubit
   int a, b;  // sorted sites for 2-qubit gates (a < b)
+  int wm;    // TDVP window: offset of its maps in DigParams::wm, -1 for TEBD
   cplx mat[16];
 };
 
 struct DigParams {
+  const WMat* wm;  // per TDVP gate with window length n: heff1[n], heff2[n-1], envL[n], envR[n]
   const DevGate* gates;
   const int* layer_off;   // [n_layers + 1] into gates
   const int* sample_col;  // [n_layers] measurement column after the layer, -1 for none
@@ -68,6 +70,40 @@ __device__ void apply_window_tebd(Ctx& c, const DState& s, const DevGate& g) {
   } else {
     tebd_apply(c, s, g.mat, g.a);
   }
+}
+
+// apply_window! with method :TDVP (DigitalTJM.jl:335-358): the window
+// a..b evolves under the product MPO coeff g1 (x) 1 ... 1 (x) g2
+// (construct_window_mpo, DigitalTJM.jl:192-236) by one forward circuit 2-site
+// sweep (_tdvp_sweep_circuit_2site!, Algorithms.jl:606-627): each pair by +1
+// with the right site back-evolved by -1 (:631-672), the last pair by +1
+// split to the right (:762-800); the centre ends on b.
+__device__ void apply_window_tdvp(Ctx& c, const DState& s, const DevGate& g, const WMat* wm) {
+  const int s1 = g.a, s2 = g.b, n = s2 - s1 + 1;
+  const WMat* h1 = wm;
+  const WMat* h2 = wm + n;
+  const WMat* eL = wm + 2 * n - 1;
+  const WMat* eR = wm + 3 * n - 1;
+  cplx* th = c.ws + c.P.lay.th;
+  shift_oc(c, s, s1);
+  if (c.sm.fail) return;
+  identity_env(c, envL(c, s1), s.chi[s1], 1);
+  identity_env(c, envR(c, s2 + 1), s.chi[s2 + 1], 1);
+  for (int j = n - 1; j >= 1; --j) update_right_w(c, s, s1 + j, eR[j]);
+  for (int j = 0; j + 2 < n && !c.sm.fail; ++j) {
+    const int i = s1 + j, l = s.chi[i], r = s.chi[i + 2];
+    merge(c, s, i, th);
+    evolve(c, th, l, 4, r, i, i + 2, h2[j], 1.0);
+    split(c, s, i, th, l, r, 0, false);
+    if (c.sm.fail) return;
+    update_left_w(c, s, i, eL[j]);
+    evolve(c, site_ptr(c, s, i + 1), s.chi[i + 1], 2, r, i + 1, i + 2, h1[j + 1], -1.0);
+  }
+  if (c.sm.fail) return;
+  const int i = s2 - 1, l = s.chi[i], r = s.chi[i + 2];
+  merge(c, s, i, th);
+  evolve(c, th, l, 4, r, i, i + 2, h2[n - 2], 1.0);
+  split(c, s, i, th, l, r, 0, false);  // the centre moves to s2
 }
 
 // Local dissipation (dt = 1) and jump step after a 2-qubit gate on (s1, s2),
@@ -276,7 +312,10 @@ __device__ void run_digital_step(Ctx& c, const DigParams& D, int launch) {
   for (int g = D.layer_off[l]; g < D.layer_off[l + 1] && !c.sm.fail; ++g) {
     const DevGate& G = D.gates[g];
     if (G.kind != 2) continue;
-    apply_window_tebd(c, st, G);
+    if (G.wm >= 0)
+      apply_window_tdvp(c, st, G, D.wm + G.wm);
+    else
+      apply_window_tebd(c, st, G);
     if (c.sm.fail) return;
     digital_noise(c, st, G.a, G.b);
     if (c.sm.fail) return;

@@ -336,6 +336,52 @@ HostWMat build_wmat(int no, int ni, F f) {
   return m;
 }
 
+// The sparse maps of an MPO (W(i, m, p_out, p_in, m') via Wat) in the order
+// heff1[L], heff2[L-1] (merged two-site W of Algorithms.jl:639-643),
+// envL[L], envR[L].
+template <class F>
+void append_mpo_wmats(int L, const int* w, F Wat, std::vector<HostWMat>& all) {
+  for (int i = 0; i < L; ++i) {  // heff1: M[(p' + 2 m'), (m + wl p)]
+    int wl = w[i], wr = w[i + 1];
+    all.push_back(build_wmat(2 * wr, wl * 2, [&](int o, int in) {
+      int pp = o % 2, mp = o / 2, m = in % wl, p = in / wl;
+      return Wat(i, m, pp, p, mp);
+    }));
+  }
+  for (int i = 0; i + 1 < L; ++i) {  // heff2 (merged)
+    int wl = w[i], wm = w[i + 1], wr = w[i + 2];
+    std::vector<hcd> G((size_t)wl * 16 * wr, 0.0);
+    for (int l = 0; l < wl; ++l)
+      for (int r = 0; r < wr; ++r)
+        for (int p1o = 0; p1o < 2; ++p1o)
+          for (int p2o = 0; p2o < 2; ++p2o)
+            for (int p1i = 0; p1i < 2; ++p1i)
+              for (int p2i = 0; p2i < 2; ++p2i) {
+                hcd s = 0;
+                for (int k = 0; k < wm; ++k) s += Wat(i, l, p1o, p1i, k) * Wat(i + 1, k, p2o, p2i, r);
+                G[l + (size_t)wl * ((p1o + 2 * p2o) + 4 * ((p1i + 2 * p2i) + 4 * (size_t)r))] = s;
+              }
+    all.push_back(build_wmat(4 * wr, wl * 4, [&](int o, int in) {
+      int pp = o % 4, mp = o / 4, m = in % wl, p = in / wl;
+      return G[m + (size_t)wl * (pp + 4 * (p + 4 * (size_t)mp))];
+    }));
+  }
+  for (int i = 0; i < L; ++i) {  // envL: M[(po + 2 m'), (ml + wl pi)]
+    int wl = w[i], wr = w[i + 1];
+    all.push_back(build_wmat(2 * wr, wl * 2, [&](int o, int in) {
+      int po = o % 2, mp = o / 2, ml = in % wl, pi = in / wl;
+      return Wat(i, ml, po, pi, mp);
+    }));
+  }
+  for (int i = 0; i < L; ++i) {  // envR: M[(po + 2 ml), (pi + 2 mr)]
+    int wl = w[i], wr = w[i + 1];
+    all.push_back(build_wmat(2 * wl, 2 * wr, [&](int o, int in) {
+      int po = o % 2, ml = o / 2, pi = in % 2, mr = in / 2;
+      return Wat(i, ml, po, pi, mr);
+    }));
+  }
+}
+
 // exp(c * H) for a small Hermitian H (cyclic complex Jacobi).
 void herm_expm(int n, const hcd* Hm, double c, hcd* out) {
   std::vector<hcd> A(Hm, Hm + n * n), V(n * n, 0.0);
@@ -836,45 +882,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
     return cload(H->tensors[i], (size_t)m + (size_t)w[i] * (po + 2 * (pi + 2 * (size_t)mr)));
   };
   std::vector<HostWMat> all;
-  for (int i = 0; i < L; ++i) {  // heff1
-    int wl = w[i], wr = w[i + 1];
-    all.push_back(build_wmat(2 * wr, wl * 2, [&](int o, int in) {
-      int pp = o % 2, mp = o / 2, m = in % wl, p = in / wl;
-      return Wat(i, m, pp, p, mp);
-    }));
-  }
-  for (int i = 0; i + 1 < L; ++i) {  // heff2 (merged)
-    int wl = w[i], wm = w[i + 1], wr = w[i + 2];
-    std::vector<hcd> G((size_t)wl * 16 * wr, 0.0);
-    for (int l = 0; l < wl; ++l)
-      for (int r = 0; r < wr; ++r)
-        for (int p1o = 0; p1o < 2; ++p1o)
-          for (int p2o = 0; p2o < 2; ++p2o)
-            for (int p1i = 0; p1i < 2; ++p1i)
-              for (int p2i = 0; p2i < 2; ++p2i) {
-                hcd s = 0;
-                for (int k = 0; k < wm; ++k) s += Wat(i, l, p1o, p1i, k) * Wat(i + 1, k, p2o, p2i, r);
-                G[l + (size_t)wl * ((p1o + 2 * p2o) + 4 * ((p1i + 2 * p2i) + 4 * (size_t)r))] = s;
-              }
-    all.push_back(build_wmat(4 * wr, wl * 4, [&](int o, int in) {
-      int pp = o % 4, mp = o / 4, m = in % wl, p = in / wl;
-      return G[m + (size_t)wl * (pp + 4 * (p + 4 * (size_t)mp))];
-    }));
-  }
-  for (int i = 0; i < L; ++i) {  // envL: M[(po + 2 m'), (ml + wl pi)]
-    int wl = w[i], wr = w[i + 1];
-    all.push_back(build_wmat(2 * wr, wl * 2, [&](int o, int in) {
-      int po = o % 2, mp = o / 2, ml = in % wl, pi = in / wl;
-      return Wat(i, ml, po, pi, mp);
-    }));
-  }
-  for (int i = 0; i < L; ++i) {  // envR: M[(po + 2 ml), (pi + 2 mr)]
-    int wl = w[i], wr = w[i + 1];
-    all.push_back(build_wmat(2 * wl, 2 * wr, [&](int o, int in) {
-      int po = o % 2, ml = o / 2, pi = in % 2, mr = in / 2;
-      return Wat(i, ml, po, pi, mr);
-    }));
-  }
+  append_mpo_wmats(L, w.data(), Wat, all);
   for (int b = 0; b <= L; ++b) {  // bond: identity on the MPO bond, physical dimension 1
     all.push_back(build_wmat(w[b], w[b], [&](int o, int in) { return hcd(o == in ? 1.0 : 0.0, 0.0); }));
     all.back().ident = 1;
@@ -1186,8 +1194,9 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   for (int b = 0; b <= L; ++b)
     if (psi0->chi[b] < 1) return set_err(ctx, YAQS_E_ARG, "bond dimension < 1");
   if (cfg->num_traj < 1 || cfg->max_bond_dim < 1) return set_err(ctx, YAQS_E_ARG, "bad config (num_traj, max_bond_dim)");
-  if (cfg->local_method != YAQS_METHOD_TEBD || cfg->long_range_method != YAQS_METHOD_TEBD)
-    return set_err(ctx, YAQS_E_UNSUPPORTED, "only TEBD gate application is served by this build");
+  if (cfg->local_method < YAQS_METHOD_TEBD || cfg->local_method > YAQS_METHOD_TDVP ||
+      cfg->long_range_method < YAQS_METHOD_TEBD || cfg->long_range_method > YAQS_METHOD_TDVP)
+    return set_err(ctx, YAQS_E_ARG, "gate methods must be YAQS_METHOD_TEBD or YAQS_METHOD_TDVP");
   if (cfg->precision != YAQS_PREC_FP64)
     return set_err(ctx, YAQS_E_UNSUPPORTED,
                    "digital runs are served in ComplexF64 only (their work is SVD/QR, which stays FP64)");
@@ -1200,13 +1209,27 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   HostCircuit C;
   int st = plan_circuit(ctx, gates, n_gates, L, C);
   if (st != YAQS_OK) return st;
+  // gates applied through a TDVP window need their generators
+  auto by_tdvp = [&](const yaqs_gate_desc& q) {
+    if (q.kind != YAQS_GATE_2Q) return false;
+    const bool lr = std::abs(q.site[0] - q.site[1]) > 1;
+    return (lr ? cfg->long_range_method : cfg->local_method) == YAQS_METHOD_TDVP;
+  };
+  bool any_tdvp = false;
+  for (int g = 0; g < n_gates; ++g)
+    if (by_tdvp(gates[g])) {
+      any_tdvp = true;
+      if (!gates[g].has_generator)
+        return set_err(ctx, YAQS_E_ARG, "a gate applied by TDVP needs its generator (GateLibrary.generator)");
+    }
+  const int kdim = 25;  // expm_krylov(..., 25) of the circuit sweeps (Algorithms.jl:185)
 
-  // ---- capacities and layout (no environments or Krylov basis) ----
+  // ---- capacities and layout (environments and Krylov basis only for TDVP windows) ----
   std::vector<int> chi0(psi0->chi, psi0->chi + L + 1), w(L + 1, 1);
   Caps caps;
   if (!plan_caps(L, chi0.data(), w.data(), cfg->max_bond_dim, caps))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
-  const WsLayout lay = plan_layout(L, caps, w.data(), false, 0, false);
+  const WsLayout lay = plan_layout(L, caps, w.data(), any_tdvp, kdim, false);
   const std::vector<int>& cap = caps.cap;
   const std::vector<long long>& mps_off = caps.mps_off;
   const std::vector<long long>& env_off = caps.env_off;
@@ -1264,6 +1287,9 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   P.ncols = ncols;
   P.dt = 1.0;
   P.thr = cfg->truncation_threshold;
+  P.kc.kdim = kdim;
+  P.kc.tol = 1e-10;
+  P.kc.exit_tol = 1e-12;
   P.seed = rng->seed;
   P.stride = rng->stride;
   P.mps_size = mps_size;
@@ -1276,8 +1302,9 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, n_layers + 1, pool);
   if (st != YAQS_OK) return st;
 
-  // ---- gates in layer order ----
+  // ---- gates in layer order; window maps of the TDVP gates ----
   std::vector<DevGate> hg;
+  std::vector<HostWMat> wall;
   std::vector<int> layer_off(1, 0), sample_col(std::max(n_layers, 1), -1);
   int col = C.sample_at_start ? 1 : 0;
   for (int l = 0; l < n_layers; ++l) {
@@ -1288,8 +1315,24 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
       d.kind = q.kind;
       d.a = q.kind == YAQS_GATE_2Q ? std::min(q.site[0], q.site[1]) : q.site[0];
       d.b = q.kind == YAQS_GATE_2Q ? std::max(q.site[0], q.site[1]) : q.site[0];
+      d.wm = -1;
       const int dd = q.kind == YAQS_GATE_2Q ? 4 : 2;
       for (int e = 0; e < dd * dd; ++e) d.mat[e] = make_double2(q.matrix[2 * e], q.matrix[2 * e + 1]);
+      if (by_tdvp(q)) {
+        // construct_window_mpo (DigitalTJM.jl:192-236): coeff g(s1) on the
+        // first window site, g(s2) on the last, identities between, bond 1
+        const int n = d.b - d.a + 1;
+        const double* gs1 = q.site[0] == d.a ? q.gen1 : q.gen2;
+        const double* gs2 = q.site[0] == d.a ? q.gen2 : q.gen1;
+        std::vector<int> wone(n + 1, 1);
+        auto Wat = [&](int j, int, int po, int pi, int) {
+          if (j == 0) return q.coeff * cload(gs1, po + 2 * pi);
+          if (j == n - 1) return cload(gs2, po + 2 * pi);
+          return hcd(po == pi ? 1.0 : 0.0, 0.0);
+        };
+        d.wm = (int)wall.size();
+        append_mpo_wmats(n, wone.data(), Wat, wall);
+      }
       hg.push_back(d);
     }
     layer_off.push_back((int)hg.size());
@@ -1305,6 +1348,16 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   CUDA_TRY(ctx, cudaMemcpy(d_layer_off, layer_off.data(), layer_off.size() * sizeof(int), cudaMemcpyHostToDevice));
   CUDA_TRY(ctx, cudaMemcpy(d_sample_col, sample_col.data(), sample_col.size() * sizeof(int), cudaMemcpyHostToDevice));
   DigParams& D = run->D;
+  D.wm = nullptr;
+  if (!wall.empty()) {
+    std::vector<WMat> views;
+    st = upload_wmats(ctx, run->dm, wall, views);
+    if (st != YAQS_OK) return st;
+    WMat* d_wm;
+    CUDA_TRY(ctx, run->dm.alloc(&d_wm, views.size()));
+    CUDA_TRY(ctx, cudaMemcpy(d_wm, views.data(), views.size() * sizeof(WMat), cudaMemcpyHostToDevice));
+    D.wm = d_wm;
+  }
   D.gates = d_gates;
   D.layer_off = d_layer_off;
   D.sample_col = d_sample_col;

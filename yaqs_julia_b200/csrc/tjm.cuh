@@ -316,8 +316,8 @@ __device__ void identity_env(Ctx& c, cplx* E, int dim, int w) {
   __syncthreads();
 }
 
-// EL[i+1] from EL[i], A_i, W_i  (update_left_environment)
-__device__ void update_left(Ctx& c, const DState& s, int i) {
+// EL[i+1] from EL[i], A_i and the map Wenv of W_i (update_left_environment)
+__device__ void update_left_w(Ctx& c, const DState& s, int i, const WMat& Wenv) {
   ProfScope prof_scope_(PF_ENV);
   const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
   const cplx* A = site_ptr(c, s, i);
@@ -351,18 +351,20 @@ __device__ void update_left(Ctx& c, const DState& s, int i) {
   g.oo1 = l;
   g.oo2 = 2 * l;
   if (c.P.mixed) {
-    dev_wapply<cflt>(T1f, T2f, c.P.wm_envL[i], g, c.sm.e.u.gw.w);
+    dev_wapply<cflt>(T1f, T2f, Wenv, g, c.sm.e.u.gw.w);
     cta_gemm_tf32<cplx>(gemm_args_f(r, wr * r, 2 * l, Af, 2 * l, 1, T2f, 1, 2 * l, envL(c, i + 1), 1, r, true, false),
                         gf);
   } else {
-    dev_wapply<cplx>(T1, T2, c.P.wm_envL[i], g, c.sm.e.u.gw.w);
+    dev_wapply<cplx>(T1, T2, Wenv, g, c.sm.e.u.gw.w);
     cta_gemm(gemm_args(r, wr * r, 2 * l, A, 2 * l, 1, T2, 1, 2 * l, envL(c, i + 1), 1, r, true, false),
              c.sm.e.u.gw.g);
   }
 }
 
-// ER[i] from ER[i+1], A_i, W_i  (update_right_environment)
-__device__ void update_right(Ctx& c, const DState& s, int i) {
+__device__ void update_left(Ctx& c, const DState& s, int i) { update_left_w(c, s, i, c.P.wm_envL[i]); }
+
+// ER[i] from ER[i+1], A_i and the map Wenv of W_i (update_right_environment)
+__device__ void update_right_w(Ctx& c, const DState& s, int i, const WMat& Wenv) {
   ProfScope prof_scope_(PF_ENV);
   const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
   const cplx* A = site_ptr(c, s, i);
@@ -395,13 +397,15 @@ __device__ void update_right(Ctx& c, const DState& s, int i) {
   g.oo1 = 1;
   g.oo2 = 2 * r;
   if (c.P.mixed) {
-    dev_wapply<cflt>(T1f, T2f, c.P.wm_envR[i], g, c.sm.e.u.gw.w);
+    dev_wapply<cflt>(T1f, T2f, Wenv, g, c.sm.e.u.gw.w);
     cta_gemm_tf32<cplx>(gemm_args_f(l, wl * l, 2 * r, Af, 1, l, T2f, 1, 2 * r, envR(c, i), 1, l, true, false), gf);
   } else {
-    dev_wapply<cplx>(T1, T2, c.P.wm_envR[i], g, c.sm.e.u.gw.w);
+    dev_wapply<cplx>(T1, T2, Wenv, g, c.sm.e.u.gw.w);
     cta_gemm(gemm_args(l, wl * l, 2 * r, A, 1, l, T2, 1, 2 * r, envR(c, i), 1, l, true, false), c.sm.e.u.gw.g);
   }
 }
+
+__device__ void update_right(Ctx& c, const DState& s, int i) { update_right_w(c, s, i, c.P.wm_envR[i]); }
 
 // ---------------------------------------------------------------------------
 // Two-site TDVP (Algorithms.jl:580-760)
