@@ -481,8 +481,11 @@ vector<cd> expm_krylov(Op&& op, const vector<cd>& v, double dt, const KrylovPara
   for (int k = 1; k <= kp.kdim; ++k) {
     op(Q[k - 1], w);
     cnt.matvecs++;
-    // two-pass classical Gram-Schmidt against q_1..q_k
+    // classical Gram-Schmidt against q_1..q_k with one refinement pass when
+    // the first kept less than 1/sqrt(2) of the norm (DGKS criterion, the
+    // eta of KrylovKit's iteratively refined Gram-Schmidt)
     double a_k = 0.0;
+    double nprev = nrm2(w.data(), n), b_k = nprev;
     for (int pass = 0; pass < 2; ++pass) {
       vector<cd> h(k);
       for (int j = 0; j < k; ++j) {
@@ -497,9 +500,11 @@ vector<cd> expm_krylov(Op&& op, const vector<cd>& v, double dt, const KrylovPara
         for (long i = 0; i < n; ++i) w[i] -= hj * qj[i];
       }
       a_k += h[k - 1].real();
+      b_k = nrm2(w.data(), n);
+      if (b_k >= 0.7071067811865476 * nprev) break;
+      nprev = b_k;
     }
     alpha.push_back(a_k);
-    double b_k = nrm2(w.data(), n);
     m = k;
     if (b_k <= tau * kp.tol) break;  // invariant subspace (KrylovKit normres test)
     if (k == kp.kdim) break;

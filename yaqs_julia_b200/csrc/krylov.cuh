@@ -5,8 +5,9 @@
 //   T2[a,p',m',c] = sum_{m,p} W[m,p',p,m'] T1[a,m,p,c]         (sparse MPO apply)
 //   y[a,p',b]     = sum_{m',c} T2[a,p',m',c] R[b,m',c]         (GEMM)
 // dev_expm_krylov restates expm_krylov (Algorithms.jl:144-187) / KrylovKit
-// exponentiate: Lanczos with two-pass classical Gram-Schmidt against the
-// whole basis, stopping at krylov_dim, at breakdown (beta <= |dt| tol), or
+// exponentiate: Lanczos with classical Gram-Schmidt against the whole basis,
+// refined by a second pass when the first kept less than 1/sqrt(2) of the
+// norm (DGKS), stopping at krylov_dim, at breakdown (beta <= |dt| tol), or
 // once prod(beta_i |dt|)/k! <= exit_tol; the small tridiagonal exponential
 // is taken on one warp by Taylor series over substeps of norm <= 1/2.
 #pragma once
@@ -250,7 +251,10 @@ __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt,
     dev_heff(h, Q + qs * (k - 1), w, sm);
     ++mv;
     ProfScope orth_scope_(PF_ORTH);
+    // classical Gram-Schmidt with one refinement pass when the first kept
+    // less than 1/sqrt(2) of the norm (DGKS criterion)
     double a_k = 0.0;
+    double nprev = sqrt(cta_norm2(w, n, sm.r)), b_k = nprev;
     for (int pass = 0; pass < 2; ++pass) {
       for (int j0 = 0; j0 < k; j0 += 8) {
         double d[16];
@@ -271,15 +275,18 @@ __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt,
         if (tid < 8 && j0 + tid < k) sm.k.h[j0 + tid] = make_double2(d[2 * tid], d[2 * tid + 1]);
       }
       __syncthreads();
+      double part = 0.0;
       for (long long i = tid; i < n; i += NT) {
         cplx v = w[i];
         for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
         w[i] = v;
+        part += cabs2(v);
       }
       a_k += sm.k.h[k - 1].x;
-      __syncthreads();
+      b_k = sqrt(block_sum(part, sm.r));
+      if (b_k >= 0.7071067811865476 * nprev) break;
+      nprev = b_k;
     }
-    const double b_k = sqrt(cta_norm2(w, n, sm.r));
     if (tid == 0) sm.k.alpha[k - 1] = a_k;
     m = k;
     if (b_k <= tau * kc.tol) break;
