@@ -213,3 +213,19 @@ def test_tdvp_local_tebd_long_range_mix(oracle):
     got = api.run_circuit_descriptors(d)
     assert np.abs(got.trajectories - ref).max() < 1e-10
     assert np.array_equal(got.max_bond, chi_ref)
+
+
+@pytest.mark.parametrize("unravel", ["projector", "unitary_gauss"])
+def test_unraveled_gate_noise(oracle, unravel):
+    """Gate-local noise with unraveled processes (the paper's digital
+    unraveling studies): device vs oracle on injected draws."""
+    L = 6
+    c = _brickwork(L, 2, seed=21)
+    info = [{"name": n, "sites": [i], "strength": 0.05, "unraveling": unravel}
+            for i in range(1, L + 1) for n in ("pauli_x", "pauli_z")]
+    info += [{"name": "crosstalk_zz", "sites": [i, i + 1], "strength": 0.05, "unraveling": unravel}
+             for i in range(1, L)]
+    nm = api.NoiseModel(info, L)
+    u = np.random.default_rng(5).random((8, api.max_draws_digital(c)))
+    got, _ = _compare(oracle, L, c, _zs(L), nm=nm, num_traj=8, uniforms=u)
+    assert got.stats["jumps"] > 0

@@ -241,3 +241,22 @@ def test_dynamic_tdvp_mixed_precision(oracle):
     ref, _, _ = oracle.analog_run(d)
     got = api.run_descriptors(d)
     assert np.abs(got.trajectories - ref).max() < 1e-5
+
+
+@pytest.mark.parametrize("unravel", ["projector", "unitary_2pt", "unitary_gauss"])
+def test_unraveled_noise_matches_oracle(oracle, unravel):
+    """Unraveling expansions (Noise.jl:134-252) on the device: non-Pauli
+    2-site projectors take the merge/SVD sweeps, unitaries the norm fast path."""
+    L = 6
+    H = api.init_ising(L, 1.0, 0.6)
+    obs = [api.Observable(f"X{i}", api.X, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.6, dt=0.05, num_traj=6, max_bond_dim=16)
+    info = [{"name": "pauli_z", "sites": [i], "strength": 0.2} for i in range(1, L + 1)]
+    info += [{"name": "crosstalk_xx", "sites": [2, 3], "strength": 0.3}]
+    for d in info:
+        d["unraveling"] = unravel
+        d["theta0"] = np.pi / 3
+    nm = api.NoiseModel(info, L)
+    u = np.random.default_rng(17).random((6, api.max_draws(cfg)))
+    got, _ = _compare(oracle, api.MPS(L, state="x+"), H, cfg, nm, uniforms=u)
+    assert got.stats["jumps"] > 0

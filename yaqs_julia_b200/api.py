@@ -365,12 +365,99 @@ class LocalNoiseProcess:
         self.matrix = np.asarray(matrix, dtype=np.complex128)
 
 
-class NoiseModel:
-    """NoiseModel(processes_info, num_qubits) with the "standard" unraveling
-    (src/Noise.jl:299-420).  Long-range and unraveling expansions are not
-    served by this engine and raise NotImplementedError."""
+def _expm(a: np.ndarray) -> np.ndarray:
+    from scipy.linalg import expm
+    return expm(np.asarray(a, dtype=np.complex128))
 
-    def __init__(self, processes, num_qubits: int | None = None):
+
+def _proc_operator(p: dict) -> np.ndarray:
+    """Noise.get_operator_from_proc (src/Noise.jl:422-433): the "matrix" key
+    wins, else the operator named by "name"."""
+    if "matrix" in p:
+        return np.asarray(p["matrix"], dtype=np.complex128)
+    return get_operator(p["name"])
+
+
+def _projector_expansion(p, sites, P, gamma):
+    """add_projector_expansion! (src/Noise.jl:134-154): jump operators I +- P
+    at rate gamma/2 each, named projector_plus_<name> / projector_minus_<name>."""
+    eye = np.eye(P.shape[0], dtype=np.complex128)
+    return [LocalNoiseProcess(f"projector_{comp}_{p['name']}", sites, gamma / 2.0, eye + sgn * P)
+            for comp, sgn in (("plus", 1.0), ("minus", -1.0))]
+
+
+def _unitary_2pt_expansion(p, sites, P, gamma, theta0):
+    """add_unitary_2pt_expansion! (src/Noise.jl:184-197): U = exp(+-i theta0 P)
+    at rate (gamma / sin^2 theta0) / 2 each, named unitary2pt_plus/minus_<name>."""
+    s_val = math.sin(theta0) ** 2
+    if not s_val > 0:
+        raise ValueError("theta0 too small")
+    lam = gamma / s_val
+    return [LocalNoiseProcess(f"unitary2pt_{comp}_{p['name']}", sites, lam / 2.0, _expm(1j * sgn * theta0 * P))
+            for comp, sgn in (("plus", 1.0), ("minus", -1.0))]
+
+
+def gauss_angles(sigma: float, M: int, theta_max: float):
+    """The angle grid and weights of add_unitary_gauss_expansion!
+    (src/Noise.jl:225-240): (M+1)//2 equispaced angles on [0, theta_max]
+    mirrored to negative angles, Gaussian weights exp(-theta^2 / 2 sigma^2)
+    normalised to sum 1 and symmetrised."""
+    n_pos = (M + 1) // 2
+    if n_pos == 1 and theta_max != 0.0:
+        raise ValueError("range(0, theta_max, length=1) needs theta_max == 0")
+    pos = np.linspace(0.0, theta_max, n_pos)
+    thetas = np.concatenate([-pos[1:][::-1], pos])
+    w = np.exp(-0.5 * (thetas / sigma) ** 2)
+    w = w / w.sum()
+    w = 0.5 * (w + w[::-1])
+    return thetas, w
+
+
+def _unitary_gauss_expansion(p, sites, P, gamma, sigma, M, k):
+    """add_unitary_gauss_expansion! (src/Noise.jl:225-252): one unitary
+    U = exp(i theta_k P) per grid angle at rate lambda * w_k with
+    lambda = gamma / sum_k w_k sin^2 theta_k, named unitary_gauss_<k>_<name>
+    (k from 0).  Per-process "M" and "theta_max" override the grid."""
+    M = int(p.get("M", M))
+    theta_max = float(p.get("theta_max", k * sigma))
+    thetas, w = gauss_angles(sigma, M, theta_max)
+    s_weight = float(np.sum(w * np.sin(thetas) ** 2))
+    if not s_weight > 1e-12:
+        raise ValueError("E[sin^2 theta] too small")
+    lam = gamma / s_weight
+    return [LocalNoiseProcess(f"unitary_gauss_{idx}_{p['name']}", sites, lam * wk, _expm(1j * th * P))
+            for idx, (wk, th) in enumerate(zip(w, thetas)) if wk > 0.0]
+
+
+UNRAVELINGS = ("standard", "projector", "unitary_2pt", "unitary_gauss", "analog_auto")
+
+
+class NoiseModel:
+    """NoiseModel(processes_info, num_qubits; theta0, dt, sigma, gauss_M,
+    gauss_k) (src/Noise.jl:299-420).
+
+    Each process dict has "name", "sites", "strength" and optionally
+    "matrix" and "unraveling":
+      - "standard": the jump operator itself (the matrix, or the named one);
+      - "projector": I +- P at gamma/2 each;
+      - "unitary_2pt": exp(+-i theta0 P) at gamma / (2 sin^2 theta0) each
+        (per-process "theta0" overrides the keyword);
+      - "unitary_gauss": exp(i theta_k P) on a Gaussian angle grid (per-process
+        "sigma", "M", "gauss_k", "theta_max" override the keywords);
+      - "analog_auto": deprecated, warns and falls back to "standard".
+    All of these give the same Lindbladian for a Pauli P; they differ in the
+    trajectories.  Expanded processes keep the given site order sorted (the
+    reference keeps the unsorted order for expansions, so a descending
+    adjacent pair would never be a jump candidate there).  With dt given, a
+    unitary_2pt rate with lambda*dt > 0.1 warns as in the reference.
+
+    Long-range processes (two sites more than one apart) are MPO noise
+    processes in the reference (Noise.jl:71-131,155-182,199-223,254-290);
+    this engine does not serve them and raises NotImplementedError."""
+
+    def __init__(self, processes, num_qubits: int | None = None, *, theta0: float = math.pi / 2,
+                 dt: float | None = None, sigma: float = 1.0, gauss_M: int = 11, gauss_k: float = 4.0):
+        import warnings
         self.processes = []
         for p in processes:
             if isinstance(p, LocalNoiseProcess):
@@ -378,17 +465,36 @@ class NoiseModel:
                 continue
             name = p["name"]
             sites = list(p["sites"])
+            strength = float(p["strength"])
             unravel = p.get("unraveling", "standard")
-            if unravel not in ("standard",):
-                raise NotImplementedError(f"unraveling {unravel!r} is not served")
+            if unravel not in UNRAVELINGS:
+                raise ValueError(f"unknown unraveling {unravel!r}")
             if len(sites) == 2:
                 sites = sorted(sites)
             if not sites or len(sites) > 2:
                 raise ValueError("Invalid sites")
             if len(sites) == 2 and sites[1] - sites[0] > 1:
                 raise NotImplementedError("long-range (MPO) noise processes are not served")
-            mat = np.asarray(p["matrix"], dtype=np.complex128) if "matrix" in p else get_operator(name)
-            self.processes.append(LocalNoiseProcess(name, sites, p["strength"], mat))
+            if unravel == "projector":
+                self.processes += _projector_expansion(p, sites, _proc_operator(p), strength)
+                continue
+            if unravel == "unitary_2pt":
+                th = float(p.get("theta0", theta0))
+                s_val = math.sin(th) ** 2
+                if s_val > 1e-12 and dt is not None and strength / s_val * dt > 0.1:
+                    warnings.warn(f"Stability Warning: theta0={th} is too small for dt={dt} "
+                                  f"(lambda*dt = {strength / s_val * dt} > 0.1)")
+                self.processes += _unitary_2pt_expansion(p, sites, _proc_operator(p), strength, th)
+                continue
+            if unravel == "unitary_gauss":
+                self.processes += _unitary_gauss_expansion(
+                    p, sites, _proc_operator(p), strength, float(p.get("sigma", sigma)),
+                    int(p.get("M", gauss_M)), float(p.get("gauss_k", gauss_k)))
+                continue
+            if unravel == "analog_auto":
+                warnings.warn("Unraveling mode 'analog_auto' is deprecated. "
+                              "Please choose 'unitary_2pt' or 'unitary_gauss' manually.")
+            self.processes.append(LocalNoiseProcess(name, sites, strength, _proc_operator(p)))
 
 
 # ---------------------------------------------------------------------------
