@@ -849,6 +849,14 @@ struct NoiseProc {
   bool pauli_name, pauli_proc;
   cd diss_half[16];  // expm(-0.5*dt*gamma*L^dag L) for dt/2 (computed per run)
   cd diss_full[16];  // ... for dt
+  // Long-range process (MPONoiseProcess, Noise.jl:22-33) on s0 < s1 - 1:
+  // O = alpha*1 + beta*(sig at s0)(tau at s1) (build_mpo_phys, Noise.jl:71-131).
+  // pauli_proc marks the "pauli_long_range" candidate (StochasticProcess.jl:
+  // 176-185), otherwise "mpo_general"; diss_rate is the scalar decay rate of
+  // handle_longrange_scalar! (Dissipation.jl:161-204).
+  bool lr = false;
+  cd sig[4], tau[4], alpha, beta;
+  double diss_rate = 0.0;
 };
 
 struct Obs {
@@ -1233,7 +1241,10 @@ void apply_dissipation(const Problem& P, const NoiseSet& N, State& s, bool full_
     if (i > 0) {
       for (const auto& pr : N.procs) {
         if (pr.nsites == 2 && pr.s1 == i) {
-          if (pr.pauli_name) {
+          if (pr.lr) {  // handle_longrange_scalar! (Dissipation.jl:161-204)
+            double f = std::exp(-0.5 * dt * pr.diss_rate);
+            for (auto& x : s.t[i].v) x *= f;
+          } else if (pr.pauli_name) {
             double f = std::exp(-0.5 * dt * pr.gamma);
             for (auto& x : s.t[i].v) x *= f;
           } else {
@@ -1254,6 +1265,70 @@ void apply_dissipation(const Problem& P, const NoiseSet& N, State& s, bool full_
 // ---------------------------------------------------------------------------
 // Stochastic process (StochasticProcess.jl:35-38, 89-212, 219-330)
 // ---------------------------------------------------------------------------
+// MPS.truncate! (MPS.jl:320-440): centre to site 1, one SVD sweep 1 -> L-1
+// with the absolute min-2 rule (keep the crossing value, at most
+// max_bond_dim), then normalize!.
+void mps_truncate(const Problem& P, State& s, Counters& cnt) {
+  shift_oc(s, 0);
+  for (int i = 0; i + 1 < s.L; ++i) {
+    Ten Th = merge(s.t[i], s.t[i + 1]);
+    Ten U, V;
+    split_theta(Th, 0, P.thr, P.max_bond, false, U, V, cnt);
+    s.t[i] = std::move(U);
+    s.t[i + 1] = std::move(V);
+  }
+  s.oc = s.L - 1;
+  normalize_mps(s);
+}
+
+// MPO of a long-range process (build_mpo_phys, Noise.jl:71-131): identity
+// outside [s0, s1]; row [1, sig] at s0; diag(1, 1) in between; column
+// [alpha 1; beta tau] at s1.  Tensors (wl, out, in, wr).
+Wt lr_mpo_site(const NoiseProc& pr, int k) {
+  const int a = pr.s0, b = pr.s1;
+  const int wl = (k > a && k <= b) ? 2 : 1, wr = (k >= a && k < b) ? 2 : 1;
+  Wt W(wl, 2, wr);
+  for (int po = 0; po < 2; ++po)
+    for (int pi = 0; pi < 2; ++pi) {
+      const cd id = po == pi ? 1.0 : 0.0;
+      if (k < a || k > b) {
+        W.at(0, po, pi, 0) = id;
+      } else if (k == a) {
+        W.at(0, po, pi, 0) = id;
+        W.at(0, po, pi, 1) = pr.sig[po + 2 * pi];
+      } else if (k < b) {
+        W.at(0, po, pi, 0) = id;
+        W.at(1, po, pi, 1) = id;
+      } else {
+        W.at(0, po, pi, 0) = pr.alpha * id;
+        W.at(1, po, pi, 0) = pr.beta * pr.tau[po + 2 * pi];
+      }
+    }
+  return W;
+}
+
+// apply_mpo_jump! (StochasticProcess.jl:46-82): contract the MPO into the
+// MPS site by site, C[la,lw,po,ra,rw] = sum_pi A[la,pi,ra] W[lw,po,pi,rw]
+// reshaped to (la*lw, po, ra*rw), then truncate!.
+void apply_mpo_jump(const Problem& P, State& s, const NoiseProc& pr, Counters& cnt) {
+  for (int k = 0; k < s.L; ++k) {
+    const Ten& A = s.t[k];
+    const Wt W = lr_mpo_site(pr, k);
+    Ten C(A.l * W.wl, 2, A.r * W.wr);
+    for (int rw = 0; rw < W.wr; ++rw)
+      for (int ra = 0; ra < A.r; ++ra)
+        for (int po = 0; po < 2; ++po)
+          for (int lw = 0; lw < W.wl; ++lw)
+            for (int la = 0; la < A.l; ++la) {
+              cd acc = 0;
+              for (int pi = 0; pi < 2; ++pi) acc += A.at(la, pi, ra) * W.at(lw, po, pi, rw);
+              C.at(la + A.l * lw, po, ra + A.r * rw) = acc;
+            }
+    s.t[k] = std::move(C);
+  }
+  mps_truncate(P, s, cnt);
+}
+
 struct Cand {
   const NoiseProc* pr;
   double dp;
@@ -1286,7 +1361,7 @@ bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt
     }
     if (site < L - 1) {
       for (const auto& pr : N.procs) {
-        if (pr.nsites == 2 && pr.s0 == site) {
+        if (pr.nsites == 2 && !pr.lr && pr.s0 == site) {
           double nr;
           if (pr.pauli_proc) {
             nr = tnorm2(s.t[site]);
@@ -1299,6 +1374,20 @@ bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt
         }
       }
     }
+  }
+  // long-range processes, after every local candidate (StochasticProcess.jl:169-202)
+  for (const auto& pr : N.procs) {
+    if (!pr.lr) continue;
+    double nr;
+    if (pr.pauli_proc) {
+      nr = tnorm2(s.t[s.oc]);
+    } else {  // applied to a copy, truncated and renormalised, then its norm
+      State tmp = s;
+      Counters scratch{};
+      apply_mpo_jump(P, tmp, pr, scratch);
+      nr = tnorm2(tmp.t[tmp.oc]);
+    }
+    cands.push_back({&pr, dt * pr.gamma * nr});
   }
   double total = 0;
   for (auto& c : cands) total += c.dp;
@@ -1318,7 +1407,12 @@ bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt
     }
   }
   const NoiseProc& pr = *cands[chosen].pr;
-  if (pr.nsites == 1) {
+  if (pr.lr) {
+    // "pauli_long_range" has no branch of its own in the reference
+    // (StochasticProcess.jl:311 tests "mpo_pauli"), so only the final
+    // normalisation acts; "mpo_general" applies the operator.
+    if (!pr.pauli_proc) apply_mpo_jump(P, s, pr, cnt);
+  } else if (pr.nsites == 1) {
     shift_oc(s, pr.s0);
     apply_1site(s.t[pr.s0], pr.mat);
   } else {
@@ -1477,9 +1571,26 @@ bool load_noise(Problem& P, const yaqs_noise_desc* noise, std::string& err) {
     pr.gamma = q.strength;
     pr.pauli_name = q.pauli_name != 0;
     pr.pauli_proc = q.pauli_proc != 0;
-    if (q.nsites == 2 && pr.s1 != pr.s0 + 1) {
-      err = "only adjacent 2-site processes are supported";
+    if (q.nsites < 1 || q.nsites > 2 || pr.s0 < 0 || pr.s1 >= P.L || pr.s1 < pr.s0) {
+      err = "bad noise process sites";
       return false;
+    }
+    if (q.nsites == 2 && pr.s1 > pr.s0 + 1) {  // long-range: sig, tau, alpha, beta, dissipation rate
+      if (!pr.pauli_name) {
+        err = "Non-Pauli long-range processes not fully implemented";
+        return false;
+      }
+      pr.lr = true;
+      for (int e = 0; e < 4; ++e) {
+        pr.sig[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);
+        pr.tau[e] = cd(q.matrix[8 + 2 * e], q.matrix[9 + 2 * e]);
+      }
+      pr.alpha = cd(q.matrix[16], q.matrix[17]);
+      pr.beta = cd(q.matrix[18], q.matrix[19]);
+      pr.diss_rate = q.matrix[20];
+      if (pr.gamma != 0.0) P.noise.all_zero = false;
+      P.noise.procs.push_back(pr);
+      continue;
     }
     int dd = q.nsites == 1 ? 2 : 4;
     for (int e = 0; e < dd * dd; ++e) pr.mat[e] = cd(q.matrix[2 * e], q.matrix[2 * e + 1]);

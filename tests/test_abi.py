@@ -64,7 +64,8 @@ def test_abi_struct_layouts_match_header(tmp_path):
 
 def test_descriptor_validation_host_side():
     from yaqs_julia_b200 import api
-    with pytest.raises(NotImplementedError):
+    # a long-range process needs a Pauli pair in its name or factors (Noise.jl:399-404)
+    with pytest.raises(ValueError, match="Pauli pair"):
         api.NoiseModel([{"name": "pauli_z", "sites": [1, 3], "strength": 0.1}], 4)
     with pytest.raises(ValueError):
         H = api.init_ising(4, 1, 1)

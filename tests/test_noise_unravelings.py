@@ -73,9 +73,9 @@ def test_analog_auto_is_deprecated_standard():
     assert [p.name for p in m.processes] == ["lowering"] and np.array_equal(m.processes[0].matrix, api.LOWERING)
 
 
-def test_long_range_unravelings_are_not_served():
-    with pytest.raises(NotImplementedError):
-        api.NoiseModel([{"name": "crosstalk_xy", "sites": [1, 3], "strength": 0.05, "unraveling": "projector"}], 4)
+def test_long_range_processes_need_the_chain_length():
+    with pytest.raises(ValueError, match="num_qubits"):
+        api.NoiseModel([{"name": "crosstalk_xy", "sites": [1, 3], "strength": 0.05, "unraveling": "projector"}])
 
 
 def _dissipator(ops, rho):

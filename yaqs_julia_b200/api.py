@@ -365,6 +365,69 @@ class LocalNoiseProcess:
         self.matrix = np.asarray(matrix, dtype=np.complex128)
 
 
+class MPONoiseProcess:
+    """MPONoiseProcess(name, sites, strength, mpo, factors) (src/Noise.jl:22-33):
+    a process on two sites i < j that are not neighbours.  Its operator is
+    O = a*1 + b*(sigma at i)(tau at j), the MPO of build_mpo_phys
+    (Noise.jl:71-131), which ``mpo`` builds.  ``factors`` is (sigma, tau)
+    for the standard unraveling and empty for the expansions, as in the
+    reference."""
+
+    def __init__(self, name, sites, strength, sigma, tau, a, b, num_qubits, factors=()):
+        self.name = name
+        self.sites = sorted(int(x) for x in sites)
+        self.strength = float(strength)
+        self.sigma = np.asarray(sigma, dtype=np.complex128)
+        self.tau = np.asarray(tau, dtype=np.complex128)
+        self.a = complex(a)
+        self.b = complex(b)
+        self.num_qubits = int(num_qubits)
+        self.factors = [np.asarray(f, dtype=np.complex128) for f in factors]
+
+    @property
+    def mpo(self) -> "MPO":
+        return build_mpo_phys(self.num_qubits, self.sites[0], self.sites[1], self.sigma, self.tau, self.a, self.b)
+
+
+def build_mpo_phys(L: int, i: int, j: int, sigma, tau, a, b) -> "MPO":
+    """MPO of O = a*1 + b*(sigma_i tau_j), 1 <= i < j <= L (Noise.jl:71-131):
+    identity (1x1) outside [i, j], the row [1, sigma] at i, diag(1, 1)
+    between, the column [a 1; b tau] at j.  Tensors (left, out, in, right)."""
+    if not 1 <= i < j <= L:
+        raise ValueError("Require 1 <= i < j <= L")
+    tens = []
+    for k in range(1, L + 1):
+        if k < i or k > j:
+            T = np.zeros((1, 2, 2, 1), dtype=np.complex128)
+            T[0, :, :, 0] = I2
+        elif k == i:
+            T = np.zeros((1, 2, 2, 2), dtype=np.complex128)
+            T[0, :, :, 0] = I2
+            T[0, :, :, 1] = sigma
+        elif k < j:
+            T = np.zeros((2, 2, 2, 2), dtype=np.complex128)
+            T[0, :, :, 0] = I2
+            T[1, :, :, 1] = I2
+        else:
+            T = np.zeros((2, 2, 2, 1), dtype=np.complex128)
+            T[0, :, :, 0] = a * I2
+            T[1, :, :, 0] = b * np.asarray(tau)
+        tens.append(T)
+    return MPO(L, tens)
+
+
+def _lr_factors(p: dict):
+    """(sigma, tau) of a long-range process: the "factors" key, else the two
+    Pauli letters that end the name, as in "crosstalk_xy" (Noise.jl:162-171)."""
+    if "factors" in p:
+        sig, tau = p["factors"]
+        return np.asarray(sig, dtype=np.complex128), np.asarray(tau, dtype=np.complex128)
+    suffix = p["name"].split("_")[-1]
+    if len(suffix) != 2 or any(ch not in "xyz" for ch in suffix):
+        raise ValueError(f"Unknown Pauli pair in {p['name']!r}")
+    return _pauli(suffix[0]), _pauli(suffix[1])
+
+
 def _expm(a: np.ndarray) -> np.ndarray:
     from scipy.linalg import expm
     return expm(np.asarray(a, dtype=np.complex128))
@@ -432,6 +495,82 @@ def _unitary_gauss_expansion(p, sites, P, gamma, sigma, M, k):
 UNRAVELINGS = ("standard", "projector", "unitary_2pt", "unitary_gauss", "analog_auto")
 
 
+def _long_range_processes(p, sites, gamma, unravel, L, theta0, dt, sigma, gauss_M, gauss_k):
+    """The long-range branches of the NoiseModel constructor (Noise.jl:
+    155-182 projector, 199-223 unitary_2pt, 254-290 unitary_gauss, 355-400
+    standard)."""
+    import warnings
+    sig, tau = _lr_factors(p)
+    name = p["name"]
+    if unravel == "projector":
+        return [MPONoiseProcess(f"projector_{comp}_{name}", sites, gamma / 2.0, sig, tau, 1.0, sgn, L)
+                for comp, sgn in (("plus", 1.0), ("minus", -1.0))]
+    if unravel == "unitary_2pt":
+        th = float(p.get("theta0", theta0))
+        s_val = math.sin(th) ** 2
+        if not s_val > 1e-12:
+            raise ValueError("theta0 too small")
+        lam = gamma / s_val
+        if dt is not None and lam * dt > 0.1:
+            warnings.warn(f"Stability Warning: theta0={th} is too small for dt={dt} (lambda*dt = {lam * dt} > 0.1)")
+        return [MPONoiseProcess(f"unitary2pt_{comp}_{name}", sites, lam / 2.0, sig, tau, math.cos(th),
+                                1j * sgn * math.sin(th), L) for comp, sgn in (("plus", 1.0), ("minus", -1.0))]
+    if unravel == "unitary_gauss":
+        sg = float(p.get("sigma", sigma))
+        M = int(p.get("M", gauss_M))
+        theta_max = float(p.get("theta_max", float(p.get("gauss_k", gauss_k)) * sg))
+        thetas, w = gauss_angles(sg, M, theta_max)
+        lam = gamma / float(np.sum(w * np.sin(thetas) ** 2))
+        return [MPONoiseProcess(f"unitary_gauss_{idx}_{name}", sites, lam * wk, sig, tau, math.cos(th),
+                                1j * math.sin(th), L) for idx, (wk, th) in enumerate(zip(w, thetas)) if wk > 0.0]
+    if unravel == "analog_auto":
+        warnings.warn("Unraveling mode 'analog_auto' is deprecated. "
+                      "Please choose 'unitary_2pt' or 'unitary_gauss' manually.")
+    return [MPONoiseProcess(name, sites, gamma, sig, tau, 0.0, 1.0, L, factors=(sig, tau))]
+
+
+_LR_SCALAR_PREFIXES = ("projector_", "unitary2pt_", "unitary_gauss_", "crosstalk_", "pauli_")
+
+
+def long_range_flags(processes):
+    """Per long-range process: (dissipation rate, pauli_long_range) as the
+    reference decides them.  handle_longrange_scalar! (Dissipation.jl:161-204)
+    decays the state by exp(-dt/2 * rate) at the process's right site: a
+    projector pair shares one factor with the summed rate (the first of the
+    pair carries it, the mate 0), unitary components and Pauli/crosstalk
+    names use their own rate, any other name is an error.  A candidate is
+    "pauli_long_range" when is_pauli_proc holds and factors are stored
+    (StochasticProcess.jl:176-185, 343-357)."""
+    out = {}
+    done = set()
+    for k, p in enumerate(processes):
+        if not isinstance(p, MPONoiseProcess):
+            continue
+        nm = p.name
+        if nm.startswith("projector_"):
+            base = nm.replace("projector_plus_", "").replace("projector_minus_", "")
+            key = (tuple(p.sites), base)
+            if key in done:
+                rate = 0.0
+            else:
+                mates = [q for q in processes if isinstance(q, MPONoiseProcess) and tuple(q.sites) == key[0]
+                         and q.name.endswith(base) and q.name.startswith("projector_")]
+                if len(mates) != 2:
+                    raise ValueError(f"Incomplete projector pair for long-range channel {base} on {key[0]}")
+                rate = mates[0].strength + mates[1].strength
+                done.add(key)
+        elif nm.startswith(_LR_SCALAR_PREFIXES):
+            rate = p.strength
+        else:
+            raise NotImplementedError(f"Non-Pauli long-range processes not fully implemented for: {nm}")
+        if ("pauli" in nm or "crosstalk" in nm) and "projector" not in nm:
+            pauli = True
+        else:
+            pauli = bool(p.factors) and all(is_pauli_matrix(f) for f in p.factors)
+        out[k] = (rate, pauli and bool(p.factors))
+    return out
+
+
 class NoiseModel:
     """NoiseModel(processes_info, num_qubits; theta0, dt, sigma, gauss_M,
     gauss_k) (src/Noise.jl:299-420).
@@ -451,16 +590,19 @@ class NoiseModel:
     adjacent pair would never be a jump candidate there).  With dt given, a
     unitary_2pt rate with lambda*dt > 0.1 warns as in the reference.
 
-    Long-range processes (two sites more than one apart) are MPO noise
-    processes in the reference (Noise.jl:71-131,155-182,199-223,254-290);
-    this engine does not serve them and raises NotImplementedError."""
+    Long-range processes (two sites more than one apart) become
+    MPONoiseProcess entries (Noise.jl:155-182,199-223,254-290,355-400): the
+    standard unraveling keeps O = sigma_i tau_j with its factors; projector
+    gives 1 +- sigma_i tau_j, unitary_2pt cos(theta0) 1 +- i sin(theta0)
+    sigma_i tau_j, unitary_gauss cos(theta_k) 1 + i sin(theta_k) sigma_i tau_j
+    at the local expansions' rates."""
 
     def __init__(self, processes, num_qubits: int | None = None, *, theta0: float = math.pi / 2,
                  dt: float | None = None, sigma: float = 1.0, gauss_M: int = 11, gauss_k: float = 4.0):
         import warnings
         self.processes = []
         for p in processes:
-            if isinstance(p, LocalNoiseProcess):
+            if isinstance(p, (LocalNoiseProcess, MPONoiseProcess)):
                 self.processes.append(p)
                 continue
             name = p["name"]
@@ -474,7 +616,13 @@ class NoiseModel:
             if not sites or len(sites) > 2:
                 raise ValueError("Invalid sites")
             if len(sites) == 2 and sites[1] - sites[0] > 1:
-                raise NotImplementedError("long-range (MPO) noise processes are not served")
+                if num_qubits is None:
+                    raise ValueError("long-range processes need num_qubits")
+                if "mpo" in p:
+                    raise NotImplementedError("processes given as an explicit MPO are not served")
+                self.processes += _long_range_processes(p, sites, strength, unravel, int(num_qubits), theta0,
+                                                        dt, sigma, gauss_M, gauss_k)
+                continue
             if unravel == "projector":
                 self.processes += _projector_expansion(p, sites, _proc_operator(p), strength)
                 continue
@@ -583,8 +731,21 @@ class Descriptors:
         # noise
         procs = noise_model.processes if noise_model is not None else []
         arr = (A.NoiseProc * max(1, len(procs)))()
+        lr = long_range_flags(procs)
         for k, p in enumerate(procs):
             q = arr[k]
+            if isinstance(p, MPONoiseProcess):
+                # sigma, tau (column-major 2x2), a, b, dissipation rate
+                q.nsites = 2
+                q.site[0], q.site[1] = p.sites[0] - 1, p.sites[1] - 1
+                q.strength = p.strength
+                packed = np.concatenate([_c64(p.sigma), _c64(p.tau), [p.a.real, p.a.imag, p.b.real, p.b.imag,
+                                                                      lr[k][0]]])
+                for e in range(packed.size):
+                    q.matrix[e] = packed[e]
+                q.pauli_name = 1
+                q.pauli_proc = int(lr[k][1])
+                continue
             q.nsites = len(p.sites)
             q.site[0] = p.sites[0] - 1
             q.site[1] = (p.sites[1] - 1) if len(p.sites) == 2 else (p.sites[0] - 1)
