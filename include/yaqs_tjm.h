@@ -76,6 +76,19 @@ typedef struct {
  *   pauli_proc — StochasticProcess.is_pauli(op) for 1-site processes
  *                (StochasticProcess.jl:336-341) and is_pauli_proc(proc) for
  *                2-site ones (:343-357) → jump weight uses the local norm.
+ *
+ * One MPONoiseProcess (Noise.jl:22-33): a 2-site process with
+ * site[1] > site[0] + 1 and operator O = a*1 + b*(sig at site[0])(tau at
+ * site[1]), the MPO of build_mpo_phys (Noise.jl:71-131).  matrix holds
+ * sig (doubles 0..7, column-major 2x2), tau (8..15), a (16..17), b (18..19)
+ * and the dissipation rate (20): the state decays by exp(-dt/2 * rate) at
+ * site[1] (handle_longrange_scalar!, Dissipation.jl:161-204: a projector
+ * pair's first member carries the pair's summed rate and its mate 0).
+ * pauli_name must be 1 (the reference errors on other names there);
+ * pauli_proc = 1 marks a "pauli_long_range" candidate (is_pauli_proc with
+ * stored factors, StochasticProcess.jl:176-185), which the reference selects
+ * but never applies; 0 an "mpo_general" one, applied as an MPO followed by
+ * MPS.truncate! (StochasticProcess.jl:46-82, MPS.jl:320-440).
  */
 typedef struct {
   int32_t nsites;

@@ -229,3 +229,26 @@ def test_unraveled_gate_noise(oracle, unravel):
     u = np.random.default_rng(5).random((8, api.max_draws_digital(c)))
     got, _ = _compare(oracle, L, c, _zs(L), nm=nm, num_traj=8, uniforms=u)
     assert got.stats["jumps"] > 0
+
+
+@pytest.mark.parametrize("method", ["tebd", "tdvp"])
+def test_long_range_gate_noise(oracle, method):
+    """Long-range gates take the long-range processes on their own pair
+    (DigitalTJM.jl:172-188): MPO jumps on the device vs the oracle."""
+    L = 6
+    c = _tdvp_circuit(L, 2, seed=41) if method == "tdvp" else _brickwork(L, 2, seed=41)
+    info = [{"name": "crosstalk_zz", "sites": [1, L], "strength": 0.3, "unraveling": "projector"},
+            {"name": "crosstalk_xy", "sites": [1, L], "strength": 0.2, "unraveling": "unitary_2pt"},
+            {"name": "crosstalk_xx", "sites": [2, L - 1], "strength": 0.3, "unraveling": "unitary_gauss", "M": 3},
+            {"name": "crosstalk_yy", "sites": [3, L - 1], "strength": 0.3},
+            {"name": "pauli_x", "sites": [2], "strength": 0.05}]
+    nm = api.NoiseModel(info, L)
+    u = np.random.default_rng(43).random((8, api.max_draws_digital(c)))
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=8, max_bond_dim=16)
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=u,
+                               local_method=method, long_range_method=method)
+    ref, chi_ref, st_ref = oracle.digital_run(d)
+    got = api.run_circuit_descriptors(d)
+    assert np.abs(got.trajectories - ref).max() <= 1e-10
+    assert np.array_equal(got.max_bond, chi_ref)
+    assert got.stats["jumps"] == st_ref["jumps"] > 0

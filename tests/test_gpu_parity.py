@@ -260,3 +260,44 @@ def test_unraveled_noise_matches_oracle(oracle, unravel):
     u = np.random.default_rng(17).random((6, api.max_draws(cfg)))
     got, _ = _compare(oracle, api.MPS(L, state="x+"), H, cfg, nm, uniforms=u)
     assert got.stats["jumps"] > 0
+
+
+def _long_range_model(L, state_kind):
+    info = [{"name": "crosstalk_zz", "sites": [1, 4], "strength": 0.4, "unraveling": "projector"},
+            {"name": "crosstalk_xy", "sites": [2, 5], "strength": 0.3, "unraveling": "unitary_2pt",
+             "theta0": np.pi / 3},
+            {"name": "crosstalk_zx", "sites": [1, L], "strength": 0.2, "unraveling": "unitary_gauss", "M": 5},
+            {"name": "crosstalk_xx", "sites": [3, L], "strength": 0.3},
+            {"name": "pauli_z", "sites": [2], "strength": 0.2}]
+    return api.NoiseModel(info, L)
+
+
+@pytest.mark.parametrize("state_kind", ["x+", "zeros"])
+def test_long_range_noise_matches_oracle(oracle, state_kind):
+    """Long-range processes (MPO jumps with truncate!, the reference's
+    candidate weights, scalar dissipation) on the device vs the oracle.
+    From |0...0> the projector's 1 - ZZ branch annihilates the state."""
+    L = 6
+    H = api.init_ising(L, 1.0, 0.6)
+    obs = [api.Observable(f"X{i}", api.X, i) for i in range(1, L + 1)] + \
+          [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.6, dt=0.05, num_traj=8, max_bond_dim=16)
+    nm = _long_range_model(L, state_kind)
+    u = np.random.default_rng(23).random((8, api.max_draws(cfg)))
+    got, _ = _compare(oracle, api.MPS(L, state=state_kind), H, cfg, nm, uniforms=u)
+    assert got.stats["jumps"] > 0
+
+
+def test_long_range_noise_tight_bond_cap(oracle):
+    """The applied operator doubles bonds a..b-1; truncate! cuts them back to
+    max_bond_dim = 4."""
+    L = 7
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.5, dt=0.05, num_traj=6, max_bond_dim=4)
+    nm = api.NoiseModel([{"name": "crosstalk_xx", "sites": [2, 6], "strength": 0.8, "unraveling": "unitary_2pt",
+                          "theta0": 0.8},
+                         {"name": "crosstalk_yz", "sites": [1, 7], "strength": 0.5, "unraveling": "projector"}], L)
+    u = np.random.default_rng(29).random((6, api.max_draws(cfg)))
+    got, _ = _compare(oracle, api.MPS(L, state="Neel"), H, cfg, nm, uniforms=u)
+    assert got.stats["jumps"] > 0

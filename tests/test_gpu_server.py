@@ -139,3 +139,12 @@ def test_failed_request_leaves_the_others_intact():
         st = srv.stats()
     assert np.array_equal(ra.trajectories, _alone(ok, 3).trajectories)
     assert st["failed"] == 1 and st["completed"] == 1
+
+
+def test_long_range_noise_is_refused_by_the_server():
+    psi, H, cfg, _ = _ising(6, 0.5, 0.2, 8, 8)
+    nm = api.NoiseModel([{"name": "crosstalk_zz", "sites": [1, 4], "strength": 0.1}], 6)
+    from yaqs_julia_b200._lib import EngineError
+    with api.Server(max_L=8, max_bond_dim=8, max_mpo_width=3) as srv:
+        with pytest.raises(EngineError, match="UNSUPPORTED"):
+            srv.submit(psi, H, cfg, nm, seed=1)

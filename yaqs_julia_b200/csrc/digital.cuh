@@ -115,7 +115,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
   ProfScope prof_scope_(PF_STOCH);
   const DevParams& P = c.P;
   int nloc = 0;
-  bool all_zero = true, split_diss = false, scalar_only = true;
+  bool all_zero = true, split_diss = false, scalar_only = true, has_lr = false;
   double fdiss = 1.0;
   for (int k = 0; k < P.nprocs; ++k) {
     const DevProc& pr = P.procs[k];
@@ -124,14 +124,15 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
     if (pr.gamma != 0.0) all_zero = false;
     if (pr.nsites == 2 && !pr.pauli_name) split_diss = true;
     if (pr.nsites != 1 || !pr.pauli_name || !pr.pauli_proc || !pr.unitary) scalar_only = false;
-    fdiss *= exp(-0.5 * pr.gamma);
+    if (pr.lr) has_lr = true;
+    fdiss *= exp(-0.5 * pr.drate);
   }
   if (!P.noise_present || nloc == 0) {
     finish_normalize(c, s);
     return;
   }
   const bool tight = chain_tight(c, s);
-  if ((split_diss && !all_zero) || !tight) {
+  if ((split_diss && !all_zero) || !tight || has_lr) {  // long-range jumps need the full sweeps
     apply_dissipation(c, s, true, 1.0, s1, s2);
     if (c.sm.fail) return;
     stochastic_process(c, s, 1.0, s1, s2);
@@ -202,7 +203,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
         for (int k = 0; k < P.nprocs; ++k) {
           const DevProc& pr = P.procs[k];
           if (!proc_on(pr, s1, s2) || pr.nsites != 2 || pr.s1 != i) continue;
-          cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * pr.gamma));
+          cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * pr.drate));
           __syncthreads();
         }
       }

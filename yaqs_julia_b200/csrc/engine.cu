@@ -480,13 +480,21 @@ int pack_noise(yaqs_ctx* ctx, const yaqs_noise_desc* noise, int nprocs, int L, d
     d.nsites = q.nsites;
     d.s0 = q.site[0];
     d.s1 = q.nsites == 2 ? q.site[1] : q.site[0];
-    if (q.nsites < 1 || q.nsites > 2 || d.s0 < 0 || d.s1 >= L || (q.nsites == 2 && d.s1 != d.s0 + 1))
-      return set_err(ctx, q.nsites == 2 ? YAQS_E_UNSUPPORTED : YAQS_E_ARG,
-                     "noise processes must be 1-site or adjacent 2-site with sites in range");
+    if (q.nsites < 1 || q.nsites > 2 || d.s0 < 0 || d.s1 >= L || (q.nsites == 2 && d.s1 <= d.s0))
+      return set_err(ctx, YAQS_E_ARG, "noise processes must be 1-site or 2-site (ascending) with sites in range");
     d.gamma = q.strength;
+    d.drate = q.strength;
     d.pauli_name = q.pauli_name;
     d.pauli_proc = q.pauli_proc;
     if (q.strength != 0.0) all_zero = false;
+    if (q.nsites == 2 && d.s1 > d.s0 + 1) {  // long-range: sig, tau, alpha, beta, dissipation rate
+      if (!q.pauli_name)
+        return set_err(ctx, YAQS_E_UNSUPPORTED, "Non-Pauli long-range processes not fully implemented");
+      d.lr = 1;
+      for (int e = 0; e < 10; ++e) d.mat[e] = make_double2(q.matrix[2 * e], q.matrix[2 * e + 1]);
+      d.drate = q.matrix[20];
+      continue;
+    }
     const int dd = q.nsites == 1 ? 2 : 4;
     hcd M[16], LdL[16], e1[16], e2[16];
     for (int e = 0; e < dd * dd; ++e) M[e] = cload(q.matrix, e);
@@ -575,7 +583,15 @@ bool plan_caps(int L, const int* chi0, const int* w, int max_bond, Caps& c) {
 // units, each buffer 32-byte aligned).  analog = false leaves out what the
 // digital program does not use (the sampled copy, environments, Krylov basis,
 // contraction intermediates).
-WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, bool mixed) {
+// True when the noise model holds a long-range process (two sites that are
+// not neighbours); its jumps need the long-range work buffers.
+bool has_long_range(const yaqs_noise_desc* noise, int nprocs) {
+  for (int k = 0; k < nprocs; ++k)
+    if (noise->procs[k].nsites == 2 && noise->procs[k].site[1] > noise->procs[k].site[0] + 1) return true;
+  return false;
+}
+
+WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, bool mixed, bool lr = false) {
   const long long tmp = 4LL * c.capmax * c.capmax + 16;
   WsLayout lay;
   long long off = 0;
@@ -613,6 +629,16 @@ WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, 
   lay.T1f = takef(c.t_size);
   lay.T2f = takef(c.t_size);
   lay.Af = takef(amax);
+  const long long big = lr ? 8LL * c.capmax * c.capmax + 16 : 0, small = lr ? tmp : 0;
+  lay.lrQ = take(lr ? 4 * c.mps_size : 0);
+  lay.lrPhi = take(big);
+  lay.lrM = take(big);
+  lay.lrH = take(big);
+  lay.lrQh = take(big);
+  lay.lrL = take(small);
+  lay.lrR = take(small);
+  lay.lrC0 = take(small);
+  lay.lrC1 = take(small);
   lay.total = off;
   long long ioff = 0;
   lay.i_chi = ioff;
@@ -623,6 +649,8 @@ WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, 
   ioff += SVD_MAX_COLS;
   lay.i_cand = ioff;
   ioff += MAX_PROCS;
+  lay.i_lr = ioff;
+  ioff += lr ? L + 1 : 0;
   lay.itotal = (ioff + 31) & ~31LL;
   return lay;
 }
@@ -871,7 +899,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   if (!plan_caps(L, chi0.data(), w.data(), cfg->max_bond_dim, caps))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
   const bool mixed = cfg->precision == YAQS_PREC_MIXED;
-  const WsLayout lay = plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed);
+  const WsLayout lay = plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed, has_long_range(noise, nprocs));
   const std::vector<int>& cap = caps.cap;
   const std::vector<long long>& mps_off = caps.mps_off;
   const std::vector<long long>& env_off = caps.env_off;
@@ -1229,7 +1257,7 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   Caps caps;
   if (!plan_caps(L, chi0.data(), w.data(), cfg->max_bond_dim, caps))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
-  const WsLayout lay = plan_layout(L, caps, w.data(), any_tdvp, kdim, false);
+  const WsLayout lay = plan_layout(L, caps, w.data(), any_tdvp, kdim, false, has_long_range(noise, nprocs));
   const std::vector<int>& cap = caps.cap;
   const std::vector<long long>& mps_off = caps.mps_off;
   const std::vector<long long>& env_off = caps.env_off;

@@ -146,6 +146,10 @@ bool copy_common(ReqCopy& r, const yaqs_mps_desc* psi0, const yaqs_noise_desc* n
       return false;
     }
     r.procs.assign(noise->procs, noise->procs + noise->n);
+    if (has_long_range(noise, noise->n)) {  // slots carry no long-range work buffers
+      err = "UNSUPPORTED: long-range noise processes are served by yaqs_analog_run / yaqs_digital_run only";
+      return false;
+    }
   }
   r.noise = {r.has_noise ? 1 : 0, (int32_t)r.procs.size(), r.procs.empty() ? nullptr : r.procs.data()};
   if (n_obs > 0) r.obs.assign(obs, obs + n_obs);
@@ -436,7 +440,8 @@ int yaqs_server_submit_analog(yaqs_server* srv, const yaqs_mps_desc* psi0, const
   ReqCopy& in = r->in;
   std::string err;
   if (cfg->num_traj < 1 || cfg->n_times < 1) return set_err(nullptr, YAQS_E_ARG, "bad config");
-  if (!copy_common(in, psi0, noise, obs, n_obs, rng, cfg->num_traj, err)) return set_err(nullptr, YAQS_E_ARG, err);
+  if (!copy_common(in, psi0, noise, obs, n_obs, rng, cfg->num_traj, err))
+    return set_err(nullptr, err.rfind("UNSUPPORTED", 0) == 0 ? YAQS_E_UNSUPPORTED : YAQS_E_ARG, err);
   if (H->L != psi0->L || !H->w || !H->tensors) return set_err(nullptr, YAQS_E_ARG, "bad MPO descriptor");
   in.w.assign(H->w, H->w + H->L + 1);
   in.mpo.resize(H->L);
@@ -465,7 +470,8 @@ int yaqs_server_submit_digital(yaqs_server* srv, const yaqs_mps_desc* psi0, cons
   ReqCopy& in = r->in;
   std::string err;
   if (cfg->num_traj < 1) return set_err(nullptr, YAQS_E_ARG, "bad config");
-  if (!copy_common(in, psi0, noise, obs, n_obs, rng, cfg->num_traj, err)) return set_err(nullptr, YAQS_E_ARG, err);
+  if (!copy_common(in, psi0, noise, obs, n_obs, rng, cfg->num_traj, err))
+    return set_err(nullptr, err.rfind("UNSUPPORTED", 0) == 0 ? YAQS_E_UNSUPPORTED : YAQS_E_ARG, err);
   in.digital = 1;
   in.gates.assign(gates, gates + n_gates);
   in.ccfg = *cfg;

@@ -23,7 +23,12 @@ struct DevProc {
   int nsites, s0, s1;
   int pauli_name, pauli_proc;
   int unitary;  // matrix^dag matrix = 1 (a jump then keeps every tensor's gauge)
+  // Long-range process (s1 > s0 + 1): operator alpha*1 + beta*(sig at s0)
+  // (tau at s1), mat[0..3] = sig, mat[4..7] = tau, mat[8] = alpha,
+  // mat[9] = beta; pauli_proc marks the "pauli_long_range" candidate.
+  int lr;
   double gamma;
+  double drate;  // rate of the scalar decay exp(-dt/2 * drate) when pauli_name
   cplx mat[16];
   cplx diss_half[16];
   cplx diss_full[16];
@@ -39,9 +44,12 @@ struct WsLayout {
   long long psi, EL, ER, Q, T1, T2, tA, tB, tC, th, B, X, Yo, Zo, y, dbl;
   // mixed form (FP32 buffers, offsets in complex-double units)
   long long Lf, Rf, xf, T1f, T2f, Af;
+  // long-range jumps: right-canonical tensors of the operator applied to
+  // the state (4 x the MPS arena) and work buffers
+  long long lrQ, lrPhi, lrM, lrH, lrQh, lrL, lrR, lrC0, lrC1;
   long long total;
   // int workspace (per slot)
-  long long i_chi, i_oc, i_ord, i_cand, itotal;
+  long long i_chi, i_oc, i_ord, i_cand, i_lr, itotal;
 };
 
 struct DevParams {
@@ -801,7 +809,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
     const DevProc& pr = c.P.procs[k];
     if (!proc_on(pr, f1, f2)) continue;
     if (!pr.pauli_name) scalar_only = false;
-    fscal *= exp(-0.5 * dt * pr.gamma);
+    fscal *= exp(-0.5 * dt * pr.drate);
   }
   if ((!c.P.noise_present || all_zero || scalar_only) && chain_tight(c, s)) {
     shift_oc(c, s, 0);
@@ -841,8 +849,8 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
       for (int k = 0; k < c.P.nprocs && !c.sm.fail; ++k) {
         const DevProc& pr = c.P.procs[k];
         if (pr.nsites == 2 && pr.s1 == i && proc_on(pr, f1, f2)) {
-          if (pr.pauli_name) {
-            cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * dt * pr.gamma));
+          if (pr.pauli_name) {  // Pauli names and long-range processes: a scalar at the right site
+            cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * dt * pr.drate));
             __syncthreads();
           } else {
             const int l = s.chi[i - 1], r = s.chi[i + 1];
@@ -856,6 +864,8 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
     }
   }
 }
+
+#include "longrange.cuh"
 
 // ---------------------------------------------------------------------------
 // Stochastic process (StochasticProcess.jl:219-330)
@@ -899,7 +909,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
     if (site < L - 1) {
       for (int k = 0; k < c.P.nprocs; ++k) {
         const DevProc& pr = c.P.procs[k];
-        if (pr.nsites == 2 && pr.s0 == site && proc_on(pr, f1, f2)) {
+        if (pr.nsites == 2 && !pr.lr && pr.s0 == site && proc_on(pr, f1, f2)) {
           double nr;
           if (pr.pauli_proc) {
             nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1], nullptr);
@@ -915,6 +925,19 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
         }
       }
     }
+  }
+  // long-range processes after every local candidate (StochasticProcess.jl:169-202);
+  // the centre is at site L-1
+  for (int k = 0; k < c.P.nprocs && !c.sm.fail; ++k) {
+    const DevProc& pr = c.P.procs[k];
+    if (!pr.lr || !proc_on(pr, f1, f2)) continue;
+    const double nr = pr.pauli_proc ? local_norm2(c, site_ptr(c, s, L - 1), s.chi[L - 1], 2, s.chi[L], nullptr)
+                                    : lr_weight(c, s, pr);
+    if (threadIdx.x == 0) {
+      cand[nc] = dt * pr.gamma * nr;
+      candp[nc] = k;
+    }
+    ++nc;
   }
   __syncthreads();
   double total = 0.0;
@@ -935,7 +958,11 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
   }
   const DevProc& pr = c.P.procs[candp[chosen]];
   __syncthreads();
-  if (pr.nsites == 1) {
+  if (pr.lr) {
+    // "pauli_long_range" has no branch of its own in the reference
+    // (StochasticProcess.jl:311 tests "mpo_pauli"): only the normalisation acts
+    if (!pr.pauli_proc) lr_apply(c, s, pr);
+  } else if (pr.nsites == 1) {
     shift_oc(c, s, pr.s0);
     apply_local(site_ptr(c, s, pr.s0), s.chi[pr.s0], 2, s.chi[pr.s0 + 1], pr.mat);
   } else {
