@@ -252,3 +252,25 @@ def test_long_range_gate_noise(oracle, method):
     assert np.abs(got.trajectories - ref).max() <= 1e-10
     assert np.array_equal(got.max_bond, chi_ref)
     assert got.stats["jumps"] == st_ref["jumps"] > 0
+
+
+@pytest.mark.parametrize("method", ["tebd", "tdvp"])
+def test_circuit_library_fermi_hubbard(oracle, method):
+    """A circuit-library generator (1D Fermi-Hubbard: long-range on-site
+    CPhase between j and j+L, descending hopping pairs) with gate noise."""
+    from yaqs_julia_b200 import circuits as C
+    c = C.create_1d_fermi_hubbard_circuit(3, 1.2, 0.8, 0.3, 1, 0.3, 2)
+    c.gates.insert(0, api.DigitalGate(api.Barrier(), []))
+    c.add_gate(api.Barrier(), [])
+    L = c.num_qubits
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.02} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_z")], L)
+    u = np.random.default_rng(47).random((6, api.max_draws_digital(c)))
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=6, max_bond_dim=16)
+    psi = api.MPS(L, state="Neel")
+    d = api.CircuitDescriptors(psi, c, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=u,
+                               local_method=method, long_range_method=method)
+    ref, chi_ref, st_ref = oracle.digital_run(d)
+    got = api.run_circuit_descriptors(d)
+    assert np.abs(got.trajectories - ref).max() <= 1e-10
+    assert np.array_equal(got.max_bond, chi_ref) and got.stats["jumps"] == st_ref["jumps"]
