@@ -274,3 +274,21 @@ def test_circuit_library_fermi_hubbard(oracle, method):
     got = api.run_circuit_descriptors(d)
     assert np.abs(got.trajectories - ref).max() <= 1e-10
     assert np.array_equal(got.max_bond, chi_ref) and got.stats["jumps"] == st_ref["jumps"]
+
+
+def test_run_repeated_library_circuit_defaults_to_tdvp_windows(oracle):
+    """api.run on a RepeatedDigitalCircuit of library gates: the reference's
+    default TJMOptions (TDVP windows) and its per-repetition sample plan."""
+    from yaqs_julia_b200 import circuits as C
+    L = 6
+    step = C.create_ising_circuit(L, 1.0, 0.7, 0.1, 1, periodic=True)
+    rep = api.RepeatedDigitalCircuit(step, 4)
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.03} for i in range(1, L + 1)], L)
+    obs = _zs(L)
+    cfg = api.TimeEvolutionConfig(obs, 4.0, dt=1.0, num_traj=8, max_bond_dim=16)
+    res = api.run(api.MPS(L, state="wall"), rep, cfg, nm, seed=61)
+    d = api.CircuitDescriptors(api.MPS(L, state="wall"), rep, cfg, nm, seed=61, local_method="tdvp",
+                               long_range_method="tdvp")
+    ref, chi_ref, _ = oracle.digital_run(d)
+    assert ref.shape[2] == 5
+    assert np.abs(res.trajectories - ref).max() <= 1e-10 and np.array_equal(res.max_bond, chi_ref)

@@ -1,0 +1,176 @@
+"""Host MPS/MPO algebra, shots and measurement configs (src/MPS.jl,
+src/MPO.jl:271-556, src/SimulationConfigs.jl:95-208) against dense
+linear algebra; RepeatedDigitalCircuit (DigitalTJM.jl:452-536) against the
+explicitly repeated circuit."""
+import math
+
+import numpy as np
+import pytest
+
+from yaqs_julia_b200 import api
+from yaqs_julia_b200 import tensornet as T
+from oracle import dense as D
+
+
+def _rand_mps(L, chi, seed):
+    m = api.random_mps(L, chi, seed=seed)
+    return T.normalize(m)
+
+
+def test_gauge_moves_keep_the_state_and_normalise():
+    m = _rand_mps(6, 4, 1)
+    v = m.to_vec()
+    assert abs(np.linalg.norm(v) - 1) < 1e-12 and m.orth_center == 1
+    for c in (4, 6, 2, 1):
+        T.shift_orthogonality_center(m, c)
+        assert np.allclose(m.to_vec(), v, atol=1e-12)
+        assert abs(T.mps_norm(m) - 1) < 1e-12
+    assert T.check_if_valid_mps(m) and T.write_max_bond_dim(m) == 4
+
+
+def test_overlaps_and_expectations_match_dense():
+    a, b = _rand_mps(5, 3, 2), _rand_mps(5, 4, 3)
+    va, vb = a.to_vec(), b.to_vec()
+    assert abs(T.scalar_product(a, b) - np.vdot(va, vb)) < 1e-12
+    for s in range(1, 6):
+        assert abs(T.local_expect(a, api.X, s) - np.vdot(va, D.site_op(api.X, s, 5) @ va)) < 1e-12
+    op = np.kron(api.Z, api.Y)
+    for s in range(1, 5):
+        ref = np.vdot(va, D.gate_op(op, [s, s + 1], 5) @ va)
+        assert abs(T.local_expect_two_site(a, op, s, s + 1) - ref) < 1e-12
+    ops = [api.Z, api.X, api.Y, api.Z, api.X]
+    ev = T.evaluate_all_local_expectations(a, ops)
+    assert np.allclose(ev, [np.vdot(va, D.site_op(o, i + 1, 5) @ va) for i, o in enumerate(ops)], atol=1e-12)
+
+
+def test_truncate_keeps_at_least_two_and_caps_the_bond():
+    m = _rand_mps(8, 8, 4)
+    v = m.to_vec()
+    err = T.truncate(m, threshold=1e-3, max_bond_dim=3)
+    assert T.write_max_bond_dim(m) <= 3 and min(t.shape[2] for t in m.tensors[:-1]) >= 2
+    assert abs(np.linalg.norm(m.to_vec()) - 1) < 1e-12 and err > 0
+    assert abs(np.vdot(m.to_vec(), v)) > 0.5
+    exact = _rand_mps(6, 2, 5)
+    v2 = exact.to_vec()
+    assert T.truncate(exact, threshold=1e-12) < 1e-20 and np.allclose(exact.to_vec(), v2, atol=1e-10)
+
+
+def _literal_shot(mps, u):
+    """single_shot_measure restated one site at a time with explicit tensors."""
+    import copy
+    psi = T.shift_orthogonality_center(copy.deepcopy(mps), 1)
+    bits = 0
+    for i in range(psi.length):
+        A = psi.tensors[i]
+        probs = [float(np.sum(np.abs(A[:, p, :]) ** 2)) for p in range(2)]
+        acc, chosen = 0.0, 1
+        for k in range(2):
+            acc += probs[k]
+            if u[i] <= acc:
+                chosen = k
+                break
+        bits += chosen << i
+        if i < psi.length - 1:
+            Ap = A[:, chosen, :] / max(math.sqrt(probs[chosen]), 1e-300)
+            N = psi.tensors[i + 1]
+            psi.tensors[i + 1] = np.einsum("lr,rpq->lpq", Ap, N)
+    return bits
+
+
+def test_shots_follow_the_born_rule():
+    m = _rand_mps(4, 3, 6)
+    v = m.to_vec()
+    u = np.random.default_rng(7).random((40, 4))
+    counts = T.measure_shots(m, 40, uniforms=u)
+    lit = [_literal_shot(m, u[s]) for s in range(40)]
+    want = {}
+    for b in lit:
+        want[b] = want.get(b, 0) + 1
+    assert counts == want
+    n = 40000
+    counts = T.measure_shots(m, n, rng=np.random.default_rng(8))
+    p = np.abs(v) ** 2
+    for b in range(16):
+        assert abs(counts.get(b, 0) / n - p[b]) < 5 * math.sqrt(p[b] * (1 - p[b]) / n) + 1e-9
+    bs = "".join(str((3 >> i) & 1) for i in range(4))
+    assert abs(T.project_onto_bitstring(m, bs) - p[3]) < 1e-12
+    assert T.single_shot_measure(api.MPS(3, state="basis", basis_string="101")) == 0b101
+
+
+def test_mpo_algebra_matches_dense():
+    L = 4
+    H1 = api.init_ising(L, 1.0, 0.4)
+    H2 = api.init_general_hamiltonian(L, 0.3, 0.2, 0.5, 0.1, 0.0, 0.2)
+    M1, M2 = H1.to_matrix(), H2.to_matrix()
+    assert np.allclose(T.mpo_add(H1, H2).to_matrix(), M1 + M2, atol=1e-12)
+    assert np.allclose(T.mpo_scale(2.5j, H1).to_matrix(), 2.5j * M1, atol=1e-12)
+    assert np.allclose(T.contract_mpo_mpo(H1, H2).to_matrix(), M1 @ M2, atol=1e-12)
+    assert np.allclose(T.mpo_identity(L).to_matrix(), np.eye(2 ** L))
+    assert np.allclose(T.mpo_zero(L).to_matrix(), 0)
+    psi = _rand_mps(L, 3, 9)
+    v = psi.to_vec()
+    assert np.allclose(T.contract_mpo_mps(H1, psi).to_vec(), M1 @ v, atol=1e-12)
+    assert abs(T.expect_mpo(H2, psi) - np.vdot(v, M2 @ v)) < 1e-12
+    # a doubled Hamiltonian compresses back to its own width
+    S = T.mpo_add(H1, H1)
+    assert max(S.bond_dims) == 6
+    err = T.mpo_truncate(S, threshold=1e-12)
+    assert err < 1e-20 and max(S.bond_dims) <= 3 and np.allclose(S.to_matrix(), 2 * M1, atol=1e-10)
+    O = T.orthogonalize(api.init_ising(L, 0.7, 1.1), 2)
+    assert np.allclose(O.to_matrix(), api.init_ising(L, 0.7, 1.1).to_matrix(), atol=1e-12)
+
+
+def test_measurement_configs():
+    mc = T.MeasurementConfig(3)
+    mc.measurements[0] = {1: 2, 3: 1}
+    mc.measurements[2] = {1: 1}
+    assert T.aggregate_measurements(mc) == {1: 3, 3: 1} and mc.results == {1: 3, 3: 1}
+    obs = [api.Observable("Z1", api.Z, 1)]
+    sc = T.StrongMeasurementConfig(obs, num_traj=2)
+    obs[0].trajectories = np.array([[1.0, 0.5], [0.0, 0.5]], dtype=np.complex128)
+    T.aggregate_strong(sc)
+    assert np.allclose(obs[0].results, [0.5, 0.5])
+
+
+def _step(L, seed, lead_barrier=True, tail_barrier=True):
+    rng = np.random.default_rng(seed)
+    c = api.DigitalCircuit(L)
+    if lead_barrier:
+        c.add_gate(api.Barrier(), [])
+    for i in range(1, L + 1):
+        c.add_gate(api.Rx(rng.uniform(0, 1)), [i])
+    for i in list(range(1, L, 2)) + list(range(2, L, 2)):
+        c.add_gate(api.Rzz(rng.uniform(0, 1)), [i, i + 1])
+    if tail_barrier:
+        c.add_gate(api.Barrier(), [])
+    return c
+
+
+@pytest.mark.parametrize("lead,tail", [(True, True), (False, True), (True, False)])
+def test_repeated_circuit_sample_plan(oracle, lead, tail):
+    L, R = 5, 3
+    step = _step(L, 3, lead, tail)
+    rep = api.RepeatedDigitalCircuit(step, R)
+    layers_step, _ = api.process_circuit(step)
+    start, after, n = api.sample_plan(rep)
+    s_start, s_after, _ = api.sample_plan(step)
+    assert start == s_start and len(api.process_circuit(rep)[0]) == R * len(layers_step)
+    assert n == max(1, (1 if s_start else 0) + R * len(s_after))
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=1.0, num_traj=1, max_bond_dim=32, truncation_threshold=1e-14)
+    tr, _, _ = oracle.digital_run(api.CircuitDescriptors(api.MPS(L, state="wall"), rep, cfg, None))
+    U = np.eye(2 ** L, dtype=np.complex128)
+    for g in step.gates:
+        if not isinstance(g.op, api.Barrier):
+            U = D.gate_op(g.op, g.sites, L) @ U
+    psi = D.product_state([[1, 0]] * (L // 2) + [[0, 1]] * (L - L // 2))
+    zs = lambda v: [np.real(np.vdot(v, D.site_op(api.Z, i, L) @ v)) for i in range(1, L + 1)]  # noqa: E731
+    cols = [zs(psi)] if lead else []
+    for _ in range(R):
+        psi = U @ psi
+        if tail:
+            cols.append(zs(psi))
+    if not cols:
+        cols = [zs(psi)]
+    assert tr.shape[2] == n == len(cols)
+    assert np.abs(tr[0] - np.array(cols).T).max() < 1e-9 and np.abs(np.array(cols)).max() > 0.1

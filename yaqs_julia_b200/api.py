@@ -847,12 +847,56 @@ class DigitalCircuit:
         return self
 
 
+class RepeatedDigitalCircuit:
+    """RepeatedDigitalCircuit(step, repeats) (DigitalTJM.jl:47-58, 452-536):
+    ``step`` run ``repeats`` times.  The step's layers are formed once; a
+    sample barrier before the step's first layer samples once at the start,
+    every other sample barrier samples after its layer in every repetition.
+
+    ``flatten`` gives the equivalent DigitalCircuit the engine runs: the step's
+    gates per repetition, a layer break (a barrier that does not sample)
+    between repetitions so layers never merge across them, and the leading
+    sample barriers kept only in the first repetition."""
+
+    def __init__(self, step: DigitalCircuit, repeats: int):
+        if repeats < 0:
+            raise ValueError("repeats must be >= 0")
+        self.step = step
+        self.repeats = int(repeats)
+
+    @property
+    def num_qubits(self) -> int:
+        return self.step.num_qubits
+
+    def flatten(self) -> DigitalCircuit:
+        out = DigitalCircuit(self.step.num_qubits)
+        lead = 0
+        while lead < len(self.step.gates) and isinstance(self.step.gates[lead].op, Barrier):
+            lead += 1
+        for r in range(self.repeats):
+            if r > 0:
+                out.gates.append(DigitalGate(Barrier("LAYER_BREAK"), []))
+            for k, g in enumerate(self.step.gates):
+                if r > 0 and k < lead:
+                    continue
+                out.gates.append(g)
+        if self.repeats == 0:
+            out.gates = [g for g in self.step.gates[:lead]]
+        return out
+
+
+def as_circuit(circ) -> DigitalCircuit:
+    """A DigitalCircuit for the engine (a RepeatedDigitalCircuit is flattened)."""
+    return circ.flatten() if isinstance(circ, RepeatedDigitalCircuit) else circ
+
+
 def add_gate(circ: DigitalCircuit, op, sites, generator=None):
     return circ.add_gate(op, sites, generator)
 
 
 def process_circuit(circ: DigitalCircuit):
     """Greedy layering and barrier map (DigitalTJM.jl:86-145)."""
+    circ = as_circuit(circ)
     layers, barrier_map, cur, busy = [], {}, [], set()
     for g in circ.gates:
         if isinstance(g.op, Barrier):
@@ -889,6 +933,7 @@ class CircuitDescriptors:
                  uniforms: np.ndarray | None = None, traj_offset: int = 0, num_traj: int | None = None,
                  local_method: str = "tebd", long_range_method: str = "tebd"):
         L = psi0.length
+        circ = as_circuit(circ)
         if circ.num_qubits != L:
             raise ValueError("circuit and MPS sizes differ")
         # reuse the analog packer for the state, noise, observables and rng
@@ -952,6 +997,7 @@ def create_local_noise_model(noise_model: NoiseModel, site1: int, site2: int) ->
 
 def max_draws_digital(circ: DigitalCircuit) -> int:
     """Upper bound on uniforms one digital trajectory consumes (2 per 2-qubit gate)."""
+    circ = as_circuit(circ)
     return 2 * max(1, sum(1 for g in circ.gates if not isinstance(g.op, Barrier) and len(g.sites) == 2))
 
 
@@ -1001,6 +1047,7 @@ def digital_plan(circ: DigitalCircuit) -> tuple[int, int]:
     """(number of layers, number of measurement columns) as the library plans them."""
     from . import _lib
     L = _lib.lib()
+    circ = as_circuit(circ)
     gd = CircuitDescriptors.pack_gates(circ)
     nl, ns = C.c_int32(0), C.c_int32(0)
     st = L.yaqs_digital_plan(gd, len(circ.gates), C.byref(nl), C.byref(ns))
@@ -1096,9 +1143,9 @@ class Server:
                precision: str = "fp64", traj_offset: int = 0, tdvp: str = "2site") -> int:
         mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
         rid = C.c_int64(0)
-        if isinstance(operator, DigitalCircuit):
+        if isinstance(operator, (DigitalCircuit, RepeatedDigitalCircuit)):
             d = CircuitDescriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
-                                   uniforms=uniforms, traj_offset=traj_offset)
+                                   uniforms=uniforms, traj_offset=traj_offset)  # server slots: TEBD gates
             st = self._lib.yaqs_server_submit_digital(self.handle, C.byref(d.mps), d.gates, d.n_gates,
                                                       C.byref(d.noise), d.obs, d.n_obs, C.byref(d.cfg),
                                                       C.byref(d.rng), C.byref(rid))
@@ -1171,9 +1218,22 @@ def random_mps(length: int, chi: int, seed: int = 0) -> MPS:
 TDVP_MODES = {"2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE, "dynamic": A.YAQS_TDVP_DYNAMIC}
 
 
+def _methods(circ, local_method, long_range_method):
+    """Digital gate methods: the given ones, else the reference's default
+    TJMOptions() (TDVP windows for every gate, DigitalTJM.jl:70-76) when every
+    2-qubit gate carries a generator; gates given as bare matrices (which the
+    reference's typed gates cannot express) run by TEBD."""
+    circ = as_circuit(circ)
+    all_gen = all(g.generator is not None for g in circ.gates
+                  if not isinstance(g.op, Barrier) and len(g.sites) == 2)
+    default = "tdvp" if all_gen else "tebd"
+    return {"local_method": local_method or default, "long_range_method": long_range_method or default}
+
+
 def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
         *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12,
-        precision: str = "fp64", tdvp: str = "2site", ctx=None) -> RunResult:
+        precision: str = "fp64", tdvp: str = "2site", local_method: str | None = None,
+        long_range_method: str | None = None, ctx=None) -> RunResult:
     """Simulator.run (Simulator.jl:127-141) for an MPO (analog TJM) or a
     DigitalCircuit (digital TJM, TEBD gate application).  Fills every
     observable's ``trajectories`` and ``results`` like _run_analog /
@@ -1185,8 +1245,13 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
     norms and jump probabilities stay FP64).  ``tdvp`` selects the sweep:
     "2site" (two_site_tdvp!, the reference's analog path), "1site"
     (single_site_tdvp!) or "dynamic" (1-site TDVP with 2-site growth up to
-    max_bond_dim, the Python lineage's local_dynamic_tdvp)."""
+    max_bond_dim, the Python lineage's local_dynamic_tdvp).  For circuits,
+    ``local_method`` / ``long_range_method`` ("tebd" or "tdvp") are the
+    TJMOptions; left unset they follow the reference's default (see
+    _methods).  A RepeatedDigitalCircuit runs as its flattened circuit."""
     prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
+    if isinstance(operator, RepeatedDigitalCircuit):
+        operator = operator.flatten()
     if not isinstance(operator, (MPO, DigitalCircuit)):
         raise TypeError("Simulation requires MPO (Analog) or DigitalCircuit (Digital).")
     if noise_model is None or all(p.strength == 0 for p in noise_model.processes):
@@ -1194,7 +1259,7 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
     mode = A.YAQS_RNG_INJECTED if uniforms is not None else A.YAQS_RNG_PHILOX
     if isinstance(operator, DigitalCircuit):  # _run_digital, Simulator.jl:71-125
         desc = CircuitDescriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
-                                  uniforms=uniforms)
+                                  uniforms=uniforms, **_methods(operator, local_method, long_range_method))
         res = run_circuit_descriptors(desc, ctx)
     else:
         desc = Descriptors(initial_state, operator, sim_params, noise_model, rng_mode=mode, seed=seed,
