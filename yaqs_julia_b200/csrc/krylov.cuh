@@ -14,7 +14,7 @@
 #include "common.cuh"
 #include "gemm_tf32.cuh"
 
-#define WAPPLY_PT 64
+#define WAPPLY_IN_CPLX 2560  // staged inputs: ni x PT values, PT = 256, 128 or 64 by what fits
 #define WAPPLY_MAXI 32
 #define WAPPLY_MAXNNZ 512
 #define KRYLOV_MAX 32
@@ -37,7 +37,7 @@ struct WApplyGeom {
 };
 
 struct WApplySmem {
-  cplx in[WAPPLY_MAXI][WAPPLY_PT];
+  cplx in[WAPPLY_IN_CPLX];
   cplx val[WAPPLY_MAXNNZ];
   int col[WAPPLY_MAXNNZ];
   int rowp[WAPPLY_MAXI + 1];
@@ -45,10 +45,12 @@ struct WApplySmem {
   int out_off[WAPPLY_MAXI];
 };
 
-// out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.  Each thread
-// owns pair slot tid % WAPPLY_PT of every tile and input/output rows
-// tid / WAPPLY_PT + k NT / WAPPLY_PT, so index arithmetic is per tile, not
-// per element.  T is cplx (FP64 form) or float2 (mixed form, FP32 products).
+// out[q0,q1,o] = sum_i M[o,i] in[q0,q1,i].  CTA-collective.  A tile holds PT
+// pairs (the largest of 256, 128, 64 whose ni inputs fit the staging
+// buffer); each thread owns pair slot tid % PT of every tile and
+// input/output rows tid / PT + k NT / PT, so index arithmetic is per tile,
+// not per element, and with PT = NT a thread issues all ni loads of its pair
+// back to back.  T is cplx (FP64 form) or float2 (mixed form, FP32 products).
 __device__ __forceinline__ void wfma(cplx& acc, cplx v, cplx x) { cfma(acc, v, x); }
 __device__ __forceinline__ void wfma(float2& acc, cplx v, float2 x) {
   const float vr = (float)v.x, vi = (float)v.y;
@@ -62,7 +64,9 @@ template <class T>
 __device__ __noinline__ void dev_wapply(const T* __restrict__ in, T* __restrict__ out, const WMat W,
                                         const WApplyGeom g, WApplySmem& ws) {
   ProfScope prof_scope_(PF_WAPPLY);
-  T(*sin)[WAPPLY_PT] = reinterpret_cast<T(*)[WAPPLY_PT]>(&ws.in[0][0]);
+  T* sin = reinterpret_cast<T*>(&ws.in[0]);
+  const int cap = (int)(WAPPLY_IN_CPLX * sizeof(cplx) / sizeof(T));
+  const int PT = W.ni * NT <= cap ? NT : (W.ni * (NT / 2) <= cap ? NT / 2 : NT / 4);
   const int tid = threadIdx.x;
   for (int e = tid; e < W.nnz; e += NT) {
     ws.val[e] = W.val[e];
@@ -72,22 +76,22 @@ __device__ __noinline__ void dev_wapply(const T* __restrict__ in, T* __restrict_
   for (int i = tid; i < W.ni; i += NT) ws.in_off[i] = (int)((i % g.ni1) * g.ii1 + (i / g.ni1) * g.ii2);
   for (int o = tid; o < W.no; o += NT) ws.out_off[o] = (int)((o % g.no1) * g.oo1 + (o / g.no1) * g.oo2);
   const int npair = g.n0 * g.n1;
-  const int pl = tid % WAPPLY_PT, r0 = tid / WAPPLY_PT;
-  constexpr int RS = NT / WAPPLY_PT;
+  const int pl = tid % PT, r0 = tid / PT;
+  const int RS = NT / PT;
   T zero;
   wzero(zero);
-  for (int base = 0; base < npair; base += WAPPLY_PT) {
+  for (int base = 0; base < npair; base += PT) {
     const int pair = base + pl;
     const bool live = pair < npair;
     const int q0 = live ? pair % g.n0 : 0, q1 = live ? pair / g.n0 : 0;
     const long long ib = q0 * g.is0 + q1 * g.is1, ob = q0 * g.os0 + q1 * g.os1;
     __syncthreads();
-    for (int i = r0; i < W.ni; i += RS) sin[i][pl] = live ? in[ib + ws.in_off[i]] : zero;
+    for (int i = r0; i < W.ni; i += RS) sin[i * PT + pl] = live ? in[ib + ws.in_off[i]] : zero;
     __syncthreads();
     if (live) {
       for (int o = r0; o < W.no; o += RS) {
         T acc = zero;
-        for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) wfma(acc, ws.val[z], sin[ws.col[z]][pl]);
+        for (int z = ws.rowp[o]; z < ws.rowp[o + 1]; ++z) wfma(acc, ws.val[z], sin[ws.col[z] * PT + pl]);
         out[ob + ws.out_off[o]] = acc;
       }
     }
