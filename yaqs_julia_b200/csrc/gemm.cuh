@@ -7,7 +7,7 @@
 // Every tensor contraction of the TDVP path (Algorithms.jl:199-226) is
 // written as one such GEMM over the reference's column-major layouts.
 //
-// Tiling: 64x64 output tiles, 8-deep K slices staged in shared memory by
+// Tiling: 64x64 output tiles, 16-deep K slices staged in shared memory by
 // cp.async (double buffered, zero-filled outside the matrix), each of the
 // 256 threads owning a 4x4 register tile with rows tx+16i and columns
 // ty+16j (so stores along m are coalesced).  Conjugation is applied when a
@@ -17,7 +17,7 @@
 
 #define GBM 64
 #define GBN 64
-#define GBK 8
+#define GBK 16
 
 struct GemmSmem {
   cplx As[2][GBK][GBM + 1];
@@ -105,22 +105,22 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
       auto issue = [&](int kc, int buf) {
         const int k0 = kc * GBK;
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
+        for (int e = 0; e < GBM * GBK / NT; ++e) {
           const int idx = tid + NT * e;
           int mi, ki, ni, kj;
           if (a_m_fast) {
-            mi = idx & 63;
-            ki = idx >> 6;
+            mi = idx & (GBM - 1);
+            ki = idx / GBM;
           } else {
-            ki = idx & 7;
-            mi = idx >> 3;
+            ki = idx & (GBK - 1);
+            mi = idx / GBK;
           }
           if (b_n_fast) {
-            ni = idx & 63;
-            kj = idx >> 6;
+            ni = idx & (GBN - 1);
+            kj = idx / GBN;
           } else {
-            kj = idx & 7;
-            ni = idx >> 3;
+            kj = idx & (GBK - 1);
+            ni = idx / GBK;
           }
           const int mm = tm + mi, ka = k0 + ki, nn = tn + ni, kb = k0 + kj;
           const bool va = mm < g.M && ka < g.K, vb = nn < g.N && kb < g.K;

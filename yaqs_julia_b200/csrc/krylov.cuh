@@ -128,7 +128,7 @@ struct KrySmem {
 #define SVD_SMEM_CPLX_K 4096
 struct EngineSmem {
   union {
-    struct {
+    union {  // the GEMM and the MPO apply run one after the other, never together
       GemmSmem g;
       WApplySmem w;
     } gw;
