@@ -481,28 +481,43 @@ vector<cd> expm_krylov(Op&& op, const vector<cd>& v, double dt, const KrylovPara
   for (int k = 1; k <= kp.kdim; ++k) {
     op(Q[k - 1], w);
     cnt.matvecs++;
-    // classical Gram-Schmidt against q_1..q_k with one refinement pass when
-    // the first kept less than 1/sqrt(2) of the norm (DGKS criterion, the
-    // eta of KrylovKit's iteratively refined Gram-Schmidt)
-    double a_k = 0.0;
-    double nprev = nrm2(w.data(), n), b_k = nprev;
-    for (int pass = 0; pass < 2; ++pass) {
-      vector<cd> h(k);
+    // classical Gram-Schmidt against q_1..q_k.  h_j = <q_j, w> and |w|^2 come
+    // from one pass; when the projection keeps at least 1/sqrt(2) of the norm
+    // (DGKS criterion, the eta of KrylovKit's iteratively refined
+    // Gram-Schmidt, tested as |w|^2 - |h|^2 >= |w|^2 / 2) the residual norm
+    // is sqrt(|w|^2 - |h|^2) and q_k = (w - Q h) / b_k; otherwise one
+    // refinement pass projects again and the norm is taken directly.
+    auto dots = [&](vector<cd>& h) {
       for (int j = 0; j < k; ++j) {
-        cd s = 0;
+        cd sacc = 0;
         const cd* qj = Q[j].data();
-        for (long i = 0; i < n; ++i) s += std::conj(qj[i]) * w[i];
-        h[j] = s;
+        for (long i = 0; i < n; ++i) sacc += std::conj(qj[i]) * w[i];
+        h[j] = sacc;
       }
-      for (int j = 0; j < k; ++j) {
-        const cd* qj = Q[j].data();
-        cd hj = h[j];
-        for (long i = 0; i < n; ++i) w[i] -= hj * qj[i];
+    };
+    auto subtract = [&](const vector<cd>& h) {
+      for (long i = 0; i < n; ++i) {
+        cd v = w[i];
+        for (int j = 0; j < k; ++j) v -= h[j] * Q[j][i];
+        w[i] = v;
       }
+    };
+    vector<cd> h(k);
+    dots(h);
+    double nw2 = 0.0, hh = 0.0;
+    for (long i = 0; i < n; ++i) nw2 += std::norm(w[i]);
+    for (int j = 0; j < k; ++j) hh += std::norm(h[j]);
+    double a_k = h[k - 1].real(), b_k;
+    const double r2 = nw2 - hh;
+    const bool accept = r2 >= 0.5 * nw2;
+    if (accept) {
+      b_k = std::sqrt(r2);
+    } else {
+      subtract(h);
+      dots(h);
       a_k += h[k - 1].real();
+      subtract(h);
       b_k = nrm2(w.data(), n);
-      if (b_k >= 0.7071067811865476 * nprev) break;
-      nprev = b_k;
     }
     alpha.push_back(a_k);
     m = k;
@@ -511,6 +526,7 @@ vector<cd> expm_krylov(Op&& op, const vector<cd>& v, double dt, const KrylovPara
     bound *= b_k * tau / k;
     if (kp.exit_tol > 0.0 && bound <= kp.exit_tol) break;
     beta.push_back(b_k);
+    if (accept) subtract(h);
     vector<cd> qn(n);
     for (long i = 0; i < n; ++i) qn[i] = w[i] / b_k;
     Q.push_back(std::move(qn));

@@ -236,6 +236,59 @@ __device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
   if (on) ks.y[j] = v;
 }
 
+// h_j = <q_j, w> (j < k) into ks.h and |w|^2 in the same pass over w: the
+// first group takes seven vectors and the norm, later groups eight.
+__device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w, long long n, int k, EngineSmem& sm) {
+  const int tid = threadIdx.x;
+  double nw2 = 0.0;
+  for (int j0 = 0, first = 1; j0 < k || first; first = 0) {
+    const int G = first ? 7 : 8;
+    double d[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) d[e] = 0.0;
+    for (long long i = tid; i < n; i += NT) {
+      const cplx wi = w[i];
+      if (first) d[15] += cabs2(wi);
+#pragma unroll
+      for (int e = 0; e < 7; ++e) {
+        if (j0 + e < k) {
+          const cplx p = cmulc(Q[qs * (j0 + e) + i], wi);
+          d[2 * e] += p.x;
+          d[2 * e + 1] += p.y;
+        }
+      }
+      if (!first && j0 + 7 < k) {
+        const cplx p = cmulc(Q[qs * (j0 + 7) + i], wi);
+        d[14] += p.x;
+        d[15] += p.y;
+      }
+    }
+    block_sum_n<16>(d, sm.r);
+    if (tid < G && j0 + tid < k) sm.k.h[j0 + tid] = make_double2(d[2 * tid], d[2 * tid + 1]);
+    if (first) nw2 = d[15];
+    j0 += G;
+  }
+  __syncthreads();
+  return nw2;
+}
+
+// w <- w - sum_j h_j q_j (j < k); with norm, returns |w|^2 after the update.
+__device__ double lanczos_subtract(const cplx* Q, long long qs, cplx* w, long long n, int k, EngineSmem& sm,
+                                   bool norm) {
+  double part = 0.0;
+  for (long long i = threadIdx.x; i < n; i += NT) {
+    cplx v = w[i];
+    for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
+    w[i] = v;
+    part += cabs2(v);
+  }
+  if (!norm) {
+    __syncthreads();
+    return 0.0;
+  }
+  return block_sum(part, sm.r);
+}
+
 // In place: x <- exp(-i dt H_eff) x.  Q holds kdim+1 vectors of stride qs.
 // Returns the number of H_eff products.  CTA-collective.
 __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt, const KrylovCfg& kc, cplx* Q,
@@ -255,41 +308,25 @@ __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt,
     dev_heff(h, Q + qs * (k - 1), w, sm);
     ++mv;
     ProfScope orth_scope_(PF_ORTH);
-    // classical Gram-Schmidt with one refinement pass when the first kept
-    // less than 1/sqrt(2) of the norm (DGKS criterion)
-    double a_k = 0.0;
-    double nprev = sqrt(cta_norm2(w, n, sm.r)), b_k = nprev;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int j0 = 0; j0 < k; j0 += 8) {
-        double d[16];
-#pragma unroll
-        for (int e = 0; e < 16; ++e) d[e] = 0.0;
-        for (long long i = tid; i < n; i += NT) {
-          cplx wi = w[i];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            if (j0 + e < k) {
-              cplx p = cmulc(Q[qs * (j0 + e) + i], wi);
-              d[2 * e] += p.x;
-              d[2 * e + 1] += p.y;
-            }
-          }
-        }
-        block_sum_n<16>(d, sm.r);
-        if (tid < 8 && j0 + tid < k) sm.k.h[j0 + tid] = make_double2(d[2 * tid], d[2 * tid + 1]);
-      }
-      __syncthreads();
-      double part = 0.0;
-      for (long long i = tid; i < n; i += NT) {
-        cplx v = w[i];
-        for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
-        w[i] = v;
-        part += cabs2(v);
-      }
+    // classical Gram-Schmidt.  One pass gives h_j = <q_j, w> and |w|^2; when
+    // the projection keeps at least 1/sqrt(2) of the norm (DGKS criterion,
+    // |w - Q h|^2 = |w|^2 - |h|^2 >= |w|^2 / 2) the residual norm follows from
+    // Pythagoras and one more pass forms q_k = (w - Q h) / b_k; otherwise a
+    // refinement pass projects again and the norm is taken directly.
+    const double nw2 = lanczos_dots(Q, qs, w, n, k, sm);
+    double hh = 0.0;
+    for (int j = 0; j < k; ++j) hh += cabs2(sm.k.h[j]);
+    double a_k = sm.k.h[k - 1].x;
+    const double r2 = nw2 - hh;
+    const bool accept = r2 >= 0.5 * nw2;
+    double b_k;
+    if (accept) {
+      b_k = sqrt(r2);
+    } else {
+      lanczos_subtract(Q, qs, w, n, k, sm, false);
+      lanczos_dots(Q, qs, w, n, k, sm);
       a_k += sm.k.h[k - 1].x;
-      b_k = sqrt(block_sum(part, sm.r));
-      if (b_k >= 0.7071067811865476 * nprev) break;
-      nprev = b_k;
+      b_k = sqrt(lanczos_subtract(Q, qs, w, n, k, sm, true));
     }
     if (tid == 0) sm.k.alpha[k - 1] = a_k;
     m = k;
@@ -298,7 +335,16 @@ __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt,
     bound *= b_k * tau / k;
     if (kc.exit_tol > 0.0 && bound <= kc.exit_tol) break;
     if (tid == 0) sm.k.beta[k - 1] = b_k;
-    for (long long i = tid; i < n; i += NT) w[i] = cscale(w[i], 1.0 / b_k);
+    const double inv = 1.0 / b_k;
+    if (accept) {
+      for (long long i = tid; i < n; i += NT) {
+        cplx v = w[i];
+        for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
+        w[i] = cscale(v, inv);
+      }
+    } else {
+      for (long long i = tid; i < n; i += NT) w[i] = cscale(w[i], inv);
+    }
     __syncthreads();
   }
   __syncthreads();
