@@ -51,6 +51,8 @@ struct WApplySmem {
 // input/output rows tid / PT + k NT / PT, so index arithmetic is per tile,
 // not per element, and with PT = NT a thread issues all ni loads of its pair
 // back to back.  T is cplx (FP64 form) or float2 (mixed form, FP32 products).
+// in and out may be the same buffer when every pair's inputs and outputs
+// occupy the same addresses (a tile reads all its inputs before it writes).
 __device__ __forceinline__ void wfma(cplx& acc, cplx v, cplx x) { cfma(acc, v, x); }
 __device__ __forceinline__ void wfma(float2& acc, cplx v, float2 x) {
   const float vr = (float)v.x, vi = (float)v.y;
@@ -61,7 +63,7 @@ __device__ __forceinline__ void wzero(cplx& z) { z = make_double2(0.0, 0.0); }
 __device__ __forceinline__ void wzero(float2& z) { z = make_float2(0.f, 0.f); }
 
 template <class T>
-__device__ __noinline__ void dev_wapply(const T* __restrict__ in, T* __restrict__ out, const WMat W,
+__device__ __noinline__ void dev_wapply(const T* in, T* out, const WMat W,
                                         const WApplyGeom g, WApplySmem& ws) {
   ProfScope prof_scope_(PF_WAPPLY);
   T* sin = reinterpret_cast<T*>(&ws.in[0]);
@@ -167,13 +169,18 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   g.no1 = D;
   g.oo1 = chil;
   g.oo2 = (long long)chil * D;
-  // an identity W with D = 1 (the bond operator) leaves T1 in T2's layout
+  // an identity W with D = 1 (the bond operator) leaves T1 in T2's layout.
+  // With wl == wr the pair (a, b) holds its wl*D inputs and its wr*D outputs
+  // at the same addresses (a + chil * j within the block of b), so the MPO
+  // apply runs in place: T2's stores land on the lines T1 just left in L2
+  // and one buffer per slot is written back instead of two.
+  const bool inplace = wl == wr;
   if (h.mixed) {
     GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(sm.u.gw.g);
     const cflt* T2 = h.T1f;
     if (!h.W.ident) {
-      dev_wapply<cflt>(h.T1f, h.T2f, h.W, g, sm.u.gw.w);
-      T2 = h.T2f;
+      dev_wapply<cflt>(h.T1f, inplace ? h.T1f : h.T2f, h.W, g, sm.u.gw.w);
+      T2 = inplace ? h.T1f : h.T2f;
     }
     cta_gemm_tf32<cplx>(gemm_args_f(chil * D, chir, wr * chir, T2, 1, (long long)chil * D, h.Rf, chir, 1, y, 1,
                                     (long long)chil * D),
@@ -181,8 +188,8 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   } else {
     const cplx* T2 = h.T1;
     if (!h.W.ident) {
-      dev_wapply<cplx>(h.T1, h.T2, h.W, g, sm.u.gw.w);
-      T2 = h.T2;
+      dev_wapply<cplx>(h.T1, inplace ? h.T1 : h.T2, h.W, g, sm.u.gw.w);
+      T2 = inplace ? h.T1 : h.T2;
     }
     cta_gemm(gemm_args(chil * D, chir, wr * chir, T2, 1, (long long)chil * D, h.R, chir, 1, y, 1,
                        (long long)chil * D),
