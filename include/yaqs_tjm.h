@@ -308,6 +308,22 @@ int yaqs_analog_finish(yaqs_run* run, double* traj_out, double* mean_out,
                        int32_t* maxchi_out, yaqs_run_stats* stats);
 
 /*
+ * Snapshot of one trajectory of a run between begin and finish: its
+ * evolving state (the MPS that the next advance continues from; for the
+ * analog program the state phi of analog_tjm_2, AnalogTJM.jl:104-137, not
+ * the sampled copy) copied to host buffers.  chi_out[L+1] receives the bond
+ * dimensions, oc_out the 0-based orthogonality centre, tensors_out the site
+ * tensors (chi[i], 2, chi[i+1]) column-major interleaved complex,
+ * concatenated site after site: sum_i 4 chi[i] chi[i+1] doubles, returned in
+ * *needed.  With tensors_out NULL (or capacity below *needed) only chi_out,
+ * oc_out and *needed are filled; the status is YAQS_OK either way unless an
+ * argument is invalid.  No counterpart in the reference, whose trajectories
+ * return only their observables (Simulator.jl:41-47).
+ */
+int yaqs_run_state(yaqs_run* run, int32_t traj, int32_t* chi_out, int32_t* oc_out, double* tensors_out,
+                   int64_t capacity, int64_t* needed);
+
+/*
  * Device time per engine phase so far (clock cycles summed over CTAs, 16
  * entries: GEMM, MPO apply, Lanczos orthogonalisation, tridiagonal
  * exponential, SVD sweeps, SVD vectors, QR factor, QR form-Q, norm

@@ -292,3 +292,23 @@ def test_run_repeated_library_circuit_defaults_to_tdvp_windows(oracle):
     ref, chi_ref, _ = oracle.digital_run(d)
     assert ref.shape[2] == 5
     assert np.abs(res.trajectories - ref).max() <= 1e-10 and np.array_equal(res.max_bond, chi_ref)
+
+
+def test_session_state_snapshot():
+    """yaqs_run_state: a trajectory's final state copied from the device
+    reproduces the observables recorded at the last sample."""
+    from yaqs_julia_b200 import tensornet as T
+    L = 6
+    c = _brickwork(L, 2, seed=71)
+    nm = api.NoiseModel([{"name": "pauli_x", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=5, max_bond_dim=16)
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, seed=9)
+    sess = api.Session(d)
+    sess.advance(sess.remaining)
+    states = [sess.state(k) for k in range(5)]
+    res = sess.finish()
+    for k, m in enumerate(states):
+        assert T.check_if_valid_mps(m) and abs(np.linalg.norm(m.to_vec()) - 1) < 1e-10
+        z = [T.local_expect(m, api.Z, i).real for i in range(1, L + 1)]
+        assert np.abs(np.array(z) - res.trajectories[k, :, -1]).max() < 1e-10
+        assert T.write_max_bond_dim(m) == res.max_bond[k, -1]

@@ -42,6 +42,8 @@ def lib():
         L.yaqs_analog_remaining.argtypes = [C.c_void_p]
         L.yaqs_analog_profile.argtypes = [C.c_void_p, A.DPTR]
         L.yaqs_analog_stats.argtypes = [C.c_void_p, P(A.RunStats)]
+        L.yaqs_run_state.argtypes = [C.c_void_p, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_double), C.c_int64,
+                                     P(C.c_int64)]
         L.yaqs_analog_finish.argtypes = [C.c_void_p, A.DPTR, A.DPTR, P(C.c_int32), P(A.RunStats)]
         L.yaqs_digital_plan.argtypes = [P(A.GateDesc), C.c_int32, P(C.c_int32), P(C.c_int32)]
         L.yaqs_digital_run.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),

@@ -1097,6 +1097,29 @@ class Session:
         self.ctx.check(self.ctx._lib.yaqs_analog_stats(self.handle, C.byref(st)))
         return st.as_dict()
 
+    def state(self, traj: int) -> MPS:
+        """The evolving state of trajectory ``traj`` (0-based within this
+        run) after the last advance, copied from the device (yaqs_run_state)."""
+        L = self.desc.mps.L
+        chi = np.zeros(L + 1, dtype=np.int32)
+        oc = C.c_int32(0)
+        need = C.c_int64(0)
+        ip = C.POINTER(C.c_int32)
+        self.ctx.check(self.ctx._lib.yaqs_run_state(self.handle, traj, chi.ctypes.data_as(ip), C.byref(oc), None,
+                                                    0, C.byref(need)))
+        buf = np.zeros(need.value, dtype=np.float64)
+        self.ctx.check(self.ctx._lib.yaqs_run_state(self.handle, traj, chi.ctypes.data_as(ip), C.byref(oc),
+                                                    A.dptr(buf), need.value, C.byref(need)))
+        z = buf.view(np.complex128)
+        tens, pos = [], 0
+        for i in range(L):
+            n = int(chi[i]) * 2 * int(chi[i + 1])
+            tens.append(z[pos:pos + n].reshape(int(chi[i]), 2, int(chi[i + 1]), order="F"))
+            pos += n
+        m = MPS(L, tensors=tens)
+        m.orth_center = int(oc.value) + 1
+        return m
+
     def profile(self) -> dict:
         out = np.zeros(16)
         self.ctx.check(self.ctx._lib.yaqs_analog_profile(self.handle, A.dptr(out)))

@@ -1047,6 +1047,34 @@ int yaqs_analog_stats(yaqs_run* run, yaqs_run_stats* stats) {
   return collect_stats(run, stats);
 }
 
+int yaqs_run_state(yaqs_run* run, int32_t traj, int32_t* chi_out, int32_t* oc_out, double* tensors_out,
+                   int64_t capacity, int64_t* needed) {
+  if (!run || !chi_out || !oc_out || !needed) return set_err(nullptr, YAQS_E_ARG, "null argument");
+  yaqs_ctx* ctx = run->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (traj < 0 || traj >= run->P.num_traj) return set_err(ctx, YAQS_E_ARG, "trajectory index out of range");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(run->stream));
+  const int L = run->P.L;
+  std::vector<long long> off(L);
+  CUDA_TRY(ctx, cudaMemcpy(off.data(), run->P.mps_off, L * sizeof(long long), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(chi_out, run->P.phi_chi + (size_t)traj * (L + 1), (L + 1) * sizeof(int32_t),
+                           cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(oc_out, run->P.phi_oc + traj, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  long long need = 0;
+  for (int i = 0; i < L; ++i) need += 4LL * chi_out[i] * chi_out[i + 1];
+  *needed = need;
+  if (!tensors_out || capacity < need) return YAQS_OK;
+  const cplx* base = run->P.phi + (size_t)traj * run->P.mps_size;
+  double* dst = tensors_out;
+  for (int i = 0; i < L; ++i) {
+    const size_t n = (size_t)chi_out[i] * 2 * chi_out[i + 1];
+    CUDA_TRY(ctx, cudaMemcpy(dst, base + off[i], n * sizeof(cplx), cudaMemcpyDeviceToHost));
+    dst += 2 * n;
+  }
+  return YAQS_OK;
+}
+
 int yaqs_analog_profile(yaqs_run* run, double* cycles) {
   if (!run || !cycles) return set_err(nullptr, YAQS_E_ARG, "null argument");
   for (int k = 0; k < PROF_N; ++k) cycles[k] = 0.0;
