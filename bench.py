@@ -51,6 +51,10 @@ sys.path.insert(0, ROOT)
 from yaqs_julia_b200 import _abi as A  # noqa: E402
 from yaqs_julia_b200 import api  # noqa: E402
 
+# DRAM bytes (read + write) of the timed launch, from one ncu capture of the
+# same command: (precision, tdvp, L, chi, trajectories, timed steps) -> bytes
+TIMED_TRAFFIC = {("fp64", "dynamic", 30, 64, 1024, 2): 10.53346e12 + 4.24245e12}
+
 METRIC = "TJM trajectory-steps/s (L=30 Heisenberg, chi=64, 1024 trajectories)"
 TDVP_NAMES = {"dynamic": A.YAQS_TDVP_DYNAMIC, "2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE}
 TDVP = [A.YAQS_TDVP_DYNAMIC]  # set from --tdvp
@@ -392,7 +396,7 @@ def run_digital(args):
                            "l2": "working set below L2 (bond dimensions stay small); every layer rereads the "
                                  "trajectory states, no flush"},
                 "gpu_launches": 1,  # one digital_step_kernel launch covers the timed layers
-                "roofline": {"bound": "fp64", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
+                "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
                              "frac": achieved / pk.value if pk.value else None, "traffic": None,
                              "kernel": "digital_step_kernel",
                              "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run",
@@ -592,8 +596,12 @@ def run_ours(args):
                                nt, sum(min(2 ** min(b, L - b), chi) * 2 * min(2 ** min(b + 1, L - b - 1), chi)
                                        for b in range(L)) * 16 / 1e6)},
                 "gpu_launches": 1,  # one tjm_step_kernel launch covers the K time indices
-                "roofline": {"bound": "fp64", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
-                             "frac": achieved / pk.value if pk.value else None, "traffic": None,
+                "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
+                             "frac": achieved / pk.value if pk.value else None,
+                             "traffic": TIMED_TRAFFIC.get((args.precision, args.tdvp, L, chi, nt, args.steps)),
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the timed "
+                                               "launch (profiles/tjm_step_kernel_L30_chi64_1024traj_dynamic_"
+                                               "launches.md); null for configurations not captured",
                              "kernel": "tjm_step_kernel",
                              "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run; "
                                             "MEASURED_PEAKS.json has no FP64 entry",
