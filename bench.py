@@ -281,6 +281,18 @@ def cpu_sample_digital(L, depth):
     return 2 * cores * depth / dt, cores, f"{2 * cores} trajectories x {depth} layers of the same circuit, {dt:.1f} s"
 
 
+def analog_config(args, L, chi, nt, ws):
+    """The analog workload's config object (shared by both bench arms)."""
+    return {"workload": f"analog TJM, L={L} Heisenberg XXX h=0.3, dephasing gamma=0.05, dt=0.05, "
+                        f"{TDVP_DESC[args.tdvp]} chi_max={chi}, thr=1e-9, {nt} trajectories per GPU, "
+                        f"start={'saturated chi MPS' if args.start == 'sat' else 'Neel'}",
+            "L": L, "chi": chi, "num_traj": nt, "dt": 0.05, "parallelism": f"replicas x{ws}",
+            "precision": args.precision, "tdvp": args.tdvp,
+            "l2": "inputs larger than L2: %d trajectory states of up to %.1f MB each" % (
+                nt, sum(min(2 ** min(b, L - b), chi) * 2 * min(2 ** min(b + 1, L - b - 1), chi)
+                        for b in range(L)) * 16 / 1e6)}
+
+
 def run_reference(args):
     ws, rank, local, dist = dist_setup()
     if rank != 0:
@@ -310,9 +322,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": f"L={args.L} Heisenberg h=0.3, chi={args.chi}, dephasing 0.05, dt=0.05, "
-                                   f"{TDVP_DESC[args.tdvp]}, "
-                                   f"start={args.start}", "L": args.L, "chi": args.chi},
+            "config": analog_config(args, args.L, args.chi, args.traj, args.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference Julia (Yaqs.jl) cannot run here; CPU restatement (oracle/tjm_oracle.cpp)"}
@@ -587,14 +597,7 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "c64 contractions (3xTF32 tensor cores) + c128 Lanczos/SVD/QR/norms"
                 if args.precision == "mixed" else "c128", "data": "synthetic",
-                "config": {"workload": f"analog TJM, L={L} Heisenberg XXX h=0.3, dephasing gamma=0.05, dt=0.05, "
-                                       f"{TDVP_DESC[args.tdvp]} chi_max={chi}, thr=1e-9, {nt} trajectories per GPU, "
-                                       f"start={'saturated chi MPS' if args.start == 'sat' else 'Neel'}",
-                           "L": L, "chi": chi, "num_traj": nt, "dt": 0.05, "parallelism": f"replicas x{ws}",
-                           "precision": args.precision, "tdvp": args.tdvp,
-                           "l2": "inputs larger than L2: %d trajectory states of up to %.1f MB each" % (
-                               nt, sum(min(2 ** min(b, L - b), chi) * 2 * min(2 ** min(b + 1, L - b - 1), chi)
-                                       for b in range(L)) * 16 / 1e6)},
+                "config": analog_config(args, L, chi, nt, ws),
                 "gpu_launches": 1,  # one tjm_step_kernel launch covers the K time indices
                 "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
                              "frac": achieved / pk.value if pk.value else None,
