@@ -1,0 +1,62 @@
+"""The multi-GPU form is replicas: each rank runs its own block of
+trajectories (global index = rank * n + local index, which keys the Philox
+streams) and only the timing is reduced.  Two gloo ranks on the CPU check
+that the blocks reproduce one run of all trajectories and that the bench's
+max/sum reductions combine the ranks as the bench line reports them."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _problem(nt, offset):
+    from yaqs_julia_b200 import api
+    L = 4
+    H = api.init_ising(L, 1.0, 0.7)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.3, dt=0.1, num_traj=nt, max_bond_dim=8)
+    nm = api.NoiseModel([{"name": "lowering", "sites": [i], "strength": 0.3} for i in range(1, L + 1)], L)
+    return api.Descriptors(api.MPS(L, state="ones"), H, cfg, nm, seed=1234, traj_offset=offset)
+
+
+def _rank(rank, world, port, nt, out_dir):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import bench
+    from oracle import oracle as O
+    ws, r, _, dist = bench.dist_setup()
+    assert (ws, r) == (world, rank)
+    traj, _, st = O.analog_run(_problem(nt, rank * nt))
+    np.save(os.path.join(out_dir, f"traj{rank}.npy"), traj)
+    t_max = bench.reduce_max(dist, 1.0 + rank)      # per-rank device seconds
+    units = bench.reduce_sum(dist, nt * 3)          # trajectory-steps of this rank
+    np.save(os.path.join(out_dir, f"red{rank}.npy"), np.array([t_max, units, st["jumps"]]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_replicas_reproduce_one_run(oracle, tmp_path):
+    import torch.multiprocessing as mp
+    nt, world = 6, 2
+    port = _free_port()
+    mp.start_processes(_rank, args=(world, port, nt, str(tmp_path)), nprocs=world, start_method="spawn", join=True)
+    parts = [np.load(tmp_path / f"traj{r}.npy") for r in range(world)]
+    whole, _, st = oracle.analog_run(_problem(world * nt, 0))
+    assert np.array_equal(np.concatenate(parts, axis=0), whole)
+    for r in range(world):
+        t_max, units, _ = np.load(tmp_path / f"red{r}.npy")
+        assert t_max == 2.0 and units == world * nt * 3
+    jumps = sum(int(np.load(tmp_path / f"red{r}.npy")[2]) for r in range(world))
+    assert jumps == st["jumps"] > 0
