@@ -82,7 +82,7 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
 // blocks of 8x8, each block accumulating re and im with four real MMAs.
 // Conjugation is a template parameter (a sign flip of the imaginary
 // fragment).
-template <bool CA, bool CB>
+template <bool CA, bool CB, int BK>
 __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   ProfScope prof_scope_(PF_GEMM);
   const int tid = threadIdx.x;
@@ -91,7 +91,7 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   const int gq = lane >> 2, tq = lane & 3;
   const bool a_m_fast = (g.am == 1) || (g.ak != 1);
   const bool b_n_fast = (g.bn == 1) || (g.bk != 1);
-  const int nk = (g.K + GBK - 1) / GBK;
+  const int nk = (g.K + BK - 1) / BK;
   for (int tm = 0; tm < g.M; tm += GBM) {
     for (int tn = 0; tn < g.N; tn += GBN) {
       double cr[4][2][2], ci[4][2][2];
@@ -103,24 +103,24 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
           ci[i][j][0] = ci[i][j][1] = 0.0;
         }
       auto issue = [&](int kc, int buf) {
-        const int k0 = kc * GBK;
+        const int k0 = kc * BK;
 #pragma unroll
-        for (int e = 0; e < GBM * GBK / NT; ++e) {
+        for (int e = 0; e < GBM * BK / NT; ++e) {
           const int idx = tid + NT * e;
           int mi, ki, ni, kj;
           if (a_m_fast) {
             mi = idx & (GBM - 1);
             ki = idx / GBM;
           } else {
-            ki = idx & (GBK - 1);
-            mi = idx / GBK;
+            ki = idx & (BK - 1);
+            mi = idx / BK;
           }
           if (b_n_fast) {
             ni = idx & (GBN - 1);
             kj = idx / GBN;
           } else {
-            kj = idx & (GBK - 1);
-            ni = idx / GBK;
+            kj = idx & (BK - 1);
+            ni = idx / BK;
           }
           const int mm = tm + mi, ka = k0 + ki, nn = tn + ni, kb = k0 + kj;
           const bool va = mm < g.M && ka < g.K, vb = nn < g.N && kb < g.K;
@@ -141,7 +141,7 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
         }
         __syncthreads();
 #pragma unroll
-        for (int k4 = 0; k4 < GBK; k4 += 4) {
+        for (int k4 = 0; k4 < BK; k4 += 4) {
           double ar[4], ai[4], br[2], bi[2];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
@@ -188,12 +188,22 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   __syncthreads();
 }
 
-__device__ __forceinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
+// K slices 16 deep for long reductions, 8 deep for short ones (a short K
+// would otherwise stage mostly zero padding).
+template <int BK>
+__device__ __forceinline__ void cta_gemm_k(const GemmArgs g, GemmSmem& sm) {
   if (g.conjA) {
-    if (g.conjB) cta_gemm_t<true, true>(g, sm);
-    else cta_gemm_t<true, false>(g, sm);
+    if (g.conjB) cta_gemm_t<true, true, BK>(g, sm);
+    else cta_gemm_t<true, false, BK>(g, sm);
   } else {
-    if (g.conjB) cta_gemm_t<false, true>(g, sm);
-    else cta_gemm_t<false, false>(g, sm);
+    if (g.conjB) cta_gemm_t<false, true, BK>(g, sm);
+    else cta_gemm_t<false, false, BK>(g, sm);
   }
+}
+
+__device__ __forceinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
+  if (g.K >= 32)
+    cta_gemm_k<GBK>(g, sm);
+  else
+    cta_gemm_k<8>(g, sm);
 }
