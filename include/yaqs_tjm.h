@@ -324,6 +324,23 @@ int yaqs_run_state(yaqs_run* run, int32_t traj, int32_t* chi_out, int32_t* oc_ou
                    int64_t capacity, int64_t* needed);
 
 /*
+ * Checkpoint and restore within a stepped run (no counterpart in the
+ * reference).  yaqs_run_position gives the next launch-list position (the
+ * number of advance steps taken); yaqs_run_rng the number of uniforms a
+ * trajectory has drawn (its Philox counter or its offset in the injected
+ * stream).  yaqs_run_restore writes a trajectory's state (as yaqs_run_state
+ * returns it; bond dimensions within this run's capacities) and draw count;
+ * yaqs_run_seek(run, p) makes the next advance run position p again
+ * (1 <= p <= positions), so a run restored from a checkpoint taken at
+ * position p repeats the trajectories it recorded from there.
+ */
+int yaqs_run_position(const yaqs_run* run, int32_t* position);
+int yaqs_run_rng(yaqs_run* run, int32_t traj, int64_t* draws);
+int yaqs_run_restore(yaqs_run* run, int32_t traj, const int32_t* chi, int32_t oc, const double* tensors,
+                     int64_t draws);
+int yaqs_run_seek(yaqs_run* run, int32_t position);
+
+/*
  * Device time per engine phase so far (clock cycles summed over CTAs, 16
  * entries: GEMM, MPO apply, Lanczos orthogonalisation, tridiagonal
  * exponential, SVD sweeps, SVD vectors, QR factor, QR form-Q, norm

@@ -312,3 +312,21 @@ def test_session_state_snapshot():
         z = [T.local_expect(m, api.Z, i).real for i in range(1, L + 1)]
         assert np.abs(np.array(z) - res.trajectories[k, :, -1]).max() < 1e-10
         assert T.write_max_bond_dim(m) == res.max_bond[k, -1]
+
+
+def test_checkpoint_restore_digital():
+    L = 6
+    c = _brickwork(L, 3, seed=73)
+    nm = api.NoiseModel([{"name": "pauli_y", "sites": [i], "strength": 0.06} for i in range(1, L + 1)], L)
+    cfg = api.TimeEvolutionConfig(_zs(L), 1.0, dt=1.0, num_traj=5, max_bond_dim=16)
+    d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, seed=19)
+    straight = api.run_circuit_descriptors(d)
+    sess = api.Session(d)
+    sess.advance(3)
+    cp = sess.checkpoint()
+    sess.advance(2)
+    sess.restore(cp)
+    sess.advance(sess.remaining)
+    res = sess.finish()
+    assert np.array_equal(res.trajectories, straight.trajectories)
+    assert np.array_equal(res.max_bond, straight.max_bond)

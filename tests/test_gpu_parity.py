@@ -301,3 +301,24 @@ def test_long_range_noise_tight_bond_cap(oracle):
     u = np.random.default_rng(29).random((6, api.max_draws(cfg)))
     got, _ = _compare(oracle, api.MPS(L, state="Neel"), H, cfg, nm, uniforms=u)
     assert got.stats["jumps"] > 0
+
+
+def test_checkpoint_restore_repeats_the_run():
+    """yaqs_run_state / _rng / _restore / _seek: a run put back to a
+    checkpoint after running ahead records exactly what the straight run
+    records (the state and the draw count are a trajectory's whole carry)."""
+    psi, H, cfg, nm = _cfg1(num_traj=6, T=1.0)
+    d = api.Descriptors(psi, H, cfg, nm, seed=77, tdvp_mode=api.TDVP_MODES["dynamic"])
+    straight = api.run_descriptors(d)
+    sess = api.Session(d)
+    n0 = sess.remaining
+    sess.advance(4)
+    cp = sess.checkpoint()
+    assert cp["position"] == 4 and max(cp["draws"]) > 0
+    sess.advance(3)
+    sess.restore(cp)
+    assert sess.remaining == n0 - 4
+    sess.advance(sess.remaining)
+    res = sess.finish()
+    assert np.array_equal(res.trajectories, straight.trajectories)
+    assert np.array_equal(res.max_bond, straight.max_bond)

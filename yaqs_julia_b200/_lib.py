@@ -44,6 +44,10 @@ def lib():
         L.yaqs_analog_stats.argtypes = [C.c_void_p, P(A.RunStats)]
         L.yaqs_run_state.argtypes = [C.c_void_p, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_double), C.c_int64,
                                      P(C.c_int64)]
+        L.yaqs_run_position.argtypes = [C.c_void_p, P(C.c_int32)]
+        L.yaqs_run_rng.argtypes = [C.c_void_p, C.c_int32, P(C.c_int64)]
+        L.yaqs_run_restore.argtypes = [C.c_void_p, C.c_int32, P(C.c_int32), C.c_int32, P(C.c_double), C.c_int64]
+        L.yaqs_run_seek.argtypes = [C.c_void_p, C.c_int32]
         L.yaqs_analog_finish.argtypes = [C.c_void_p, A.DPTR, A.DPTR, P(C.c_int32), P(A.RunStats)]
         L.yaqs_digital_plan.argtypes = [P(A.GateDesc), C.c_int32, P(C.c_int32), P(C.c_int32)]
         L.yaqs_digital_run.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),

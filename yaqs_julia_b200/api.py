@@ -1120,6 +1120,31 @@ class Session:
         m.orth_center = int(oc.value) + 1
         return m
 
+    def checkpoint(self) -> dict:
+        """Every trajectory's state and draw count at the current position
+        (yaqs_run_position / yaqs_run_state / yaqs_run_rng)."""
+        pos = C.c_int32(0)
+        self.ctx.check(self.ctx._lib.yaqs_run_position(self.handle, C.byref(pos)))
+        states, draws = [], []
+        for k in range(self.desc.num_traj):
+            states.append(self.state(k))
+            d = C.c_int64(0)
+            self.ctx.check(self.ctx._lib.yaqs_run_rng(self.handle, k, C.byref(d)))
+            draws.append(d.value)
+        return {"position": pos.value, "states": states, "draws": draws}
+
+    def restore(self, cp: dict) -> None:
+        """Put every trajectory back to a checkpoint of this run and make the
+        next advance continue from its position (yaqs_run_restore /
+        yaqs_run_seek)."""
+        ip = C.POINTER(C.c_int32)
+        for k, (m, d) in enumerate(zip(cp["states"], cp["draws"])):
+            chi = np.array(m.bond_dims, dtype=np.int32)
+            buf = np.concatenate([_c64(t) for t in m.tensors])
+            self.ctx.check(self.ctx._lib.yaqs_run_restore(self.handle, k, chi.ctypes.data_as(ip), m.orth_center - 1,
+                                                          A.dptr(buf), int(d)))
+        self.ctx.check(self.ctx._lib.yaqs_run_seek(self.handle, cp["position"]))
+
     def profile(self) -> dict:
         out = np.zeros(16)
         self.ctx.check(self.ctx._lib.yaqs_analog_profile(self.handle, A.dptr(out)))

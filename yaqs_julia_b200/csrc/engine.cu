@@ -1075,6 +1075,74 @@ int yaqs_run_state(yaqs_run* run, int32_t traj, int32_t* chi_out, int32_t* oc_ou
   return YAQS_OK;
 }
 
+int yaqs_run_position(const yaqs_run* run, int32_t* position) {
+  if (!run || !position) return set_err(nullptr, YAQS_E_ARG, "null argument");
+  *position = (int32_t)run->next;
+  return YAQS_OK;
+}
+
+int yaqs_run_rng(yaqs_run* run, int32_t traj, int64_t* draws) {
+  if (!run || !draws) return set_err(nullptr, YAQS_E_ARG, "null argument");
+  yaqs_ctx* ctx = run->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (traj < 0 || traj >= run->P.num_traj) return set_err(ctx, YAQS_E_ARG, "trajectory index out of range");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(run->stream));
+  long long v = 0;
+  CUDA_TRY(ctx, cudaMemcpy(&v, run->P.rng_pos + traj, sizeof(long long), cudaMemcpyDeviceToHost));
+  *draws = v;
+  return YAQS_OK;
+}
+
+int yaqs_run_restore(yaqs_run* run, int32_t traj, const int32_t* chi, int32_t oc, const double* tensors,
+                     int64_t draws) {
+  if (!run || !chi || !tensors) return set_err(nullptr, YAQS_E_ARG, "null argument");
+  yaqs_ctx* ctx = run->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int L = run->P.L;
+  if (traj < 0 || traj >= run->P.num_traj) return set_err(ctx, YAQS_E_ARG, "trajectory index out of range");
+  if (oc < 0 || oc >= L || draws < 0) return set_err(ctx, YAQS_E_ARG, "bad centre or draw count");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(run->stream));
+  std::vector<int> cap(L + 1);
+  std::vector<long long> off(L);
+  CUDA_TRY(ctx, cudaMemcpy(cap.data(), run->P.cap, (L + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  CUDA_TRY(ctx, cudaMemcpy(off.data(), run->P.mps_off, L * sizeof(long long), cudaMemcpyDeviceToHost));
+  if (chi[0] != 1 || chi[L] != 1) return set_err(ctx, YAQS_E_ARG, "boundary bonds must be 1");
+  for (int b = 0; b <= L; ++b)
+    if (chi[b] < 1 || chi[b] > cap[b]) return set_err(ctx, YAQS_E_ARG, "bond dimension beyond this run's capacity");
+  cplx* base = run->P.phi + (size_t)traj * run->P.mps_size;
+  const double* src = tensors;
+  for (int i = 0; i < L; ++i) {
+    const size_t n = (size_t)chi[i] * 2 * chi[i + 1];
+    CUDA_TRY(ctx, cudaMemcpy(base + off[i], src, n * sizeof(cplx), cudaMemcpyHostToDevice));
+    src += 2 * n;
+  }
+  const long long d = draws;
+  CUDA_TRY(ctx, cudaMemcpy(run->P.phi_chi + (size_t)traj * (L + 1), chi, (L + 1) * sizeof(int32_t),
+                           cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(run->P.phi_oc + traj, &oc, sizeof(int32_t), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(run->P.rng_pos + traj, &d, sizeof(long long), cudaMemcpyHostToDevice));
+  return YAQS_OK;
+}
+
+int yaqs_run_seek(yaqs_run* run, int32_t position) {
+  if (!run) return set_err(nullptr, YAQS_E_ARG, "null run");
+  yaqs_ctx* ctx = run->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int np = (int)run->launches.size();
+  if (position < 1 || position > np) return set_err(ctx, YAQS_E_ARG, "position must be in [1, positions]");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaStreamSynchronize(run->stream));
+  // launches from here on pull fresh unit counters, and every trajectory
+  // counts as having completed exactly the position before
+  CUDA_TRY(ctx, cudaMemset(run->P.queue + position, 0, (size_t)(np - position) * sizeof(int)));
+  std::vector<int> done(run->P.num_traj, position - 1);
+  CUDA_TRY(ctx, cudaMemcpy(run->P.done, done.data(), done.size() * sizeof(int), cudaMemcpyHostToDevice));
+  run->next = position;
+  return YAQS_OK;
+}
+
 int yaqs_analog_profile(yaqs_run* run, double* cycles) {
   if (!run || !cycles) return set_err(nullptr, YAQS_E_ARG, "null argument");
   for (int k = 0; k < PROF_N; ++k) cycles[k] = 0.0;
