@@ -1011,6 +1011,18 @@ class RunResult:
         self.max_bond = maxchi        # [num_traj, n_out]
         self.stats = stats
 
+    @property
+    def variance(self) -> np.ndarray:
+        """Unbiased ensemble variance per observable and sample (an addition:
+        the reference aggregates means only, SimulationConfigs.jl:168-181)."""
+        n = self.trajectories.shape[0]
+        return self.trajectories.var(axis=0, ddof=1) if n > 1 else np.zeros_like(self.mean)
+
+    @property
+    def standard_error(self) -> np.ndarray:
+        """Standard error of the ensemble mean, sqrt(variance / num_traj)."""
+        return np.sqrt(self.variance / self.trajectories.shape[0])
+
 
 def run_descriptors(desc: Descriptors, ctx=None) -> RunResult:
     """Runs a packed problem through yaqs_analog_run."""
