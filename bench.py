@@ -54,6 +54,8 @@ from yaqs_julia_b200 import api  # noqa: E402
 # DRAM bytes (read + write) of the timed launch, from one ncu capture of the
 # same command: (precision, tdvp, L, chi, trajectories, timed steps) -> bytes
 TIMED_TRAFFIC = {("fp64", "dynamic", 30, 64, 1024, 2): 10.53346e12 + 4.24245e12}
+# the same for the digital workload: (L, trajectories, timed layers) -> bytes
+DIG_TIMED_TRAFFIC = {(40, 512, 57): 4.458638080e9 + 15.767363584e9}
 
 METRIC = "TJM trajectory-steps/s (L=30 Heisenberg, chi=64, 1024 trajectories)"
 TDVP_NAMES = {"dynamic": A.YAQS_TDVP_DYNAMIC, "2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE}
@@ -380,9 +382,12 @@ def run_digital(args):
     pk = C.c_double(0.0)
     ctx.check(ctx._lib.yaqs_fp64_peak(ctx.handle, C.byref(pk)))
     achieved = (st1["flops"] - st0["flops"]) / (dev_ms / 1e3) / 1e12
+    # end to end: the public call on host buffers (marshalling, uploads,
+    # the run, result reads); the circuit object is the caller's input and
+    # is built before the clock starts, as the analog leg builds its MPS/MPO
+    e2e_psi = digital_workload(L, depth, nt)
     barrier_sync(dist)
     t0 = time.perf_counter()
-    e2e_psi = digital_workload(L, depth, nt)
     e2e_desc = api.CircuitDescriptors(*e2e_psi, seed=DIG_SEED, traj_offset=rank * nt)
     api.run_circuit_descriptors(e2e_desc, ctx)
     barrier_sync(dist)
@@ -407,7 +412,11 @@ def run_digital(args):
                                  "trajectory states, no flush"},
                 "gpu_launches": 1,  # one digital_step_kernel launch covers the timed layers
                 "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
-                             "frac": achieved / pk.value if pk.value else None, "traffic": None,
+                             "frac": achieved / pk.value if pk.value else None,
+                             "traffic": DIG_TIMED_TRAFFIC.get((L, nt, K)),
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the timed "
+                                               "launch (profiles/digital_step_kernel_L40_ising_512traj.md); "
+                                               "null for configurations not captured",
                              "kernel": "digital_step_kernel",
                              "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run",
                              "achieved_counts": "nominal TEBD work: theta merge GEMM + 4x4 gate + SVD as "
