@@ -43,6 +43,11 @@ def lib():
         L.orc_digital_plan.argtypes = [P(A.GateDesc), C.c_int32, P(C.c_int32), P(C.c_int32)]
         L.orc_tdvp_evolve.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.ObsDesc), C.c_int32, P(A.TevConfig),
                                       C.c_int32, A.DPTR]
+        L.orc_tdvp_overlap.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.TevConfig), C.c_int32, A.DPTR]
+        L.orc_stochastic_factor.argtypes = [P(A.MpsDesc), A.DPTR]
+        L.orc_probability_distribution.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.NoiseDesc), P(A.TevConfig),
+                                                   C.c_double, C.c_int32, A.DPTR, P(C.c_int32), P(C.c_int32),
+                                                   P(C.c_int32)]
         L.orc_svd.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR, A.DPTR]
         L.orc_qr.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR]
         L.orc_truncation_rank.argtypes = [C.c_int32, A.DPTR, C.c_double, C.c_int32, C.c_int32]
@@ -105,6 +110,44 @@ def tdvp_evolve(desc, n_steps):
     _check(lib().orc_tdvp_evolve(C.byref(desc.mps), C.byref(desc.mpo), desc.obs, desc.n_obs, C.byref(desc.cfg),
                                  n_steps, A.dptr(out)))
     return out[:, :desc.n_obs]
+
+
+def tdvp_overlap(desc, n_steps) -> complex:
+    """scalar_product(psi(t), psi0) in the reference's convention after
+    n_steps noise-free sweeps of the configured TDVP mode."""
+    out = np.zeros(2)
+    _check(lib().orc_tdvp_overlap(C.byref(desc.mps), C.byref(desc.mpo), C.byref(desc.cfg), n_steps,
+                                  A.dptr(out)))
+    return complex(out[0], out[1])
+
+
+def stochastic_factor(desc) -> float:
+    """calculate_stochastic_factor of the packed initial state, as given."""
+    out = np.zeros(1)
+    _check(lib().orc_stochastic_factor(C.byref(desc.mps), A.dptr(out)))
+    return float(out[0])
+
+
+CANDIDATE_TYPES = ("local_1", "local_2", "pauli_long_range", "mpo_general")
+
+
+def probability_distribution(desc, dt):
+    """create_probability_distribution on the packed initial state:
+    (probabilities, [(type, sites 1-based)]) in the reference's order."""
+    cap = max(1, desc.noise.n)  # one candidate per process at most
+    probs = np.zeros(cap)
+    kinds = np.zeros(cap, dtype=np.int32)
+    sites = np.zeros(2 * cap, dtype=np.int32)
+    n = C.c_int32(0)
+    I32 = C.POINTER(C.c_int32)
+    _check(lib().orc_probability_distribution(C.byref(desc.mps), C.byref(desc.mpo), C.byref(desc.noise),
+                                              C.byref(desc.cfg), dt, cap, A.dptr(probs),
+                                              kinds.ctypes.data_as(I32), sites.ctypes.data_as(I32), C.byref(n)))
+    k = n.value
+    cands = [(CANDIDATE_TYPES[kinds[i]],
+              [int(sites[2 * i]) + 1] if kinds[i] == 0 else [int(sites[2 * i]) + 1, int(sites[2 * i + 1]) + 1])
+             for i in range(k)]
+    return probs[:k], cands
 
 
 def svd(M):

@@ -770,6 +770,30 @@ cd scalar_product(const State& s) {  // scalar_product(psi, psi), MPS.jl:528-585
   return E[0];
 }
 
+// scalar_product(psi, phi) of MPS.jl:528-585 for two states: the code
+// contracts psi with conj(phi), so this is sum psi * conj(phi) = <phi|psi>.
+cd scalar_product(const State& psi, const State& phi) {
+  vector<cd> E(1, 1.0);  // E[la, lb], leading dimension ea
+  int ea = 1;
+  for (int i = 0; i < psi.L; ++i) {
+    const Ten& A = psi.t[i];
+    const Ten& B = phi.t[i];
+    vector<cd> En((size_t)A.r * B.r, 0.0);
+    for (int rb = 0; rb < B.r; ++rb)
+      for (int ra = 0; ra < A.r; ++ra) {
+        cd acc = 0;
+        for (int p = 0; p < A.d; ++p)
+          for (int lb = 0; lb < B.l; ++lb)
+            for (int la = 0; la < A.l; ++la)
+              acc += E[la + (size_t)ea * lb] * A.at(la, p, ra) * std::conj(B.at(lb, p, rb));
+        En[ra + (size_t)A.r * rb] = acc;
+      }
+    E.swap(En);
+    ea = A.r;
+  }
+  return E[0];
+}
+
 void apply_1site(Ten& A, const cd* op) {  // T[l,p,r] <- sum_k op[p,k] T[l,k,r]
   Ten B(A.l, A.d, A.r);
   for (int r = 0; r < A.r; ++r)
@@ -1350,15 +1374,12 @@ struct Cand {
   double dp;
 };
 
-bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt, Draws& rng, Counters& cnt) {
+// create_probability_distribution (StochasticProcess.jl:89-212): the jump
+// candidates in the reference's order with their unnormalised weights
+// dt gamma ||L psi||^2 (1-site in site order, then 2-site adjacent, then the
+// long-range processes).  Moves the orthogonality centre.
+vector<Cand> jump_candidates(const Problem& P, const NoiseSet& N, State& s, double dt) {
   const int L = s.L;
-  double dp = 1.0 - scalar_product(s).real();
-  if (N.procs.empty() || rng.next() >= dp) {
-    shift_oc(s, 0);
-    normalize_mps(s);
-    return false;
-  }
-  // create_probability_distribution
   vector<Cand> cands;
   for (int site = 0; site < L; ++site) {
     shift_oc(s, site);
@@ -1405,6 +1426,17 @@ bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt
     }
     cands.push_back({&pr, dt * pr.gamma * nr});
   }
+  return cands;
+}
+
+bool stochastic_process(const Problem& P, const NoiseSet& N, State& s, double dt, Draws& rng, Counters& cnt) {
+  double dp = 1.0 - scalar_product(s).real();
+  if (N.procs.empty() || rng.next() >= dp) {
+    shift_oc(s, 0);
+    normalize_mps(s);
+    return false;
+  }
+  vector<Cand> cands = jump_candidates(P, N, s, dt);
   double total = 0;
   for (auto& c : cands) total += c.dp;
   if (total == 0.0) {
@@ -2056,6 +2088,68 @@ int orc_tdvp_evolve(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaq
     sw.sweep(s);
     for (int k = 0; k < n_obs; ++k) out[(size_t)t * n_obs + k] = measure(P.obs[k], s);
   }
+  return YAQS_OK;
+}
+
+// calculate_stochastic_factor (StochasticProcess.jl:35-38): dp = 1 - <psi|psi>
+// of the state as given (no normalisation first).
+int orc_stochastic_factor(const yaqs_mps_desc* psi, double* dp) {
+  if (!psi || !dp || psi->L < 1) return fail(YAQS_E_ARG, "null argument");
+  Problem P;
+  load_state(P, psi);
+  *dp = 1.0 - scalar_product(P.psi0).real();
+  return YAQS_OK;
+}
+
+// create_probability_distribution (StochasticProcess.jl:89-212) on the
+// initial state of a problem: the normalised weights in the reference's
+// candidate order, each candidate's type (0 local_1, 1 local_2,
+// 2 pauli_long_range, 3 mpo_general) and its two sites (0-based; the second
+// repeats the first for 1-site candidates).  *n_out = 0 when every weight is
+// zero, as the reference returns empty lists then.
+int orc_probability_distribution(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                                 const yaqs_tev_config* cfg, double dt, int32_t cap, double* probs, int32_t* kinds,
+                                 int32_t* sites, int32_t* n_out) {
+  if (!probs || !kinds || !sites || !n_out) return fail(YAQS_E_ARG, "null argument");
+  Problem P;
+  std::string err;
+  yaqs_rng_desc rng{YAQS_RNG_PHILOX, 0, nullptr, 0};
+  if (!load_problem(P, psi0, H, noise, nullptr, 0, cfg, &rng, err)) return fail(YAQS_E_ARG, err);
+  State s = P.psi0;
+  vector<Cand> cands = jump_candidates(P, P.noise, s, dt);
+  double total = 0;
+  for (auto& c : cands) total += c.dp;
+  *n_out = 0;
+  if (total == 0.0) return YAQS_OK;
+  if ((int)cands.size() > cap) return fail(YAQS_E_ARG, "candidate capacity too small");
+  for (size_t i = 0; i < cands.size(); ++i) {
+    const NoiseProc& pr = *cands[i].pr;
+    probs[i] = cands[i].dp / total;
+    kinds[i] = pr.lr ? (pr.pauli_proc ? 2 : 3) : (pr.nsites == 1 ? 0 : 1);
+    sites[2 * i] = pr.s0;
+    sites[2 * i + 1] = pr.nsites == 1 ? pr.s0 : pr.s1;
+  }
+  *n_out = (int32_t)cands.size();
+  return YAQS_OK;
+}
+
+// Plain TDVP evolution without noise, returning <psi0|psi(t)> after n_steps
+// sweeps of the configured mode (single_site_tdvp! / two_site_tdvp!, the
+// eigenstate-phase checks of test/test_Algorithms.jl:37-95).
+int orc_tdvp_overlap(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_tev_config* cfg, int32_t n_steps,
+                     double* overlap) {
+  if (!overlap || n_steps < 0) return fail(YAQS_E_ARG, "bad argument");
+  Problem P;
+  std::string err;
+  yaqs_rng_desc rng{YAQS_RNG_PHILOX, 0, nullptr, 0};
+  if (!load_problem(P, psi0, H, nullptr, nullptr, 0, cfg, &rng, err)) return fail(YAQS_E_ARG, err);
+  Counters c;
+  State s = P.psi0;
+  Sweeper sw(P, c);
+  for (int t = 0; t < n_steps; ++t) sw.sweep(s);
+  cd ov = scalar_product(s, P.psi0);  // scalar_product(mps, mps0) of the reference test
+  overlap[0] = ov.real();
+  overlap[1] = ov.imag();
   return YAQS_OK;
 }
 

@@ -31,7 +31,9 @@ def test_gauge_moves_keep_the_state_and_normalise():
 def test_overlaps_and_expectations_match_dense():
     a, b = _rand_mps(5, 3, 2), _rand_mps(5, 4, 3)
     va, vb = a.to_vec(), b.to_vec()
-    assert abs(T.scalar_product(a, b) - np.vdot(va, vb)) < 1e-12
+    # the reference's convention: sum a * conj(b) = <b|a> (MPS.jl:528-585)
+    assert abs(T.scalar_product(a, b) - np.vdot(vb, va)) < 1e-12
+    assert abs(T.scalar_product(a, b) - np.conj(T.scalar_product(b, a))) < 1e-12
     for s in range(1, 6):
         assert abs(T.local_expect(a, api.X, s) - np.vdot(va, D.site_op(api.X, s, 5) @ va)) < 1e-12
     op = np.kron(api.Z, api.Y)

@@ -99,10 +99,15 @@ def mps_norm(mps: MPS) -> float:
 
 
 def scalar_product(psi: MPS, phi: MPS) -> complex:
-    """<psi|phi> by a left-to-right transfer contraction (MPS.jl:528-585)."""
+    """scalar_product(psi, phi) as the reference computes it (MPS.jl:528-585):
+    a left-to-right transfer contraction of psi with conj(phi), i.e.
+    sum psi * conj(phi) = <phi|psi>.  The reference's docstring reads <a|b>,
+    but its code conjugates the second argument; this follows the code, so
+    scalar_product(psi(t), psi0) of an eigenstate is e^{-iEt} as in
+    test_Algorithms.jl:37-95."""
     E = np.ones((1, 1), dtype=np.complex128)
     for A, B in zip(psi.tensors, phi.tensors):
-        E = np.einsum("ab,apc,bpd->cd", E, A.conj(), B)
+        E = np.einsum("ab,apc,bpd->cd", E, A, B.conj())
     return complex(E[0, 0])
 
 
