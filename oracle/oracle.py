@@ -48,6 +48,8 @@ def lib():
         L.orc_probability_distribution.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.NoiseDesc), P(A.TevConfig),
                                                    C.c_double, C.c_int32, A.DPTR, P(C.c_int32), P(C.c_int32),
                                                    P(C.c_int32)]
+        L.orc_apply_dissipation.argtypes = [P(A.MpsDesc), P(A.MpoDesc), P(A.NoiseDesc), P(A.TevConfig),
+                                            C.c_int32, C.c_int64, A.DPTR, P(C.c_int32), P(C.c_int32)]
         L.orc_svd.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR, A.DPTR]
         L.orc_qr.argtypes = [C.c_int32, C.c_int32, A.DPTR, A.DPTR, A.DPTR]
         L.orc_truncation_rank.argtypes = [C.c_int32, A.DPTR, C.c_double, C.c_int32, C.c_int32]
@@ -148,6 +150,26 @@ def probability_distribution(desc, dt):
               [int(sites[2 * i]) + 1] if kinds[i] == 0 else [int(sites[2 * i]) + 1, int(sites[2 * i + 1]) + 1])
              for i in range(k)]
     return probs[:k], cands
+
+
+def apply_dissipation(desc, full_dt=True):
+    """apply_dissipation on the packed initial state at cfg.dt (or dt/2).
+    Returns (tensors as (left, phys, right) arrays, 1-based centre)."""
+    L = desc.mps.L
+    cap = 4 * L * max(int(desc.mps.chi[i]) for i in range(L + 1)) ** 2 * 2 + 64
+    buf = np.zeros(2 * cap)
+    chi = np.zeros(L + 1, dtype=np.int32)
+    oc = C.c_int32(0)
+    _check(lib().orc_apply_dissipation(C.byref(desc.mps), C.byref(desc.mpo), C.byref(desc.noise),
+                                       C.byref(desc.cfg), int(full_dt), cap, A.dptr(buf),
+                                       chi.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(oc)))
+    z = buf.view(np.complex128)
+    out, o = [], 0
+    for i in range(L):
+        n = chi[i] * 2 * chi[i + 1]
+        out.append(np.reshape(z[o:o + n], (chi[i], 2, chi[i + 1]), order="F").copy())
+        o += n
+    return out, oc.value + 1
 
 
 def svd(M):

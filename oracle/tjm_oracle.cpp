@@ -2153,6 +2153,39 @@ int orc_tdvp_overlap(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const ya
   return YAQS_OK;
 }
 
+// apply_dissipation (Dissipation.jl:37-159) once on the initial state of a
+// problem, with the process rates at cfg->dt (full_dt != 0) or cfg->dt / 2.
+// The resulting tensors are written packed, site after site, in the
+// (left, phys, right) column-major layout; chi_out gets the L+1 bond
+// dimensions and *oc_out the 0-based orthogonality centre.
+int orc_apply_dissipation(const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H, const yaqs_noise_desc* noise,
+                          const yaqs_tev_config* cfg, int32_t full_dt, int64_t capacity, double* tensors_out,
+                          int32_t* chi_out, int32_t* oc_out) {
+  if (!tensors_out || !chi_out || !oc_out) return fail(YAQS_E_ARG, "null argument");
+  Problem P;
+  std::string err;
+  yaqs_rng_desc rng{YAQS_RNG_PHILOX, 0, nullptr, 0};
+  if (!load_problem(P, psi0, H, noise, nullptr, 0, cfg, &rng, err)) return fail(YAQS_E_ARG, err);
+  Counters c;
+  State s = P.psi0;
+  apply_dissipation(P, P.noise, s, full_dt != 0, full_dt ? P.dt : P.dt / 2, c);
+  int64_t n = 0;
+  for (int i = 0; i < s.L; ++i) n += (int64_t)s.t[i].v.size();
+  if (n > capacity) return fail(YAQS_E_ARG, "tensor capacity too small");
+  int64_t o = 0;
+  for (int i = 0; i < s.L; ++i) {
+    chi_out[i] = s.t[i].l;
+    for (const cd& x : s.t[i].v) {
+      tensors_out[2 * o] = x.real();
+      tensors_out[2 * o + 1] = x.imag();
+      ++o;
+    }
+  }
+  chi_out[s.L] = s.t[s.L - 1].r;
+  *oc_out = s.oc;
+  return YAQS_OK;
+}
+
 // Component entry points used by the unit tests.
 int orc_svd(int32_t m, int32_t n, const double* M, double* U, double* S, double* Vt) {
   vector<cd> A((size_t)m * n);

@@ -1,7 +1,8 @@
 """Known answers of the reference's own unit tests, restated against the
 oracle's building blocks: the TDVP eigenstate phase of both sweeps
 (test/test_Algorithms.jl:37-95), calculate_stochastic_factor and
-create_probability_distribution (test/test_StochasticProcess.jl:16-99)."""
+create_probability_distribution (test/test_StochasticProcess.jl:16-99) and
+apply_dissipation (test/test_Dissipation.jl:24-85)."""
 import cmath
 
 import numpy as np
@@ -106,3 +107,86 @@ def test_probability_distribution_order_and_weights(oracle):
     w.append(dt * 0.15 * np.linalg.norm(v) ** 2)  # Pauli long-range: the state norm
     assert np.allclose(probs, np.array(w) / sum(w), atol=1e-13)
     assert abs(probs.sum() - 1.0) < 1e-14
+
+
+def _product_state(L, seed):
+    """A random normalised product state, as test_Dissipation.jl:24-37 builds it."""
+    rng = np.random.default_rng(seed)
+    psi = api.MPS(L)
+    for i in range(L):
+        v = rng.normal(size=2) + 1j * rng.normal(size=2)
+        psi.tensors[i] = (v / np.linalg.norm(v)).reshape(1, 2, 1)
+    return psi
+
+
+def _right_canonical(A):
+    l = A.shape[0]
+    M = np.reshape(A, (l, -1), order="F")
+    return np.allclose(M @ M.conj().T, np.eye(l), atol=1e-12)
+
+
+def _dense_dissipation(psi, nm, dt):
+    """prod exp(-dt gamma L^dag L / 2) in the reference's order: sites from
+    right to left, at each site its 1-site processes, then the 2-site ones
+    that end there (Dissipation.jl:37-159)."""
+    from scipy.linalg import expm
+    from oracle import dense as D
+    L = psi.length
+    v = psi.to_vec()
+    for i in range(L, 0, -1):
+        for p in nm.processes:
+            if len(p.sites) == 1 and p.sites[0] == i:
+                m = np.asarray(p.matrix)
+                v = D.site_op(expm(-0.5 * dt * p.strength * m.conj().T @ m), i, L) @ v
+        for p in nm.processes:
+            if len(p.sites) == 2 and p.sites[1] == i:
+                m = np.asarray(p.matrix)
+                v = D.gate_op(expm(-0.5 * dt * p.strength * m.conj().T @ m), p.sites, L) @ v
+    return v
+
+
+def _to_vec(tensors):
+    st = api.MPS(len(tensors))
+    st.tensors = tensors
+    return st.to_vec()
+
+
+@pytest.mark.parametrize("case", ["one_site", "two_site"])
+def test_dissipation_leaves_the_centre_at_site_1(oracle, case):
+    """test_Dissipation.jl:24-85: lowering + pauli_z on every site, or
+    crosstalk_xx + crosstalk_yy on every bond, of a random product state:
+    afterwards the recorded centre is site 1 (the reference's
+    check_canonical_form returns the recorded centre, MPS.jl:510-512) and
+    the state equals the dense product of the dissipators.  The product
+    state's recorded centre is site 1, so the first shift moves right and
+    the last site, dissipated off-centre, is not re-gauged, in the reference
+    as here."""
+    L, dt = 3, 0.1
+    psi = _product_state(L, 1234 if case == "one_site" else 4321)
+    if case == "one_site":
+        info = [{"name": n, "sites": [i], "strength": 0.1} for i in range(1, L + 1) for n in ("lowering", "pauli_z")]
+    else:
+        info = [{"name": n, "sites": [i, i + 1], "strength": 0.1} for i in range(1, L)
+                for n in ("crosstalk_xx", "crosstalk_yy")]
+    nm = api.NoiseModel(info, L)
+    cfg = api.TimeEvolutionConfig([], 0.1, dt=dt, num_traj=1, max_bond_dim=10, truncation_threshold=1e-10)
+    out, oc = oracle.apply_dissipation(api.Descriptors(psi, api.init_ising(L, 1, 0.5), cfg, nm))
+    assert oc == 1
+    assert np.allclose(_to_vec(out), _dense_dissipation(psi, nm, dt), atol=1e-13)
+
+
+def test_dissipation_non_pauli_two_site_process(oracle):
+    """An entangled start (centre at site 1) and a non-Pauli 2-site process
+    (merged, the 4x4 dissipator applied, split with the relative rule):
+    equal to the dense dissipators, and sites 2..L right-canonical since no
+    process acts on the last site."""
+    L, dt = 5, 0.2
+    psi = api.random_mps(L, 3, seed=21)
+    T.normalize(psi)
+    proc = api.LocalNoiseProcess("custom_lr", [2, 3], 0.4, np.kron(api.LOWERING, api.LOWERING.T))
+    nm = api.NoiseModel([proc, {"name": "lowering", "sites": [4], "strength": 0.3},
+                         {"name": "pauli_x", "sites": [2], "strength": 0.2}], L)
+    cfg = api.TimeEvolutionConfig([], 0.2, dt=dt, num_traj=1, max_bond_dim=16, truncation_threshold=1e-14)
+    out, oc = oracle.apply_dissipation(api.Descriptors(psi, api.init_ising(L, 1, 0.5), cfg, nm))
+    assert oc == 1 and all(_right_canonical(A) for A in out[1:])
+    assert np.allclose(_to_vec(out), _dense_dissipation(psi, nm, dt), atol=1e-12)
