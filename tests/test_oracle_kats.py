@@ -190,3 +190,19 @@ def test_dissipation_non_pauli_two_site_process(oracle):
     out, oc = oracle.apply_dissipation(api.Descriptors(psi, api.init_ising(L, 1, 0.5), cfg, nm))
     assert oc == 1 and all(_right_canonical(A) for A in out[1:])
     assert np.allclose(_to_vec(out), _dense_dissipation(psi, nm, dt), atol=1e-12)
+
+
+@pytest.mark.parametrize("order", [2, 1])
+@pytest.mark.parametrize("sample", [False, True])
+def test_analog_tjm_result_shapes(oracle, order, sample):
+    """test_AnalogTJM.jl:44-100: identity Hamiltonian on |00000>, T = 0.2,
+    dt = 0.1, no noise: one column without sampling, len(0:dt:T) = 3 with
+    it, for analog_tjm_2 and analog_tjm_1; <Z_i> stays 1."""
+    L = 5
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.2, dt=0.1, num_traj=1, max_bond_dim=8, sample_timesteps=sample,
+                                  order=order)
+    tr, chi, _ = oracle.analog_run(api.Descriptors(api.MPS(L, state="zeros"), T.mpo_identity(L), cfg, None))
+    assert tr.shape == (1, L, 3 if sample else 1)
+    # the 2-site split keeps at least two Schmidt values (Algorithms.jl:428-438)
+    assert np.allclose(tr, 1.0, atol=1e-14) and chi.max() <= 2
