@@ -176,3 +176,33 @@ def test_repeated_circuit_sample_plan(oracle, lead, tail):
         cols = [zs(psi)]
     assert tr.shape[2] == n == len(cols)
     assert np.abs(tr[0] - np.array(cols).T).max() < 1e-9 and np.abs(np.array(cols)).max() > 0.1
+
+
+def test_simulation_config_known_answers():
+    """test_SimulationConfigs.jl:28-114: times, defaults, buffer shapes of
+    initialize!, expect on |++++>, and the trajectory mean."""
+    c = api.TimeEvolutionConfig([api.Observable("X", api.X, 1)], 1.0, dt=0.2, sample_timesteps=True, num_traj=50)
+    assert np.allclose(c.times, np.arange(0.0, 1.0 + 1e-12, 0.2), atol=1e-10) and c.num_traj == 50
+    d = api.TimeEvolutionConfig([], 2.0)
+    assert (d.dt, d.sample_timesteps, d.num_traj, d.max_bond_dim, d.truncation_threshold) == \
+        (0.1, True, 1000, 4096, 1e-9)
+    assert abs(d.times[-1] - 2.0) < 1e-10
+    o = api.Observable("X", api.X, 1)
+    T.initialize_observable(o, api.TimeEvolutionConfig([o], 1.0, dt=0.5, sample_timesteps=True, num_traj=10))
+    assert o.results.shape == (3,) and o.trajectories.shape == (10, 3)
+    T.initialize_observable(o, api.TimeEvolutionConfig([o], 1.0, dt=0.25, sample_timesteps=False, num_traj=5))
+    assert o.results.shape == (1,) and o.trajectories.shape == (5, 1)
+    s = T.StrongMeasurementConfig([o], num_traj=4, sample_layers=True)
+    T.initialize_observable(o, s, num_layers=3)
+    assert o.trajectories.shape == (4, 4)
+    psi = api.MPS(4, state="x+")
+    assert abs(T.expect(psi, api.Observable("X", api.X, 1)) - 1.0) < 1e-10
+    assert abs(T.expect(psi, api.Observable("Z", api.Z, 1))) < 1e-10
+    assert abs(T.expect(psi, api.Observable("XX", np.kron(api.X, api.X), [3, 2])) - 1.0) < 1e-10
+    with pytest.raises(ValueError):
+        T.expect(psi, api.Observable("XXX", np.eye(8), [1, 2, 3]))
+    agg = api.TimeEvolutionConfig([o], 1.0, num_traj=2, sample_timesteps=False)
+    T.initialize_observable(o, agg)
+    o.trajectories[0, 0], o.trajectories[1, 0] = 1.0, 0.5
+    T.aggregate_trajectories(agg)
+    assert abs(o.results[0] - 0.75) < 1e-10

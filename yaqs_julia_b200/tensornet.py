@@ -6,9 +6,10 @@ states).  Plain numpy; nothing here runs on the device.
   local expectations, projective shots and bitstring projections.
 * MPO (src/MPO.jl:271-556): canonical form, compression, MPO x MPS,
   <psi|W|psi>, sums, scalar multiples and products.
-* Measurement configs (src/SimulationConfigs.jl:95-137, 168-208):
+* Measurement configs (src/SimulationConfigs.jl:42-56, 95-208):
   MeasurementConfig (shots) and StrongMeasurementConfig (trajectories) with
-  their aggregation.
+  their aggregation; expect, initialize! and aggregate_trajectories! for
+  observables of either config.
 
 Tensors follow the engine's layouts: MPS (left, phys, right), MPO (left,
 out, in, right), column-major reshapes as in the reference; sites 1-based.
@@ -363,7 +364,7 @@ def contract_mpo_mpo(a: MPO, b: MPO) -> MPO:
 
 
 # ---------------------------------------------------------------------------
-# Measurement configs (src/SimulationConfigs.jl:95-137, 168-208)
+# Measurement configs (src/SimulationConfigs.jl:42-56, 95-208)
 # ---------------------------------------------------------------------------
 class MeasurementConfig:
     """MeasurementConfig (shots): per-shot outcome tallies and their sum."""
@@ -403,6 +404,43 @@ class StrongMeasurementConfig:
         self.min_bond_dim = int(min_bond_dim)
         self.truncation_threshold = float(truncation_threshold)
         self.sample_layers = bool(sample_layers)
+
+
+def expect(mps: MPS, obs: Observable) -> float:
+    """expect(psi, obs) (SimulationConfigs.jl:42-56): the real part of
+    local_expect for a 1-site observable, of local_expect_two_site on the
+    sorted pair for a 2-site one; more sites are an error, as there."""
+    if obs.op is None:
+        raise ValueError("expect needs an operator observable")
+    if len(obs.sites) == 1:
+        return float(local_expect(mps, obs.op, obs.sites[0]).real)
+    if len(obs.sites) == 2:
+        s1, s2 = sorted(obs.sites)
+        return float(local_expect_two_site(mps, obs.op, s1, s2).real)
+    raise ValueError("multi-site expectation is not implemented (as in the reference)")
+
+
+def initialize_observable(obs: Observable, config, num_layers: int = 0) -> None:
+    """initialize! (SimulationConfigs.jl:146-160): zeroed buffers for one
+    observable.  A TimeEvolutionConfig gets len(times) columns when it
+    samples every time step, else 1; a StrongMeasurementConfig gets
+    num_layers + 1 columns when it samples layers, else 1."""
+    if isinstance(config, StrongMeasurementConfig):
+        n = num_layers + 1 if config.sample_layers else 1
+    else:
+        n = len(config.times) if config.sample_timesteps else 1
+    obs.trajectories = np.zeros((config.num_traj, n), dtype=np.complex128)
+    obs.results = np.zeros(n)
+
+
+def aggregate_trajectories(config) -> None:
+    """aggregate_trajectories! (SimulationConfigs.jl:168-190) for either
+    config: results = sum of the real parts over trajectories / num_traj,
+    for every observable that has trajectories."""
+    for o in config.observables:
+        tr = getattr(o, "trajectories", None)
+        if tr is not None and np.size(tr):
+            o.results = np.real(np.asarray(tr)).sum(axis=0) / config.num_traj
 
 
 def aggregate_strong(config: StrongMeasurementConfig) -> None:
