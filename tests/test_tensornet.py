@@ -206,3 +206,21 @@ def test_simulation_config_known_answers():
     o.trajectories[0, 0], o.trajectories[1, 0] = 1.0, 0.5
     T.aggregate_trajectories(agg)
     assert abs(o.results[0] - 0.75) < 1e-10
+
+
+def test_mps_random_state_and_padding():
+    """MPS(L; state="random") is normalised with bonds of at most 4
+    (MPS.jl:92-103); pad= and pad_bond_dimension! grow every bond to the
+    target and leave a normalised state that is the padded one up to the
+    noise (MPS.jl:453-494)."""
+    r = api.MPS(6, state="random", seed=3)
+    assert T.check_if_valid_mps(r) and max(r.bond_dims) <= 4 and r.orth_center == 1
+    assert abs(np.linalg.norm(r.to_vec()) - 1) < 1e-12
+    p = api.MPS(5, state="x+", pad=4, seed=1)
+    # padded to 4, then normalize!'s LQ sweep (L -> 2) trims the last bond to its rank
+    assert p.bond_dims == [1, 4, 4, 4, 2, 1]
+    assert abs(np.linalg.norm(p.to_vec()) - 1) < 1e-12
+    plus = api.MPS(5, state="x+").to_vec()
+    assert abs(abs(np.vdot(plus, p.to_vec())) - 1) < 1e-6
+    with pytest.raises(ValueError):
+        api.MPS(3).pad_bond_dimension(0)

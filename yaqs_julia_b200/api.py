@@ -190,7 +190,12 @@ class MPS:
     """Matrix product state; tensors are (left, phys, right) arrays."""
 
     def __init__(self, length: int, tensors=None, physical_dimensions=None, state: str = "zeros",
-                 basis_string: str | None = None):
+                 basis_string: str | None = None, pad: int | None = None, seed: int | None = None):
+        """MPS(length; tensors, physical_dimensions, state, pad, basis_string)
+        (MPS.jl:52-144).  state "random" draws complex Gaussian tensors with
+        interior bonds 4 and normalises them (MPS.jl:92-103; ``seed`` seeds
+        the draws, which the reference takes from the global RNG); ``pad``
+        grows every bond to that dimension afterwards (pad_bond_dimension!)."""
         self.length = int(length)
         if physical_dimensions not in (None, 2) and not (
                 isinstance(physical_dimensions, (list, tuple)) and set(physical_dimensions) == {2}):
@@ -200,6 +205,20 @@ class MPS:
         if tensors is not None:
             assert len(tensors) == self.length
             self.tensors = [np.asfortranarray(np.asarray(t, dtype=np.complex128)) for t in tensors]
+            return
+        if state == "random":
+            rng = np.random.default_rng(seed)
+            ts = []
+            for i in range(1, self.length + 1):
+                l = 1 if i == 1 else 4
+                r = 1 if i == self.length else 4
+                z = (rng.standard_normal((l, 2, r)) + 1j * rng.standard_normal((l, 2, r))) / math.sqrt(2)
+                ts.append(np.asfortranarray(z))
+            self.tensors = ts
+            from .tensornet import normalize
+            normalize(self)
+            if pad is not None:
+                self.pad_bond_dimension(pad, seed=seed or 0)
             return
         ts = []
         for i in range(1, self.length + 1):  # MPS.jl:105-134
@@ -227,16 +246,22 @@ class MPS:
                 raise ValueError(f"Unknown state: {state}")
             ts.append(np.asfortranarray(v.reshape(1, 2, 1)))
         self.tensors = ts
+        if pad is not None:
+            self.pad_bond_dimension(pad, seed=seed or 0)
 
     @property
     def bond_dims(self):
         return [1] + [t.shape[2] for t in self.tensors]
 
     def pad_bond_dimension(self, target_dim: int, noise_scale: float = 1e-8, seed: int = 0):
-        """pad_bond_dimension! (MPS.jl:453-494): grow every bond below
-        target_dim to target_dim, filling the new slices with complex noise of
-        amplitude noise_scale (seeded here; the reference draws from the global
-        RNG).  The engine normalises the state before it evolves it."""
+        """pad_bond_dimension! (MPS.jl:453-494): normalize!, then grow every
+        bond below target_dim to target_dim, filling the new slices with
+        complex noise of amplitude noise_scale (seeded here; the reference
+        draws from the global RNG), then normalize! again."""
+        from .tensornet import normalize
+        if target_dim <= 0:
+            raise ValueError("target_dim must be positive")
+        normalize(self)
         rng = np.random.default_rng(seed)
         for i in range(self.length - 1):
             A, B = self.tensors[i], self.tensors[i + 1]
@@ -253,6 +278,7 @@ class MPS:
                                     1j * rng.standard_normal((target_dim - r, B.shape[1], B.shape[2])))
             self.tensors[i] = np.asfortranarray(nA)
             self.tensors[i + 1] = np.asfortranarray(nB)
+        normalize(self)
         return self
 
     def to_vec(self) -> np.ndarray:
