@@ -102,3 +102,40 @@ def test_argument_checks():
     d.rng.uniforms = None
     with pytest.raises(EngineError, match="injected"):
         api.run_descriptors(d)
+
+
+@pytest.mark.parametrize("order", [2, 1])
+@pytest.mark.parametrize("sample", [False, True])
+def test_identity_hamiltonian_result_shapes(oracle, order, sample):
+    """test_AnalogTJM.jl:44-100 through the C-ABI: identity MPO (bond width
+    1), T = 0.2, dt = 0.1: one column without sampling, three with it."""
+    from yaqs_julia_b200 import tensornet as T
+    L = 5
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.2, dt=0.1, num_traj=1, max_bond_dim=8, sample_timesteps=sample,
+                                  order=order)
+    d = api.Descriptors(api.MPS(L, state="zeros"), T.mpo_identity(L), cfg, None)
+    got = api.run_descriptors(d)
+    ref, _, _ = oracle.analog_run(d)
+    assert got.trajectories.shape == ref.shape == (1, L, 3 if sample else 1)
+    assert np.abs(got.trajectories - ref).max() <= 1e-12 and np.allclose(got.trajectories, 1.0, atol=1e-12)
+
+
+def test_simulator_run_without_sampling(oracle):
+    """test_Simulator.jl:34-64: Simulator.run with lowering + pauli_z at 0.1,
+    10 trajectories, max_bond_dim 4, threshold 1e-6, order 2, no sampling:
+    one result per observable and one row per trajectory, equal to the
+    oracle on the same Philox draws."""
+    from yaqs_julia_b200 import tensornet as T
+    L = 5
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=0.1, num_traj=10, max_bond_dim=4, truncation_threshold=1e-6,
+                                  order=2, sample_timesteps=False)
+    info = [{"name": n, "sites": [i], "strength": 0.1} for n in ("lowering", "pauli_z") for i in range(1, L + 1)]
+    nm = api.NoiseModel(info, L)
+    res = api.run(api.MPS(L, state="zeros"), T.mpo_identity(L), cfg, nm, seed=3)
+    assert res.trajectories.shape == (10, L, 1)
+    for o in cfg.observables:
+        assert len(o.results) == 1 and o.trajectories.shape[0] == 10
+    ref, _, _ = oracle.analog_run(api.Descriptors(api.MPS(L, state="zeros"), T.mpo_identity(L), cfg, nm, seed=3))
+    assert np.abs(res.trajectories - ref).max() <= 1e-10
