@@ -224,3 +224,47 @@ def test_mps_random_state_and_padding():
     assert abs(abs(np.vdot(plus, p.to_vec())) - 1) < 1e-6
     with pytest.raises(ValueError):
         api.MPS(3).pad_bond_dimension(0)
+
+
+def _randc(rng, *dims):
+    return rng.normal(size=dims) + 1j * rng.normal(size=dims)
+
+
+def test_decompositions_known_answers():
+    """test_Decompositions.jl:18-117: right_qr / left_qr shapes,
+    reconstruction and isometry; two_site_svd reconstruction, truncation by
+    a large threshold and by max_bond_dim."""
+    rng = np.random.default_rng(9)
+    X = _randc(rng, 4, 2, 5)
+    Q, R = T.right_qr(X)
+    nb = Q.shape[2]
+    assert Q.shape == (4, 2, nb) and R.shape == (nb, 5)
+    assert np.allclose(np.einsum("lpk,kr->lpr", Q, R), X, atol=1e-12)
+    Qm = np.reshape(Q, (8, nb), order="F")
+    assert np.allclose(Qm.conj().T @ Qm, np.eye(nb), atol=1e-12)
+    Y = _randc(rng, 5, 2, 4)
+    Lm, Q2 = T.left_qr(Y)
+    nb = Q2.shape[0]
+    assert Lm.shape == (5, nb) and Q2.shape == (nb, 2, 4)
+    assert np.allclose(np.einsum("lk,kpr->lpr", Lm, Q2), Y, atol=1e-12)
+    Qm = np.reshape(Q2, (nb, 8), order="F")
+    assert np.allclose(Qm @ Qm.conj().T, np.eye(nb), atol=1e-12)
+    A, B = _randc(rng, 3, 2, 4), _randc(rng, 4, 2, 5)
+    An, Bn = T.two_site_svd(A, B, 1e-15)
+    assert np.allclose(np.einsum("lak,kbr->labr", A, B), np.einsum("lak,kbr->labr", An, Bn), atol=1e-11)
+    At, _ = T.two_site_svd(A, B, 2.0)
+    assert At.shape[2] < 6
+    Al, Bl = T.two_site_svd(A, B, 1e-15, max_bond_dim=2)
+    assert Al.shape[2] == 2 and Bl.shape[0] == 2
+
+
+def test_two_site_svd_rank_rule_matches_the_oracle(oracle):
+    """The kept count is the oracle's absolute rule (rule 0) on the same
+    singular values, for thresholds across the spectrum."""
+    rng = np.random.default_rng(2)
+    A, B = _randc(rng, 4, 2, 6), _randc(rng, 6, 2, 4)
+    S = np.linalg.svd(np.reshape(A, (8, 6), order="F") @ np.reshape(B, (6, 8), order="F"), compute_uv=False)
+    for thr in (1e-15, 1e-3, 1.0, 10.0, 1e3, 1e6):
+        for chi in (None, 3):
+            An, _ = T.two_site_svd(A, B, thr, max_bond_dim=chi)
+            assert An.shape[2] == oracle.truncation_rank(S, thr, chi or 1 << 30, 0), (thr, chi)

@@ -2,6 +2,7 @@
 engine (building and compressing Hamiltonians, inspecting and sampling
 states).  Plain numpy; nothing here runs on the device.
 
+* Decompositions (src/Decompositions.jl): right_qr, left_qr, two_site_svd.
 * MPS (src/MPS.jl): gauge moves, normalisation, truncation, overlaps,
   local expectations, projective shots and bitstring projections.
 * MPO (src/MPO.jl:271-556): canonical form, compression, MPO x MPS,
@@ -39,6 +40,48 @@ def _lq(M):
 
 def _f(a, shape):
     return np.reshape(a, shape, order="F")
+
+
+def right_qr(tensor):
+    """right_qr (Decompositions.jl:18-33): thin QR of the (left*phys, right)
+    matricisation; returns Q as (left, phys, k) and R as (k, right)."""
+    l, p, r = tensor.shape
+    Q, R = _qr(_f(np.asarray(tensor, dtype=np.complex128), (l * p, r)))
+    return _f(Q, (l, p, Q.shape[1])), R
+
+
+def left_qr(tensor):
+    """left_qr (Decompositions.jl:35-58): thin LQ of the (left, phys*right)
+    matricisation; returns L as (left, k) and Q as (k, phys, right)."""
+    l, p, r = tensor.shape
+    Lm, Q = _lq(_f(np.asarray(tensor, dtype=np.complex128), (l, p * r)))
+    return Lm, _f(Q, (Q.shape[0], p, r))
+
+
+def two_site_svd(A, B, threshold: float, max_bond_dim: int | None = None):
+    """two_site_svd (Decompositions.jl:85-164): merge A (l, pa, k) and
+    B (k, pb, r), SVD the (l*pa, pb*r) matrix, keep by the absolute rule
+    (discard from the smallest while the discarded weight stays below
+    threshold, keep the crossing value, at least 2), at most max_bond_dim;
+    returns U as (l, pa, keep) and S*Vt as (keep, pb, r).  The kept count is
+    also capped at the number of singular values, where the reference would
+    index past them."""
+    la, pa, ra = A.shape
+    lb, pb, rb = B.shape
+    if ra != lb:
+        raise ValueError("bond dimensions of A and B differ")
+    theta = _f(A, (la * pa, ra)) @ _f(B, (lb, pb * rb))
+    U, S, Vt = np.linalg.svd(theta, full_matrices=False)
+    keep, disc = len(S), 0.0
+    for k in range(len(S), 0, -1):
+        disc += S[k - 1] ** 2
+        if disc >= threshold:
+            keep = max(k, 2)
+            break
+    if max_bond_dim is not None:
+        keep = min(keep, max_bond_dim)
+    keep = max(min(keep, len(S)), 1)
+    return _f(U[:, :keep], (la, pa, keep)), _f(S[:keep, None] * Vt[:keep], (keep, pb, rb))
 
 
 # ---------------------------------------------------------------------------
