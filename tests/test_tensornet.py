@@ -268,3 +268,36 @@ def test_two_site_svd_rank_rule_matches_the_oracle(oracle):
         for chi in (None, 3):
             An, _ = T.two_site_svd(A, B, thr, max_bond_dim=chi)
             assert An.shape[2] == oracle.truncation_rank(S, thr, chi or 1 << 30, 0), (thr, chi)
+
+
+def test_mps_known_answers():
+    """test_MPS.jl:97-214: scalar products of random / orthogonal states,
+    local expectations, all-site expectations, shots on basis states, the
+    recorded centre after a shift and normalize!, truncate! to bond 2."""
+    rng = np.random.default_rng(4)
+    r = api.MPS(3, state="random", seed=5)
+    assert abs(T.scalar_product(r, r) - 1) < 1e-12
+    assert abs(T.scalar_product(api.MPS(3, state="zeros"), api.MPS(3, state="ones"))) < 1e-12
+    z = api.MPS(2, state="zeros")
+    assert abs(T.local_expect(z, api.Z, 1) - 1) < 1e-12 and abs(T.local_expect(z, api.Z, 2) - 1) < 1e-12
+    assert abs(T.local_expect(api.MPS(2, state="x+"), api.X, 1) - 1) < 1e-12
+    r4 = api.MPS(4, state="random", seed=6)
+    ind = [T.local_expect(r4, api.Z, i) for i in range(1, 5)]
+    assert np.allclose(ind, T.evaluate_all_local_expectations(r4, [api.Z] * 4), atol=1e-12)
+    assert T.measure_single_shot(api.MPS(3, state="zeros")) == 0
+    ones = api.MPS(3, state="ones")
+    assert T.measure_single_shot(ones) == 7
+    assert T.measure_shots(ones, 100, rng=rng) == {7: 100}
+    assert sum(T.measure_shots(api.MPS(4, state="x+"), 100, rng=rng).values()) == 100
+    m = _rand_mps(4, 4, 8)
+    T.shift_orthogonality_center(m, 2)
+    assert T.check_canonical_form(m) == [2]
+    T.normalize(m)
+    assert m.orth_center == 1 and abs(T.scalar_product(m, m) - 1) < 1e-12
+    big = api.MPS(6, tensors=[_randc(rng, 1, 2, 8)] + [_randc(rng, 8, 2, 8) for _ in range(4)] +
+                  [_randc(rng, 8, 2, 1)])
+    T.normalize(big)
+    T.truncate(big, max_bond_dim=2)
+    assert max(max(t.shape[0], t.shape[2]) for t in big.tensors) <= 2
+    T.normalize(big)
+    assert abs(T.scalar_product(big, big) - 1) < 1e-10

@@ -92,6 +92,12 @@ def check_if_valid_mps(mps: MPS) -> bool:
     return all(mps.tensors[i].shape[2] == mps.tensors[i + 1].shape[0] for i in range(mps.length - 1))
 
 
+def check_canonical_form(mps: MPS) -> list[int]:
+    """check_canonical_form (MPS.jl:510-512): the recorded centre, as a
+    one-element list (the reference does not inspect the tensors)."""
+    return [mps.orth_center]
+
+
 def write_max_bond_dim(mps: MPS) -> int:
     """write_max_bond_dim (MPS.jl:168-174)."""
     return max(t.shape[2] for t in mps.tensors)
