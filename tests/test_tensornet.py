@@ -301,3 +301,34 @@ def test_mps_known_answers():
     assert max(max(t.shape[0], t.shape[2]) for t in big.tensors) <= 2
     T.normalize(big)
     assert abs(T.scalar_product(big, big) - 1) < 1e-10
+
+
+def test_mpo_known_answers():
+    """test_MPO.jl:10-150: identity / zero MPOs, orthogonalize! keeps
+    <psi|W|psi> and records the centre, truncate! caps the bonds and leaves
+    the centre at L, H1 + H2 = init_ising(L, 1, 1) and compresses, c * W,
+    X * X = I."""
+    rng = np.random.default_rng(12)
+    I4 = T.mpo_identity(4)
+    assert I4.tensors[0][0, 0, 0, 0] == 1 and I4.tensors[0][0, 1, 1, 0] == 1 and I4.tensors[0][0, 0, 1, 0] == 0
+    assert np.abs(T.mpo_zero(4).tensors[0]).sum() == 0 and I4.orth_center == 0
+    W = api.MPO(4, [_randc(rng, 1, 2, 2, 4)] + [_randc(rng, 4, 2, 2, 4) for _ in range(2)] + [_randc(rng, 4, 2, 2, 1)])
+    psi = api.MPS(4, state="random", seed=3)
+    v0 = T.expect_mpo(W, psi)
+    T.orthogonalize(W, 1)
+    assert W.orth_center == 1 and abs(T.expect_mpo(W, psi) - v0) < 1e-10
+    T.mpo_truncate(W, max_bond_dim=2)
+    assert W.orth_center == 4 and max(max(t.shape[0], t.shape[3]) for t in W.tensors) <= 2
+    assert np.isfinite(T.expect_mpo(W, psi))
+    H1, H2 = api.init_ising(3, 1.0, 0.0), api.init_ising(3, 0.0, 1.0)
+    Hs = H1 + H2
+    p3 = api.MPS(3, state="random", seed=4)
+    assert abs(T.expect_mpo(Hs, p3) - T.expect_mpo(api.init_ising(3, 1.0, 1.0), p3)) < 1e-10
+    T.orthogonalize(Hs, 1)
+    T.mpo_truncate(Hs, threshold=1e-10)
+    assert Hs.tensors[1].shape[3] <= 5
+    assert abs(T.expect_mpo(2.5 * H1, p3) - 2.5 * T.expect_mpo(H1, p3)) < 1e-12
+    assert abs(T.expect_mpo(H1 * 2.5, p3) - 2.5 * T.expect_mpo(H1, p3)) < 1e-12
+    X = api.MPO(2, [api.X.reshape(1, 2, 2, 1)] * 2)
+    XX = T.contract_mpo_mpo(X, X)
+    assert abs(T.expect_mpo(XX, api.MPS(2)) - 1) < 1e-10 and XX.tensors[0].shape[3] == 1

@@ -300,10 +300,26 @@ class MPO:
         self.length = int(length)
         self.tensors = [np.asfortranarray(np.asarray(t, dtype=np.complex128)) for t in tensors]
         self.phys_dims = [2] * self.length
+        self.orth_center = 0  # unknown until orthogonalize! (MPO.jl:44)
 
     @property
     def bond_dims(self):
         return [1] + [t.shape[3] for t in self.tensors]
+
+    def __add__(self, other: "MPO") -> "MPO":
+        """a + b (MPO.jl:486-521): the block-diagonal sum."""
+        from .tensornet import mpo_add
+        return mpo_add(self, other)
+
+    def __mul__(self, c) -> "MPO":
+        """mpo * c = c * mpo (MPO.jl:523-529): the first tensor scaled."""
+        import numbers
+        if not isinstance(c, numbers.Number):
+            return NotImplemented
+        from .tensornet import mpo_scale
+        return mpo_scale(c, self)
+
+    __rmul__ = __mul__
 
     def to_matrix(self) -> np.ndarray:
         """Dense operator in the to_vec basis (site 1 fastest); tests only."""

@@ -396,7 +396,9 @@ def mpo_scale(c: complex, mpo: MPO) -> MPO:
     """c * mpo: the first tensor scaled (MPO.jl:523-529)."""
     ts = [t.copy() for t in mpo.tensors]
     ts[0] = c * ts[0]
-    return MPO(mpo.length, ts)
+    out = MPO(mpo.length, ts)
+    out.orth_center = mpo.orth_center
+    return out
 
 
 def contract_mpo_mpo(a: MPO, b: MPO) -> MPO:
