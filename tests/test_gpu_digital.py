@@ -330,3 +330,26 @@ def test_checkpoint_restore_digital():
     res = sess.finish()
     assert np.array_equal(res.trajectories, straight.trajectories)
     assert np.array_equal(res.max_bond, straight.max_bond)
+
+
+def test_ising_circuit_bitflip_run(oracle):
+    """test_Ising_Digital_TJM.jl:11-58 through run(): create_ising_circuit
+    with custom-named bit-flip processes, a TimeEvolutionConfig of 51 time
+    points (T = 50, dt = 1) holding the 11 samples, 200 trajectories; the
+    results equal the oracle on the same draws and keep the reference's
+    buffer length."""
+    from yaqs_julia_b200 import circuits as CL
+    L, steps, nt = 6, 10, 200
+    c = CL.create_ising_circuit(L, 1.0, 1.0, 0.1, steps)
+    nm = api.NoiseModel([{"name": f"bitflip_{i}", "sites": [i], "strength": 0.05, "matrix": api.X}
+                         for i in range(1, L + 1)], L)
+    obs = [api.Observable(f"Z_{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 50.0, dt=1.0, num_traj=nt, sample_timesteps=True)
+    res = api.run(api.MPS(L, state="zeros"), c, cfg, nm, seed=4)
+    z1 = obs[0].results
+    assert len(z1) == 51 > steps and abs(z1[0] - 1.0) < 1e-12
+    assert np.all(np.abs(z1) <= 1 + 1e-9) and np.all(z1[steps + 1:] == 0)
+    d = api.CircuitDescriptors(api.MPS(L, state="zeros"), c, cfg, nm, seed=4,
+                               **api._methods(c, None, None))
+    ref, _, _ = oracle.digital_run(d)
+    assert np.abs(res.trajectories - ref).max() <= 1e-10
