@@ -332,3 +332,20 @@ def test_mpo_known_answers():
     X = api.MPO(2, [api.X.reshape(1, 2, 2, 1)] * 2)
     XX = T.contract_mpo_mpo(X, X)
     assert abs(T.expect_mpo(XX, api.MPS(2)) - 1) < 1e-10 and XX.tensors[0].shape[3] == 1
+
+
+def test_available_cpus(monkeypatch):
+    """test_Simulator.jl:23-32: the host's CPU count, or SLURM_CPUS_ON_NODE."""
+    import os
+    monkeypatch.delenv("SLURM_CPUS_ON_NODE", raising=False)
+    assert api.available_cpus() == os.cpu_count()
+    monkeypatch.setenv("SLURM_CPUS_ON_NODE", "8")
+    assert api.available_cpus() == 8
+
+
+def test_run_rejects_other_operators():
+    """test_Simulator.jl:91-96: an operator that is neither an MPO nor a
+    circuit is an error before anything runs (and parallel= is accepted)."""
+    cfg = api.TimeEvolutionConfig([], 1.0)
+    with pytest.raises(TypeError):
+        api.run(api.MPS(2), "InvalidOperator", cfg, parallel=False)

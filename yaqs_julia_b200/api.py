@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 
 import numpy as np
 
@@ -1332,8 +1333,16 @@ def _methods(circ, local_method, long_range_method):
     return {"local_method": local_method or default, "long_range_method": long_range_method or default}
 
 
+def available_cpus() -> int:
+    """available_cpus (Simulator.jl:14-20): SLURM_CPUS_ON_NODE when set, else
+    the host's logical CPU count."""
+    if "SLURM_CPUS_ON_NODE" in os.environ:
+        return int(os.environ["SLURM_CPUS_ON_NODE"])
+    return os.cpu_count() or 1
+
+
 def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_model: NoiseModel | None = None,
-        *, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12,
+        *, parallel: bool = True, seed: int = 0, uniforms: np.ndarray | None = None, krylov_exit_tol: float = 1e-12,
         precision: str = "fp64", tdvp: str = "2site", local_method: str | None = None,
         long_range_method: str | None = None, ctx=None) -> RunResult:
     """Simulator.run (Simulator.jl:127-141) for an MPO (analog TJM) or a
@@ -1350,7 +1359,9 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
     max_bond_dim, the Python lineage's local_dynamic_tdvp).  For circuits,
     ``local_method`` / ``long_range_method`` ("tebd" or "tdvp") are the
     TJMOptions; left unset they follow the reference's default (see
-    _methods).  A RepeatedDigitalCircuit runs as its flattened circuit."""
+    _methods).  A RepeatedDigitalCircuit runs as its flattened circuit.
+    ``parallel`` is accepted for the reference's signature; every trajectory
+    of the run advances together on the device either way."""
     prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
     if isinstance(operator, RepeatedDigitalCircuit):
         operator = operator.flatten()
