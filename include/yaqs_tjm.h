@@ -195,6 +195,17 @@ const char* yaqs_last_error(const yaqs_ctx* ctx);
 const char* yaqs_version(void);
 
 /*
+ * Relative Frobenius norm ||H - H^dag|| / ||H|| of an MPO, computed on the
+ * host (no device work, no context).  Stands in for the reference's
+ * _ishermitian_check (src/Algorithms.jl:120-137), which decides between
+ * Lanczos and Arnoldi in the :auto Krylov mode; this engine only runs
+ * Lanczos, so yaqs_analog_run / _begin refuse a Hamiltonian whose defect
+ * exceeds 1e-5 with YAQS_E_UNSUPPORTED.  The estimate is a difference of
+ * squared norms: values below about 1e-7 are rounding.
+ */
+int yaqs_mpo_hermitian_defect(const yaqs_mpo_desc* H, double* defect);
+
+/*
  * Analog TJM run: replaces the trajectory loop of Simulator._run_analog
  * (Simulator.jl:22-69) with every trajectory of the run advancing together
  * on one GPU; each trajectory follows analog_tjm_2 (AnalogTJM.jl:104-137)

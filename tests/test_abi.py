@@ -74,3 +74,47 @@ def test_descriptor_validation_host_side():
 
 
 import numpy as np  # noqa: E402
+
+
+def _dagger(W):
+    from yaqs_julia_b200 import api
+    return api.MPO(W.length, [np.conj(np.transpose(t, (0, 2, 1, 3))) for t in W.tensors])
+
+
+def test_hamiltonian_hermiticity_check():
+    """yaqs_mpo_hermitian_defect (host arithmetic, no device) stands in for
+    the reference's _ishermitian_check (Algorithms.jl:120-137): zero for the
+    library Hamiltonians, their sums and multiples and a Hermitian random
+    MPO; the true relative defect for non-Hermitian ones, which runs refuse."""
+    from yaqs_julia_b200 import api
+    from yaqs_julia_b200 import tensornet as T
+    rng = np.random.default_rng(3)
+    herm = [api.init_ising(30, 1.0, 0.5), api.init_ising(6, [0.6, 1.2, 0.8, 1.4, 0.9], [0.7, 1.3, 0.5, 1.1, 0.8, 1.2]),
+            api.init_general_hamiltonian(12, 0.3, -1.2, 0.7, 0.4, 0.9, -0.2), T.mpo_identity(5), T.mpo_zero(4),
+            api.init_ising(8, 1, 0) + api.init_ising(8, 0, 1), 2.5 * api.init_general_hamiltonian(256, 1, 1, 1, 0, 0, 0.3)]
+    W = api.MPO(5, [rng.normal(size=(1 if i == 0 else 3, 2, 2, 1 if i == 4 else 3)) +
+                    1j * rng.normal(size=(1 if i == 0 else 3, 2, 2, 1 if i == 4 else 3)) for i in range(5)])
+    herm.append(W + _dagger(W))
+    for H in herm:
+        assert api.hermitian_defect(H) < 1e-7
+    # non-Hermitian: i H, a random MPO, a small anti-Hermitian admixture; dense check of the value
+    for H in (1j * api.init_ising(6, 1, 0.5), W, (1 + 1e-3j) * (W + _dagger(W))):
+        M = H.to_matrix()
+        ref = np.linalg.norm(M - M.conj().T) / np.linalg.norm(M)
+        assert abs(api.hermitian_defect(H) - ref) <= 1e-6 * max(ref, 1.0) + 1e-7
+        assert ref > 1e-5
+
+
+def test_descriptors_refuse_non_hermitian_hamiltonians():
+    """The host check (numpy) equals the library's, and Descriptors refuses a
+    Hamiltonian above the tolerance before anything reaches the device."""
+    from yaqs_julia_b200 import api
+    rng = np.random.default_rng(5)
+    W = api.MPO(4, [rng.normal(size=(1 if i == 0 else 2, 2, 2, 1 if i == 3 else 2)) +
+                    1j * rng.normal(size=(1 if i == 0 else 2, 2, 2, 1 if i == 3 else 2)) for i in range(4)])
+    for H in (api.init_ising(10, 1, 0.5), W + _dagger(W), W, 1j * api.init_ising(4, 1, 0.2)):
+        assert abs(api.mpo_antihermitian_part(H) - api.hermitian_defect(H)) < 1e-7
+    cfg = api.TimeEvolutionConfig([api.Observable("Z1", api.Z, 1)], 0.2, dt=0.1, num_traj=1, max_bond_dim=4)
+    with pytest.raises(ValueError, match="not Hermitian"):
+        api.Descriptors(api.MPS(4), W, cfg, None)
+    api.Descriptors(api.MPS(4), W + _dagger(W), cfg, None)

@@ -50,6 +50,7 @@ def lib():
         L.yaqs_run_seek.argtypes = [C.c_void_p, C.c_int32]
         L.yaqs_analog_finish.argtypes = [C.c_void_p, A.DPTR, A.DPTR, P(C.c_int32), P(A.RunStats)]
         L.yaqs_digital_plan.argtypes = [P(A.GateDesc), C.c_int32, P(C.c_int32), P(C.c_int32)]
+        L.yaqs_mpo_hermitian_defect.argtypes = [P(A.MpoDesc), P(C.c_double)]
         L.yaqs_digital_run.argtypes = [C.c_void_p, P(A.MpsDesc), P(A.GateDesc), C.c_int32, P(A.NoiseDesc),
                                        P(A.ObsDesc), C.c_int32, P(A.CircuitConfig), P(A.RngDesc), A.DPTR, A.DPTR,
                                        P(C.c_int32), P(A.RunStats)]

@@ -771,6 +771,10 @@ class Descriptors:
         wp = (A.DPTR * L)(*[A.dptr(b) for b in wb])
         self._keep += [w, wb, wp]
         self.mpo = A.MpoDesc(L, w.ctypes.data_as(C.POINTER(C.c_int32)), wp)
+        defect = mpo_antihermitian_part(H)
+        if not defect <= HERMITIAN_TOL:
+            raise ValueError(f"the Hamiltonian MPO is not Hermitian (relative anti-Hermitian part {defect:.3g}): "
+                             "the engine runs Lanczos, where the reference's :auto Krylov mode switches to Arnoldi")
         # noise
         procs = noise_model.processes if noise_model is not None else []
         arr = (A.NoiseProc * max(1, len(procs)))()
@@ -1096,6 +1100,44 @@ def run_circuit_descriptors(desc: CircuitDescriptors, ctx=None) -> RunResult:
                                         A.dptr(traj), A.dptr(mean), chi.ctypes.data_as(C.POINTER(C.c_int32)),
                                         C.byref(st)))
     return RunResult(traj[:, :nobs, :], mean[:nobs, :], chi, st.as_dict())
+
+
+HERMITIAN_TOL = 1e-5  # largest relative anti-Hermitian part a run accepts
+
+
+def mpo_antihermitian_part(H: MPO) -> float:
+    """||H - H^dag||_F / ||H||_F by the transfer contractions the library uses
+    (tr(H^dag H) and tr(H H) over two copies' bonds), in numpy: the host-side
+    form of the check, so descriptors fail early without the library.
+    Values below about 1e-7 are rounding."""
+    e1 = np.ones((1, 1), dtype=np.complex128)
+    e2 = np.ones((1, 1), dtype=np.complex128)
+    for t in H.tensors:
+        e1 = np.einsum("ab,aoir,bois->rs", e1, t.conj(), t)
+        e2 = np.einsum("ab,aoir,bios->rs", e2, t, t)
+    n1 = e1[0, 0].real
+    if n1 == 0.0:
+        return 0.0
+    q = (2.0 * n1 - 2.0 * e2[0, 0].real) / n1
+    return math.sqrt(q) if q > 0.0 else (0.0 if q == q else q)
+
+
+def hermitian_defect(H: MPO) -> float:
+    """||H - H^dag||_F / ||H||_F as yaqs_mpo_hermitian_defect computes it (host
+    arithmetic in the library, no device): the check that stands in for the
+    reference's _ishermitian_check (Algorithms.jl:120-137).  Runs refuse a
+    Hamiltonian above 1e-5; values below about 1e-7 are rounding."""
+    from . import _lib
+    L = _lib.lib()
+    w = np.array([1] + [t.shape[3] for t in H.tensors], dtype=np.int32)
+    wb = [_c64(t) for t in H.tensors]
+    wp = (A.DPTR * H.length)(*[A.dptr(b) for b in wb])
+    desc = A.MpoDesc(H.length, w.ctypes.data_as(C.POINTER(C.c_int32)), wp)
+    out = C.c_double(0.0)
+    st = L.yaqs_mpo_hermitian_defect(C.byref(desc), C.byref(out))
+    if st != 0:
+        raise _lib.EngineError(st, L.yaqs_last_error(None).decode())
+    return out.value
 
 
 def digital_plan(circ: DigitalCircuit) -> tuple[int, int]:

@@ -822,6 +822,50 @@ static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, 
 
 // Uploads the launch list (time index or layer per position) and marks no
 // position done for any trajectory.
+// ||W - W^dag||_F^2 / ||W||_F^2 of an MPO (host arithmetic only), formed as
+// (2 tr(W^dag W) - 2 Re tr(W W)) / tr(W^dag W) from two transfer
+// contractions over the bonds of two copies.  Being a difference of squared
+// norms it carries rounding of about 1e-15 relative, so only values well
+// above that mean anything.  0 for the zero operator; NaN for non-finite
+// tensors.
+static double mpo_antihermitian_sq(const yaqs_mpo_desc* H) {
+  std::vector<hcd> E1(1, 1.0), E2(1, 1.0);
+  int wl = 1;
+  for (int site = 0; site < H->L; ++site) {
+    const int wr = H->w[site + 1];
+    const double* T = H->tensors[site];
+    auto at = [&](int a, int o, int i, int r) {
+      return cload(T, (size_t)a + (size_t)wl * (o + 2 * (i + 2 * (size_t)r)));
+    };
+    std::vector<hcd> N1((size_t)wr * wr, 0.0), N2((size_t)wr * wr, 0.0);
+    for (int b = 0; b < wl; ++b)
+      for (int a = 0; a < wl; ++a) {
+        const hcd e1 = E1[a + (size_t)wl * b], e2 = E2[a + (size_t)wl * b];
+        for (int rb = 0; rb < wr; ++rb)
+          for (int ra = 0; ra < wr; ++ra) {
+            hcd s1 = 0.0, s2 = 0.0;
+            for (int o = 0; o < 2; ++o)
+              for (int i = 0; i < 2; ++i) {
+                s1 += std::conj(at(a, o, i, ra)) * at(b, o, i, rb);  // tr(W^dag W)
+                s2 += at(a, o, i, ra) * at(b, i, o, rb);             // tr(W W)
+              }
+            N1[ra + (size_t)wr * rb] += e1 * s1;
+            N2[ra + (size_t)wr * rb] += e2 * s2;
+          }
+      }
+    E1.swap(N1);
+    E2.swap(N2);
+    wl = wr;
+  }
+  const double n1 = E1[0].real();
+  if (n1 == 0.0) return 0.0;
+  return (2.0 * n1 - 2.0 * E2[0].real()) / n1;
+}
+
+// Largest squared relative anti-Hermitian part accepted for a Hamiltonian:
+// a relative defect of 1e-5, far above the rounding of the estimate.
+constexpr double HERMITIAN_TOL_SQ = 1e-10;
+
 static int upload_positions(yaqs_ctx* ctx, yaqs_run* run) {
   int *d_jlist, *d_done;
   const size_t np = run->launches.size();
@@ -837,6 +881,18 @@ static int upload_positions(yaqs_ctx* ctx, yaqs_run* run) {
 extern "C" {
 
 const char* yaqs_version(void) { return "yaqs-b200 0.1.0 (sm_100a, FP64 trajectory engine)"; }
+
+int yaqs_mpo_hermitian_defect(const yaqs_mpo_desc* H, double* defect) {
+  if (!H || !defect || H->L < 1 || !H->w || !H->tensors) return set_err(nullptr, YAQS_E_ARG, "null MPO descriptor");
+  if (H->w[0] != 1 || H->w[H->L] != 1) return set_err(nullptr, YAQS_E_ARG, "boundary bond dimensions must be 1");
+  for (int b = 0; b <= H->L; ++b)
+    if (H->w[b] < 1 || H->w[b] > 8) return set_err(nullptr, YAQS_E_UNSUPPORTED, "MPO bond width must be in [1, 8]");
+  for (int i = 0; i < H->L; ++i)
+    if (!H->tensors[i]) return set_err(nullptr, YAQS_E_ARG, "null MPO tensor");
+  const double q = mpo_antihermitian_sq(H);
+  *defect = q > 0.0 ? std::sqrt(q) : (q == q ? 0.0 : q);
+  return YAQS_OK;
+}
 
 int yaqs_ctx_create(int32_t device, yaqs_ctx** out) {
   if (!out) return set_err(nullptr, YAQS_E_ARG, "null out pointer");
@@ -877,6 +933,16 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   for (int b = 0; b <= L; ++b) {
     if (psi0->chi[b] < 1) return set_err(ctx, YAQS_E_ARG, "bond dimension < 1");
     if (H->w[b] < 1 || H->w[b] > 8) return set_err(ctx, YAQS_E_UNSUPPORTED, "MPO bond width must be in [1, 8]");
+  }
+  for (int i = 0; i < L; ++i)
+    if (!H->tensors[i]) return set_err(ctx, YAQS_E_ARG, "null MPO tensor");
+  {  // the Krylov solver is Lanczos: refuse what the reference would hand to Arnoldi
+    const double q = mpo_antihermitian_sq(H);
+    if (!(q <= HERMITIAN_TOL_SQ))
+      return set_err(ctx, YAQS_E_UNSUPPORTED,
+                     "the Hamiltonian MPO is not Hermitian (relative anti-Hermitian part " +
+                         std::to_string(q > 0.0 ? std::sqrt(q) : q) +
+                         "); the engine runs Lanczos, where the reference's :auto Krylov mode switches to Arnoldi");
   }
   if (cfg->n_times < 1 || cfg->num_traj < 1 || cfg->max_bond_dim < 1 || !(cfg->dt == cfg->dt))
     return set_err(ctx, YAQS_E_ARG, "bad config (n_times, num_traj, max_bond_dim, dt)");
