@@ -349,3 +349,38 @@ def test_run_rejects_other_operators():
     cfg = api.TimeEvolutionConfig([], 1.0)
     with pytest.raises(TypeError):
         api.run(api.MPS(2), "InvalidOperator", cfg, parallel=False)
+
+
+def test_run_host_logic(oracle, monkeypatch):
+    """Simulator.run's host side (Simulator.jl:22-141) on CPU: the device
+    call is replaced by the oracle here, so only the host logic is under
+    test: the config check comes first, a noiseless model runs one
+    trajectory, the observables' buffers follow _run_analog / _run_digital,
+    and the caller's initial state is left normalised with its centre at 1."""
+    def fake_analog(desc, ctx=None):
+        tr, chi, st = oracle.analog_run(desc)
+        return api.RunResult(tr, tr.mean(0), chi, st)
+
+    def fake_digital(desc, ctx=None):
+        tr, chi, st = oracle.digital_run(desc)
+        return api.RunResult(tr, tr.mean(0), chi, st)
+
+    monkeypatch.setattr(api, "run_descriptors", fake_analog)
+    monkeypatch.setattr(api, "run_circuit_descriptors", fake_digital)
+    with pytest.raises(TypeError, match="Only TimeEvolutionConfig"):
+        api.run(api.MPS(2), "InvalidOperator", T.StrongMeasurementConfig([]))
+    L = 4
+    psi = api.MPS(L, tensors=[2.0 * t for t in api.MPS(L, state="x+").tensors])  # norm 16
+    psi.orth_center = 3
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.3, dt=0.1, num_traj=7, max_bond_dim=4)
+    res = api.run(psi, api.init_ising(L, 1, 0.5), cfg, None)
+    assert cfg.num_traj == 1 and res.trajectories.shape == (1, L, 4)
+    assert obs[0].trajectories.shape == (1, 4) and obs[0].results.shape == (4,)
+    assert psi.orth_center == 1 and abs(np.linalg.norm(psi.to_vec()) - 1) < 1e-12
+    c = api.DigitalCircuit(L).add_gate(api.Barrier("SAMPLE_OBSERVABLES"), []).add_gate(api.Rx(0.4), [2])
+    c.add_gate(api.Barrier("SAMPLE_OBSERVABLES"), [])
+    cfg = api.TimeEvolutionConfig(obs, 5.0, dt=1.0, num_traj=3, max_bond_dim=4)
+    api.run(api.MPS(L), c, cfg, None)
+    assert obs[1].trajectories.shape == (1, 6) and abs(obs[1].results[1] - np.cos(0.4)) < 1e-12
+    assert np.all(obs[1].results[2:] == 0)

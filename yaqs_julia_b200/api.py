@@ -1403,10 +1403,14 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
     TJMOptions; left unset they follow the reference's default (see
     _methods).  A RepeatedDigitalCircuit runs as its flattened circuit.
     ``parallel`` is accepted for the reference's signature; every trajectory
-    of the run advances together on the device either way."""
+    of the run advances together on the device either way.  As in the
+    reference, ``initial_state`` is left normalised (centre at site 1) and a
+    configuration other than TimeEvolutionConfig is an error."""
     prec = {"fp64": A.YAQS_PREC_FP64, "mixed": A.YAQS_PREC_MIXED}[precision]
     if isinstance(operator, RepeatedDigitalCircuit):
         operator = operator.flatten()
+    if not isinstance(sim_params, TimeEvolutionConfig):
+        raise TypeError("Only TimeEvolutionConfig is supported.")
     if not isinstance(operator, (MPO, DigitalCircuit)):
         raise TypeError("Simulation requires MPO (Analog) or DigitalCircuit (Digital).")
     if noise_model is None or all(p.strength == 0 for p in noise_model.processes):
@@ -1429,8 +1433,14 @@ def run(initial_state: MPS, operator, sim_params: TimeEvolutionConfig, noise_mod
             o.trajectories = np.zeros((sim_params.num_traj, ncol), dtype=np.complex128)
             o.trajectories[:, :n_copy] = res.trajectories[:, k, :n_copy]
             o.results = o.trajectories.real.sum(axis=0) / sim_params.num_traj
-        return res
-    for k, o in enumerate(sim_params.observables):
-        o.trajectories = res.trajectories[:, k, :].astype(np.complex128)
-        o.results = res.mean[k].copy()
+    else:
+        for k, o in enumerate(sim_params.observables):
+            o.trajectories = res.trajectories[:, k, :].astype(np.complex128)
+            o.results = res.mean[k].copy()
+    # the reference normalises the caller's initial state in place
+    # (Simulator.jl:128, normalize! with the centre at site 1); the engine
+    # normalised its own copy, so the caller's object is brought to the same
+    # form here, after the run, leaving what the device received unchanged
+    from .tensornet import normalize
+    normalize(initial_state)
     return res
