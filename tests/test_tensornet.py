@@ -384,3 +384,12 @@ def test_run_host_logic(oracle, monkeypatch):
     api.run(api.MPS(L), c, cfg, None)
     assert obs[1].trajectories.shape == (1, 6) and abs(obs[1].results[1] - np.cos(0.4)) < 1e-12
     assert np.all(obs[1].results[2:] == 0)
+
+
+def test_truncate_refuses_non_finite_tensors():
+    """MPS.truncate! raises on NaN/Inf in a two-site tensor (MPS.jl:356-360)."""
+    m = _rand_mps(4, 2, 3)
+    m.tensors[2] = m.tensors[2].copy()
+    m.tensors[2][0, 0, 0] = np.nan
+    with pytest.raises(ValueError, match="non-finite"):
+        T.truncate(m, max_bond_dim=2)

@@ -173,6 +173,9 @@ def truncate(mps: MPS, threshold: float = 1e-12, max_bond_dim: int | None = None
         l, d1, k = A.shape
         _, d2, r = B.shape
         theta = _f(A, (l * d1, k)) @ _f(B, (k, d2 * r))
+        scale = np.abs(theta).max() if theta.size else 0.0
+        if not np.isfinite(scale):  # MPS.jl:356-360
+            raise ValueError(f"truncate!: non-finite entries encountered in Theta (scale={scale})")
         U, S, Vh = np.linalg.svd(theta, full_matrices=False)
         keep, disc = len(S), 0.0
         for kk in range(len(S), 0, -1):
