@@ -22,6 +22,13 @@ def test_header_declares_entry_points():
     assert {"yaqs_analog_run", "yaqs_ctx_create", "yaqs_batched_svd", "yaqs_batched_expm_site"} <= names
 
 
+def test_integration_guide_covers_every_entry_point():
+    """Every declared entry point has its line in the integration guide."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = sorted(n for n in _declared() if n not in guide)
+    assert not missing, missing
+
+
 def test_library_exports_every_declared_symbol():
     from yaqs_julia_b200 import _lib
     if not os.path.exists(_lib.LIB_PATH):
