@@ -1,8 +1,9 @@
 """The multi-GPU form is replicas: each rank runs its own block of
 trajectories (global index = rank * n + local index, which keys the Philox
 streams) and only the timing is reduced.  Two gloo ranks on the CPU check
-that the blocks reproduce one run of all trajectories and that the bench's
-max/sum reductions combine the ranks as the bench line reports them."""
+that the blocks reproduce one run of all trajectories, analog and digital,
+and that the bench's max/sum reductions combine the ranks as the bench line
+reports them."""
 import os
 import socket
 
@@ -60,3 +61,43 @@ def test_two_replicas_reproduce_one_run(oracle, tmp_path):
         assert t_max == 2.0 and units == world * nt * 3
     jumps = sum(int(np.load(tmp_path / f"red{r}.npy")[2]) for r in range(world))
     assert jumps == st["jumps"] > 0
+
+
+def _circuit_problem(nt, offset):
+    from yaqs_julia_b200 import api
+    from yaqs_julia_b200 import circuits as CL
+    L = 5
+    c = CL.create_ising_circuit(L, 1.0, 0.7, 0.1, 3)
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.05} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_z")], L)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 3.0, dt=1.0, num_traj=nt, max_bond_dim=8)
+    return api.CircuitDescriptors(api.MPS(L), c, cfg, nm, seed=77, traj_offset=offset)
+
+
+def _digital_rank(rank, world, port, nt, out_dir):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import bench
+    from oracle import oracle as O
+    _, _, _, dist = bench.dist_setup()
+    traj, _, _ = O.digital_run(_circuit_problem(nt, rank * nt))
+    np.save(os.path.join(out_dir, f"dig{rank}.npy"), traj)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_digital_replicas_reproduce_one_run(oracle, tmp_path):
+    """The digital workload shards the same way: each rank's block of
+    trajectories (Philox streams keyed by the global index) concatenates to
+    one run of all of them."""
+    import torch.multiprocessing as mp
+    nt, world = 5, 2
+    mp.start_processes(_digital_rank, args=(world, _free_port(), nt, str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    parts = [np.load(tmp_path / f"dig{r}.npy") for r in range(world)]
+    whole, _, st = oracle.digital_run(_circuit_problem(world * nt, 0))
+    assert np.array_equal(np.concatenate(parts, axis=0), whole) and st["jumps"] > 0
