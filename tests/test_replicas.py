@@ -8,7 +8,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 
 
 def _free_port():
