@@ -175,3 +175,20 @@ def test_generated_circuits_run_on_the_oracle(oracle, make):
     psi = _unitary(circ) @ psi
     ref = [np.real(np.vdot(psi, D.site_op(api.Z, i, L) @ psi)) for i in range(1, L + 1)]
     assert np.abs(tr[0, :, -1] - ref).max() < 1e-9
+
+
+def test_ingestion_reference_circuit_layers():
+    """test_CircuitIngestion.jl:25-88: h(0), cx(0,1), rx(0.5, 2), barrier,
+    rzz(0.2, 1, 2) -> layer 1 holds H on 1 and Rx(0.5) on 3, layer 2 CX on
+    (1, 2), layer 3 Rzz(0.2) on (2, 3)."""
+    items = [("h", [], [0]), ("cx", [], [0, 1]), ("rx", [0.5], [2]), ("barrier", [], [0, 1, 2]),
+             ("rzz", [0.2], [1, 2])]
+    circ = C.ingest_qiskit_circuit(_fake_qiskit(3, items))
+    assert isinstance(circ, api.DigitalCircuit) and circ.num_qubits == 3
+    layers, _ = api.process_circuit(circ)
+    assert len(layers) >= 2
+    l1 = {tuple(g.sites): g.op for g in layers[0]}
+    assert set(l1) == {(1,), (3,)}
+    assert np.allclose(l1[(1,)], api.H) and np.allclose(l1[(3,)], api.Rx(0.5))
+    assert [tuple(g.sites) for g in layers[1]] == [(1, 2)] and np.allclose(layers[1][0].op, api.CX)
+    assert [tuple(g.sites) for g in layers[2]] == [(2, 3)] and np.allclose(layers[2][0].op, api.Rzz(0.2))
