@@ -48,6 +48,19 @@ int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D
                            const double* x, double dt, int32_t krylov_dim, double krylov_tol,
                            double krylov_exit_tol, double* out, int32_t* matvecs);
 
+/* Complex FP32 product C = op(A) op(B) on the tensor cores, the building
+ * block of the mixed-precision form's H_eff and environment contractions
+ * (the @tensor products of src/Algorithms.jl:199-226, :330-361, in complex
+ * FP32): tcgen05 MMAs in the 3-product complex form with the 3xTF32 split,
+ * operand tiles loaded by TMA.  A: batch x (M x K), column-major
+ * (a_kmajor = 0) or row-major (a_kmajor = 1); B: batch x (K x N), row-major
+ * (b_kmajor = 0) or column-major (b_kmajor = 1); C: batch x (M x N)
+ * column-major; interleaved complex64.  conj_a / conj_b conjugate the
+ * operand. */
+int yaqs_batched_cgemm_tf32(yaqs_ctx* ctx, int32_t batch, int32_t M, int32_t N, int32_t K, const float* A,
+                            int32_t a_kmajor, int32_t conj_a, const float* B, int32_t b_kmajor, int32_t conj_b,
+                            float* C);
+
 /*
  * yaqs_batched_svd without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc: a host whose device
@@ -59,9 +72,11 @@ int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D
  * Scratch comes from a fixed 8 MiB array compiled into the library (held by
  * every GPU that loads it until exit): batch * (4 max(m,n)^2 + max(m,n) +
  * 256) complex values plus 256 ints per problem must fit, otherwise the call
- * returns YAQS_E_ARG before launching anything.  The first call on a device
- * looks up the array's device address and sets the kernel's shared-memory
- * limit; make that first call before any stream capture.  All calls share
+ * returns YAQS_E_ARG before launching anything.  yaqs_ctx_create looks up
+ * the array's device address for its device and sets the kernel's
+ * shared-memory limit (this loads the library onto that GPU), so a call does
+ * no set-up of its own; create the context before any stream capture, and
+ * create a new one after a cudaDeviceReset.  All calls share
  * the one array and every call rewrites the scratch words it reads, so a
  * call never depends on an earlier one; calls that overlap on the GPU (two
  * streams, two threads) race on the array and must be serialised by the

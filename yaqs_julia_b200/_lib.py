@@ -77,6 +77,9 @@ def lib():
         L.yaqs_batched_svd.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4
         L.yaqs_batched_qr.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 3
         L.yaqs_batched_project_site.argtypes = [C.c_void_p] + [C.c_int32] * 6 + [A.DPTR] * 5
+        FPTR = P(C.c_float)
+        L.yaqs_batched_cgemm_tf32.argtypes = ([C.c_void_p] + [C.c_int32] * 4 + [FPTR, C.c_int32, C.c_int32, FPTR,
+                                              C.c_int32, C.c_int32, FPTR])
         L.yaqs_batched_expm_site.argtypes = ([C.c_void_p] + [C.c_int32] * 6 + [A.DPTR] * 4 +
                                              [C.c_double, C.c_int32, C.c_double, C.c_double, A.DPTR,
                                               P(C.c_int32)])

@@ -22,6 +22,7 @@
 #include "../../include/yaqs_tjm.h"
 #include "../../include/yaqs_tjm_components.h"
 #include "digital.cuh"
+#include "tcgemm.cuh"
 
 // ---------------------------------------------------------------------------
 // Device program
@@ -246,6 +247,30 @@ __global__ void __launch_bounds__(NT, 1) expm_kernel(int chil, int D, int chir, 
   if (threadIdx.x == 0) matvecs[b] = mv;
 }
 
+// Shared memory of a kernel that runs tc_gemm: the pipeline buffers and
+// barriers, aligned to 1024 bytes inside the dynamic allocation.
+struct CgemmSmem {
+  TcSmem t;
+  TcState st;
+};
+__device__ __forceinline__ unsigned char* align_smem_1024(unsigned char* p) {
+  const unsigned off = smem_u32(p);
+  return p + ((1024u - (off & 1023u)) & 1023u);
+}
+
+// One complex FP32 product per CTA on the tensor cores (tcgen05 + TMA).
+__global__ void __launch_bounds__(NT, 1) cgemm_tc_kernel(int M, int N, int K, const CUtensorMap* maps, int a_mn,
+                                                         int conj_a, int b_mn, int conj_b, float2* C, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CgemmSmem& sm = *reinterpret_cast<CgemmSmem*>(align_smem_1024(smraw));
+  tc_setup(sm.st);
+  const TcOp A{maps + 2 * blockIdx.x, a_mn, conj_a};
+  const TcOp B{maps + 2 * blockIdx.x + 1, b_mn, conj_b};
+  const bool ok = tc_gemm<float2>(M, N, K, A, B, C + (long long)M * N * blockIdx.x, 1, M, false, sm.t, sm.st);
+  if (threadIdx.x == 0) status[blockIdx.x] = ok ? 0 : 1;
+  tc_teardown(sm.st);
+}
+
 // FP64 FMA throughput probe: 8 independent chains per thread.
 __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
@@ -308,6 +333,46 @@ struct DevMem {
     return e;
   }
 };
+
+// Tensor maps of staged tc_gemm operands (cuTensorMapEncodeTiled, reached
+// through the runtime's driver entry point so the library links no driver
+// stub).  A staged operand is a 2D FP32 array of `rows` rows of
+// 2 * pitch floats (pitch complex values, even, so every row starts on a
+// 16-byte boundary); the box is fixed by the operand's role (tcgemm.cuh).
+enum TcRole { TC_A_MN = 0, TC_A_K = 1, TC_B_MN = 2, TC_B_K = 3 };
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// Fills *out for a staged operand at `base` (16-byte aligned).  Returns false
+// when the driver refuses the map or the geometry breaks the alignment rules.
+bool make_tc_map(CUtensorMap* out, const void* base, long long pitch, long long rows, int role) {
+  EncodeTiledFn fn = encode_tiled_fn();
+  if (!fn || pitch < 2 || (pitch & 1) || rows < 1 || (reinterpret_cast<uintptr_t>(base) & 15)) return false;
+  const int inner_c = role == TC_A_MN ? TC_BM : role == TC_B_MN ? TC_BN : TC_BK;
+  const int box_rows = role == TC_A_K ? TC_BM : role == TC_B_K ? TC_BN : TC_BK;
+  cuuint64_t dims[2] = {(cuuint64_t)(2 * pitch), (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(2 * pitch * sizeof(float))};
+  cuuint32_t box[2] = {(cuuint32_t)(2 * inner_c), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 // Sparse M[o, i] built from a dense lambda, in CSR.
 struct HostWMat {
@@ -820,8 +885,6 @@ static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, 
   return YAQS_OK;
 }
 
-// Uploads the launch list (time index or layer per position) and marks no
-// position done for any trajectory.
 // ||W - W^dag||_F^2 / ||W||_F^2 of an MPO (host arithmetic only), formed as
 // (2 tr(W^dag W) - 2 Re tr(W W)) / tr(W^dag W) from two transfer
 // contractions over the bonds of two copies.  Being a difference of squared
@@ -866,6 +929,8 @@ static double mpo_antihermitian_sq(const yaqs_mpo_desc* H) {
 // a relative defect of 1e-5, far above the rounding of the estimate.
 constexpr double HERMITIAN_TOL_SQ = 1e-10;
 
+// Uploads the launch list (time index or layer per position) and marks no
+// position done for any trajectory.
 static int upload_positions(yaqs_ctx* ctx, yaqs_run* run) {
   int *d_jlist, *d_done;
   const size_t np = run->launches.size();
@@ -879,6 +944,8 @@ static int upload_positions(yaqs_ctx* ctx, yaqs_run* run) {
 }
 
 extern "C" {
+
+static cudaError_t noalloc_prepare(int device);
 
 const char* yaqs_version(void) { return "yaqs-b200 0.1.0 (sm_100a, FP64 trajectory engine)"; }
 
@@ -900,9 +967,15 @@ int yaqs_ctx_create(int32_t device, yaqs_ctx** out) {
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) return set_err(nullptr, YAQS_E_CUDA, "no CUDA device visible");
   if (device < 0 || device >= n) return set_err(nullptr, YAQS_E_ARG, "device index out of range");
+  if (cudaSetDevice(device) != cudaSuccess) return set_err(nullptr, YAQS_E_CUDA, "cudaSetDevice failed");
+  // Loads the module onto the device now (the no-allocation entry point's
+  // scratch array is part of it) and caches that array's device address, so
+  // no later call has to load the module mid-run.  Refreshed by every new
+  // context: after a cudaDeviceReset, create a new context.
+  e = noalloc_prepare(device);
+  if (e != cudaSuccess) return set_err(nullptr, YAQS_E_CUDA, std::string("module set-up: ") + cudaGetErrorString(e));
   yaqs_ctx* c = new yaqs_ctx();
   c->device = device;
-  cudaSetDevice(device);
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   *out = c;
   return YAQS_OK;
@@ -1652,6 +1725,21 @@ std::mutex g_noalloc_mu;
 void* g_noalloc_base[64] = {};  // device address of g_noalloc_scratch, per device ordinal
 }  // namespace
 
+// With `device` current: looks up the array's device address (the first
+// lookup on a device loads the module there) and sets svd_kernel's
+// shared-memory limit.  Run by yaqs_ctx_create for its device.
+static cudaError_t noalloc_prepare(int device) {
+  if (device < 0 || device >= 64) return cudaSuccess;  // the entry point refuses such ordinals
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CompSmem));
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  g_noalloc_base[device] = p;
+  return cudaSuccess;
+}
+
 int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M, double* U,
                              double* S, double* SVt, void* stream) {
   if (!ctx) return set_err(nullptr, YAQS_E_ARG, "null context");
@@ -1673,14 +1761,9 @@ int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n,
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_base[ctx->device]) {  // once per device, with that device current
-      void* p = nullptr;
-      CUDA_TRY(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch));
-      CUDA_TRY(ctx, cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      g_noalloc_base[ctx->device] = p;
-    }
-    base = g_noalloc_base[ctx->device];
+    base = g_noalloc_base[ctx->device];  // set when the context was created
   }
+  if (!base) return set_err(ctx, YAQS_E_CUDA, "scratch address not resolved for this device");
   cplx* work = static_cast<cplx*>(base);
   int* iwork = reinterpret_cast<int*>(work + (long long)batch * wstride);
   svd_kernel<<<batch, NT, smem, static_cast<cudaStream_t>(stream)>>>(
@@ -1794,6 +1877,60 @@ int yaqs_batched_expm_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D
                            int32_t* matvecs) {
   return expm_common(ctx, batch, chil, D, chir, wl, wr, L, R, W, x, dt, krylov_dim, krylov_tol, krylov_exit_tol, out,
                      matvecs, 0);
+}
+
+int yaqs_batched_cgemm_tf32(yaqs_ctx* ctx, int32_t batch, int32_t M, int32_t N, int32_t K, const float* A,
+                            int32_t a_kmajor, int32_t conj_a, const float* B, int32_t b_kmajor, int32_t conj_b,
+                            float* C) {
+  if (!ctx || batch < 1 || M < 1 || N < 1 || K < 1 || M > 4096 || N > 4096 || K > 4096 || !A || !B || !C)
+    return set_err(ctx, YAQS_E_ARG, "bad cgemm arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  // staged layouts: A MN-major = rows k, inner m; K-major = rows m, inner k (likewise B with n)
+  const int a_mn = a_kmajor ? 0 : 1, b_mn = b_kmajor ? 0 : 1;
+  const long long a_rows = a_mn ? K : M, a_inner = a_mn ? M : K, b_rows = b_mn ? K : N, b_inner = b_mn ? N : K;
+  const long long pa = (a_inner + 1) & ~1LL, pb = (b_inner + 1) & ~1LL;
+  std::vector<float> ha((size_t)batch * a_rows * pa * 2, 0.f), hb((size_t)batch * b_rows * pb * 2, 0.f);
+  for (long long b = 0; b < batch; ++b) {
+    for (long long r = 0; r < a_rows; ++r)
+      for (long long i = 0; i < a_inner; ++i)
+        for (int c = 0; c < 2; ++c)
+          ha[((b * a_rows + r) * pa + i) * 2 + c] = A[((b * a_rows + r) * a_inner + i) * 2 + c];
+    for (long long r = 0; r < b_rows; ++r)
+      for (long long i = 0; i < b_inner; ++i)
+        for (int c = 0; c < 2; ++c)
+          hb[((b * b_rows + r) * pb + i) * 2 + c] = B[((b * b_rows + r) * b_inner + i) * 2 + c];
+  }
+  DevMem dm;
+  float *dA, *dB;
+  float2* dC;
+  CUtensorMap* dmaps;
+  int* dst;
+  CUDA_TRY(ctx, dm.alloc(&dA, ha.size()));
+  CUDA_TRY(ctx, dm.alloc(&dB, hb.size()));
+  CUDA_TRY(ctx, dm.alloc(&dC, (size_t)batch * M * N));
+  CUDA_TRY(ctx, dm.alloc(&dmaps, 2 * (size_t)batch));
+  CUDA_TRY(ctx, dm.alloc(&dst, batch));
+  CUDA_TRY(ctx, cudaMemcpy(dA, ha.data(), ha.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(dB, hb.data(), hb.size() * sizeof(float), cudaMemcpyHostToDevice));
+  std::vector<CUtensorMap> maps(2 * (size_t)batch);
+  for (long long b = 0; b < batch; ++b) {
+    if (!make_tc_map(&maps[2 * b], dA + b * a_rows * pa * 2, pa, a_rows, a_mn ? TC_A_MN : TC_A_K) ||
+        !make_tc_map(&maps[2 * b + 1], dB + b * b_rows * pb * 2, pb, b_rows, b_mn ? TC_B_MN : TC_B_K))
+      return set_err(ctx, YAQS_E_CUDA, "cuTensorMapEncodeTiled refused a staged operand");
+  }
+  CUDA_TRY(ctx, cudaMemcpy(dmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  const size_t smem = sizeof(CgemmSmem) + 1024;
+  CUDA_TRY(ctx, cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cgemm_tc_kernel<<<batch, NT, smem>>>(M, N, K, dmaps, a_mn, conj_a ? 1 : 0, b_mn, conj_b ? 1 : 0, dC, dst);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaDeviceSynchronize());
+  std::vector<int> st(batch);
+  CUDA_TRY(ctx, cudaMemcpy(st.data(), dst, batch * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int v : st)
+    if (v) return set_err(ctx, YAQS_E_TIMEOUT, "tensor-core pipeline wait gave up");
+  CUDA_TRY(ctx, cudaMemcpy(C, dC, (size_t)batch * M * N * sizeof(float2), cudaMemcpyDeviceToHost));
+  return YAQS_OK;
 }
 
 int yaqs_batched_project_site(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, int32_t chir, int32_t wl,
