@@ -22,10 +22,30 @@ def test_header_declares_entry_points():
     assert {"yaqs_analog_run", "yaqs_ctx_create", "yaqs_batched_svd", "yaqs_batched_expm_site"} <= names
 
 
-def test_integration_guide_covers_every_entry_point():
-    """Every declared entry point has its line in the integration guide."""
-    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    missing = sorted(n for n in _declared() if n not in guide)
+# The C-ABI surface as the bindings (yaqs_julia_b200/_lib.py) and the Julia
+# shim know it; a new or removed declaration must be added here too.
+ENTRY_POINTS = {
+    "yaqs_version", "yaqs_last_error", "yaqs_ctx_create", "yaqs_ctx_destroy", "yaqs_mpo_hermitian_defect",
+    "yaqs_analog_run", "yaqs_analog_begin", "yaqs_analog_advance", "yaqs_analog_remaining", "yaqs_analog_stats",
+    "yaqs_analog_profile", "yaqs_analog_finish", "yaqs_run_state", "yaqs_run_position", "yaqs_run_rng",
+    "yaqs_run_restore", "yaqs_run_seek", "yaqs_digital_plan", "yaqs_digital_begin", "yaqs_digital_run",
+    "yaqs_server_create", "yaqs_server_submit_analog", "yaqs_server_submit_digital", "yaqs_server_poll",
+    "yaqs_server_wait", "yaqs_server_take", "yaqs_server_last_error", "yaqs_server_stats_get",
+    "yaqs_server_destroy", "yaqs_batched_svd", "yaqs_batched_qr", "yaqs_batched_project_site",
+    "yaqs_batched_expm_site", "yaqs_batched_cgemm_tf32", "yaqs_batched_svd_noalloc", "yaqs_fp64_peak",
+}
+
+
+def test_headers_declare_exactly_the_bound_entry_points():
+    """The headers declare the entry points the bindings know, no more, no fewer."""
+    names = _declared()
+    assert names == ENTRY_POINTS, (sorted(names - ENTRY_POINTS), sorted(ENTRY_POINTS - names))
+
+
+def test_bindings_set_argtypes_for_every_entry_point():
+    """Every entry point taking arguments has its ctypes signature in _lib.py."""
+    src = open(os.path.join(ROOT, "yaqs_julia_b200", "_lib.py")).read()
+    missing = sorted(n for n in ENTRY_POINTS if n != "yaqs_version" and f"L.{n}." not in src)
     assert not missing, missing
 
 

@@ -14,8 +14,13 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 
 
 def sources():
-    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh"))] + [
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh", ".h"))] + [
         os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include")))]
+
+
+# translation units: engine.cu (every kernel without tcgen05 code) and
+# engine_tc.cu (the tensor-core trajectory kernel), compiled in parallel
+UNITS = ["engine.cu", "engine_tc.cu"]
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -23,8 +28,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
         newest = max(os.path.getmtime(s) for s in sources())
         if os.path.getmtime(OUT) >= newest:
             return OUT
-    cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", OUT, os.path.join(CSRC, "engine.cu")]
-    subprocess.run(cmd, check=True)
+    objs, procs = [], []
+    for u in UNITS:
+        o = os.path.join(CSRC, u.replace(".cu", ".o"))
+        cmd = [NVCC] + [f for f in FLAGS if f != "-shared"] + (["-Xptxas", "-v"] if verbose else []) + [
+            "-c", "-o", o, os.path.join(CSRC, u)]
+        procs.append(subprocess.Popen(cmd))
+        objs.append(o)
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
+    subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT] + objs, check=True)
+    for o in objs:
+        os.remove(o)
     return OUT
 
 

@@ -37,11 +37,11 @@ struct DigParams {
   int any_sample;
 };
 
-__device__ __constant__ cplx c_swap[16] = {{1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}, {0, 0},
+static __device__ __constant__ cplx c_swap[16] = {{1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}, {0, 0},
                                            {0, 0}, {1, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {1, 0}};
 
 // apply_local_gate_exact! on sites (s1, s1+1).
-__device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
+static __device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
   ProfScope prof_scope_(PF_SWEEP);
   shift_oc(c, s, s1);
   if (c.sm.fail) return;
@@ -51,18 +51,18 @@ __device__ void tebd_apply(Ctx& c, const DState& s, const cplx* op, int s1) {
   merge(c, s, s1, th);
   apply_local(th, l, 4, r, op);
   split(c, s, s1, th, l, r, 2, false);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  cta_sync();
+  if (ltid() == 0) {
     *s.oc = s1 + 1;
     // nominal work: theta merge GEMM, 4x4 gate, SVD counted as 4 m n min(m, n) complex MACs
     const double m = 2.0 * l, n = 2.0 * r;
     *c.fl += 8.0 * (m * n * k + 4.0 * m * n + 4.0 * m * n * fmin(m, n));
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // apply_window! with method :TEBD (DigitalTJM.jl:307-334).
-__device__ void apply_window_tebd(Ctx& c, const DState& s, const DevGate& g) {
+static __device__ void apply_window_tebd(Ctx& c, const DState& s, const DevGate& g) {
   if (g.b > g.a + 1) {
     for (int k = g.b - 1; k >= g.a + 1 && !c.sm.fail; --k) tebd_apply(c, s, c_swap, k);
     if (!c.sm.fail) tebd_apply(c, s, g.mat, g.a);
@@ -78,7 +78,7 @@ __device__ void apply_window_tebd(Ctx& c, const DState& s, const DevGate& g) {
 // sweep (_tdvp_sweep_circuit_2site!, Algorithms.jl:606-627): each pair by +1
 // with the right site back-evolved by -1 (:631-672), the last pair by +1
 // split to the right (:762-800); the centre ends on b.
-__device__ void apply_window_tdvp(Ctx& c, const DState& s, const DevGate& g, const WMat* wm) {
+static __device__ void apply_window_tdvp(Ctx& c, const DState& s, const DevGate& g, const WMat* wm) {
   const int s1 = g.a, s2 = g.b, n = s2 - s1 + 1;
   const WMat* h1 = wm;
   const WMat* h2 = wm + n;
@@ -111,7 +111,7 @@ __device__ void apply_window_tdvp(Ctx& c, const DState& s, const DevGate& g, con
 // dissipator needs a two-site split, every operation of the reference sweeps
 // away from the gate's sites is a gauge move, and only the gate's sites are
 // visited; otherwise the reference sweeps run as they are.
-__device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
+static __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
   ProfScope prof_scope_(PF_STOCH);
   const DevParams& P = c.P;
   int nloc = 0;
@@ -147,7 +147,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
     const long long n = (long long)s.chi[oc] * 2 * s.chi[oc + 1];
     if (!all_zero) {
       cta_scale(A, n, fdiss);
-      __syncthreads();
+      cta_sync();
     }
     const double nrm = cta_norm2(A, n, c.sm.e.r);
     const double u1 = draw_uniform(c);
@@ -177,7 +177,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
     if (chosen < 0) chosen = first;  // rounding left the cumulative sum below r: the first candidate
     const DevProc& pr = P.procs[chosen];
     apply_local(site_ptr(c, s, pr.s0), s.chi[pr.s0], 2, s.chi[pr.s0 + 1], pr.mat);
-    if (threadIdx.x == 0) c.cnt[3] += 1;
+    if (ltid() == 0) c.cnt[3] += 1;
     normalize_center(c, s);
     return;
   }
@@ -194,7 +194,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
         cplx* A = site_ptr(c, s, i);
         if (pr.pauli_name) {
           cta_scale(A, (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * pr.gamma));
-          __syncthreads();
+          cta_sync();
         } else {
           apply_local(A, s.chi[i], 2, s.chi[i + 1], pr.diss_full);
         }
@@ -204,7 +204,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
           const DevProc& pr = P.procs[k];
           if (!proc_on(pr, s1, s2) || pr.nsites != 2 || pr.s1 != i) continue;
           cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * pr.drate));
-          __syncthreads();
+          cta_sync();
         }
       }
     }
@@ -230,7 +230,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
       const DevProc& pr = P.procs[k];
       if (!proc_on(pr, s1, s2) || pr.nsites != 1 || pr.s0 != site) continue;
       double nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1], pr.pauli_proc ? nullptr : pr.mat);
-      if (threadIdx.x == 0) {
+      if (ltid() == 0) {
         cand[nc] = pr.gamma * nr;
         candp[nc] = k;
       }
@@ -247,7 +247,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
           merge(c, s, site, th);
           nr = local_norm2(c, th, s.chi[site], 4, s.chi[site + 2], pr.mat);
         }
-        if (threadIdx.x == 0) {
+        if (ltid() == 0) {
           cand[nc] = pr.gamma * nr;
           candp[nc] = k;
         }
@@ -255,7 +255,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
       }
     }
   }
-  __syncthreads();
+  cta_sync();
   double total = 0.0;
   for (int e = 0; e < nc; ++e) total += cand[e];
   if (total == 0.0) {
@@ -273,7 +273,7 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
     }
   }
   const DevProc& pr = P.procs[candp[chosen]];
-  __syncthreads();
+  cta_sync();
   shift_oc(c, s, pr.s0);
   if (pr.nsites == 1) {
     apply_local(site_ptr(c, s, pr.s0), s.chi[pr.s0], 2, s.chi[pr.s0 + 1], pr.mat);
@@ -283,23 +283,23 @@ __device__ void digital_noise(Ctx& c, const DState& s, int s1, int s2) {
     apply_local(th, l, 4, rr, pr.mat);
     split(c, s, pr.s0, th, l, rr, 1, false);
   }
-  if (threadIdx.x == 0) c.cnt[3] += 1;
+  if (ltid() == 0) c.cnt[3] += 1;
   finish_normalize(c, s);
 }
 
 // Launch 0: initial state, normalisation and the start sample; launch l >= 1:
 // layer l-1 (its 1-qubit gates first, then each 2-qubit gate followed by the
 // noise step) and the sample after it.
-__device__ void run_digital_step(Ctx& c, const DigParams& D, int launch) {
+static __device__ void run_digital_step(Ctx& c, const DigParams& D, int launch) {
   ProfScope prof_scope_(PF_STEP);
   const DevParams& P = c.P;
   const int L = P.L;
   DState st{P.phi + (long long)c.traj * P.mps_size, P.phi_chi + (long long)c.traj * (L + 1), P.phi_oc + c.traj};
   if (launch == 0) {
     cta_copy(st.a, P.psi0, P.mps_size);
-    for (int b = threadIdx.x; b <= L; b += NT) st.chi[b] = P.chi0[b];
-    if (threadIdx.x == 0) *st.oc = 0;
-    __syncthreads();
+    for (int b = ltid(); b <= L; b += NT) st.chi[b] = P.chi0[b];
+    if (ltid() == 0) *st.oc = 0;
+    cta_sync();
     normalize_state(c, st);  // Simulator.jl:128
     if (D.sample_at_start) evaluate(c, st, 0);
     if (D.n_layers == 0 && !D.any_sample && P.nobs > 0) evaluate(c, st, 0);
@@ -320,7 +320,7 @@ __device__ void run_digital_step(Ctx& c, const DigParams& D, int launch) {
     if (c.sm.fail) return;
     digital_noise(c, st, G.a, G.b);
     if (c.sm.fail) return;
-    if (threadIdx.x == 0) c.cnt[6] += 1;
+    if (ltid() == 0) c.cnt[6] += 1;
   }
   if (c.sm.fail) return;
   if (D.sample_col[l] >= 0) evaluate(c, st, D.sample_col[l]);

@@ -24,136 +24,12 @@
 #include "digital.cuh"
 #include "tcgemm.cuh"
 
-// ---------------------------------------------------------------------------
-// Device program
-// ---------------------------------------------------------------------------
-__device__ void copy_state(Ctx& c, const DState& dst, const DState& src) {
-  ProfScope prof_scope_(PF_COPY);
-  cta_copy(dst.a, src.a, c.P.mps_size);
-  for (int b = threadIdx.x; b <= c.P.L; b += NT) dst.chi[b] = src.chi[b];
-  if (threadIdx.x == 0) *dst.oc = *src.oc;
-  __syncthreads();
-}
-
-__device__ void sample(Ctx& c, const DState& phi, const DState& psi, int col) {
-  copy_state(c, psi, phi);
-  tdvp_sweep(c, psi);
-  if (c.sm.fail) return;
-  apply_dissipation(c, psi, false, c.P.dt / 2);
-  if (c.sm.fail) return;
-  if (c.P.noise_present) stochastic_process(c, psi, c.P.dt);
-  if (c.sm.fail) return;
-  evaluate(c, psi, col);
-}
-
-__device__ void run_step(Ctx& c, int j) {
-  ProfScope prof_scope_(PF_STEP);
-  const DevParams& P = c.P;
-  const int L = P.L;
-  DState phi{P.phi + (long long)c.traj * P.mps_size, P.phi_chi + (long long)c.traj * (L + 1), P.phi_oc + c.traj};
-  DState psi{c.ws + P.lay.psi, c.wsi + P.lay.i_chi, c.wsi + P.lay.i_oc};
-  if (j == 0) {
-    cta_copy(phi.a, P.psi0, P.mps_size);
-    for (int b = threadIdx.x; b <= L; b += NT) phi.chi[b] = P.chi0[b];
-    if (threadIdx.x == 0) *phi.oc = 0;
-    __syncthreads();
-    normalize_state(c, phi);  // Simulator.jl:128
-    if (P.sample_ts) evaluate(c, phi, 0);
-    if (P.order == 2) {
-      apply_dissipation(c, phi, false, P.dt / 2);  // initialize, AnalogTJM.jl:21-33
-      if (c.sm.fail) return;
-      if (P.noise_present) stochastic_process(c, phi, P.dt);
-      if (c.sm.fail) return;
-      if (P.sample_ts && P.n_times > 1) sample(c, phi, psi, 1);
-    }
-    return;
-  }
-  tdvp_sweep(c, phi);
-  if (c.sm.fail) return;
-  if (P.order == 2) {
-    apply_dissipation(c, phi, true, P.dt);  // step_through, AnalogTJM.jl:40-55
-    if (c.sm.fail) return;
-    if (P.noise_present) stochastic_process(c, phi, P.dt);
-    if (c.sm.fail) return;
-    if (P.sample_ts || j == P.n_times - 1) sample(c, phi, psi, P.sample_ts ? j : 0);
-  } else {
-    if (P.noise_present) {  // AnalogTJM.jl:160-173
-      apply_dissipation(c, phi, true, P.dt);
-      if (c.sm.fail) return;
-      stochastic_process(c, phi, P.dt);
-      if (c.sm.fail) return;
-    }
-    if (P.sample_ts)
-      evaluate(c, phi, j);
-    else if (j == P.n_times - 1)
-      evaluate(c, phi, 0);
-  }
-}
-
-// Work units of a launch are (position, trajectory) pairs in position-major
-// order, where the positions first .. first+count-1 index P.jlist.  Each CTA
-// pulls the next unit from an atomic counter, so work is balanced at the
-// granularity of one time index (or circuit layer) of one trajectory, not of
-// whole trajectories.  A unit runs only after the same trajectory's previous
-// position has finished: that unit was pulled earlier by a CTA that is
-// executing it, so the wait always ends; it is still bounded (about 100 s)
-// and gives up with ST_TIMEOUT.
-#define DONE_WAIT_POLLS 100000000LL
-__device__ bool wait_done(const DevParams& P, int t, int need, CtaSmem& sm) {
-  if (threadIdx.x == 0) {
-    volatile int* d = P.done + t;
-    int ok = 0;
-    for (long long it = 0; it < DONE_WAIT_POLLS; ++it) {
-      if (*d >= need) {
-        ok = 1;
-        break;
-      }
-      __nanosleep(1000);
-    }
-    __threadfence();
-    sm.bcast_i[6] = ok;
-  }
-  __syncthreads();
-  const int ok = sm.bcast_i[6];
-  __syncthreads();
-  return ok != 0;
-}
-
-template <class StepFn>
-__device__ void run_units(const DevParams& P, CtaSmem& sm, int first, int count, StepFn step) {
-  const int slot = blockIdx.x;
-  cplx* ws = P.ws + (long long)slot * P.lay.total;
-  int* wsi = P.wsi + (long long)slot * P.lay.itotal;
-  const int nt = P.num_traj;
-  const int total = count * nt;
-  for (;;) {
-    if (threadIdx.x == 0) sm.bcast_i[7] = atomicAdd(&P.queue[first], 1);
-    __syncthreads();
-    const int u = sm.bcast_i[7];
-    __syncthreads();
-    if (u >= total) break;
-    const int k = u / nt, t = u - k * nt, pos = first + k;
-    bool ready = true;
-    if (k > 0) ready = wait_done(P, t, pos - 1, sm);
-    if (threadIdx.x == 0) sm.fail = ready ? 0 : ST_TIMEOUT;
-    __syncthreads();
-    if (ready && P.status[t] == 0) {
-      Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
-      step(c, P.jlist[pos]);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      if (sm.fail && P.status[t] == 0) P.status[t] = sm.fail;
-      __threadfence();
-      atomicExch(P.done + t, pos);
-    }
-    __syncthreads();
-  }
-}
+#include "program.cuh"
+#include "engine_tc.h"
 
 __global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int first, int count) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(align_smem_1024(smraw));
   run_units(P, sm, first, count, [](Ctx& c, int j) { run_step(c, j); });
 }
 
@@ -162,7 +38,7 @@ __global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int 
 __global__ void __launch_bounds__(NT, 2) digital_step_kernel(const DevParams P, const DigParams D, int first,
                                                              int count) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(align_smem_1024(smraw));
   run_units(P, sm, first, count, [&D](Ctx& c, int j) { run_digital_step(c, D, j); });
 }
 
@@ -177,7 +53,7 @@ struct CompSmem {
 __global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M, cplx* U, double* S, cplx* SVt,
                                                     cplx* work, long long wstride, int* iwork) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
+  CompSmem& sm = *reinterpret_cast<CompSmem*>(align_smem_1024(smraw));
   const int b = blockIdx.x;
   const int k = min(m, n);
   const long long big = (long long)max(m, n) * max(m, n);
@@ -196,21 +72,21 @@ __global__ void __launch_bounds__(NT, 1) svd_kernel(int m, int n, const cplx* M,
   cplx* Ub = U + (long long)m * k * b;
   cplx* Sb = SVt + (long long)k * n * b;
   cta_copy(Ub, w.Yo, (long long)m * k);
-  __syncthreads();
+  cta_sync();
   cta_gemm(gemm_args(k, n, m, w.Yo, m, 1, Mb, 1, m, Sb, 1, k, true, false), sm.e.u.gw.g);
-  for (int e = threadIdx.x; e < k * n; e += NT)
+  for (int e = ltid(); e < k * n; e += NT)
     if ((int)(e % k) >= r.rank) Sb[e] = make_double2(0.0, 0.0);
-  for (int e = threadIdx.x; e < k; e += NT) S[(long long)k * b + e] = w.sig[e];
+  for (int e = ltid(); e < k; e += NT) S[(long long)k * b + e] = w.sig[e];
 }
 
 __global__ void __launch_bounds__(NT, 1) qr_kernel(int m, int n, const cplx* M, cplx* Q, cplx* R, cplx* work) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
+  CompSmem& sm = *reinterpret_cast<CompSmem*>(align_smem_1024(smraw));
   const int b = blockIdx.x;
   const int k = min(m, n);
   cplx* H = work + (long long)m * n * b;
   cta_copy(H, M + (long long)m * n * b, (long long)m * n);
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(H, m, n, sm.la, sm.e.r);
   dev_qr_formq(H, m, n, Q + (long long)m * k * b, sm.la);
   dev_qr_extract_r(H, m, n, R + (long long)k * n * b);
@@ -221,7 +97,7 @@ __global__ void __launch_bounds__(NT, 1) expm_kernel(int chil, int D, int chir, 
                                                      cplx* work, long long wstride, int* matvecs, int heff_only,
                                                      cplx* out) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  CompSmem& sm = *reinterpret_cast<CompSmem*>(smraw);
+  CompSmem& sm = *reinterpret_cast<CompSmem*>(align_smem_1024(smraw));
   const int b = blockIdx.x;
   const long long n = (long long)chil * D * chir;
   const long long tsz = (long long)chil * chir * max(wl, wr) * D;
@@ -244,7 +120,7 @@ __global__ void __launch_bounds__(NT, 1) expm_kernel(int chil, int D, int chir, 
     return;
   }
   int mv = dev_expm_krylov(h, xb, dt, kc, Q, n, sm.e);
-  if (threadIdx.x == 0) matvecs[b] = mv;
+  if (ltid() == 0) matvecs[b] = mv;
 }
 
 // Shared memory of a kernel that runs tc_gemm: the pipeline buffers and
@@ -253,11 +129,6 @@ struct CgemmSmem {
   TcSmem t;
   TcState st;
 };
-__device__ __forceinline__ unsigned char* align_smem_1024(unsigned char* p) {
-  const unsigned off = smem_u32(p);
-  return p + ((1024u - (off & 1023u)) & 1023u);
-}
-
 // One complex FP32 product per CTA on the tensor cores (tcgen05 + TMA).
 __global__ void __launch_bounds__(NT, 1) cgemm_tc_kernel(int M, int N, int K, const CUtensorMap* maps, int a_mn,
                                                          int conj_a, int b_mn, int conj_b, float2* C, int* status) {
@@ -267,13 +138,13 @@ __global__ void __launch_bounds__(NT, 1) cgemm_tc_kernel(int M, int N, int K, co
   const TcOp A{maps + 2 * blockIdx.x, a_mn, conj_a};
   const TcOp B{maps + 2 * blockIdx.x + 1, b_mn, conj_b};
   const bool ok = tc_gemm<float2>(M, N, K, A, B, C + (long long)M * N * blockIdx.x, 1, M, false, sm.t, sm.st);
-  if (threadIdx.x == 0) status[blockIdx.x] = ok ? 0 : 1;
+  if (ltid() == 0) status[blockIdx.x] = ok ? 0 : 1;
   tc_teardown(sm.st);
 }
 
 // FP64 FMA throughput probe: 8 independent chains per thread.
 __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
-  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  double x0 = ltid(), x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
   for (int i = 0; i < iters; ++i) {
     x0 = fma(x0, a, b);
     x1 = fma(x1, a, b);
@@ -656,7 +527,8 @@ bool has_long_range(const yaqs_noise_desc* noise, int nprocs) {
   return false;
 }
 
-WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, bool mixed, bool lr = false) {
+WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, bool mixed, bool lr = false,
+                     bool tc = false) {
   const long long tmp = 4LL * c.capmax * c.capmax + 16;
   WsLayout lay;
   long long off = 0;
@@ -694,6 +566,24 @@ WsLayout plan_layout(int L, const Caps& c, const int* w, bool analog, int kdim, 
   lay.T1f = takef(c.t_size);
   lay.T2f = takef(c.t_size);
   lay.Af = takef(amax);
+  // tcgen05 operands of the H_eff products (rows x pitch complex FP32 each;
+  // even pitches keep every staged row on a 16-byte boundary)
+  int wmax = 1;
+  for (int b = 0; b <= L; ++b) wmax = std::max(wmax, w[b]);
+  auto even = [](long long v) { return (int)((v + 1) & ~1LL); };
+  lay.pL = even((long long)c.capmax * wmax);
+  lay.rL = c.capmax;
+  lay.px = even(c.capmax);
+  lay.rx = 4 * c.capmax;
+  lay.pT2 = even(4LL * c.capmax);
+  lay.rT2 = wmax * c.capmax;
+  lay.pR = even(c.capmax);
+  lay.rR = wmax * c.capmax;
+  const bool st = mf && tc;
+  lay.sL = takef(st ? (long long)lay.pL * lay.rL : 0);
+  lay.sx = takef(st ? (long long)lay.px * lay.rx : 0);
+  lay.sT2 = takef(st ? (long long)lay.pT2 * lay.rT2 : 0);
+  lay.sR = takef(st ? (long long)lay.pR * lay.rR : 0);
   const long long big = lr ? 8LL * c.capmax * c.capmax + 16 : 0, small = lr ? tmp : 0;
   lay.lrQ = take(lr ? 4 * c.mps_size : 0);
   lay.lrPhi = take(big);
@@ -756,6 +646,7 @@ struct yaqs_run {
     if (d_prof) {
       unsigned long long* z = nullptr;
       cudaMemcpyToSymbol(g_prof, &z, sizeof(z));
+      tc_set_prof(nullptr);
     }
     if (stream) cudaStreamSynchronize(stream);
     if (e0) cudaEventDestroy(e0);
@@ -878,6 +769,7 @@ static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, 
     CUDA_TRY(ctx, dm.alloc(&run->d_prof, (size_t)slots * PROF_N));
     CUDA_TRY(ctx, cudaMemset(run->d_prof, 0, (size_t)slots * PROF_N * sizeof(unsigned long long)));
     CUDA_TRY(ctx, cudaMemcpyToSymbol(g_prof, &run->d_prof, sizeof(run->d_prof)));
+    CUDA_TRY(ctx, tc_set_prof(run->d_prof));  // the tensor-core kernel's translation unit
   }
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&run->e0));
@@ -1038,7 +930,12 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   if (!plan_caps(L, chi0.data(), w.data(), cfg->max_bond_dim, caps))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "bond dimension above 128 is not served");
   const bool mixed = cfg->precision == YAQS_PREC_MIXED;
-  const WsLayout lay = plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed, has_long_range(noise, nprocs));
+  // the mixed H_eff products run on tcgen05 in direct runs (the tensor-core
+  // kernel, engine_tc.cu); server slots are shared by runs of different
+  // shapes and keep the mma.sync form
+  const bool use_tc = mixed && !pool;
+  const WsLayout lay =
+      plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed, has_long_range(noise, nprocs), use_tc);
   const std::vector<int>& cap = caps.cap;
   const std::vector<long long>& mps_off = caps.mps_off;
   const std::vector<long long>& env_off = caps.env_off;
@@ -1072,10 +969,15 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   // ---- slots and memory admission ----
   const int num_traj = cfg->num_traj;
   const int ncols = cfg->sample_timesteps ? cfg->n_times : 1;
-  const size_t smem = sizeof(CtaSmem);
-  CUDA_TRY(ctx, cudaFuncSetAttribute(tjm_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  size_t smem = cta_smem_bytes();
   int per_sm = 0;
-  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tjm_step_kernel, NT, smem));
+  if (use_tc) {  // two programs per 512-thread CTA
+    CUDA_TRY(ctx, tc_kernel_prepare(smem, &per_sm, &smem));
+    per_sm = std::min(per_sm, TMEM_PROGRAMS_PER_SM);
+  } else {
+    CUDA_TRY(ctx, cudaFuncSetAttribute(tjm_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tjm_step_kernel, NT, smem));
+  }
   if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
   if (pool && (lay.total > pool->ws_stride || lay.itotal > pool->wsi_stride))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "the request's workspace exceeds the server's slot shape");
@@ -1090,6 +992,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
     return set_err(ctx, YAQS_E_OOM, "trajectory states do not fit in device memory");
   int slots = std::min(num_traj, ctx->sms * per_sm);
   while (slots > 1 && fixed + (size_t)num_traj * per_traj + (size_t)slots * per_slot > budget) --slots;
+  if (use_tc) slots = (slots + 1) & ~1;  // whole CTAs of two programs
   if (pool) slots = pool->slots;
 
   yaqs_run* run = new yaqs_run();
@@ -1102,6 +1005,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   P.n_times = cfg->n_times;
   P.order = cfg->order;
   P.mixed = mixed ? 1 : 0;
+  P.tc = use_tc ? 1 : 0;
   P.tdvp_mode = cfg->tdvp_mode;
   P.sample_ts = cfg->sample_timesteps != 0;
   P.max_bond = cfg->max_bond_dim;
@@ -1130,6 +1034,22 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   run->ncols = ncols;
   int st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, cfg->n_times, pool);
   if (st != YAQS_OK) return st;
+  if (use_tc) {  // four tensor maps per slot over its staged operands
+    std::vector<CUtensorMap> maps(4 * (size_t)slots);
+    for (int sl = 0; sl < slots; ++sl) {
+      const cplx* base = P.ws + (long long)sl * P.lay.total;
+      const WsLayout& y = P.lay;
+      if (!make_tc_map(&maps[4 * sl + 0], base + y.sL, y.pL, y.rL, TC_A_MN) ||
+          !make_tc_map(&maps[4 * sl + 1], base + y.sx, y.px, y.rx, TC_B_K) ||
+          !make_tc_map(&maps[4 * sl + 2], base + y.sT2, y.pT2, y.rT2, TC_A_MN) ||
+          !make_tc_map(&maps[4 * sl + 3], base + y.sR, y.pR, y.rR, TC_B_MN))
+        return set_err(ctx, YAQS_E_CUDA, "cuTensorMapEncodeTiled refused a staged H_eff operand");
+    }
+    CUtensorMap* d_maps;
+    CUDA_TRY(ctx, dm.alloc(&d_maps, maps.size()));
+    CUDA_TRY(ctx, cudaMemcpy(d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    P.tmaps = d_maps;
+  }
   std::vector<WMat> views;
   st = upload_wmats(ctx, dm, all, views);
   if (st != YAQS_OK) return st;
@@ -1316,7 +1236,10 @@ int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms) {
     if (run->digital)
       digital_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, run->D, first, cnt);
     else
-      tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, first, cnt);
+      if (run->P.tc)
+        CUDA_TRY(ctx, tc_kernel_launch(run->slots, run->smem, run->stream, run->P, first, cnt));
+      else
+        tjm_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, first, cnt);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return set_err(ctx, YAQS_E_CUDA, std::string("launch: ") + cudaGetErrorString(le));
   }
@@ -1511,7 +1434,7 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   const int num_traj = cfg->num_traj;
   const int ncols = C.n_samples;
   const int n_layers = (int)C.layers.size();
-  const size_t smem = sizeof(CtaSmem);
+  const size_t smem = cta_smem_bytes();
   CUDA_TRY(ctx, cudaFuncSetAttribute(digital_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, digital_step_kernel, NT, smem));
@@ -1695,7 +1618,7 @@ int yaqs_batched_svd(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const d
   CUDA_TRY(ctx, dm.alloc(&dw, (size_t)batch * wstride));
   CUDA_TRY(ctx, dm.alloc(&di, (size_t)batch * SVD_MAX_COLS));
   CUDA_TRY(ctx, cudaMemcpy(dM, M, (size_t)batch * m * n * sizeof(cplx), cudaMemcpyHostToDevice));
-  const size_t smem = sizeof(CompSmem);
+  const size_t smem = sizeof(CompSmem) + 1024;
   CUDA_TRY(ctx, cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   svd_kernel<<<batch, NT, smem>>>(m, n, dM, dU, dS, dVt, dw, wstride, di);
   CUDA_TRY(ctx, cudaGetLastError());
@@ -1733,7 +1656,7 @@ static cudaError_t noalloc_prepare(int device) {
   void* p = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CompSmem));
+  e = cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(CompSmem) + 1024));
   if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> g(g_noalloc_mu);
   g_noalloc_base[device] = p;
@@ -1757,7 +1680,7 @@ int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n,
                    "yaqs_batched_svd_noalloc; use fewer or smaller problems per call");
   std::lock_guard<std::mutex> lk(ctx->mu);
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
-  const size_t smem = sizeof(CompSmem);
+  const size_t smem = sizeof(CompSmem) + 1024;
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
@@ -1815,7 +1738,7 @@ int yaqs_batched_qr(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const do
   CUDA_TRY(ctx, dm.alloc(&dR, (size_t)batch * k * n));
   CUDA_TRY(ctx, dm.alloc(&dw, (size_t)batch * m * n));
   CUDA_TRY(ctx, cudaMemcpy(dM, M, (size_t)batch * m * n * sizeof(cplx), cudaMemcpyHostToDevice));
-  const size_t smem = sizeof(CompSmem);
+  const size_t smem = sizeof(CompSmem) + 1024;
   CUDA_TRY(ctx, cudaFuncSetAttribute(qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   qr_kernel<<<batch, NT, smem>>>(m, n, dM, dQ, dR, dw);
   CUDA_TRY(ctx, cudaGetLastError());
@@ -1860,7 +1783,7 @@ static int expm_common(yaqs_ctx* ctx, int32_t batch, int32_t chil, int32_t D, in
   kc.kdim = kdim;
   kc.tol = tol;
   kc.exit_tol = exit_tol;
-  const size_t smem = sizeof(CompSmem);
+  const size_t smem = sizeof(CompSmem) + 1024;
   CUDA_TRY(ctx, cudaFuncSetAttribute(expm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   expm_kernel<<<batch, NT, smem>>>(chil, D, chir, wl, wr, dL, dR, views[0], dx, dt, kc, dw, wstride, dmv, heff_only,
                                    dout);

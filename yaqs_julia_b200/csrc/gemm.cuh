@@ -24,14 +24,14 @@ struct GemmSmem {
   cplx Bs[2][GBK][GBN + 1];
 };
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+static __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   const int sz = valid ? 16 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+static __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 struct GemmArgs {
   int M, N, K;
@@ -44,7 +44,7 @@ struct GemmArgs {
   bool conjA, conjB, accumulate;
 };
 
-__device__ __forceinline__ GemmArgs gemm_args(int M, int N, int K, const cplx* A, long long am, long long ak,
+static __device__ __forceinline__ GemmArgs gemm_args(int M, int N, int K, const cplx* A, long long am, long long ak,
                                               const cplx* B, long long bk, long long bn, cplx* C, long long cm,
                                               long long cn, bool conjA = false, bool conjB = false,
                                               bool accumulate = false) {
@@ -70,22 +70,22 @@ __device__ __forceinline__ GemmArgs gemm_args(int M, int N, int K, const cplx* A
 // FP64 tensor-core product: D (8x8) += A (8x4, row) * B (4x8, col).
 // Fragments (per lane, g = lane/4, t = lane%4): A[g][t], B[t][g],
 // D[g][2t], D[g][2t+1].
-__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+static __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
 }
 
-// CTA-collective.  Ends with a __syncthreads() so C is visible to all.
+// CTA-collective.  Ends with a cta_sync() so C is visible to all.
 // Complex products run on the FP64 tensor cores (mma.sync m8n8k4): each of
 // the 8 warps owns a 32x16 complex sub-tile of the 64x64 CTA tile as 4x2
 // blocks of 8x8, each block accumulating re and im with four real MMAs.
 // Conjugation is a template parameter (a sign flip of the imaginary
 // fragment).
 template <bool CA, bool CB, int BK>
-__device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
+static __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   ProfScope prof_scope_(PF_GEMM);
-  const int tid = threadIdx.x;
+  const int tid = ltid();
   const int lane = tid & 31, wid = tid >> 5;
   const int wm = wid & 1, wn = wid >> 1;  // 2 x 4 warps
   const int gq = lane >> 2, tq = lane & 3;
@@ -129,7 +129,7 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
         }
         cp_async_commit();
       };
-      __syncthreads();
+      cta_sync();
       issue(0, 0);
       for (int kc = 0; kc < nk; ++kc) {
         const int buf = kc & 1;
@@ -139,7 +139,7 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
         } else {
           cp_async_wait_all();
         }
-        __syncthreads();
+        cta_sync();
 #pragma unroll
         for (int k4 = 0; k4 < BK; k4 += 4) {
           double ar[4], ai[4], br[2], bi[2];
@@ -165,7 +165,7 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
               dmma884(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
             }
         }
-        __syncthreads();
+        cta_sync();
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -185,13 +185,13 @@ __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
       }
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // K slices 16 deep for long reductions, 8 deep for short ones (a short K
 // would otherwise stage mostly zero padding).
 template <int BK>
-__device__ __forceinline__ void cta_gemm_k(const GemmArgs g, GemmSmem& sm) {
+static __device__ __forceinline__ void cta_gemm_k(const GemmArgs g, GemmSmem& sm) {
   if (g.conjA) {
     if (g.conjB) cta_gemm_t<true, true, BK>(g, sm);
     else cta_gemm_t<true, false, BK>(g, sm);
@@ -201,7 +201,7 @@ __device__ __forceinline__ void cta_gemm_k(const GemmArgs g, GemmSmem& sm) {
   }
 }
 
-__device__ __forceinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
+static __device__ __forceinline__ void cta_gemm(const GemmArgs g, GemmSmem& sm) {
   if (g.K >= 32)
     cta_gemm_k<GBK>(g, sm);
   else

@@ -39,7 +39,7 @@ struct GemmArgsF {
   bool conjA, conjB, accumulate;
 };
 
-__device__ __forceinline__ GemmArgsF gemm_args_f(int M, int N, int K, const cflt* A, long long am, long long ak,
+static __device__ __forceinline__ GemmArgsF gemm_args_f(int M, int N, int K, const cflt* A, long long am, long long ak,
                                                  const cflt* B, long long bk, long long bn, void* C, long long cm,
                                                  long long cn, bool conjA = false, bool conjB = false,
                                                  bool accumulate = false) {
@@ -62,19 +62,19 @@ __device__ __forceinline__ GemmArgsF gemm_args_f(int M, int N, int K, const cflt
   return g;
 }
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+static __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   const int sz = valid ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz) : "memory");
 }
 
-__device__ __forceinline__ unsigned to_tf32(float x) {
+static __device__ __forceinline__ unsigned to_tf32(float x) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return r;
 }
 
-__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+static __device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
   hi = to_tf32(x);
   lo = to_tf32(x - __uint_as_float(hi));
 }
@@ -82,7 +82,7 @@ __device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) 
 // D (16x8) += A (16x8, row) * B (8x8, col).  Fragments (g = lane/4,
 // t = lane%4): a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]},
 // b = {B[t][g], B[t+4][g]}, d = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}.
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+static __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
   asm volatile(
       "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
       "{%0, %1, %2, %3};\n"
@@ -91,14 +91,14 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], 
 }
 
 // d += x * y with the 3xTF32 split (small terms first).
-__device__ __forceinline__ void mma3(float (&d)[4], const unsigned (&xh)[4], const unsigned (&xl)[4],
+static __device__ __forceinline__ void mma3(float (&d)[4], const unsigned (&xh)[4], const unsigned (&xl)[4],
                                      const unsigned (&yh)[2], const unsigned (&yl)[2]) {
   mma_tf32(d, xl, yh);
   mma_tf32(d, xh, yl);
   mma_tf32(d, xh, yh);
 }
 
-__device__ __forceinline__ void store_c(cflt* c, float re, float im, bool acc) {
+static __device__ __forceinline__ void store_c(cflt* c, float re, float im, bool acc) {
   if (acc) {
     cflt o = *c;
     re += o.x;
@@ -106,7 +106,7 @@ __device__ __forceinline__ void store_c(cflt* c, float re, float im, bool acc) {
   }
   *c = make_float2(re, im);
 }
-__device__ __forceinline__ void store_c(cplx* c, float re, float im, bool acc) {
+static __device__ __forceinline__ void store_c(cplx* c, float re, float im, bool acc) {
   double r = re, i = im;
   if (acc) {
     cplx o = *c;
@@ -116,11 +116,11 @@ __device__ __forceinline__ void store_c(cplx* c, float re, float im, bool acc) {
   *c = make_double2(r, i);
 }
 
-// CTA-collective.  Ends with a __syncthreads() so C is visible to all.
+// CTA-collective.  Ends with a cta_sync() so C is visible to all.
 template <bool CA, bool CB, class TC>
-__device__ __noinline__ void cta_gemm_tf32_t(const GemmArgsF g, GemmSmemF& sm) {
+static __device__ __noinline__ void cta_gemm_tf32_t(const GemmArgsF g, GemmSmemF& sm) {
   ProfScope prof_scope_(PF_GEMM);
-  const int tid = threadIdx.x;
+  const int tid = ltid();
   const int lane = tid & 31, wid = tid >> 5;
   const int wm = wid & 1, wn = wid >> 1;  // 2 x 4 warps
   const int gq = lane >> 2, tq = lane & 3;
@@ -165,7 +165,7 @@ __device__ __noinline__ void cta_gemm_tf32_t(const GemmArgsF g, GemmSmemF& sm) {
         }
         cp_async_commit();
       };
-      __syncthreads();
+      cta_sync();
       issue(0, 0);
       for (int kc = 0; kc < nk; ++kc) {
         const int buf = kc & 1;
@@ -175,7 +175,7 @@ __device__ __noinline__ void cta_gemm_tf32_t(const GemmArgsF g, GemmSmemF& sm) {
         } else {
           cp_async_wait_all();
         }
-        __syncthreads();
+        cta_sync();
         unsigned arh[2][4], arl[2][4], aih[2][4], ail[2][4];
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
@@ -214,7 +214,7 @@ __device__ __noinline__ void cta_gemm_tf32_t(const GemmArgsF g, GemmSmemF& sm) {
             mma3(ci[i][j], aih[i], ail[i], brh[j], brl[j]);
           }
         }
-        __syncthreads();
+        cta_sync();
       }
 #pragma unroll
       for (int i = 0; i < 2; ++i)
@@ -229,11 +229,11 @@ __device__ __noinline__ void cta_gemm_tf32_t(const GemmArgsF g, GemmSmemF& sm) {
           }
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 template <class TC>
-__device__ __forceinline__ void cta_gemm_tf32(const GemmArgsF g, GemmSmemF& sm) {
+static __device__ __forceinline__ void cta_gemm_tf32(const GemmArgsF g, GemmSmemF& sm) {
   if (g.conjA) {
     if (g.conjB) cta_gemm_tf32_t<true, true, TC>(g, sm);
     else cta_gemm_tf32_t<true, false, TC>(g, sm);
@@ -244,10 +244,10 @@ __device__ __forceinline__ void cta_gemm_tf32(const GemmArgsF g, GemmSmemF& sm) 
 }
 
 // FP64 -> FP32 conversion of n complex values.  CTA-collective.
-__device__ __forceinline__ void cta_to_f32(cflt* __restrict__ dst, const cplx* __restrict__ src, long long n) {
-  for (long long i = threadIdx.x; i < n; i += NT) {
+static __device__ __forceinline__ void cta_to_f32(cflt* __restrict__ dst, const cplx* __restrict__ src, long long n) {
+  for (long long i = ltid(); i < n; i += NT) {
     const cplx v = src[i];
     dst[i] = make_float2((float)v.x, (float)v.y);
   }
-  __syncthreads();
+  cta_sync();
 }

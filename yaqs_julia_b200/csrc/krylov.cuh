@@ -13,6 +13,7 @@
 #pragma once
 #include "common.cuh"
 #include "gemm_tf32.cuh"
+#include "tcgemm.cuh"
 
 #define WAPPLY_IN_CPLX 2560  // staged inputs: ni x PT values, PT = 256, 128 or 64 by what fits
 #define WAPPLY_MAXI 32
@@ -53,23 +54,23 @@ struct WApplySmem {
 // back to back.  T is cplx (FP64 form) or float2 (mixed form, FP32 products).
 // in and out may be the same buffer when every pair's inputs and outputs
 // occupy the same addresses (a tile reads all its inputs before it writes).
-__device__ __forceinline__ void wfma(cplx& acc, cplx v, cplx x) { cfma(acc, v, x); }
-__device__ __forceinline__ void wfma(float2& acc, cplx v, float2 x) {
+static __device__ __forceinline__ void wfma(cplx& acc, cplx v, cplx x) { cfma(acc, v, x); }
+static __device__ __forceinline__ void wfma(float2& acc, cplx v, float2 x) {
   const float vr = (float)v.x, vi = (float)v.y;
   acc.x = fmaf(vr, x.x, fmaf(-vi, x.y, acc.x));
   acc.y = fmaf(vr, x.y, fmaf(vi, x.x, acc.y));
 }
-__device__ __forceinline__ void wzero(cplx& z) { z = make_double2(0.0, 0.0); }
-__device__ __forceinline__ void wzero(float2& z) { z = make_float2(0.f, 0.f); }
+static __device__ __forceinline__ void wzero(cplx& z) { z = make_double2(0.0, 0.0); }
+static __device__ __forceinline__ void wzero(float2& z) { z = make_float2(0.f, 0.f); }
 
 template <class T>
-__device__ __noinline__ void dev_wapply(const T* in, T* out, const WMat W,
+static __device__ __noinline__ void dev_wapply(const T* in, T* out, const WMat W,
                                         const WApplyGeom g, WApplySmem& ws) {
   ProfScope prof_scope_(PF_WAPPLY);
   T* sin = reinterpret_cast<T*>(&ws.in[0]);
   const int cap = (int)(WAPPLY_IN_CPLX * sizeof(cplx) / sizeof(T));
   const int PT = W.ni * NT <= cap ? NT : (W.ni * (NT / 2) <= cap ? NT / 2 : NT / 4);
-  const int tid = threadIdx.x;
+  const int tid = ltid();
   for (int e = tid; e < W.nnz; e += NT) {
     ws.val[e] = W.val[e];
     ws.col[e] = W.col[e];
@@ -87,9 +88,9 @@ __device__ __noinline__ void dev_wapply(const T* in, T* out, const WMat W,
     const bool live = pair < npair;
     const int q0 = live ? pair % g.n0 : 0, q1 = live ? pair / g.n0 : 0;
     const long long ib = q0 * g.is0 + q1 * g.is1, ob = q0 * g.os0 + q1 * g.os1;
-    __syncthreads();
+    cta_sync();
     for (int i = r0; i < W.ni; i += RS) sin[i * PT + pl] = live ? in[ib + ws.in_off[i]] : zero;
-    __syncthreads();
+    cta_sync();
     if (live) {
       for (int o = r0; o < W.no; o += RS) {
         T acc = zero;
@@ -98,7 +99,7 @@ __device__ __noinline__ void dev_wapply(const T* in, T* out, const WMat W,
       }
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 struct HeffOp {
@@ -115,6 +116,16 @@ struct HeffOp {
   cflt* xf = nullptr;
   cflt* T1f = nullptr;
   cflt* T2f = nullptr;
+  // mixed form on tcgen05 (tc = 1): TMA-staged operands of the two products,
+  // tensor maps maps[0..3] = SL (A, MN-major), Sx (B, K-major), ST2 (A,
+  // MN-major), SR (B, MN-major); pitches in complex FP32 values
+  int tc = 0;
+  const CUtensorMap* maps = nullptr;
+  cflt* SL = nullptr;
+  cflt* Sx = nullptr;
+  cflt* ST2 = nullptr;
+  cflt* SR = nullptr;
+  int pL = 0, px = 0, pT2 = 0, pR = 0;
 };
 
 struct KrySmem {
@@ -128,23 +139,75 @@ struct KrySmem {
 // Shared memory of one CTA.  The GEMM / MPO-apply staging and the SVD block
 // buffer are never live at the same time and share storage.
 #define SVD_SMEM_CPLX_K 4096
+union EngineSmemU {
+  union {  // the GEMM and the MPO apply run one after the other, never together
+    GemmSmem g;
+    WApplySmem w;
+  } gw;
+  cplx svd[SVD_SMEM_CPLX_K];
+  TcSmem t;  // the tensor-core pipeline (mixed form), no larger than the GEMM staging
+};
 struct EngineSmem {
-  union {
-    union {  // the GEMM and the MPO apply run one after the other, never together
-      GemmSmem g;
-      WApplySmem w;
-    } gw;
-    cplx svd[SVD_SMEM_CPLX_K];
-  } u;
   RedScratch r;
   KrySmem k;
+  TcState tc;
+  EngineSmemU u;
 };
+static_assert(sizeof(TcSmem) <= sizeof(GemmSmem), "the tensor-core pipeline must not grow the CTA's shared memory");
+
+#if YAQS_TC
+// Mixed form on tcgen05 (compiled only into the tensor-core kernel,
+// engine_tc.cu: a kernel that contains tcgen05 code is given one CTA per
+// SM).  x is staged as the K-major B operand of the first product, the MPO
+// apply writes T2 straight into the MN-major A operand of the second
+// product, and both products run in tc_gemm; the environments were staged
+// once per Krylov solve.
+static __device__ void dev_heff_tc(const HeffOp& h, const cplx* x, cplx* y, EngineSmem& sm) {
+  const int chil = h.chil, D = h.D, chir = h.chir, wl = h.wl, wr = h.wr;
+  const long long n = (long long)chil * D * chir;
+  for (long long e = ltid(); e < n; e += NT) {  // Sx[nn px + k] = x[k + chil nn]
+    const cplx v = x[e];
+    const long long k = e % chil, nn = e / chil;
+    h.Sx[nn * h.px + k] = make_float2((float)v.x, (float)v.y);
+  }
+  const TcOp A1{h.maps + 0, 1, 0}, B1{h.maps + 1, 0, 0}, A2{h.maps + 2, 1, 0}, B2{h.maps + 3, 1, 0};
+  tc_gemm<cflt>(chil * wl, D * chir, chil, A1, B1, h.T1f, 1, (long long)chil * wl, false, sm.u.t, sm.tc);
+  if (h.W.ident) {  // bond (D = 1, wl = wr): T2 is T1 re-laid into ST2
+    for (long long e = ltid(); e < (long long)chil * wl * chir; e += NT) {
+      const long long a = e % chil, m = (e / chil) % wl, c = e / ((long long)chil * wl);
+      h.ST2[(m + (long long)wr * c) * h.pT2 + a] = h.T1f[e];
+    }
+  } else {
+    WApplyGeom g;
+    g.n0 = chil;
+    g.n1 = chir;
+    g.is0 = 1;
+    g.is1 = (long long)chil * wl * D;
+    g.ni1 = wl;
+    g.ii1 = chil;
+    g.ii2 = (long long)chil * wl;
+    g.os0 = 1;                      // a
+    g.os1 = (long long)h.pT2 * wr;  // c: rows m' + wr c of ST2
+    g.no1 = D;
+    g.oo1 = chil;   // p'
+    g.oo2 = h.pT2;  // m'
+    dev_wapply<cflt>(h.T1f, h.ST2, h.W, g, sm.u.gw.w);
+  }
+  tc_gemm<cplx>(chil * D, chir, wr * chir, A2, B2, y, 1, (long long)chil * D, false, sm.u.t, sm.tc);
+}
+#endif
 
 // y = H_eff x.  CTA-collective.  In the mixed form x is rounded to FP32, the
 // three contractions run in FP32 (tensor cores for the two GEMMs) and y is
 // written back in FP64.
-__device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, EngineSmem& sm) {
+static __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, EngineSmem& sm) {
   const int chil = h.chil, D = h.D, chir = h.chir, wl = h.wl, wr = h.wr;
+#if YAQS_TC
+  if (h.tc) {
+    dev_heff_tc(h, x, y, sm);
+    return;
+  }
+#endif
   if (h.mixed) {
     GemmSmemF& gf = reinterpret_cast<GemmSmemF&>(sm.u.gw.g);
     cta_to_f32(h.xf, x, (long long)chil * D * chir);
@@ -197,7 +260,7 @@ __device__ __noinline__ void dev_heff(const HeffOp& h, const cplx* x, cplx* y, E
   }
 }
 
-__device__ __forceinline__ double heff_flops(int chil, int wl, int D, int chir, int wr) {
+static __device__ __forceinline__ double heff_flops(int chil, int wl, int D, int chir, int wr) {
   return 8.0 * ((double)chil * chil * wl * D * chir + (double)chil * chir * D * D * wl * wr +
                 (double)chil * D * chir * chir * wr);
 }
@@ -209,10 +272,10 @@ struct KrylovCfg {
 };
 
 // Warp 0: y = exp(-i dt T) e_1 for the m x m Lanczos matrix in ks.
-__device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
+static __device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
   ProfScope prof_scope_(PF_TRIDIAG);
-  if (threadIdx.x >= 32) return;
-  const int j = threadIdx.x;
+  if (ltid() >= 32) return;
+  const int j = ltid();
   const bool on = j < m;
   const double a = on ? ks.alpha[j] : 0.0;
   const double bl = (on && j > 0) ? ks.beta[j - 1] : 0.0;
@@ -245,8 +308,8 @@ __device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
 
 // h_j = <q_j, w> (j < k) into ks.h and |w|^2 in the same pass over w: the
 // first group takes seven vectors and the norm, later groups eight.
-__device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w, long long n, int k, EngineSmem& sm) {
-  const int tid = threadIdx.x;
+static __device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w, long long n, int k, EngineSmem& sm) {
+  const int tid = ltid();
   double nw2 = 0.0;
   for (int j0 = 0, first = 1; j0 < k || first; first = 0) {
     const int G = first ? 7 : 8;
@@ -275,22 +338,22 @@ __device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w, long 
     if (first) nw2 = d[15];
     j0 += G;
   }
-  __syncthreads();
+  cta_sync();
   return nw2;
 }
 
 // w <- w - sum_j h_j q_j (j < k); with norm, returns |w|^2 after the update.
-__device__ double lanczos_subtract(const cplx* Q, long long qs, cplx* w, long long n, int k, EngineSmem& sm,
+static __device__ double lanczos_subtract(const cplx* Q, long long qs, cplx* w, long long n, int k, EngineSmem& sm,
                                    bool norm) {
   double part = 0.0;
-  for (long long i = threadIdx.x; i < n; i += NT) {
+  for (long long i = ltid(); i < n; i += NT) {
     cplx v = w[i];
     for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
     w[i] = v;
     part += cabs2(v);
   }
   if (!norm) {
-    __syncthreads();
+    cta_sync();
     return 0.0;
   }
   return block_sum(part, sm.r);
@@ -298,15 +361,15 @@ __device__ double lanczos_subtract(const cplx* Q, long long qs, cplx* w, long lo
 
 // In place: x <- exp(-i dt H_eff) x.  Q holds kdim+1 vectors of stride qs.
 // Returns the number of H_eff products.  CTA-collective.
-__device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt, const KrylovCfg& kc, cplx* Q,
+static __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt, const KrylovCfg& kc, cplx* Q,
                                             long long qs, EngineSmem& sm) {
-  const int tid = threadIdx.x;
+  const int tid = ltid();
   const long long n = (long long)h.chil * h.D * h.chir;
   const double beta0 = sqrt(cta_norm2(x, n, sm.r));
   if (beta0 == 0.0) return 0;
   const double tau = fabs(dt);
   for (long long i = tid; i < n; i += NT) Q[i] = cscale(x[i], 1.0 / beta0);
-  __syncthreads();
+  cta_sync();
   double bound = 1.0;
   int m = 0;
   int mv = 0;
@@ -352,16 +415,16 @@ __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, double dt,
     } else {
       for (long long i = tid; i < n; i += NT) w[i] = cscale(w[i], inv);
     }
-    __syncthreads();
+    cta_sync();
   }
-  __syncthreads();
+  cta_sync();
   dev_tridiag_expm(m, dt, sm.k);
-  __syncthreads();
+  cta_sync();
   for (long long i = tid; i < n; i += NT) {
     cplx v = make_double2(0.0, 0.0);
     for (int j = 0; j < m; ++j) cfma(v, sm.k.y[j], Q[qs * j + i]);
     x[i] = cscale(v, beta0);
   }
-  __syncthreads();
+  cta_sync();
   return mv;
 }

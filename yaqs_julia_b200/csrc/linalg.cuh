@@ -31,9 +31,9 @@ struct LinalgSmem {
 // ---------------------------------------------------------------------------
 // Factor H (m x n, col-major, ld m) in place: R in the upper triangle,
 // reflector vectors below, scalars in ls.tau.  CTA-collective.
-__device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls, RedScratch& rs) {
+static __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls, RedScratch& rs) {
   ProfScope prof_scope_(PF_QR);
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = ltid(), lane = tid & 31, wid = tid >> 5;
   const int kq = min(m, n);
   double fro2 = cta_norm2(H, (long long)m * n, rs);
   const double null_abs = QR_NULL_TOL * sqrt(fro2);
@@ -44,11 +44,11 @@ __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls
     const double xn2 = block_sum(s, rs);
     const cplx alpha = col[j];
     const double full = sqrt(cabs2(alpha) + xn2);
-    __syncthreads();
+    cta_sync();
     if (full <= null_abs || (xn2 == 0.0 && alpha.y == 0.0)) {
       for (int i = j + 1 + tid; i < m; i += NT) col[i] = make_double2(0.0, 0.0);
       if (tid == 0) ls.tau[j] = make_double2(0.0, 0.0);
-      __syncthreads();
+      cta_sync();
       continue;
     }
     const double beta = (alpha.x >= 0.0) ? -full : full;
@@ -57,7 +57,7 @@ __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls
     const double d = cabs2(amb);
     const cplx scale = make_double2(amb.x / d, -amb.y / d);
     for (int i = j + 1 + tid; i < m; i += NT) col[i] = cmul(col[i], scale);
-    __syncthreads();
+    cta_sync();
     if (tid == 0) {
       col[j] = make_double2(beta, 0.0);
       ls.tau[j] = t;
@@ -125,20 +125,20 @@ __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgSmem& ls
         if (lane == 0) x[j] = csub(x[j], acc);
       }
     }
-    __syncthreads();
+    cta_sync();
   }
 }
 
 // Q (m x kq) of a factored H.  CTA-collective.
-__device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, LinalgSmem& ls) {
+static __device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, LinalgSmem& ls) {
   ProfScope prof_scope_(PF_QRQ);
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = ltid(), lane = tid & 31, wid = tid >> 5;
   const int kq = min(m, n);
   for (int e = tid; e < m * kq; e += NT) {
     int r = (int)(e % m), c = (int)(e / m);
     Q[e] = make_double2(r == c ? 1.0 : 0.0, 0.0);
   }
-  __syncthreads();
+  cta_sync();
   for (int j = kq - 1; j >= 0; --j) {
     const cplx t = ls.tau[j];
     if (t.x == 0.0 && t.y == 0.0) continue;
@@ -204,18 +204,18 @@ __device__ __noinline__ void dev_qr_formq(const cplx* H, int m, int n, cplx* Q, 
         if (lane == 0) q[j] = csub(q[j], acc);
       }
     }
-    __syncthreads();
+    cta_sync();
   }
 }
 
 // R (kq x n) of a factored H into Rout (ld kq), zero below the diagonal.
-__device__ __forceinline__ void dev_qr_extract_r(const cplx* H, int m, int n, cplx* Rout) {
+static __device__ __forceinline__ void dev_qr_extract_r(const cplx* H, int m, int n, cplx* Rout) {
   const int kq = min(m, n);
-  for (int e = threadIdx.x; e < kq * n; e += NT) {
+  for (int e = ltid(); e < kq * n; e += NT) {
     int r = (int)(e % kq), c = (int)(e / kq);
     Rout[e] = (r <= c) ? H[r + (long long)m * c] : make_double2(0.0, 0.0);
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -238,10 +238,10 @@ struct SvdResult {
 };
 
 // Orthonormal completion of column k of Y (rows x *) against columns 0..k-1.
-__device__ void dev_complete_column(cplx* Y, int rows, int k, cplx* y, RedScratch& rs) {
+static __device__ void dev_complete_column(cplx* Y, int rows, int k, cplx* y, RedScratch& rs) {
   for (int c = 0; c < rows; ++c) {
     // pass 1: y = e_c - sum_h conj(Y_h[c]) Y_h
-    for (int i = threadIdx.x; i < rows; i += NT) {
+    for (int i = ltid(); i < rows; i += NT) {
       cplx v = make_double2(i == c ? 1.0 : 0.0, 0.0);
       for (int h = 0; h < k; ++h) {
         cplx yc = Y[c + (long long)rows * h];
@@ -250,13 +250,13 @@ __device__ void dev_complete_column(cplx* Y, int rows, int k, cplx* y, RedScratc
       }
       y[i] = v;
     }
-    __syncthreads();
+    cta_sync();
     // pass 2: y -= sum_h (Y_h^H y) Y_h, dot products in chunks of 8
     for (int h0 = 0; h0 < k; h0 += 8) {
       double d[16];
 #pragma unroll
       for (int e = 0; e < 16; ++e) d[e] = 0.0;
-      for (int i = threadIdx.x; i < rows; i += NT) {
+      for (int i = ltid(); i < rows; i += NT) {
         cplx yi = y[i];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -269,19 +269,19 @@ __device__ void dev_complete_column(cplx* Y, int rows, int k, cplx* y, RedScratc
         }
       }
       block_sum_n<16>(d, rs);
-      for (int i = threadIdx.x; i < rows; i += NT) {
+      for (int i = ltid(); i < rows; i += NT) {
         cplx v = y[i];
 #pragma unroll
         for (int e = 0; e < 8; ++e)
           if (h0 + e < k) v = csub(v, cmul(make_double2(d[2 * e], d[2 * e + 1]), Y[i + (long long)rows * (h0 + e)]));
         y[i] = v;
       }
-      __syncthreads();
+      cta_sync();
     }
     double nr = sqrt(cta_norm2(y, rows, rs));
     if (nr > 0.5) {
-      for (int i = threadIdx.x; i < rows; i += NT) Y[i + (long long)rows * k] = cscale(y[i], 1.0 / nr);
-      __syncthreads();
+      for (int i = ltid(); i < rows; i += NT) Y[i + (long long)rows * k] = cscale(y[i], 1.0 / nr);
+      cta_sync();
       return;
     }
   }
@@ -306,7 +306,7 @@ __host__ __device__ __forceinline__ int svd_block_size(int q, int p) {
 // written with fewer dependent divisions/square roots:
 //   t = sign(d) 2|g| / (|d| + sqrt(d^2 + 4|g|^2)),  d = be - al.
 // Returns false when the pair is already orthogonal to tolerance.
-__device__ __forceinline__ bool jacobi_params(double al, double be, double gx, double gy, double tol, double& c,
+static __device__ __forceinline__ bool jacobi_params(double al, double be, double gx, double gy, double tol, double& c,
                                               cplx& se, cplx& sec) {
   const double g2 = gx * gx + gy * gy;
   if (!(g2 > tol * tol * (al * be))) return false;
@@ -328,10 +328,10 @@ __device__ __forceinline__ bool jacobi_params(double al, double be, double gx, d
 // k-th pair as (i, j) local column indices, -1 to skip.  Each half-warp
 // takes one pair.
 template <class PairFn>
-__device__ __forceinline__ void smem_rotate_round(cplx* sb, int ld, int q, int rows, int npairs, PairFn pairs,
+static __device__ __forceinline__ void smem_rotate_round(cplx* sb, int ld, int q, int rows, int npairs, PairFn pairs,
                                                   double tol, int* rot) {
-  const int hl = threadIdx.x & 15, hw = threadIdx.x >> 4;
-  const unsigned mask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  const int hl = ltid() & 15, hw = ltid() >> 4;
+  const unsigned mask = (ltid() & 16) ? 0xffff0000u : 0x0000ffffu;
   for (int k = hw; k < npairs; k += NT / 16) {
     int i, j;
     pairs(k, i, j);
@@ -363,22 +363,22 @@ __device__ __forceinline__ void smem_rotate_round(cplx* sb, int ld, int q, int r
       bj[r] = cadd(cmul(se, x), cscale(y, c));
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // Stage columns [c0, c0+nc0) and [c1, c1+nc1) of B into sb (ld = q), or
 // write them back.
-__device__ __forceinline__ void svd_stage(cplx* sb, int ld, const SvdWork& w, int q, int c0, int nc0, int c1, int nc1,
+static __device__ __forceinline__ void svd_stage(cplx* sb, int ld, const SvdWork& w, int q, int c0, int nc0, int c1, int nc1,
                                           bool store) {
   const int nc = nc0 + nc1;
-  for (int e = threadIdx.x; e < nc * ld; e += NT) {
+  for (int e = ltid(); e < nc * ld; e += NT) {
     int r = (int)(e % ld), lc = (int)(e / ld);
     int col = lc < nc0 ? c0 + lc : c1 + (lc - nc0);
     cplx* g = w.B + (long long)q * col + r;
     if (store) *g = sb[e];
     else sb[e] = *g;
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // SVD of M (m x n, col-major ld m), phase 1.  side LEFT asks for the left
@@ -393,10 +393,10 @@ __device__ __forceinline__ void svd_stage(cplx* sb, int ld, const SvdWork& w, in
 // shared buffer sb (SVD_SMEM_CPLX elements).  Leaves the sorted singular
 // values in w.sig (nulls set to 0).  CTA-collective; returns metadata.
 enum { SVD_LEFT = 0, SVD_RIGHT = 1 };
-__device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side, SvdWork& w, LinalgSmem& ls,
+static __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side, SvdWork& w, LinalgSmem& ls,
                                           RedScratch& rs, cplx* sb) {
   ProfScope prof_scope_(PF_SVD);
-  const int tid = threadIdx.x;
+  const int tid = ltid();
   SvdResult res;
   res.tr = side == SVD_RIGHT;
   const int mm = res.tr ? m : n;  // rows of the factored matrix H
@@ -411,14 +411,14 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
     int r = (int)(e % mm), c = (int)(e / mm);
     H[e] = res.tr ? M[e] : cconj(M[c + (long long)m * r]);
   }
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(H, mm, nn, ls, rs);
   // B = R^H (nn x k): B[r, c] = conj(R[c, r]) for c <= r
   for (int e = tid; e < q * p; e += NT) {
     int r = (int)(e % q), c = (int)(e / q);
     w.B[e] = (c <= r) ? cconj(H[c + (long long)mm * r]) : make_double2(0.0, 0.0);
   }
-  __syncthreads();
+  cta_sync();
   const double tol = 2.220446049250313e-16 * q;
   const int ld = q;
   const int b = svd_block_size(q, p);
@@ -427,7 +427,7 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
   const int be2 = b + (b & 1);
   for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS; ++sweep) {
     if (tid == 0) ls.rot_count = 0;
-    __syncthreads();
+    cta_sync();
     for (int I = 0; I < nb; ++I) {
       const int c0 = I * b, nc = min(b, p - c0);
       svd_stage(sb, ld, w, q, c0, nc, 0, 0, false);
@@ -471,7 +471,7 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
       }
     }
     int rc = ls.rot_count;
-    __syncthreads();
+    cta_sync();
     res.sweeps = sweep + 1;
     if (rc == 0) break;
   }
@@ -484,7 +484,7 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
     s = warp_sum(s);
     if (lane == 0) w.sig[c] = sqrt(s);
   }
-  __syncthreads();
+  cta_sync();
   // stable descending order
   for (int c = tid; c < p; c += NT) {
     double sc = w.sig[c];
@@ -495,7 +495,7 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
     }
     w.ord[rank] = c;
   }
-  __syncthreads();
+  cta_sync();
   const double smax = p > 0 ? w.sig[w.ord[0]] : 0.0;
   // rank of non-null values (sorted prefix)
   int cnt = 0;
@@ -511,31 +511,31 @@ __device__ __noinline__ SvdResult dev_svd(const cplx* M, int m, int n, int side,
     double s = w.sig[w.ord[myk]];
     sk = (smax > 0.0 && s > SVD_NULL_TOL * smax) ? s : 0.0;
   }
-  __syncthreads();
+  cta_sync();
   if (myk < p) w.sig[myk] = sk;
-  __syncthreads();
+  cta_sync();
   return res;
 }
 
 // Phase 2: the requested orthonormal vectors Yo (q x need): column k is
 // B[:, ord[k]] / sigma_k for non-null k and an orthonormal completion for
 // null k < need.  CTA-collective.
-__device__ __noinline__ void dev_svd_vectors(const SvdResult& res, int need, SvdWork& w, RedScratch& rs) {
+static __device__ __noinline__ void dev_svd_vectors(const SvdResult& res, int need, SvdWork& w, RedScratch& rs) {
   ProfScope prof_scope_(PF_SVDVEC);
-  const int tid = threadIdx.x, q = res.q, p = res.p;
+  const int tid = ltid(), q = res.q, p = res.p;
   need = min(need, p);
   const int ng = min(need, res.rank);
   for (int e = tid; e < q * ng; e += NT) {
     int r = (int)(e % q), k = (int)(e / q);
     w.Yo[e] = cscale(w.B[r + (long long)q * w.ord[k]], 1.0 / w.sig[k]);
   }
-  __syncthreads();
+  cta_sync();
   for (int k = res.rank; k < need; ++k) dev_complete_column(w.Yo, q, k, w.y, rs);
 }
 
 // Truncation ranks (see the oracle for the reference lines they restate).
 // split_mps_tensor_svd / two_site_svd: absolute, keep crossing value, min 2.
-__device__ __forceinline__ int keep_tdvp(const double* S, int n, double thr, int max_bond) {
+static __device__ __forceinline__ int keep_tdvp(const double* S, int n, double thr, int max_bond) {
   double disc = 0.0;
   int keep = n;
   for (int k = n; k >= 1; --k) {
@@ -548,7 +548,7 @@ __device__ __forceinline__ int keep_tdvp(const double* S, int n, double thr, int
   return max(1, min(keep, max_bond));
 }
 // Dissipation / jump split: relative, min 1.
-__device__ __forceinline__ int keep_relative(const double* S, int n, double thr, int max_bond) {
+static __device__ __forceinline__ int keep_relative(const double* S, int n, double thr, int max_bond) {
   double nsq = 0.0;
   for (int k = 0; k < n; ++k) nsq += S[k] * S[k];
   double cur = 0.0;
@@ -565,7 +565,7 @@ __device__ __forceinline__ int keep_relative(const double* S, int n, double thr,
 
 // apply_local_gate_exact! (DigitalTJM.jl:282-292): absolute, drop while the
 // running sum plus s^2 stays <= thr, no minimum.
-__device__ __forceinline__ int keep_tebd(const double* S, int n, double thr, int max_bond) {
+static __device__ __forceinline__ int keep_tebd(const double* S, int n, double thr, int max_bond) {
   double cur = 0.0;
   int keep = n;
   for (int k = n; k >= 1; --k) {

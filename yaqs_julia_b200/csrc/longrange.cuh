@@ -30,7 +30,7 @@ struct LrBufs {
   int* bd;  // [L+1] bond dimensions of the operator-applied chain
 };
 
-__device__ __forceinline__ LrBufs lr_bufs(const Ctx& c) {
+static __device__ __forceinline__ LrBufs lr_bufs(const Ctx& c) {
   LrBufs b;
   b.Q = c.ws + c.P.lay.lrQ;
   b.Phi = c.ws + c.P.lay.lrPhi;
@@ -47,14 +47,14 @@ __device__ __forceinline__ LrBufs lr_bufs(const Ctx& c) {
 
 // Right-canonical factor of site k in the lrQ arena (room for twice the
 // state's caps on both bonds).
-__device__ __forceinline__ cplx* lr_qslot(const Ctx& c, const LrBufs& b, int k) {
+static __device__ __forceinline__ cplx* lr_qslot(const Ctx& c, const LrBufs& b, int k) {
   return b.Q + 4 * c.P.mps_off[k];
 }
 
 // Site k of O|psi> as a dense (lo, 2, ro) tensor: the contraction
 // C[la, lw, po, ra, rw] of apply_mpo_jump! with (la, lw) and (ra, rw) merged,
 // la and ra fastest.  A is the state's tensor (l, 2, r).
-__device__ void lr_phi(const DevProc& pr, int k, const cplx* A, int l, int r, cplx* out, int& lo, int& ro) {
+static __device__ void lr_phi(const DevProc& pr, int k, const cplx* A, int l, int r, cplx* out, int& lo, int& ro) {
   const int a = pr.s0, b = pr.s1;
   const cplx* sig = pr.mat;
   const cplx* tau = pr.mat + 4;
@@ -73,7 +73,7 @@ __device__ void lr_phi(const DevProc& pr, int k, const cplx* A, int l, int r, cp
     ro = r;
   }
   const long long n = (long long)lo * 2 * ro;
-  for (long long e = threadIdx.x; e < n; e += NT) {
+  for (long long e = ltid(); e < n; e += NT) {
     const int L_ = (int)(e % lo);
     const int p = (int)((e / lo) % 2);
     const int R_ = (int)(e / (2LL * lo));
@@ -93,31 +93,31 @@ __device__ void lr_phi(const DevProc& pr, int k, const cplx* A, int l, int r, cp
     }
     out[e] = v;
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // LQ of M (rows x cols, ld rows) = Lout (rows x rn) Qout (rn x cols),
 // rn = min(rows, cols), through the Householder QR of M^H (the factorisation
 // lq_left uses).  rows <= SVD_MAX_COLS.
-__device__ int lr_lq(Ctx& c, const LrBufs& b, const cplx* M, int rows, int cols, cplx* Lout, cplx* Qout) {
+static __device__ int lr_lq(Ctx& c, const LrBufs& b, const cplx* M, int rows, int cols, cplx* Lout, cplx* Qout) {
   const int rn = min(rows, cols);
-  for (long long e = threadIdx.x; e < (long long)cols * rows; e += NT) {
+  for (long long e = ltid(); e < (long long)cols * rows; e += NT) {
     const int cc = (int)(e % cols), ii = (int)(e / cols);
     b.H[e] = cconj(M[ii + (long long)rows * cc]);
   }
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(b.H, cols, rows, c.sm.la, c.sm.e.r);
   dev_qr_formq(b.H, cols, rows, b.Qh, c.sm.la);
   dev_qr_extract_r(b.H, cols, rows, b.R);  // rn x rows
-  for (long long e = threadIdx.x; e < (long long)rn * cols; e += NT) {
+  for (long long e = ltid(); e < (long long)rn * cols; e += NT) {
     const int k = (int)(e % rn), cc = (int)(e / rn);
     Qout[e] = cconj(b.Qh[cc + (long long)cols * k]);
   }
-  for (long long e = threadIdx.x; e < (long long)rows * rn; e += NT) {
+  for (long long e = ltid(); e < (long long)rows * rn; e += NT) {
     const int i = (int)(e % rows), k = (int)(e / rows);
     Lout[e] = cconj(b.R[k + (long long)rn * i]);
   }
-  __syncthreads();
+  cta_sync();
   return rn;
 }
 
@@ -125,7 +125,7 @@ __device__ int lr_lq(Ctx& c, const LrBufs& b, const cplx* M, int rows, int cols,
 // O|psi> is not null, else its (tiny) norm squared.  The state's centre
 // sits at site L-1 with sites 0..L-2 left-canonical, so the sweep starts at
 // site a with an identity on the left.  Reads the state only.
-__device__ __noinline__ double lr_weight(Ctx& c, const DState& s, const DevProc& pr) {
+static __device__ __noinline__ double lr_weight(Ctx& c, const DState& s, const DevProc& pr) {
   const int L = c.P.L;
   LrBufs b = lr_bufs(c);
   int lo, ro;
@@ -141,7 +141,7 @@ __device__ __noinline__ double lr_weight(Ctx& c, const DState& s, const DevProc&
       cta_gemm(gemm_args(kq, 2 * ro, lo, b.R, 1, kq, b.Phi, 1, lo, b.M, 1, kq), c.sm.e.u.gw.g);
       rows = 2 * kq;
     }
-    __syncthreads();
+    cta_sync();
     if (k == L - 1) {
       nrm2 = cta_norm2(b.M, (long long)rows * ro, c.sm.e.r);
       break;
@@ -155,7 +155,7 @@ __device__ __noinline__ double lr_weight(Ctx& c, const DState& s, const DevProc&
 
 // apply_mpo_jump! followed by MPS.truncate! (see above).  Expects the
 // centre at site L-1; leaves the state normalised with the centre at 0.
-__device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr) {
+static __device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr) {
   const int L = c.P.L, a = pr.s0, bb = pr.s1;
   LrBufs b = lr_bufs(c);
   // ---- LQ walk L-1 -> 1 of O|psi> ----
@@ -164,7 +164,7 @@ __device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr
   int lo, ro;
   lr_phi(pr, bb, site_ptr(c, s, bb), s.chi[bb], s.chi[bb + 1], b.Phi, lo, ro);
   int rn = lr_lq(c, b, b.Phi, lo, 2 * ro, b.Lf, lr_qslot(c, b, bb));
-  if (threadIdx.x == 0) {
+  if (ltid() == 0) {
     b.bd[bb] = rn;
     for (int k = bb + 1; k <= L; ++k) b.bd[k] = s.chi[k];
   }
@@ -174,10 +174,10 @@ __device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr
   for (int k = bb - 1; k >= a && !c.sm.fail; --k) {
     lr_phi(pr, k, site_ptr(c, s, k), s.chi[k], s.chi[k + 1], b.Phi, lo, ro);  // ro == lf_rows
     cta_gemm(gemm_args(2 * lo, lf_cols, ro, b.Phi, 1, 2 * lo, b.Lf, 1, lf_rows, b.M, 1, 2 * lo), c.sm.e.u.gw.g);
-    __syncthreads();
+    cta_sync();
     if (k == 0) {  // site 0 is never factorised: it is the centre
       cta_copy(C, b.M, (long long)lo * 2 * lf_cols);
-      if (threadIdx.x == 0) {
+      if (ltid() == 0) {
         b.bd[0] = lo;
         b.bd[1] = lf_cols;
       }
@@ -185,7 +185,7 @@ __device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr
       break;
     }
     rn = lr_lq(c, b, b.M, lo, 2 * lf_cols, b.Lf, lr_qslot(c, b, k));
-    if (threadIdx.x == 0) b.bd[k] = rn;
+    if (ltid() == 0) b.bd[k] = rn;
     lf_rows = lo;
     lf_cols = rn;
   }
@@ -195,16 +195,16 @@ __device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr
     const int lp = s.chi[a - 1];
     cplx* Ap = site_ptr(c, s, a - 1);
     cta_gemm(gemm_args(2 * lp, lf_cols, lf_rows, Ap, 1, 2 * lp, b.Lf, 1, lf_rows, b.M, 1, 2 * lp), c.sm.e.u.gw.g);
-    __syncthreads();
+    cta_sync();
     cta_copy(Ap, b.M, (long long)2 * lp * lf_cols);
     set_chi(c, s, a, lf_cols);
     for (int i = a - 1; i >= 1 && !c.sm.fail; --i) lq_left(c, s, i);
     if (c.sm.fail) return;
     cta_copy(C, site_ptr(c, s, 0), (long long)s.chi[0] * 2 * s.chi[1]);
-    if (threadIdx.x == 0)
+    if (ltid() == 0)
       for (int k = 0; k <= a; ++k) b.bd[k] = s.chi[k];
   }
-  __syncthreads();
+  cta_sync();
   // ---- SVD sweep 0 -> L-2 (absolute rule, min 2, at most max_bond) ----
   cplx* Cn = b.C1;
   for (int k = 0; k + 1 < L && !c.sm.fail; ++k) {
@@ -212,41 +212,41 @@ __device__ __noinline__ void lr_apply(Ctx& c, const DState& s, const DevProc& pr
     const int m = 2 * l;
     SvdWork w = svd_work(c);
     SvdResult res = dev_svd(C, m, r, SVD_LEFT, w, c.sm.la, c.sm.e.r, c.sm.e.u.svd);
-    if (threadIdx.x == 0) {
+    if (ltid() == 0) {
       c.sm.bcast_i[0] = keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond);
       c.cnt[2] += 1;
       c.cnt[5] += res.sweeps;
     }
-    __syncthreads();
+    cta_sync();
     const int keep = c.sm.bcast_i[0];
-    __syncthreads();
+    cta_sync();
     if (keep > c.P.cap[k + 1]) {
-      if (threadIdx.x == 0) c.sm.fail = ST_UNSUPPORTED;
-      __syncthreads();
+      if (ltid() == 0) c.sm.fail = ST_UNSUPPORTED;
+      cta_sync();
       return;
     }
     dev_svd_vectors(res, keep, w, c.sm.e.r);
     cta_copy(site_ptr(c, s, k), w.Yo, (long long)m * keep);
     // S V^H = U^H C (keep x r), rows past the rank exactly zero
     cta_gemm(gemm_args(keep, r, m, w.Yo, m, 1, C, 1, m, b.R, 1, keep, true, false), c.sm.e.u.gw.g);
-    __syncthreads();
-    for (int e = threadIdx.x; e < keep * r; e += NT)
+    cta_sync();
+    for (int e = ltid(); e < keep * r; e += NT)
       if ((e % keep) >= res.rank) b.R[e] = make_double2(0.0, 0.0);
-    __syncthreads();
+    cta_sync();
     const cplx* Bn = (k + 1 >= a && k + 1 <= bb) ? lr_qslot(c, b, k + 1) : site_ptr(c, s, k + 1);
     cta_gemm(gemm_args(keep, 2 * r2, r, b.R, 1, keep, Bn, 1, r, Cn, 1, keep), c.sm.e.u.gw.g);
-    __syncthreads();
+    cta_sync();
     set_chi(c, s, k + 1, keep);
-    if (threadIdx.x == 0) b.bd[k + 1] = keep;
-    __syncthreads();
+    if (ltid() == 0) b.bd[k + 1] = keep;
+    cta_sync();
     cplx* t = C;
     C = Cn;
     Cn = t;
   }
   if (c.sm.fail) return;
   cta_copy(site_ptr(c, s, L - 1), C, (long long)b.bd[L - 1] * 2 * b.bd[L]);
-  __syncthreads();
-  if (threadIdx.x == 0) *s.oc = L - 1;
-  __syncthreads();
+  cta_sync();
+  if (ltid() == 0) *s.oc = L - 1;
+  cta_sync();
   normalize_state(c, s);  // truncate! ends with normalize!
 }

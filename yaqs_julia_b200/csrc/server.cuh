@@ -31,27 +31,27 @@ struct BatchRun {
 __global__ void __launch_bounds__(NT, 2) serve_kernel(const BatchRun* runs, int nruns, int total_units,
                                                       int* counter) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smraw);
+  CtaSmem& sm = *reinterpret_cast<CtaSmem*>(align_smem_1024(smraw));
   __shared__ __align__(16) BatchRun br;
-  const int slot = blockIdx.x;
+  const int slot = cta_slot();
   for (;;) {
-    if (threadIdx.x == 0) {
+    if (ltid() == 0) {
       const int u = atomicAdd(counter, 1);
       int r = 0;
       while (r + 1 < nruns && runs[r + 1].unit_begin <= u) ++r;
       sm.bcast_i[7] = u;
       sm.bcast_i[5] = r;
     }
-    __syncthreads();
+    cta_sync();
     const int u = sm.bcast_i[7], r = sm.bcast_i[5];
-    __syncthreads();
+    cta_sync();
     if (u >= total_units) break;
     {
       const unsigned long long* src = reinterpret_cast<const unsigned long long*>(runs + r);
       unsigned long long* dst = reinterpret_cast<unsigned long long*>(&br);
-      for (int e = threadIdx.x; e < (int)(sizeof(BatchRun) / 8); e += NT) dst[e] = src[e];
+      for (int e = ltid(); e < (int)(sizeof(BatchRun) / 8); e += NT) dst[e] = src[e];
     }
-    __syncthreads();
+    cta_sync();
     const DevParams& P = br.P;
     const int nt = P.num_traj;
     const int local = u - br.unit_begin, k = local / nt, t = local - k * nt, pos = br.first + k;
@@ -59,8 +59,8 @@ __global__ void __launch_bounds__(NT, 2) serve_kernel(const BatchRun* runs, int 
     int* wsi = P.wsi + (long long)slot * P.lay.itotal;
     bool ready = true;
     if (k > 0) ready = wait_done(P, t, pos - 1, sm);
-    if (threadIdx.x == 0) sm.fail = ready ? 0 : ST_TIMEOUT;
-    __syncthreads();
+    if (ltid() == 0) sm.fail = ready ? 0 : ST_TIMEOUT;
+    cta_sync();
     if (ready && P.status[t] == 0) {
       Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
       if (br.digital)
@@ -68,13 +68,13 @@ __global__ void __launch_bounds__(NT, 2) serve_kernel(const BatchRun* runs, int 
       else
         run_step(c, P.jlist[pos]);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    cta_sync();
+    if (ltid() == 0) {
       if (sm.fail && P.status[t] == 0) P.status[t] = sm.fail;
       __threadfence();
       atomicExch(P.done + t, pos);
     }
-    __syncthreads();
+    cta_sync();
   }
 }
 
@@ -411,7 +411,7 @@ int yaqs_server_create(yaqs_ctx* ctx, const yaqs_server_config* cfg, yaqs_server
   const WsLayout ld = plan_layout(L, cd, wone.data(), false, 0, false);
   srv->pool.ws_stride = std::max(la.total, ld.total);
   srv->pool.wsi_stride = std::max(la.itotal, ld.itotal);
-  srv->smem = sizeof(CtaSmem);
+  srv->smem = cta_smem_bytes();
   CUDA_TRY(ctx, cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)srv->smem));
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, NT, srv->smem));

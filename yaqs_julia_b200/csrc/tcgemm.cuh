@@ -18,17 +18,19 @@
 // tensor memory: nine tcgen05.mma.kind::tf32 (M = 128, N <= 64, K = 8) per
 // K step into three accumulators of 64 columns each.
 //
-// Pipeline per 128 x 64 output tile, K in steps of 8, two stages: thread 0
-// issues the TMA loads of step k+1 (raw FP32 complex tiles into shared
-// memory, completion on an mbarrier) while all 256 threads split the raw
-// tile of step k into six TF32 planes (re, im, re+im; hi and lo) laid out
-// in the canonical K-major no-swizzle layout the MMA reads (8-row x 16-byte
-// core matrices; 128 bytes between the two K halves, 256 bytes between
-// 8-row groups); thread 0 then issues the nine MMAs and commits them to the
-// stage's mbarrier, which releases the planes two steps later.  The
-// epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM lanes
-// 32 (w % 4) .. +31, warps 0-3 the first 32 columns, warps 4-7 the rest)
-// and writes C in FP32 or FP64 with general strides.
+// Pipeline per 128 x 64 output tile, K in steps of 8: thread 0 issues the
+// TMA loads of step k+1 (raw FP32 complex tiles into one of two raw
+// buffers, completion on that buffer's mbarrier) while the 256 threads of
+// the program wait for the MMAs of step k-1 to release the planes, then
+// split the raw tile of step k into six TF32 planes (re, im, re+im; hi and
+// lo) laid out in the canonical K-major no-swizzle layout the MMA reads
+// (8-row x 16-byte core matrices; 128 bytes between the two K halves, 256
+// bytes between 8-row groups); thread 0 then issues the nine MMAs and
+// commits them to the plane mbarrier.  One plane buffer keeps the pipeline
+// within the shared memory the FP64 GEMM staging already takes (60 KB).
+// The epilogue reads the accumulators with tcgen05.ld (warp w owns TMEM
+// lanes 32 (w % 4) .. +31, warps 0-3 the first 32 columns, warps 4-7 the
+// rest) and writes C in FP32 or FP64 with general strides.
 //
 // Every wait is bounded; a wait that gives up sets TcState::fatal, after
 // which every later call returns at once and the caller reports a timeout.
@@ -40,24 +42,25 @@
 #define TC_BN 64
 #define TC_BK 8
 #define TC_TMEM_COLS 256  // three accumulators of 64 columns (power of two >= 192)
+#define TMEM_PROGRAMS_PER_SM 2  // 512 TMEM columns per SM / TC_TMEM_COLS
 #define TC_WAIT_SPINS (1LL << 24)
 
 // Shared memory of the pipeline (never live together with the other GEMM or
 // SVD staging; the engine keeps it in the same union).
 struct __align__(1024) TcSmem {
-  float rawA[2][2048];           // 2 stages x 8 KB: one A box (128 x 8 complex)
-  float rawB[2][1024];           // 2 stages x 4 KB: one B box (8 x 64 complex)
-  unsigned planeA[2][6][1024];   // 2 stages x 6 planes x (128 rows x 8 k) tf32
-  unsigned planeB[2][6][512];    // 2 stages x 6 planes x (64 rows x 8 k) tf32
+  float rawA[2][2048];        // 2 buffers x 8 KB: one A box (128 x 8 complex)
+  float rawB[2][1024];        // 2 buffers x 4 KB: one B box (8 x 64 complex)
+  unsigned planeA[6][1024];   // 6 planes x (128 rows x 8 k) tf32
+  unsigned planeB[6][512];    // 6 planes x (64 rows x 8 k) tf32
 };
 
 // State that persists across calls (outside the union).
 struct TcState {
   unsigned long long bar_raw[2];
-  unsigned long long bar_mma[2];
+  unsigned long long bar_mma;
   unsigned tmem_base;
   unsigned ph_raw;  // bit s: parity of the next phase of bar_raw[s]
-  unsigned ph_mma;  // bit s: parity of the next phase of bar_mma[s]
+  unsigned ph_mma;  // parity of the next phase of bar_mma
   int fatal;
 };
 
@@ -68,15 +71,15 @@ struct TcOp {
   int conj;                // use the complex conjugate
 };
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+static __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+static __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+static __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+static __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -88,7 +91,7 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned pari
   return ok != 0;
 }
 // Bounded wait for the phase of parity `parity`; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+static __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
   for (long long it = 0; it < TC_WAIT_SPINS; ++it) {
     if (mbar_test(bar, parity)) return true;
     if (it > 64) __nanosleep(64);
@@ -96,35 +99,35 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return false;
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+static __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
           smem_u32(dst)),
       "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map) {
+static __device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
 }
 
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+static __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+static __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+static __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+static __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // Warp-collective TMEM allocation / release.
-__device__ __forceinline__ void tmem_alloc(unsigned* dst, unsigned ncols) {
+static __device__ __forceinline__ void tmem_alloc(unsigned* dst, unsigned ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
                : "memory");
 }
-__device__ __forceinline__ void tmem_relinquish() {
+static __device__ __forceinline__ void tmem_relinquish() {
   asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 }
-__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+static __device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-__device__ __forceinline__ void tc_mma_tf32(unsigned d_tmem, unsigned long long adesc, unsigned long long bdesc,
+static __device__ __forceinline__ void tc_mma_tf32(unsigned d_tmem, unsigned long long adesc, unsigned long long bdesc,
                                             unsigned idesc, unsigned accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -133,11 +136,11 @@ __device__ __forceinline__ void tc_mma_tf32(unsigned d_tmem, unsigned long long 
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
-__device__ __forceinline__ void tc_commit(unsigned long long* bar) {
+static __device__ __forceinline__ void tc_commit(unsigned long long* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
+static __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   unsigned r[16];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -148,12 +151,12 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+static __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Shared-memory matrix descriptor, canonical K-major layout without
 // swizzle: LBO = bytes between the two 16-byte K halves of an 8-row core
 // matrix group, SBO = bytes between consecutive 8-row groups.
-__device__ __forceinline__ unsigned long long tc_sdesc(const void* p, unsigned lbo, unsigned sbo) {
+static __device__ __forceinline__ unsigned long long tc_sdesc(const void* p, unsigned lbo, unsigned sbo) {
   unsigned long long d = (unsigned long long)((smem_u32(p) >> 4) & 0x3FFFu);
   d |= (unsigned long long)((lbo >> 4) & 0x3FFFu) << 16;
   d |= (unsigned long long)((sbo >> 4) & 0x3FFFu) << 32;
@@ -162,24 +165,24 @@ __device__ __forceinline__ unsigned long long tc_sdesc(const void* p, unsigned l
 }
 
 // Instruction descriptor: TF32 x TF32 -> FP32, A and B K-major, M = 128, N.
-__device__ __forceinline__ unsigned tc_idesc(int n) {
+static __device__ __forceinline__ unsigned tc_idesc(int n) {
   return (1u << 4)            // D format FP32
          | (2u << 7)          // A format TF32
          | (2u << 10)         // B format TF32
          | ((unsigned)(n >> 3) << 17) | ((unsigned)(TC_BM >> 4) << 24);
 }
 
-__device__ __forceinline__ unsigned tf32_rna(float x) {
+static __device__ __forceinline__ unsigned tf32_rna(float x) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return r;
 }
 
 // Byte offset of (row r, k quad q) inside a K-major plane.
-__device__ __forceinline__ int tc_plane_off(int r, int q) { return (r >> 3) * 256 + q * 128 + (r & 7) * 16; }
+static __device__ __forceinline__ int tc_plane_off(int r, int q) { return (r >> 3) * 256 + q * 128 + (r & 7) * 16; }
 
 // Splits four complex values (one row, one k quad) into the six planes.
-__device__ __forceinline__ void tc_split_store(unsigned* planes, int plane_words, int r, int q, const float2 (&v)[4]) {
+static __device__ __forceinline__ void tc_split_store(unsigned* planes, int plane_words, int r, int q, const float2 (&v)[4]) {
   unsigned hr[4], lr[4], hi_[4], li[4], hs[4], ls[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -202,7 +205,7 @@ __device__ __forceinline__ void tc_split_store(unsigned* planes, int plane_words
 
 // Reads the four complex values of row r (global r0 + r), k quad q of a raw
 // box; zero outside the matrix.  rows_box: 128 (A) or 64 (B).
-__device__ __forceinline__ void tc_raw_quad(const float* raw, int mn, int rows_box, int r, int q, bool row_ok, int k0,
+static __device__ __forceinline__ void tc_raw_quad(const float* raw, int mn, int rows_box, int r, int q, bool row_ok, int k0,
                                             int K, bool conj, float2 (&v)[4]) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -217,7 +220,7 @@ __device__ __forceinline__ void tc_raw_quad(const float* raw, int mn, int rows_b
   }
 }
 
-__device__ __forceinline__ void tc_store_c(float2* c, float re, float im, bool acc) {
+static __device__ __forceinline__ void tc_store_c(float2* c, float re, float im, bool acc) {
   if (acc) {
     const float2 o = *c;
     re += o.x;
@@ -225,7 +228,7 @@ __device__ __forceinline__ void tc_store_c(float2* c, float re, float im, bool a
   }
   *c = make_float2(re, im);
 }
-__device__ __forceinline__ void tc_store_c(double2* c, float re, float im, bool acc) {
+static __device__ __forceinline__ void tc_store_c(double2* c, float re, float im, bool acc) {
   double r = re, i = im;
   if (acc) {
     const double2 o = *c;
@@ -235,34 +238,33 @@ __device__ __forceinline__ void tc_store_c(double2* c, float re, float im, bool 
   *c = make_double2(r, i);
 }
 
-// Called once per CTA before the first tc_gemm (thread-0 barrier set-up and
-// a warp-0 TMEM allocation).  CTA-collective.
-__device__ __forceinline__ void tc_setup(TcState& st) {
-  if (threadIdx.x == 0) {
+// Called once per program before the first tc_gemm: thread-0 barrier
+// set-up and a warp-0 allocation of TC_TMEM_COLS columns.  Collective over
+// the program's NT threads.  The kernel relinquishes the CTA's allocation
+// permit once every program of the CTA has allocated.
+static __device__ __forceinline__ void tc_setup(TcState& st) {
+  if (ltid() == 0) {
     mbar_init(&st.bar_raw[0], 1);
     mbar_init(&st.bar_raw[1], 1);
-    mbar_init(&st.bar_mma[0], 1);
-    mbar_init(&st.bar_mma[1], 1);
+    mbar_init(&st.bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     st.ph_raw = 0;
     st.ph_mma = 0;
     st.fatal = 0;
   }
-  if (threadIdx.x < 32) {
-    tmem_alloc(&st.tmem_base, TC_TMEM_COLS);
-    tmem_relinquish();
-  }
+  if (ltid() < 32) tmem_alloc(&st.tmem_base, TC_TMEM_COLS);
   tc_fence_before();
-  __syncthreads();
+  cta_sync();
   tc_fence_after();
 }
 
-// Releases the TMEM columns.  CTA-collective; the last call of a CTA.
-__device__ __forceinline__ void tc_teardown(TcState& st) {
+// Releases the program's TMEM columns.  Collective over the program's
+// threads; its last call.
+static __device__ __forceinline__ void tc_teardown(TcState& st) {
   tc_fence_before();
-  __syncthreads();
+  cta_sync();
   tc_fence_after();
-  if (threadIdx.x < 32) tmem_dealloc(st.tmem_base, TC_TMEM_COLS);
+  if (ltid() < 32) tmem_dealloc(st.tmem_base, TC_TMEM_COLS);
 }
 
 // C = op(A) op(B) (+ C when accumulate), M x N x K, C element (m, n) at
@@ -270,15 +272,15 @@ __device__ __forceinline__ void tc_teardown(TcState& st) {
 // up (the CTA's tensor-core state is then unusable).  CTA-collective; ends
 // with C visible to the whole CTA.
 template <class TC>
-__device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, const TcOp B, TC* C, long long cm, long long cn,
+static __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, const TcOp B, TC* C, long long cm, long long cn,
                                      bool accumulate, TcSmem& s, TcState& st) {
   ProfScope prof_scope_(PF_GEMM);
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  __syncthreads();
+  const int tid = ltid(), lane = tid & 31, wid = tid >> 5;
+  cta_sync();
   if (st.fatal) return false;
   // producers of the staged operands wrote them through the generic proxy
   fence_async_global();
-  __syncthreads();
+  cta_sync();
   unsigned ph_raw = st.ph_raw, ph_mma = st.ph_mma;
   bool ok = true;
   const int nM = (M + TC_BM - 1) / TC_BM, nN = (N + TC_BN - 1) / TC_BN, nK = (K + TC_BK - 1) / TC_BK;
@@ -295,7 +297,7 @@ __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, const Tc
     else
       tma_load_2d(s.rawB[stg], B.map, 2 * k0, n0, &st.bar_raw[stg]);
   };
-  unsigned pend = 0;  // bit s: a commit on bar_mma[s] not yet waited for
+  bool pend = false;  // a commit on bar_mma not yet waited for
   int stage = 0;
   for (int t = 0; t < nM * nN; ++t) {
     const int m0 = (t / nN) * TC_BM, n0 = (t % nN) * TC_BN;
@@ -308,30 +310,30 @@ __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, const Tc
       if (tid == 0 && kc + 1 < nK) issue(kc + 1, sg ^ 1, m0, n0);
       ok &= mbar_wait(&st.bar_raw[sg], (ph_raw >> sg) & 1);
       ph_raw ^= 1u << sg;
-      if (pend & (1u << sg)) {
-        ok &= mbar_wait(&st.bar_mma[sg], (ph_mma >> sg) & 1);
-        ph_mma ^= 1u << sg;
-        pend &= ~(1u << sg);
+      if (pend) {  // the MMAs of the previous step release the planes
+        ok &= mbar_wait(&st.bar_mma, ph_mma & 1);
+        ph_mma ^= 1u;
+        pend = false;
       }
       const int k0 = kc * TC_BK;
       {  // A: 128 rows x 2 k quads, one item per thread
         const int r = tid & 127, q = tid >> 7;
         float2 v[4];
         tc_raw_quad(s.rawA[sg], A.mn, TC_BM, r, q, m0 + r < M, k0, K, A.conj != 0, v);
-        tc_split_store(&s.planeA[sg][0][0], 1024, r, q, v);
+        tc_split_store(&s.planeA[0][0], 1024, r, q, v);
       }
       if (tid < 128) {  // B: 64 rows x 2 k quads
         const int r = tid & 63, q = tid >> 6;
         float2 v[4];
         tc_raw_quad(s.rawB[sg], B.mn, TC_BN, r, q, n0 + r < N, k0, K, B.conj != 0, v);
-        tc_split_store(&s.planeB[sg][0][0], 512, r, q, v);
+        tc_split_store(&s.planeB[0][0], 512, r, q, v);
       }
       fence_async_smem();
-      __syncthreads();
+      cta_sync();
       if (tid == 0) {
         tc_fence_after();
-        const unsigned* pa = &s.planeA[sg][0][0];
-        const unsigned* pb = &s.planeB[sg][0][0];
+        const unsigned* pa = &s.planeA[0][0];
+        const unsigned* pb = &s.planeB[0][0];
 #pragma unroll
         for (int acc = 0; acc < 3; ++acc) {
           const unsigned long long ah = tc_sdesc(pa + (2 * acc) * 1024, 128, 256);
@@ -343,19 +345,16 @@ __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, const Tc
           tc_mma_tf32(d, al, bh, idesc, 1u);
           tc_mma_tf32(d, ah, bh, idesc, 1u);
         }
-        tc_commit(&st.bar_mma[sg]);
+        tc_commit(&st.bar_mma);
       }
-      pend |= 1u << sg;
+      pend = true;
     }
     stage += nK;
-    // all MMAs of the tile done (commits complete in issue order)
-    for (int sg = 0; sg < 2; ++sg) {
-      const int s2 = (stage + sg) & 1;  // older stage first
-      if (pend & (1u << s2)) {
-        ok &= mbar_wait(&st.bar_mma[s2], (ph_mma >> s2) & 1);
-        ph_mma ^= 1u << s2;
-        pend &= ~(1u << s2);
-      }
+    // all MMAs of the tile done
+    if (pend) {
+      ok &= mbar_wait(&st.bar_mma, ph_mma & 1);
+      ph_mma ^= 1u;
+      pend = false;
     }
     tc_fence_after();
     // epilogue
@@ -380,15 +379,15 @@ __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, const Tc
       }
     }
     tc_fence_before();
-    __syncthreads();
+    cta_sync();
   }
   if (!ok) st.fatal = 1;  // benign race: every writer stores 1
-  __syncthreads();
+  cta_sync();
   if (tid == 0) {
     st.ph_raw = ph_raw;
     st.ph_mma = ph_mma;
   }
   const bool good = !st.fatal;
-  __syncthreads();
+  cta_sync();
   return good;
 }

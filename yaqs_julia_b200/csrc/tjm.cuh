@@ -47,6 +47,12 @@ struct WsLayout {
   // long-range jumps: right-canonical tensors of the operator applied to
   // the state (4 x the MPS arena) and work buffers
   long long lrQ, lrPhi, lrM, lrH, lrQh, lrL, lrR, lrC0, lrC1;
+  // mixed form on tcgen05: TMA-staged FP32 operands of the H_eff products
+  // (offsets in complex-double units, pitches and row counts in complex
+  // FP32 values): SL = L as [k][a + chil m], Sx = x as [p + D c][k],
+  // ST2 = T2 as [m' + wr c][a + chil p'], SR = R as [m' + wr c][b]
+  long long sL, sx, sT2, sR;
+  int pL, px, pT2, pR, rL, rx, rT2, rR;
   long long total;
   // int workspace (per slot)
   long long i_chi, i_oc, i_ord, i_cand, i_lr, itotal;
@@ -56,6 +62,8 @@ struct DevParams {
   int L, n_times, order, sample_ts, max_bond, nobs, nprocs, noise_present, all_zero, rng_mode, num_traj,
       traj_offset, ncols;
   int mixed;  // H_eff and environment contractions in complex FP32 on the tensor cores
+  int tc;     // mixed H_eff products on tcgen05 (the tensor-core kernel, engine_tc.cu)
+  const CUtensorMap* tmaps;  // [slots][4]: SL, Sx, ST2, SR of each slot
   int tdvp_mode;  // YAQS_TDVP_2SITE / _1SITE / _DYNAMIC
   double dt, thr;
   KrylovCfg kc;
@@ -103,6 +111,14 @@ struct CtaSmem {
   int canon;  // the state is in mixed canonical form around its centre
 };
 
+// Dynamic shared memory of one trajectory program, with 1024 bytes of slack
+// for aligning the base (the tensor-core buffers want 1024-byte alignment).
+constexpr size_t cta_smem_bytes() { return sizeof(CtaSmem) + 1024; }
+static __device__ __forceinline__ unsigned char* align_smem_1024(unsigned char* p) {
+  const unsigned off = smem_u32(p);
+  return p + ((1024u - (off & 1023u)) & 1023u);
+}
+
 struct Ctx {  // per-CTA view
   const DevParams& P;
   CtaSmem& sm;
@@ -120,12 +136,12 @@ struct DState {
   int* oc;
 };
 
-__device__ __forceinline__ cplx* site_ptr(const Ctx& c, const DState& s, int i) { return s.a + c.P.mps_off[i]; }
+static __device__ __forceinline__ cplx* site_ptr(const Ctx& c, const DState& s, int i) { return s.a + c.P.mps_off[i]; }
 
 // ---------------------------------------------------------------------------
 // Philox-4x32-10 (Salmon et al., SC'11), one 53-bit double per counter.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double philox_uniform(unsigned long long seed, unsigned long long stream,
+static __device__ __forceinline__ double philox_uniform(unsigned long long seed, unsigned long long stream,
                                                  unsigned long long draw) {
   unsigned int c0 = (unsigned int)draw, c1 = (unsigned int)(draw >> 32), c2 = (unsigned int)stream,
                c3 = (unsigned int)(stream >> 32);
@@ -149,8 +165,8 @@ __device__ __forceinline__ double philox_uniform(unsigned long long seed, unsign
 }
 
 // Next uniform of this trajectory (CTA-collective; broadcast).
-__device__ double draw_uniform(Ctx& c) {
-  if (threadIdx.x == 0) {
+static __device__ double draw_uniform(Ctx& c) {
+  if (ltid() == 0) {
     long long pos = c.P.rng_pos[c.traj];
     double u;
     if (c.P.rng_mode == 1) {
@@ -166,26 +182,26 @@ __device__ double draw_uniform(Ctx& c) {
     c.P.rng_pos[c.traj] = pos + 1;
     c.sm.bcast_d[0] = u;
   }
-  __syncthreads();
+  cta_sync();
   double u = c.sm.bcast_d[0];
-  __syncthreads();
+  cta_sync();
   return u;
 }
 
 // ---------------------------------------------------------------------------
 // Gauge moves (MPS.jl:182-311)
 // ---------------------------------------------------------------------------
-__device__ void set_chi(Ctx& c, const DState& s, int b, int v) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
+static __device__ void set_chi(Ctx& c, const DState& s, int b, int v) {
+  cta_sync();
+  if (ltid() == 0) {
     if (v > c.P.cap[b]) c.sm.fail = ST_UNSUPPORTED;
     else s.chi[b] = v;
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // site i: A = Q R, Q -> site i, R absorbed into site i+1.
-__device__ void qr_right(Ctx& c, const DState& s, int i) {
+static __device__ void qr_right(Ctx& c, const DState& s, int i) {
   const int l = s.chi[i], r = s.chi[i + 1], m = 2 * l, rn = min(m, r);
   const int r2 = s.chi[i + 2];
   cplx* A = site_ptr(c, s, i);
@@ -194,7 +210,7 @@ __device__ void qr_right(Ctx& c, const DState& s, int i) {
   cplx* Rb = c.ws + c.P.lay.tB;
   cplx* T = c.ws + c.P.lay.tC;
   cta_copy(H, A, (long long)m * r);
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(H, m, r, c.sm.la, c.sm.e.r);
   dev_qr_formq(H, m, r, A, c.sm.la);
   dev_qr_extract_r(H, m, r, Rb);
@@ -204,7 +220,7 @@ __device__ void qr_right(Ctx& c, const DState& s, int i) {
 }
 
 // site i: A = L Q, Q -> site i, L absorbed into site i-1.
-__device__ void lq_left(Ctx& c, const DState& s, int i) {
+static __device__ void lq_left(Ctx& c, const DState& s, int i) {
   const int l = s.chi[i], r = s.chi[i + 1], n2 = 2 * r, rn = min(l, n2);
   const int lp = s.chi[i - 1];
   cplx* A = site_ptr(c, s, i);
@@ -212,63 +228,63 @@ __device__ void lq_left(Ctx& c, const DState& s, int i) {
   cplx* H = c.ws + c.P.lay.tA;
   cplx* Qh = c.ws + c.P.lay.tB;
   cplx* Rb = c.ws + c.P.lay.tC;
-  for (int e = threadIdx.x; e < n2 * l; e += NT) {
+  for (int e = ltid(); e < n2 * l; e += NT) {
     int cc = (int)(e % n2), ii = (int)(e / n2);
     H[e] = cconj(A[ii + (long long)l * cc]);
   }
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(H, n2, l, c.sm.la, c.sm.e.r);
   dev_qr_formq(H, n2, l, Qh, c.sm.la);
   dev_qr_extract_r(H, n2, l, Rb);
-  for (int e = threadIdx.x; e < rn * n2; e += NT) {
+  for (int e = ltid(); e < rn * n2; e += NT) {
     int k = (int)(e % rn), cc = (int)(e / rn);
     A[e] = cconj(Qh[cc + (long long)n2 * k]);
   }
-  __syncthreads();
+  cta_sync();
   cta_gemm(gemm_args(2 * lp, rn, l, Ap, 1, 2 * lp, Rb, rn, 1, H, 1, 2 * lp, false, true), c.sm.e.u.gw.g);
   cta_copy(Ap, H, (long long)2 * lp * rn);
   set_chi(c, s, i, rn);
 }
 
-__device__ void shift_oc(Ctx& c, const DState& s, int nc) {
+static __device__ void shift_oc(Ctx& c, const DState& s, int nc) {
   int oc = *s.oc;
-  __syncthreads();
+  cta_sync();
   if (oc == nc) return;
   if (nc > oc) {
     for (int i = oc; i < nc && !c.sm.fail; ++i) qr_right(c, s, i);
   } else {
     for (int i = oc; i > nc && !c.sm.fail; --i) lq_left(c, s, i);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) *s.oc = nc;
-  __syncthreads();
+  cta_sync();
+  if (ltid() == 0) *s.oc = nc;
+  cta_sync();
 }
 
-__device__ void normalize_state(Ctx& c, const DState& s) {
+static __device__ void normalize_state(Ctx& c, const DState& s) {
   for (int i = c.P.L - 1; i >= 1 && !c.sm.fail; --i) lq_left(c, s, i);
   cplx* A = site_ptr(c, s, 0);
   const long long n = (long long)s.chi[0] * 2 * s.chi[1];
   double nr = sqrt(cta_norm2(A, n, c.sm.e.r));
   if (nr > 1e-13) cta_scale(A, n, 1.0 / nr);
-  __syncthreads();
-  if (threadIdx.x == 0) *s.oc = 0;
-  __syncthreads();
+  cta_sync();
+  if (ltid() == 0) *s.oc = 0;
+  cta_sync();
 }
 
 // Scale the orthogonality-centre tensor to unit norm (normalize!, MPS.jl:274-311).
-__device__ void normalize_center(Ctx& c, const DState& s) {
+static __device__ void normalize_center(Ctx& c, const DState& s) {
   const int oc = *s.oc;
   cplx* A = site_ptr(c, s, oc);
   const long long n = (long long)s.chi[oc] * 2 * s.chi[oc + 1];
   double nr = sqrt(cta_norm2(A, n, c.sm.e.r));
   if (nr > 1e-13) cta_scale(A, n, 1.0 / nr);
-  __syncthreads();
+  cta_sync();
 }
 
 // True when every bond satisfies chi[b] <= 2 chi[b-1] and chi[b] <= 2 chi[b+1]:
 // then the thin QR / LQ factorisations of a gauge sweep keep every shape, so
 // a sweep is a pure gauge move.  Uniform across the CTA.
-__device__ bool chain_tight(const Ctx& c, const DState& s) {
+static __device__ bool chain_tight(const Ctx& c, const DState& s) {
   bool ok = true;
   for (int b = 1; b < c.P.L; ++b) {
     const int x = s.chi[b];
@@ -280,7 +296,7 @@ __device__ bool chain_tight(const Ctx& c, const DState& s) {
 // normalize! of a state in mixed canonical form around its centre: on a
 // tight chain the full sweep only rescales the centre tensor; otherwise run
 // the sweep.
-__device__ void finish_normalize(Ctx& c, const DState& s) {
+static __device__ void finish_normalize(Ctx& c, const DState& s) {
   if (chain_tight(c, s))
     normalize_center(c, s);
   else
@@ -288,13 +304,13 @@ __device__ void finish_normalize(Ctx& c, const DState& s) {
 }
 
 // Re <psi|psi> by full contraction (scalar_product, MPS.jl:528-585).
-__device__ double scalar_product(Ctx& c, const DState& s) {
+static __device__ double scalar_product(Ctx& c, const DState& s) {
   ProfScope prof_scope_(PF_SCALAR);
   cplx* Ea = c.ws + c.P.lay.tA;
   cplx* Eb = c.ws + c.P.lay.tB;
   cplx* T = c.ws + c.P.lay.tC;
-  if (threadIdx.x == 0) Ea[0] = make_double2(1.0, 0.0);
-  __syncthreads();
+  if (ltid() == 0) Ea[0] = make_double2(1.0, 0.0);
+  cta_sync();
   for (int i = 0; i < c.P.L; ++i) {
     const int l = s.chi[i], r = s.chi[i + 1];
     const cplx* A = site_ptr(c, s, i);
@@ -305,27 +321,27 @@ __device__ double scalar_product(Ctx& c, const DState& s) {
     Eb = t;
   }
   double v = Ea[0].x;
-  __syncthreads();
+  cta_sync();
   return v;
 }
 
 // ---------------------------------------------------------------------------
 // Environments (Algorithms.jl:191-211)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ cplx* envL(const Ctx& c, int b) { return c.ws + c.P.lay.EL + c.P.env_off[b]; }
-__device__ __forceinline__ cplx* envR(const Ctx& c, int b) { return c.ws + c.P.lay.ER + c.P.env_off[b]; }
+static __device__ __forceinline__ cplx* envL(const Ctx& c, int b) { return c.ws + c.P.lay.EL + c.P.env_off[b]; }
+static __device__ __forceinline__ cplx* envR(const Ctx& c, int b) { return c.ws + c.P.lay.ER + c.P.env_off[b]; }
 
-__device__ void identity_env(Ctx& c, cplx* E, int dim, int w) {
-  for (int e = threadIdx.x; e < dim * w * dim; e += NT) {
+static __device__ void identity_env(Ctx& c, cplx* E, int dim, int w) {
+  for (int e = ltid(); e < dim * w * dim; e += NT) {
     long long a = e % dim, rest = e / dim;
     long long m = rest % w, k = rest / w;
     E[e] = make_double2((m == 0 && a == k) ? 1.0 : 0.0, 0.0);
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // EL[i+1] from EL[i], A_i and the map Wenv of W_i (update_left_environment)
-__device__ void update_left_w(Ctx& c, const DState& s, int i, const WMat& Wenv) {
+static __device__ void update_left_w(Ctx& c, const DState& s, int i, const WMat& Wenv) {
   ProfScope prof_scope_(PF_ENV);
   const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
   const cplx* A = site_ptr(c, s, i);
@@ -369,10 +385,10 @@ __device__ void update_left_w(Ctx& c, const DState& s, int i, const WMat& Wenv) 
   }
 }
 
-__device__ void update_left(Ctx& c, const DState& s, int i) { update_left_w(c, s, i, c.P.wm_envL[i]); }
+static __device__ void update_left(Ctx& c, const DState& s, int i) { update_left_w(c, s, i, c.P.wm_envL[i]); }
 
 // ER[i] from ER[i+1], A_i and the map Wenv of W_i (update_right_environment)
-__device__ void update_right_w(Ctx& c, const DState& s, int i, const WMat& Wenv) {
+static __device__ void update_right_w(Ctx& c, const DState& s, int i, const WMat& Wenv) {
   ProfScope prof_scope_(PF_ENV);
   const int l = s.chi[i], r = s.chi[i + 1], wl = c.P.w[i], wr = c.P.w[i + 1];
   const cplx* A = site_ptr(c, s, i);
@@ -413,12 +429,12 @@ __device__ void update_right_w(Ctx& c, const DState& s, int i, const WMat& Wenv)
   }
 }
 
-__device__ void update_right(Ctx& c, const DState& s, int i) { update_right_w(c, s, i, c.P.wm_envR[i]); }
+static __device__ void update_right(Ctx& c, const DState& s, int i) { update_right_w(c, s, i, c.P.wm_envR[i]); }
 
 // ---------------------------------------------------------------------------
 // Two-site TDVP (Algorithms.jl:580-760)
 // ---------------------------------------------------------------------------
-__device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, const WMat& W, double dt) {
+static __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, const WMat& W, double dt) {
   HeffOp h;
   h.L = envL(c, bl);
   h.R = envR(c, br);
@@ -431,7 +447,29 @@ __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, con
   h.T1 = c.ws + c.P.lay.T1;
   h.T2 = c.ws + c.P.lay.T2;
   h.mixed = c.P.mixed;
-  if (c.P.mixed) {  // FP32 environments for the whole Krylov solve
+  if (c.P.tc) {  // environments staged once per Krylov solve as the TMA operands
+    const WsLayout& y = c.P.lay;
+    h.tc = 1;
+    h.maps = c.P.tmaps + 4 * c.slot;
+    h.SL = reinterpret_cast<cflt*>(c.ws + y.sL);
+    h.Sx = reinterpret_cast<cflt*>(c.ws + y.sx);
+    h.ST2 = reinterpret_cast<cflt*>(c.ws + y.sT2);
+    h.SR = reinterpret_cast<cflt*>(c.ws + y.sR);
+    h.pL = y.pL;
+    h.px = y.px;
+    h.pT2 = y.pT2;
+    h.pR = y.pR;
+    h.T1f = reinterpret_cast<cflt*>(c.ws + y.T1f);
+    const long long ml = (long long)l * h.wl;
+    for (long long e = ltid(); e < ml * l; e += NT) {  // SL[k pL + i] = L[i + ml k]
+      const cplx v = h.L[e];
+      h.SL[(e / ml) * h.pL + e % ml] = make_float2((float)v.x, (float)v.y);
+    }
+    for (long long e = ltid(); e < (long long)r * h.wr * r; e += NT) {  // SR[k pR + b] = R[b + r k]
+      const cplx v = h.R[e];
+      h.SR[(e / r) * h.pR + e % r] = make_float2((float)v.x, (float)v.y);
+    }
+  } else if (c.P.mixed) {  // FP32 environments for the whole Krylov solve
     cflt* Lf = reinterpret_cast<cflt*>(c.ws + c.P.lay.Lf);
     cflt* Rf = reinterpret_cast<cflt*>(c.ws + c.P.lay.Rf);
     cta_to_f32(Lf, h.L, (long long)l * h.wl * l);
@@ -443,7 +481,7 @@ __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, con
     h.T2f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T2f);
   }
   int mv = dev_expm_krylov(h, x, dt, c.P.kc, c.ws + c.P.lay.Q, c.P.kry_n, c.sm.e);
-  if (threadIdx.x == 0) {
+  if (ltid() == 0) {
     c.cnt[0] += mv;
     c.cnt[1] += (mv > 0);
     *c.fl += mv * heff_flops(l, h.wl, D, r, h.wr);
@@ -451,13 +489,13 @@ __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, con
 }
 
 // Theta (l,4,r) of sites i,i+1 into buffer th.
-__device__ void merge(Ctx& c, const DState& s, int i, cplx* th) {
+static __device__ void merge(Ctx& c, const DState& s, int i, cplx* th) {
   const int l = s.chi[i], m = s.chi[i + 1], r = s.chi[i + 2];
   cta_gemm(gemm_args(2 * l, 2 * r, m, site_ptr(c, s, i), 1, 2 * l, site_ptr(c, s, i + 1), 1, m, th, 1, 2 * l),
            c.sm.e.u.gw.g);
 }
 
-__device__ SvdWork svd_work(const Ctx& c) {
+static __device__ SvdWork svd_work(const Ctx& c) {
   SvdWork w;
   w.B = c.ws + c.P.lay.B;
   w.X = c.ws + c.P.lay.X;
@@ -470,9 +508,9 @@ __device__ SvdWork svd_work(const Ctx& c) {
 }
 
 // NaN/Inf -> 0 before the SVD (Algorithms.jl:414-417).
-__device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
+static __device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
   int bad = 0;
-  for (int e = threadIdx.x; e < (int)n; e += NT) {
+  for (int e = ltid(); e < (int)n; e += NT) {
     cplx v = th[e];
     if (!isfinite(v.x) || !isfinite(v.y)) {
       th[e] = make_double2(0.0, 0.0);
@@ -480,7 +518,7 @@ __device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
     }
   }
   double b = block_sum((double)bad, c.sm.e.r);
-  if (b > 0 && threadIdx.x == 0) c.cnt[4] += 1;
+  if (b > 0 && ltid() == 0) c.cnt[4] += 1;
 }
 
 // SVD split of theta (2l x 2r) into sites i (l,2,keep) and i+1 (keep,2,r).
@@ -489,12 +527,12 @@ __device__ void fix_nonfinite(Ctx& c, cplx* th, long long n) {
 // otherwise right (U | S Vt, U orthonormal, Algorithms.jl:656-663).  The
 // scaled factor is computed as a product with theta and is exactly zero for
 // null singular values.
-__device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, int rule, bool s_left) {
+static __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, int rule, bool s_left) {
   const int m = 2 * l, n = 2 * r;
   fix_nonfinite(c, th, (long long)m * n);
   SvdWork w = svd_work(c);
   SvdResult res = dev_svd(th, m, n, s_left ? SVD_RIGHT : SVD_LEFT, w, c.sm.la, c.sm.e.r, c.sm.e.u.svd);
-  if (threadIdx.x == 0) {
+  if (ltid() == 0) {
     int keep = rule == 0   ? keep_tdvp(w.sig, res.p, c.P.thr, c.P.max_bond)
                : rule == 1 ? keep_relative(w.sig, res.p, c.P.thr, c.P.max_bond)
                : rule == 2 ? keep_tebd(w.sig, res.p, c.P.thr, c.P.max_bond)
@@ -503,12 +541,12 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
     c.cnt[2] += 1;
     c.cnt[5] += res.sweeps;
   }
-  __syncthreads();
+  cta_sync();
   const int keep = c.sm.bcast_i[0];
-  __syncthreads();
+  cta_sync();
   if (keep > c.P.cap[i + 1]) {
-    if (threadIdx.x == 0) c.sm.fail = ST_UNSUPPORTED;
-    __syncthreads();
+    if (ltid() == 0) c.sm.fail = ST_UNSUPPORTED;
+    cta_sync();
     return;
   }
   dev_svd_vectors(res, keep, w, c.sm.e.r);
@@ -516,27 +554,27 @@ __device__ void split(Ctx& c, const DState& s, int i, cplx* th, int l, int r, in
   cplx* Rt = site_ptr(c, s, i + 1);
   if (!s_left) {
     cta_copy(Lt, w.Yo, (long long)m * keep);
-    __syncthreads();
+    cta_sync();
     cta_gemm(gemm_args(keep, n, m, w.Yo, m, 1, th, 1, m, Rt, 1, keep, true, false), c.sm.e.u.gw.g);
-    for (int e = threadIdx.x; e < keep * n; e += NT)
+    for (int e = ltid(); e < keep * n; e += NT)
       if ((int)(e % keep) >= res.rank) Rt[e] = make_double2(0.0, 0.0);
   } else {
-    for (int e = threadIdx.x; e < keep * n; e += NT) {
+    for (int e = ltid(); e < keep * n; e += NT) {
       int k = (int)(e % keep), cc = (int)(e / keep);
       Rt[e] = cconj(w.Yo[cc + (long long)n * k]);
     }
     cta_gemm(gemm_args(m, keep, n, th, 1, m, w.Yo, 1, n, Lt, 1, m), c.sm.e.u.gw.g);
-    for (int e = threadIdx.x; e < m * keep; e += NT)
+    for (int e = ltid(); e < m * keep; e += NT)
       if ((int)(e / m) >= res.rank) Lt[e] = make_double2(0.0, 0.0);
   }
-  __syncthreads();
+  cta_sync();
   set_chi(c, s, i + 1, keep);
-  if (threadIdx.x == 0) *s.oc = s_left ? i : i + 1;  // the scaled factor holds the centre
-  __syncthreads();
+  if (ltid() == 0) *s.oc = s_left ? i : i + 1;  // the scaled factor holds the centre
+  cta_sync();
 }
 
 // _init_envs (Algorithms.jl:802-819) after moving the centre to site 0.
-__device__ void init_envs(Ctx& c, const DState& s) {
+static __device__ void init_envs(Ctx& c, const DState& s) {
   const int L = c.P.L;
   shift_oc(c, s, 0);
   identity_env(c, envR(c, L), s.chi[L], c.P.w[L]);
@@ -545,13 +583,13 @@ __device__ void init_envs(Ctx& c, const DState& s) {
 }
 
 // exp(-i dtb H_bond) C on bond b (project_bond, Algorithms.jl:222-226), C (k x r).
-__device__ void evolve_bond(Ctx& c, cplx* C, int k, int r, int b, double dtb) {
+static __device__ void evolve_bond(Ctx& c, cplx* C, int k, int r, int b, double dtb) {
   evolve(c, C, k, 1, r, b, b, c.P.wm_bond[b], dtb);
 }
 
 // Site i = Q R (thin QR): Q -> site i, EL[i+1] from it, R evolved by dtb on
 // bond i+1 and absorbed into site i+1 (Algorithms.jl:491-505).
-__device__ void qr_bond_forward(Ctx& c, const DState& s, int i, double dtb) {
+static __device__ void qr_bond_forward(Ctx& c, const DState& s, int i, double dtb) {
   const int l = s.chi[i], r = s.chi[i + 1], m = 2 * l, rn = min(m, r);
   const int r2 = s.chi[i + 2];
   cplx* A = site_ptr(c, s, i);
@@ -560,7 +598,7 @@ __device__ void qr_bond_forward(Ctx& c, const DState& s, int i, double dtb) {
   cplx* Rb = c.ws + c.P.lay.tB;
   cplx* T = c.ws + c.P.lay.tC;
   cta_copy(H, A, (long long)m * r);
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(H, m, r, c.sm.la, c.sm.e.r);
   dev_qr_formq(H, m, r, A, c.sm.la);
   dev_qr_extract_r(H, m, r, Rb);
@@ -570,12 +608,12 @@ __device__ void qr_bond_forward(Ctx& c, const DState& s, int i, double dtb) {
   evolve_bond(c, Rb, rn, r, i + 1, dtb);
   cta_gemm(gemm_args(rn, 2 * r2, r, Rb, 1, rn, An, 1, r, T, 1, rn), c.sm.e.u.gw.g);
   cta_copy(An, T, (long long)rn * 2 * r2);
-  __syncthreads();
+  cta_sync();
 }
 
 // Site i = L Q (thin LQ): Q -> site i, ER[i] from it, L evolved by dtb on
 // bond i and absorbed into site i-1 (Algorithms.jl:515-529).
-__device__ void lq_bond_backward(Ctx& c, const DState& s, int i, double dtb) {
+static __device__ void lq_bond_backward(Ctx& c, const DState& s, int i, double dtb) {
   const int l = s.chi[i], r = s.chi[i + 1], n2 = 2 * r, rn = min(l, n2);
   const int lp = s.chi[i - 1];
   cplx* A = site_ptr(c, s, i);
@@ -583,20 +621,20 @@ __device__ void lq_bond_backward(Ctx& c, const DState& s, int i, double dtb) {
   cplx* H = c.ws + c.P.lay.tA;
   cplx* Qh = c.ws + c.P.lay.tB;
   cplx* Rb = c.ws + c.P.lay.tC;
-  for (int e = threadIdx.x; e < n2 * l; e += NT) {
+  for (int e = ltid(); e < n2 * l; e += NT) {
     int cc = (int)(e % n2), ii = (int)(e / n2);
     H[e] = cconj(A[ii + (long long)l * cc]);
   }
-  __syncthreads();
+  cta_sync();
   dev_qr_factor(H, n2, l, c.sm.la, c.sm.e.r);
   dev_qr_formq(H, n2, l, Qh, c.sm.la);
   dev_qr_extract_r(H, n2, l, Rb);
-  for (int e = threadIdx.x; e < rn * n2; e += NT) {
+  for (int e = ltid(); e < rn * n2; e += NT) {
     int k = (int)(e % rn), cc = (int)(e / rn);
     A[e] = cconj(Qh[cc + (long long)n2 * k]);
   }
   cplx* Lm = H;  // L = R^H (l x rn)
-  for (int e = threadIdx.x; e < l * rn; e += NT) {
+  for (int e = ltid(); e < l * rn; e += NT) {
     int a = (int)(e % l), k = (int)(e / l);
     Lm[e] = cconj(Rb[k + (long long)rn * a]);
   }
@@ -606,15 +644,15 @@ __device__ void lq_bond_backward(Ctx& c, const DState& s, int i, double dtb) {
   evolve_bond(c, Lm, l, rn, i, dtb);
   cta_gemm(gemm_args(2 * lp, rn, l, Ap, 1, 2 * lp, Lm, 1, l, Rb, 1, 2 * lp), c.sm.e.u.gw.g);
   cta_copy(Ap, Rb, (long long)2 * lp * rn);
-  __syncthreads();
+  cta_sync();
 }
 
-__device__ void evolve_site1(Ctx& c, const DState& s, int i, double dts) {
+static __device__ void evolve_site1(Ctx& c, const DState& s, int i, double dts) {
   evolve(c, site_ptr(c, s, i), s.chi[i], 2, s.chi[i + 1], i, i + 1, c.P.wm_heff1[i], dts);
 }
 
 // _tdvp_sweep_hamiltonian_1site! (Algorithms.jl:472-533).
-__device__ void tdvp_sweep_1site(Ctx& c, const DState& s) {
+static __device__ void tdvp_sweep_1site(Ctx& c, const DState& s) {
   const int L = c.P.L;
   const double dt = c.P.dt;
   init_envs(c, s);
@@ -626,9 +664,9 @@ __device__ void tdvp_sweep_1site(Ctx& c, const DState& s) {
     evolve_site1(c, s, i, dt / 2);
     if (i > 0) lq_bond_backward(c, s, i, -dt / 2);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) *s.oc = 0;
-  __syncthreads();
+  cta_sync();
+  if (ltid() == 0) *s.oc = 0;
+  cta_sync();
 }
 
 // local_dynamic_tdvp (mqt-yaqs/src/mqt/yaqs/core/methods/tdvp.py:667-855):
@@ -636,7 +674,7 @@ __device__ void tdvp_sweep_1site(Ctx& c, const DState& s) {
 // keeping min(rank, max_bond_dim) values), a 1-site update with bond
 // back-evolution once it has reached it; once a 1-site step reaches the
 // last bond the last site (first site on the way back) is updated alone.
-__device__ void tdvp_sweep_dynamic(Ctx& c, const DState& s) {
+static __device__ void tdvp_sweep_dynamic(Ctx& c, const DState& s) {
   const int L = c.P.L;
   const double dt = c.P.dt;
   cplx* th = c.ws + c.P.lay.th;
@@ -680,12 +718,12 @@ __device__ void tdvp_sweep_dynamic(Ctx& c, const DState& s) {
       if (i != 1) evolve(c, site_ptr(c, s, i - 1), s.chi[i - 1], 2, s.chi[i], i - 1, i, c.P.wm_heff1[i - 1], -dt / 2);
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) *s.oc = 0;
-  __syncthreads();
+  cta_sync();
+  if (ltid() == 0) *s.oc = 0;
+  cta_sync();
 }
 
-__device__ void tdvp_sweep_2site(Ctx& c, const DState& s) {
+static __device__ void tdvp_sweep_2site(Ctx& c, const DState& s) {
   const int L = c.P.L;
   const double dt = c.P.dt;
   cplx* th = c.ws + c.P.lay.th;
@@ -714,7 +752,7 @@ __device__ void tdvp_sweep_2site(Ctx& c, const DState& s) {
   }
 }
 
-__device__ void tdvp_sweep(Ctx& c, const DState& s) {
+static __device__ void tdvp_sweep(Ctx& c, const DState& s) {
   ProfScope prof_scope_(PF_SWEEP);
   if (c.P.tdvp_mode == 1)
     tdvp_sweep_1site(c, s);
@@ -728,8 +766,8 @@ __device__ void tdvp_sweep(Ctx& c, const DState& s) {
 // Local operators
 // ---------------------------------------------------------------------------
 // A[l,p,r] <- sum_k op[p,k] A[l,k,r] for a d x d op (d = 2 or 4), in place.
-__device__ void apply_local(cplx* A, int l, int d, int r, const cplx* op) {
-  for (int e = threadIdx.x; e < l * r; e += NT) {
+static __device__ void apply_local(cplx* A, int l, int d, int r, const cplx* op) {
+  for (int e = ltid(); e < l * r; e += NT) {
     long long a = e % l, b = e / l;
     cplx v[4], o[4];
     for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
@@ -740,13 +778,13 @@ __device__ void apply_local(cplx* A, int l, int d, int r, const cplx* op) {
     }
     for (int p = 0; p < d; ++p) A[a + (long long)l * (p + (long long)d * b)] = o[p];
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // sum |op . A|^2 (or sum |A|^2 when op == nullptr), d = 2 or 4.
-__device__ double local_norm2(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
+static __device__ double local_norm2(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
   double sacc = 0.0;
-  for (int e = threadIdx.x; e < l * r; e += NT) {
+  for (int e = ltid(); e < l * r; e += NT) {
     long long a = e % l, b = e / l;
     cplx v[4];
     for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
@@ -764,9 +802,9 @@ __device__ double local_norm2(Ctx& c, const cplx* A, int l, int d, int r, const 
 }
 
 // Re sum conj(A) (op A)
-__device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
+static __device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const cplx* op) {
   double sacc = 0.0;
-  for (int e = threadIdx.x; e < l * r; e += NT) {
+  for (int e = ltid(); e < l * r; e += NT) {
     long long a = e % l, b = e / l;
     cplx v[4];
     for (int p = 0; p < d; ++p) v[p] = A[a + (long long)l * (p + (long long)d * b)];
@@ -786,12 +824,12 @@ __device__ double local_expect(Ctx& c, const cplx* A, int l, int d, int r, const
 // model of a gate on sites (f1, f2) (create_local_noise_model,
 // DigitalTJM.jl:172-188): 1-site processes on either site and 2-site
 // processes on exactly that pair.
-__device__ __forceinline__ bool proc_on(const DevProc& pr, int f1, int f2) {
+static __device__ __forceinline__ bool proc_on(const DevProc& pr, int f1, int f2) {
   if (f1 < 0) return true;
   return pr.nsites == 1 ? (pr.s0 == f1 || pr.s0 == f2) : ((pr.s0 == f1 && pr.s1 == f2) || (pr.s0 == f2 && pr.s1 == f1));
 }
 
-__device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt, int f1 = -1, int f2 = -1) {
+static __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt, int f1 = -1, int f2 = -1) {
   ProfScope prof_scope_(PF_DISS);
   const int L = c.P.L;
   bool all_zero = c.P.all_zero != 0;
@@ -816,16 +854,16 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
     if (c.P.noise_present && !all_zero) {
       cplx* A = site_ptr(c, s, 0);
       cta_scale(A, (long long)s.chi[0] * 2 * s.chi[1], fscal);
-      __syncthreads();
+      cta_sync();
     }
-    if (threadIdx.x == 0) c.sm.canon = 1;
-    __syncthreads();
+    if (ltid() == 0) c.sm.canon = 1;
+    cta_sync();
     return;
   }
   // The reference sweep applies its first dissipators to site L while the
   // centre sits elsewhere, so the chain is not canonical afterwards.
-  if (threadIdx.x == 0) c.sm.canon = 0;
-  __syncthreads();
+  if (ltid() == 0) c.sm.canon = 0;
+  cta_sync();
   if (!c.P.noise_present || all_zero) {
     for (int i = L - 1; i >= 1 && !c.sm.fail; --i) shift_oc(c, s, i - 1);
     return;
@@ -839,7 +877,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
         const long long n = (long long)s.chi[i] * 2 * s.chi[i + 1];
         if (pr.pauli_name) {
           cta_scale(A, n, exp(-0.5 * dt * pr.gamma));
-          __syncthreads();
+          cta_sync();
         } else {
           apply_local(A, s.chi[i], 2, s.chi[i + 1], full ? pr.diss_full : pr.diss_half);
         }
@@ -851,7 +889,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
         if (pr.nsites == 2 && pr.s1 == i && proc_on(pr, f1, f2)) {
           if (pr.pauli_name) {  // Pauli names and long-range processes: a scalar at the right site
             cta_scale(site_ptr(c, s, i), (long long)s.chi[i] * 2 * s.chi[i + 1], exp(-0.5 * dt * pr.drate));
-            __syncthreads();
+            cta_sync();
           } else {
             const int l = s.chi[i - 1], r = s.chi[i + 1];
             merge(c, s, i - 1, th);
@@ -870,7 +908,7 @@ __device__ void apply_dissipation(Ctx& c, const DState& s, bool full, double dt,
 // ---------------------------------------------------------------------------
 // Stochastic process (StochasticProcess.jl:219-330)
 // ---------------------------------------------------------------------------
-__device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = -1, int f2 = -1) {
+static __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = -1, int f2 = -1) {
   ProfScope prof_scope_(PF_STOCH);
   const int L = c.P.L;
   const double dp = 1.0 - scalar_product(c, s);
@@ -899,7 +937,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
       if (pr.nsites == 1 && pr.s0 == site && proc_on(pr, f1, f2)) {
         double nr = local_norm2(c, site_ptr(c, s, site), s.chi[site], 2, s.chi[site + 1],
                                 pr.pauli_proc ? nullptr : pr.mat);
-        if (threadIdx.x == 0) {
+        if (ltid() == 0) {
           cand[nc] = dt * pr.gamma * nr;
           candp[nc] = k;
         }
@@ -917,7 +955,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
             merge(c, s, site, th);
             nr = local_norm2(c, th, s.chi[site], 4, s.chi[site + 2], pr.mat);
           }
-          if (threadIdx.x == 0) {
+          if (ltid() == 0) {
             cand[nc] = dt * pr.gamma * nr;
             candp[nc] = k;
           }
@@ -933,13 +971,13 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
     if (!pr.lr || !proc_on(pr, f1, f2)) continue;
     const double nr = pr.pauli_proc ? local_norm2(c, site_ptr(c, s, L - 1), s.chi[L - 1], 2, s.chi[L], nullptr)
                                     : lr_weight(c, s, pr);
-    if (threadIdx.x == 0) {
+    if (ltid() == 0) {
       cand[nc] = dt * pr.gamma * nr;
       candp[nc] = k;
     }
     ++nc;
   }
-  __syncthreads();
+  cta_sync();
   double total = 0.0;
   for (int e = 0; e < nc; ++e) total += cand[e];
   if (total == 0.0) {
@@ -957,7 +995,7 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
     }
   }
   const DevProc& pr = c.P.procs[candp[chosen]];
-  __syncthreads();
+  cta_sync();
   if (pr.lr) {
     // "pauli_long_range" has no branch of its own in the reference
     // (StochasticProcess.jl:311 tests "mpo_pauli"): only the normalisation acts
@@ -972,14 +1010,14 @@ __device__ void stochastic_process(Ctx& c, const DState& s, double dt, int f1 = 
     apply_local(th, l, 4, rr, pr.mat);
     split(c, s, pr.s0, th, l, rr, 1, false);
   }
-  if (threadIdx.x == 0) c.cnt[3] += 1;
+  if (ltid() == 0) c.cnt[3] += 1;
   finish_normalize(c, s);
 }
 
 // ---------------------------------------------------------------------------
 // Observables
 // ---------------------------------------------------------------------------
-__device__ void evaluate(Ctx& c, const DState& s, int col) {
+static __device__ void evaluate(Ctx& c, const DState& s, int col) {
   ProfScope prof_scope_(PF_EVAL);
   const int ncols = c.P.ncols;
   for (int k = 0; k < c.P.nobs && !c.sm.fail; ++k) {
@@ -998,7 +1036,7 @@ __device__ void evaluate(Ctx& c, const DState& s, int col) {
       const int l = s.chi[o.s0], r = s.chi[o.s0 + 1];
       SvdWork w = svd_work(c);
       SvdResult res = dev_svd(site_ptr(c, s, o.s0), 2 * l, r, SVD_LEFT, w, c.sm.la, c.sm.e.r, c.sm.e.u.svd);
-      if (threadIdx.x == 0) {
+      if (ltid() == 0) {
         double nsq = 0.0;
         for (int e = 0; e < res.p; ++e) nsq += w.sig[e] * w.sig[e];
         double ent = 0.0;
@@ -1008,16 +1046,16 @@ __device__ void evaluate(Ctx& c, const DState& s, int col) {
         }
         c.sm.bcast_d[1] = ent;
       }
-      __syncthreads();
+      cta_sync();
       val = c.sm.bcast_d[1];
-      __syncthreads();
+      cta_sync();
     }
-    if (threadIdx.x == 0) c.P.traj_out[((long long)c.traj * c.P.nobs + k) * ncols + col] = val;
+    if (ltid() == 0) c.P.traj_out[((long long)c.traj * c.P.nobs + k) * ncols + col] = val;
   }
-  if (threadIdx.x == 0) {
+  if (ltid() == 0) {
     int mx = 0;
     for (int b = 0; b <= c.P.L; ++b) mx = max(mx, s.chi[b]);
     if (c.P.chi_out) c.P.chi_out[(long long)c.traj * ncols + col] = mx;
   }
-  __syncthreads();
+  cta_sync();
 }
