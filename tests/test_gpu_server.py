@@ -52,11 +52,17 @@ def _ring(n, p, nt, seed):
 
 
 def _alone(problem, seed, precision="fp64"):
+    """The request run alone: FP64 requests as a direct run (the server's
+    FP64 arithmetic is the direct run's), mixed ones alone in a server of the
+    same shape (direct mixed runs take the tcgen05 products, served runs the
+    mma.sync form)."""
     psi, op, cfg, nm = problem
     if isinstance(op, api.DigitalCircuit):
         return api.run_circuit_descriptors(api.CircuitDescriptors(psi, op, cfg, nm, seed=seed))
-    prec = A.YAQS_PREC_MIXED if precision == "mixed" else A.YAQS_PREC_FP64
-    return api.run_descriptors(api.Descriptors(psi, op, cfg, nm, seed=seed, precision=prec))
+    if precision == "mixed":
+        with api.Server(max_L=16, max_bond_dim=32, max_mpo_width=5, chunk=2) as srv:
+            return srv.result(srv.submit(psi, op, cfg, nm, seed=seed, precision=precision), timeout=300)
+    return api.run_descriptors(api.Descriptors(psi, op, cfg, nm, seed=seed, precision=A.YAQS_PREC_FP64))
 
 
 def test_results_alone_equal_results_in_the_mix():
