@@ -1,21 +1,28 @@
 #!/usr/bin/env python
-"""Benchmark: TJM trajectory-steps/s of the analog engine.
+"""Benchmark: TJM trajectory-steps/s of the analog engine, mixed-precision
+form against the plain FP64 form.
 
 Workload (default): the L=30 Heisenberg chain H = sum(XX+YY+ZZ) + 0.3 sum Z
 (init_general_hamiltonian(30,1,1,1,0,0,0.3)), dephasing (pauli_z, gamma=0.05)
 on every site, dt=0.05, 1-site TDVP with 2-site growth up to bond dimension
 64 (the local dynamic TDVP of the Python lineage; --tdvp 2site runs the Julia
-reference's two_site_tdvp! instead), threshold 1e-9,
-second-order TJM with sampling at every time index, <Z_i> on all 30 sites
-plus the half-chain entropy, 1024 trajectories per GPU, Philox draws.  The
-start state is an MPS with every bulk bond already at 64 (Gaussian
-entries, normalised by the engine) so every timed step runs at chi=64; with
---start neel the run starts from the Neel state instead.
+reference's two_site_tdvp! instead), threshold 1e-9, second-order TJM with
+sampling at every time index, <Z_i> on all 30 sites plus the half-chain
+entropy, 1024 trajectories per GPU, Philox draws.  The start state is an MPS
+with every bulk bond already at 64 (Gaussian entries, normalised by the
+engine) so every timed step runs at chi=64; with --start neel the run
+starts from the Neel state instead.
+
+The default form is the mixed-precision one (H_eff products in complex FP32
+on tcgen05, Lanczos/SVD/QR/norms in FP64); the plain ComplexF64 form is
+timed beside it in the same process on the same problem and draws
+(vs_baseline = mixed / plain, the metric's comparison), and every recorded
+<Z_i> and S_half of the two runs gives the error against FP64.
 
 A step is one recorded time index of every trajectory (two TDVP sweeps,
 dissipation, jump, measurement).  W untimed steps, then K timed steps,
 bracketed by a barrier and a device synchronisation; device time from CUDA
-events on the launching stream; the trajectory states (3.6 GB) are larger
+events on the launching stream; the trajectory states (2.5 GB) are larger
 than L2.  Multi-GPU runs are independent replicas (one process per GPU,
 launched by torchrun); the value is the sum of every rank's trajectory-steps
 over the slowest rank's time.
@@ -26,11 +33,11 @@ bonds, RX(2 g dt) on every qubit, a SAMPLE_OBSERVABLES barrier; J = g = 1,
 dt = 0.05, 60 layers), Pauli X/Y/Z noise 0.01 per qubit after every 2-qubit
 gate, TEBD with chi_max = 128 and threshold 1e-9, 512 trajectories, <Z_i> on
 every qubit after every layer.  A step is one Trotter layer of every
-trajectory (three launches of the processed circuit).
+trajectory.
 
 --impl reference times the CPU restatement of the reference algorithm
-(the reference itself is Julia, not runnable here) on all host cores, on
-bounded samples of the same workload.
+(the reference itself is Julia, not runnable here) on all host cores with
+its contractions on OpenBLAS zgemm, on bounded samples of the same workload.
 """
 from __future__ import annotations
 
@@ -51,13 +58,13 @@ sys.path.insert(0, ROOT)
 from yaqs_julia_b200 import _abi as A  # noqa: E402
 from yaqs_julia_b200 import api  # noqa: E402
 
-# DRAM bytes (read + write) of the timed launch, from one ncu capture of the
-# same command: (precision, tdvp, L, chi, trajectories, timed steps) -> bytes
-TIMED_TRAFFIC = {("fp64", "dynamic", 30, 64, 1024, 2): 10.53346e12 + 4.24245e12}
 # the same for the digital workload: (L, trajectories, timed layers) -> bytes
 DIG_TIMED_TRAFFIC = {(40, 512, 57): 4.458638080e9 + 15.767363584e9}
 
-METRIC = "TJM trajectory-steps/s (L=30 Heisenberg, chi=64, 1024 trajectories)"
+METRIC = "TJM trajectory-steps/s (L=30 Heisenberg, chi=64, 1024 trajectories) vs plain FP64 GPU"
+# DRAM read + write bytes per trajectory-step of the trajectory kernel, from
+# one small-case ncu capture per configuration: (precision, tdvp, L, chi) -> bytes
+TRAFFIC_PER_TRAJ_STEP = {}
 TDVP_NAMES = {"dynamic": A.YAQS_TDVP_DYNAMIC, "2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE}
 TDVP = [A.YAQS_TDVP_DYNAMIC]  # set from --tdvp
 TDVP_DESC = {"dynamic": "1-site TDVP with 2-site growth (local dynamic TDVP)", "2site": "2-site TDVP",
@@ -256,18 +263,27 @@ def reduce_sum(dist, v):
 
 
 def cpu_sample(L, chi, start):
-    """Oracle (CPU restatement, test infrastructure) on all host cores:
-    3 recorded time indices (1.5 sweeps per trajectory-step) for one
-    trajectory per core.  Returns (trajectory-steps/s, cores, sample text)."""
+    """The reference path on the host cores: the oracle (CPU restatement,
+    test infrastructure) with its contractions on OpenBLAS zgemm (the
+    reference's backend), one trajectory per core, 4 recorded time indices
+    from the same saturated start.  Order-2 sampling runs 2 (n - 1) - 1 = 5
+    TDVP sweeps for those 3 indices, and a timed GPU step runs 2, so the rate
+    counts 5 / 2 trajectory-steps per trajectory.  Returns (trajectory-steps/s,
+    cores, sample text, BLAS description)."""
     from oracle import oracle as O
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    psi, H, cfg, nm = workload(L, chi, 3, cores, start)
+    psi, H, cfg, nm = workload(L, chi, 4, cores, start)
     d = api.Descriptors(psi, H, cfg, nm, seed=SEED, tdvp_mode=TDVP[0])
-    t0 = time.perf_counter()
-    O.analog_run(d, nthreads=cores)
-    dt = time.perf_counter() - t0
-    steps = cores * 2
-    return steps / dt, cores, f"{cores} trajectories x 2 time indices (t=0..0.1) of the same workload, {dt:.1f} s"
+    blas = O.set_blas(True)
+    try:
+        t0 = time.perf_counter()
+        O.analog_run(d, nthreads=cores)
+        dt = time.perf_counter() - t0
+    finally:
+        O.set_blas(False)
+    steps = cores * 2.5
+    return (steps / dt, cores, f"{cores} trajectories x 4 time indices (5 TDVP sweeps = 2.5 trajectory-steps each) "
+                               f"of the same workload from the same saturated start, {dt:.1f} s", blas)
 
 
 def cpu_sample_digital(L, depth):
@@ -316,18 +332,21 @@ def run_reference(args):
         print(json.dumps(line), flush=True)
         return
     vals = []
-    for k in range(args.warmup + args.steps):
-        v, cores, sample = cpu_sample(args.L, args.chi, args.start)
-        if k >= args.warmup:
+    nrep = max(1, min(args.steps, 3))  # bounded: each repetition is ~10 s of host work
+    for k in range(min(args.warmup, 1) + nrep):
+        v, cores, sample, blas = cpu_sample(args.L, args.chi, args.start)
+        if k >= min(args.warmup, 1):
             vals.append(v)
     value = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": analog_config(args, args.L, args.chi, args.traj, args.gpus),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "blas": blas,
+                             "sample": f"{nrep} timed samples after 1 untimed: " + sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "reference Julia (Yaqs.jl) cannot run here; CPU restatement (oracle/tjm_oracle.cpp)"}
+            "note": "reference Julia (Yaqs.jl) cannot run here; CPU restatement (oracle/tjm_oracle.cpp) in "
+                    "ComplexF64 with its contractions on OpenBLAS zgemm"}
     print(json.dumps(line), flush=True)
 
 
@@ -537,16 +556,23 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
-    ws, rank, local, dist = dist_setup()
-    import torch
-    torch.cuda.set_device(local)
-    from yaqs_julia_b200 import _lib
-    ctx = _lib.Context(local)
-    L, chi, nt = args.L, args.chi, args.traj
-    n_times = args.warmup + args.steps + 1
-    psi, H, cfg, nm = workload(L, chi, n_times, nt, args.start)
-    prec = A.YAQS_PREC_MIXED if args.precision == "mixed" else A.YAQS_PREC_FP64
+def measured_peaks():
+    """Roofline denominators: the driver-measured peaks of this pool's B200s
+    (MEASURED_PEAKS.json beside this file), else the stated fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    except (OSError, ValueError, KeyError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def timed_session(args, ctx, dist, local, problem, prec, rank, nt, n_steps):
+    """One resident run: W untimed time indices, then n_steps timed ones in one
+    launch (CUDA events on the launching stream, barrier + synchronize on both
+    sides); returns device ms, the run's counters before/after, its results
+    and the clock record."""
+    psi, H, cfg, nm = problem
     desc = api.Descriptors(psi, H, cfg, nm, seed=SEED, traj_offset=rank * nt, precision=prec, tdvp_mode=TDVP[0])
     sess = api.Session(desc, ctx)
     for _ in range(args.warmup):
@@ -555,80 +581,126 @@ def run_ours(args):
     clocks = ClockSampler(local)
     barrier_sync(dist)
     clocks.start()
-    dev_ms = sess.advance(args.steps)
+    dev_ms = sess.advance(n_steps)
     barrier_sync(dist)
     ck = clocks.stop()
     st1 = sess.stats()
     phases = sess.profile() if args.profile else None
     res = sess.finish()
-    t_max = reduce_max(dist, dev_ms / 1e3)
-    steps_all = reduce_sum(dist, nt * args.steps)
-    value = steps_all / t_max
-    flops_timed = st1["flops"] - st0["flops"]
-    matvecs_timed = st1["matvecs"] - st0["matvecs"]
+    return {"dev_ms": dev_ms, "st0": st0, "st1": st1, "res": res, "clocks": ck, "phases": phases}
+
+
+def run_ours(args):
+    ws, rank, local, dist = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from yaqs_julia_b200 import _lib
+    ctx = _lib.Context(local)
+    L, chi, nt = args.L, args.chi, args.traj
+    K = args.steps
+    mixed = args.precision == "mixed"
+    problem = workload(L, chi, args.warmup + K + 1, nt, args.start)
+    prec = A.YAQS_PREC_MIXED if mixed else A.YAQS_PREC_FP64
+    main = timed_session(args, ctx, dist, local, problem, prec, rank, nt, K)
+    t_max = reduce_max(dist, main["dev_ms"] / 1e3)
+    value = reduce_sum(dist, nt * K) / t_max
+    flops_timed = main["st1"]["flops"] - main["st0"]["flops"]
+    matvecs_timed = main["st1"]["matvecs"] - main["st0"]["matvecs"]
+    achieved = flops_timed / (main["dev_ms"] / 1e3) / 1e12
     import ctypes as C
     pk = C.c_double(0.0)
     ctx.check(ctx._lib.yaqs_fp64_peak(ctx.handle, C.byref(pk)))
-    achieved = flops_timed / (dev_ms / 1e3) / 1e12
-    # end to end: the public C-ABI call on host buffers, a complete run of 2K
-    # time indices from t = 0 (its first index costs one sweep, the others two)
-    e2e_steps = 2 * args.steps
-    e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm = workload(L, chi, e2e_steps + 1, nt, args.start)
+    peaks = measured_peaks()
+    # the plain ComplexF64 form on the same problem and draws, in the same
+    # process: the metric's comparison and the reference of the error
+    plain, err, ratio = None, None, None
+    if mixed and not args.no_plain:
+        Kp = min(K, args.plain_steps)
+        pl = timed_session(args, ctx, dist, local, problem, A.YAQS_PREC_FP64, rank, nt, Kp)
+        p_value = reduce_sum(dist, nt * Kp) / reduce_max(dist, pl["dev_ms"] / 1e3)
+        ratio = value / p_value
+        p_achieved = (pl["st1"]["flops"] - pl["st0"]["flops"]) / (pl["dev_ms"] / 1e3) / 1e12
+        plain = {"what": "plain ComplexF64 GPU form (FP64 tensor-core products), same problem, same Philox draws, "
+                         "same process", "value": p_value, "unit": UNIT, "steps": Kp,
+                 "ms_per_step": pl["dev_ms"] / Kp, "clocks": pl["clocks"],
+                 "roofline": {"bound": "tensor", "achieved": p_achieved, "peak": pk.value, "unit": "TFLOP/s",
+                              "frac": p_achieved / pk.value if pk.value else None,
+                              "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run"}}
+        ncol = args.warmup + Kp + 1  # time indices both runs recorded
+        a = main["res"].trajectories[:, :, :ncol]
+        b = pl["res"].trajectories[:, :, :ncol]
+        dz = np.abs(a[:, :L] - b[:, :L])
+        ds = np.abs(a[:, L] - b[:, L])
+        err = {"z_max_abs": float(dz.max()), "z_mean_abs": float(dz.mean()), "s_half_max_abs": float(ds.max()),
+               "s_half_mean_abs": float(ds.mean()),
+               "z_ensemble_mean_max_abs": float(np.abs(a[:, :L].mean(0) - b[:, :L].mean(0)).max()),
+               "trajectories_compared": nt, "time_indices_compared": ncol,
+               "run": f"every <Z_i> and S_half at {ncol} recorded time indices (saturated start, {args.warmup} "
+                      f"warm-up and {Kp} timed indices) of the two forms on the same Philox draws"}
+    # end to end: the public C-ABI call on host buffers (marshalling, uploads,
+    # allocation, a complete run of K time indices from t = 0 whose first
+    # index costs one sweep, result download)
+    e2e_problem = workload(L, chi, K + 1, nt, args.start)
     barrier_sync(dist)
     t0 = time.perf_counter()
-    e2e_desc = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt,
-                               precision=prec, tdvp_mode=TDVP[0])
-    e2e_res = api.run_descriptors(e2e_desc, ctx)
+    e2e_desc = api.Descriptors(*e2e_problem, seed=SEED, traj_offset=rank * nt, precision=prec, tdvp_mode=TDVP[0])
+    api.run_descriptors(e2e_desc, ctx)
     barrier_sync(dist)
     e2e_s = reduce_max(dist, time.perf_counter() - t0)
-    err = None
-    if args.precision == "mixed":
-        # the same run (same draws) in the FP64 form: error of every observable
-        d64 = api.Descriptors(e2e_cfg_psi, e2e_H, e2e_cfg, e2e_nm, seed=SEED, traj_offset=rank * nt,
-                              tdvp_mode=TDVP[0])
-        r64 = api.run_descriptors(d64, ctx)
-        dz = np.abs(e2e_res.trajectories[:, :L] - r64.trajectories[:, :L])
-        ds = np.abs(e2e_res.trajectories[:, L] - r64.trajectories[:, L])
-        same = np.all(np.abs(e2e_res.trajectories - r64.trajectories).reshape(nt, -1).max(1) < 1e-3)
-        err = {"z_max_abs": float(dz.max()), "z_mean_abs": float(dz.mean()), "s_half_max_abs": float(ds.max()),
-               "z_ensemble_mean_max_abs": float(np.abs(e2e_res.mean[:L] - r64.mean[:L]).max()),
-               "trajectories_compared": nt, "all_jump_records_equal": bool(same),
-               "run": f"{e2e_steps} time indices from t=0, same Philox draws"}
     h2d, d2h = desc_bytes(e2e_desc, e2e_desc.n_obs, e2e_desc.n_out, nt, L)
-    e2e_value = reduce_sum(dist, nt * e2e_steps) / e2e_s
+    e2e_value = reduce_sum(dist, nt * K) / e2e_s
     cpu = None
     if rank == 0 and not args.no_cpu and ws == 1:
-        v, cores, sample = cpu_sample(L, chi, args.start)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        v, cores, sample, blas = cpu_sample(L, chi, args.start)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "blas": blas, "sample": sample}
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
-                "dtype": "c64 contractions (3xTF32 tensor cores) + c128 Lanczos/SVD/QR/norms"
-                if args.precision == "mixed" else "c128", "data": "synthetic",
+        traffic_per = TRAFFIC_PER_TRAJ_STEP.get((args.precision, args.tdvp, L, chi))
+        if mixed:
+            tc_peak = peaks["bf16_tflops"] / 2
+            roof = {"bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
+                    "frac": achieved / tc_peak,
+                    "peak_source": f"half the {peaks['source']} dense bf16 rate (MEASURED_PEAKS.json): the rate of "
+                                   "the tcgen05 kind::tf32 MMAs the mixed products issue",
+                    "achieved_counts": "H_eff product flops only, 8 per complex MAC (the tensor pipe executes 9 "
+                                       "TF32 MMAs per 4 real MACs: 3-product complex form x 3xTF32 split)"}
+        else:
+            roof = {"bound": "tensor", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
+                    "frac": achieved / pk.value if pk.value else None,
+                    "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run; MEASURED_PEAKS.json "
+                                   "has no FP64 entry",
+                    "achieved_counts": "H_eff product flops only (8 flops per complex MAC)"}
+        tt = traffic_per * nt * K if traffic_per else None
+        roof.update({"kernel": "tjm_step_kernel_tc" if mixed else "tjm_step_kernel", "traffic": tt,
+                     "traffic_source": "DRAM read+write bytes per trajectory-step from a one-launch ncu capture "
+                                       "of a small case of the same configuration (profiles/), scaled by the "
+                                       "trajectory-steps of the timed launch; null when not captured",
+                     "traffic_gbs": tt / (main["dev_ms"] / 1e3) / 1e9 if tt else None,
+                     "hbm_frac": tt / (main["dev_ms"] / 1e3) / 1e9 / peaks["hbm_gbs"] if tt else None})
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+                "warmup": args.warmup, "ms_per_step": main["dev_ms"] / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": ratio,
+                "vs_baseline_note": "value / the plain ComplexF64 GPU form's value measured in the same run (the "
+                                    "metric's own comparison; the reference publishes no throughput)"
+                if ratio is not None else None,
+                "dtype": "c64 contractions (tcgen05 3xTF32) + c128 Lanczos/SVD/QR/norms" if mixed else "c128",
+                "data": "synthetic",
                 "config": analog_config(args, L, chi, nt, ws),
-                "gpu_launches": 1,  # one tjm_step_kernel launch covers the K time indices
-                "roofline": {"bound": "tensor", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
-                             "frac": achieved / pk.value if pk.value else None,
-                             "traffic": TIMED_TRAFFIC.get((args.precision, args.tdvp, L, chi, nt, args.steps)),
-                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the timed "
-                                               "launch (profiles/tjm_step_kernel_L30_chi64_1024traj_dynamic_"
-                                               "launches.md); null for configurations not captured",
-                             "kernel": "tjm_step_kernel",
-                             "peak_source": "measured FP64 DFMA probe (yaqs_fp64_peak) in this run; "
-                                            "MEASURED_PEAKS.json has no FP64 entry",
-                             "achieved_counts": "H_eff product flops only (8 flops per complex MAC)"},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
-                        "d2h_bytes_per_step": d2h / e2e_steps, "seconds": e2e_s, "steps": e2e_steps},
-                "cpu_baseline": cpu, "clocks": ck,
+                "gpu_launches": 1,  # one trajectory-kernel launch covers the K time indices
+                "roofline": roof,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+                        "d2h_bytes_per_step": d2h / K, "seconds": e2e_s, "steps": K,
+                        "precision": args.precision},
+                "cpu_baseline": cpu, "clocks": main["clocks"],
                 "stats": {"matvecs_timed": matvecs_timed, "flops_timed": flops_timed,
-                          "jumps": res.stats["jumps"], "svd_sweeps": res.stats["svd_sweeps"],
-                          "svds": res.stats["svds"], "max_bond": int(res.max_bond.max())}}
+                          "jumps": main["res"].stats["jumps"], "svd_sweeps": main["res"].stats["svd_sweeps"],
+                          "svds": main["res"].stats["svds"], "max_bond": int(main["res"].max_bond.max())}}
+        if plain is not None:
+            line["plain_fp64"] = plain
         if err is not None:
             line["err_vs_fp64"] = err
-        if phases:
-            tot = phases["step"] or 1.0
-            line["phases_pct_of_step"] = {k: round(100 * v / tot, 2) for k, v in phases.items()}
+        if main["phases"]:
+            tot = main["phases"]["step"] or 1.0
+            line["phases_pct_of_step"] = {k: round(100 * v / tot, 2) for k, v in main["phases"].items()}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -644,8 +716,12 @@ def main():
                          "mode), 2site (the Julia reference's two_site_tdvp!) or 1site")
     ap.add_argument("--chunk", type=int, default=2, help="batch/serve: positions each run advances per launch")
     ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of Poisson arrivals")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="analog contraction precision: fp64, or mixed (complex FP32 on the tensor cores)")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="analog contraction precision: mixed (complex FP32 on the tensor cores, the metric's "
+                         "subject; the plain FP64 form is timed beside it) or fp64 alone")
+    ap.add_argument("--plain-steps", type=int, default=8,
+                    help="mixed runs: timed time indices of the plain FP64 form measured beside it")
+    ap.add_argument("--no-plain", action="store_true", help="mixed runs: skip the plain FP64 comparison")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--traj", type=int, default=None)

@@ -85,6 +85,49 @@ def analog_run(desc, t_begin=0, t_end=None, nthreads=None):
     return traj[:, :desc.n_obs, :], chi, st.as_dict()
 
 
+_blas = {}
+
+
+def openblas_zgemm():
+    """The OpenBLAS that scipy ships (the reference's LinearAlgebra backend is
+    OpenBLAS as well, Manifest.toml), set to one thread per caller: returns
+    (address of its cblas_zgemm, description), or (None, reason)."""
+    if "fn" in _blas:
+        return _blas["fn"], _blas["desc"]
+    import glob
+
+    import scipy
+    libdir = os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs")
+    cands = sorted(glob.glob(os.path.join(libdir, "libscipy_openblas-*.so")))
+    if not cands:
+        _blas.update(fn=None, desc="scipy's OpenBLAS not found")
+        return None, _blas["desc"]
+    ob = C.CDLL(cands[0])
+    ob.scipy_openblas_set_num_threads.argtypes = [C.c_int]
+    ob.scipy_openblas_set_num_threads(1)  # trajectories run one per host thread
+    fn = C.cast(ob.scipy_cblas_zgemm, C.c_void_p).value
+    ver = ""
+    if hasattr(ob, "scipy_openblas_get_config"):
+        ob.scipy_openblas_get_config.restype = C.c_char_p
+        ver = ob.scipy_openblas_get_config().decode().split()[1] if ob.scipy_openblas_get_config() else ""
+    _blas.update(fn=fn, desc=f"OpenBLAS {ver} cblas_zgemm (scipy's build), 1 thread per trajectory", lib=ob)
+    return fn, _blas["desc"]
+
+
+def set_blas(enabled: bool):
+    """Routes the oracle's contractions through OpenBLAS zgemm (enabled) or
+    back to its plain loops.  Returns the description of what is in use."""
+    L = lib()
+    L.orc_set_zgemm.restype = C.c_void_p
+    L.orc_set_zgemm.argtypes = [C.c_void_p]
+    if not enabled:
+        L.orc_set_zgemm(None)
+        return "plain loops"
+    fn, desc = openblas_zgemm()
+    L.orc_set_zgemm(fn)
+    return desc if fn else "plain loops (" + desc + ")"
+
+
 def digital_run(desc, t_begin=0, t_end=None, nthreads=None):
     """Digital trajectories of a packed circuit problem (api.CircuitDescriptors)."""
     L = lib()

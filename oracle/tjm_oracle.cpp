@@ -94,8 +94,26 @@ struct State {
   int oc = 0;  // orth_center (0-based)
 };
 
+// Optional optimised BLAS for the timed CPU baseline: a CBLAS zgemm (the
+// reference's contractions run on OpenBLAS ZGEMM through TensorOperations,
+// Manifest.toml).  Installed by orc_set_zgemm; null (the default, and what
+// every test uses) keeps the plain loops below.  Column-major only.
+typedef void (*cblas_zgemm_t)(int order, int transa, int transb, int m, int n, int k, const void* alpha,
+                              const void* A, int lda, const void* B, int ldb, const void* beta, void* C, int ldc);
+static cblas_zgemm_t g_zgemm = nullptr;
+enum { CB_COLMAJOR = 102, CB_NOTRANS = 111, CB_TRANS = 112, CB_CONJTRANS = 113 };
+inline void blas_gemm(int ta, int tb, int m, int n, int k, const cd* A, int lda, const cd* B, int ldb, cd* C,
+                      int ldc) {
+  const cd one(1.0, 0.0), zero(0.0, 0.0);
+  g_zgemm(CB_COLMAJOR, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc);
+}
+
 // C(m x n) = A(m x k) * B(k x n), column-major with leading dims = rows.
 void matmul(int m, int n, int k, const cd* A, const cd* B, cd* C) {
+  if (g_zgemm) {
+    blas_gemm(CB_NOTRANS, CB_NOTRANS, m, n, k, A, m, B, k, C, m);
+    return;
+  }
   for (long i = 0; i < (long)m * n; ++i) C[i] = 0;
   for (int j = 0; j < n; ++j)
     for (int p = 0; p < k; ++p) {
@@ -569,6 +587,25 @@ Env update_left(const Ten& A, const Wt& W, const Env& E) {
   // T1[bra_l, ml, pin, ket_r] = sum_k E[bra_l, ml, k] A[k, pin, ket_r]
   vector<cd> T1((size_t)bl * wl * d * br);
   matmul(bl * wl, d * br, bl, E.v.data(), A.v.data(), T1.data());
+  if (g_zgemm) {  // T2 as [bra_l, pout, ket_r, mr], then E'_mr = A^H T2_mr
+    vector<cd> T2((size_t)bl * d * br * wr, 0.0);
+    for (int kr = 0; kr < br; ++kr)
+      for (int mr = 0; mr < wr; ++mr)
+        for (int po = 0; po < d; ++po)
+          for (int ml = 0; ml < wl; ++ml)
+            for (int pi = 0; pi < d; ++pi) {
+              cd w = W.at(ml, po, pi, mr);
+              if (w == cd(0)) continue;
+              const cd* t1 = &T1[(size_t)bl * (ml + (size_t)wl * (pi + (size_t)d * kr))];
+              cd* t2 = &T2[(size_t)bl * (po + (size_t)d * (kr + (size_t)br * mr))];
+              for (int a = 0; a < bl; ++a) t2[a] += t1[a] * w;
+            }
+    Env En(br, wr, br);
+    for (int mr = 0; mr < wr; ++mr)
+      blas_gemm(CB_CONJTRANS, CB_NOTRANS, br, br, bl * d, A.v.data(), bl * d, &T2[(size_t)bl * d * br * mr], bl * d,
+                &En.v[(size_t)br * mr], br * wr);
+    return En;
+  }
   // T2[bra_l, ket_r, pout, mr] = sum T1[bra_l, ml, pin, ket_r] W[ml, pout, pin, mr]
   vector<cd> T2((size_t)bl * br * d * wr, 0.0);
   for (int kr = 0; kr < br; ++kr)
@@ -600,6 +637,30 @@ Env update_left(const Ten& A, const Wt& W, const Env& E) {
 // update_right_environment (Algorithms.jl:206-211)
 Env update_right(const Ten& A, const Wt& W, const Env& E) {
   const int kl = A.l, d = A.d, kr = A.r, wl = W.wl, wr = W.wr;
+  if (g_zgemm) {  // T1 = A E^T, T2 as [pout, br, ket_l, ml] conjugated, E'_ml = conj(A conj(T2_ml))
+    vector<cd> T1((size_t)kl * d * kr * wr);
+    blas_gemm(CB_NOTRANS, CB_TRANS, kl * d, kr * wr, kr, A.v.data(), kl * d, E.v.data(), kr * wr, T1.data(), kl * d);
+    vector<cd> T2((size_t)d * kr * kl * wl, 0.0);
+    for (int b = 0; b < kr; ++b)
+      for (int a = 0; a < kl; ++a)
+        for (int ml = 0; ml < wl; ++ml)
+          for (int po = 0; po < d; ++po) {
+            cd sum = 0;
+            for (int mr = 0; mr < wr; ++mr)
+              for (int pi = 0; pi < d; ++pi) {
+                cd w = W.at(ml, po, pi, mr);
+                if (w == cd(0)) continue;
+                sum += w * T1[a + (size_t)kl * (pi + (size_t)d * (b + (size_t)kr * mr))];
+              }
+            T2[po + (size_t)d * (b + (size_t)kr * (a + (size_t)kl * ml))] = std::conj(sum);
+          }
+    Env En(kl, wl, kl);
+    for (int ml = 0; ml < wl; ++ml)
+      blas_gemm(CB_NOTRANS, CB_NOTRANS, kl, kl, d * kr, A.v.data(), kl, &T2[(size_t)d * kr * kl * ml], d * kr,
+                &En.v[(size_t)kl * ml], kl * wl);
+    for (auto& v : En.v) v = std::conj(v);
+    return En;
+  }
   // T1[ket_l, pin, bra_r, mr] = sum_k A[ket_l, pin, k] E[bra_r, mr, k]
   vector<cd> T1((size_t)kl * d * kr * wr, 0.0);
   for (int k = 0; k < kr; ++k)
@@ -649,6 +710,25 @@ void project_site(const Env& Le, const Env& Re, const Wt& W, int chil, int D, in
   // T1[a, ml, pin, c] = sum_k L[a, ml, k] x[k, pin, c]
   vector<cd> T1((size_t)chil * wl * D * chir);
   matmul(chil * wl, D * chir, chil, Le.v.data(), x.data(), T1.data());
+  if (g_zgemm) {  // T2 as [a, mr, c, pout]; out_po = T2_po R^T with R as (chir x wr chir)
+    vector<cd> T2((size_t)chil * wr * chir * D, 0.0);
+    for (int c = 0; c < chir; ++c)
+      for (int mr = 0; mr < wr; ++mr)
+        for (int po = 0; po < D; ++po)
+          for (int ml = 0; ml < wl; ++ml)
+            for (int pi = 0; pi < D; ++pi) {
+              cd w = W.at(ml, po, pi, mr);
+              if (w == cd(0)) continue;
+              const cd* t1 = &T1[(size_t)chil * (ml + (size_t)wl * (pi + (size_t)D * c))];
+              cd* t2 = &T2[(size_t)chil * (mr + (size_t)wr * (c + (size_t)chir * po))];
+              for (int a = 0; a < chil; ++a) t2[a] += t1[a] * w;
+            }
+    out.assign((size_t)chil * D * chir, 0.0);
+    for (int po = 0; po < D; ++po)
+      blas_gemm(CB_NOTRANS, CB_TRANS, chil, chir, wr * chir, &T2[(size_t)chil * wr * chir * po], chil, Re.v.data(),
+                chir, &out[(size_t)chil * po], chil * D);
+    return;
+  }
   // T2[a, c, pout, mr] = sum T1[a, ml, pin, c] W[ml, pout, pin, mr]
   vector<cd> T2((size_t)chil * chir * D * wr, 0.0);
   for (int c = 0; c < chir; ++c)
@@ -1942,6 +2022,14 @@ bool load_circuit(const yaqs_gate_desc* gates, int n, int L, vector<Gate>& out, 
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
+
+// Installs (fn != null) or removes the CBLAS zgemm the contractions use and
+// returns the previous one.  Not to be changed while a problem runs.
+void* orc_set_zgemm(void* fn) {
+  void* old = reinterpret_cast<void*>(g_zgemm);
+  g_zgemm = reinterpret_cast<cblas_zgemm_t>(fn);
+  return old;
+}
 
 // Runs trajectories [t_begin, t_end) of the problem on nthreads host threads.
 // traj_out is [num_traj][n_obs][n_out] indexed by the absolute trajectory.

@@ -9,7 +9,7 @@ which computes the same contractions.  Noise-free evolution from
 |0...0>, dt = 0.05, 20 sweeps; after every sweep <Z_i> of the dense state
 vector and the bond dimensions are written to dynamic_tdvp.csv.
 
-Usage: python tests/golden/make_dynamic_golden.py [/path/to/reference]
+Usage: python tests/golden/make_dynamic_golden.py /path/to/reference
 """
 import csv
 import os
@@ -18,7 +18,9 @@ import types
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YAQS_REFERENCE_TREE")
+if not REF:
+    sys.exit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set YAQS_REFERENCE_TREE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 

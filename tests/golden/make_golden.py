@@ -12,14 +12,16 @@ here: Julia is not installed).  This script only copies and subsets them:
                           results/tjm_vs_qutip_data.csv (benchmark_analog_tjm.jl:90-227):
                           columns t, TJM <Z_1..6>, TJM stagg, QuTiP <Z_1..6>, QuTiP stagg.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference
 """
 import csv
 import os
 import shutil
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("YAQS_REFERENCE_TREE")
+if not REF:
+    sys.exit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set YAQS_REFERENCE_TREE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

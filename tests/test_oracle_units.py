@@ -4,6 +4,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from yaqs_julia_b200 import _abi as A
 from yaqs_julia_b200 import api
 
 
@@ -148,3 +149,27 @@ def test_injected_draws_reproduce_and_exhaustion_errors(oracle):
     assert np.array_equal(a, b)
     with pytest.raises(RuntimeError, match="YAQS_E_RNG"):
         oracle.analog_run(api.Descriptors(api.MPS(L, state="x+"), H, cfg, nm, rng_mode=1, uniforms=u[:, :2]))
+
+
+def test_blas_backed_restatement_equals_the_loops(oracle):
+    """The timed CPU baseline routes the contractions through OpenBLAS zgemm;
+    its trajectories equal the plain-loop restatement's to rounding."""
+    L = 8
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.2, dt=0.05, num_traj=2, max_bond_dim=8)
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    res = {}
+    for tdvp in (A.YAQS_TDVP_2SITE, A.YAQS_TDVP_DYNAMIC):
+        d = api.Descriptors(api.random_mps(L, 8, seed=2), H, cfg, nm, seed=3, tdvp_mode=tdvp)
+        try:
+            oracle.set_blas(False)
+            ref, _, _ = oracle.analog_run(d, nthreads=2)
+            desc = oracle.set_blas(True)
+            got, _, _ = oracle.analog_run(d, nthreads=2)
+        finally:
+            oracle.set_blas(False)
+        res[tdvp] = (np.abs(got - ref).max(), desc)
+    for err, desc in res.values():
+        assert "OpenBLAS" in desc, desc
+        assert err < 1e-10, err
