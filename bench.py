@@ -631,8 +631,12 @@ def run_ours(args):
         b = pl["res"].trajectories[:, :, :ncol]
         dz = np.abs(a[:, :L] - b[:, :L])
         ds = np.abs(a[:, L] - b[:, L])
+        per_traj = dz.max(axis=(1, 2))
         err = {"z_max_abs": float(dz.max()), "z_mean_abs": float(dz.mean()), "s_half_max_abs": float(ds.max()),
                "s_half_mean_abs": float(ds.mean()),
+               "z_traj_max_percentiles": {q: float(np.percentile(per_traj, q)) for q in (50, 90, 99)},
+               "trajectories_above_1e-5": int((per_traj > 1e-5).sum()),
+               "jumps": {"mixed": int(main["res"].stats["jumps"]), "plain": int(pl["res"].stats["jumps"])},
                "z_ensemble_mean_max_abs": float(np.abs(a[:, :L].mean(0) - b[:, :L].mean(0)).max()),
                "trajectories_compared": nt, "time_indices_compared": ncol,
                "run": f"every <Z_i> and S_half at {ncol} recorded time indices (saturated start, {args.warmup} "

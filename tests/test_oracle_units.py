@@ -173,3 +173,32 @@ def test_blas_backed_restatement_equals_the_loops(oracle):
     for err, desc in res.values():
         assert "OpenBLAS" in desc, desc
         assert err < 1e-10, err
+
+
+def test_dynamic_truncation_is_rounding_sensitive(oracle):
+    """Why the dynamic sweep's parity bar is 1e-5 where a 2-site split
+    truncates (tests/test_gpu_parity.py): the oracle against itself with
+    another summation order (OpenBLAS zgemm instead of loops) on the same
+    draws.  L = 10 Heisenberg from Neel: with chi_max = 32 (never binding) the
+    two runs agree to rounding; with chi_max = 16 the middle split truncates
+    32 values to 16 and the runs separate by orders of magnitude more."""
+    L = 10
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    out = {}
+    for chi in (32, 16):
+        cfg = api.TimeEvolutionConfig(obs, 0.8, dt=0.05, num_traj=3, max_bond_dim=chi)
+        u = np.random.default_rng(22).random((3, api.max_draws(cfg)))
+        d = api.Descriptors(api.MPS(L, state="Neel"), H, cfg, nm, rng_mode=A.YAQS_RNG_INJECTED, uniforms=u,
+                            tdvp_mode=A.YAQS_TDVP_DYNAMIC)
+        try:
+            oracle.set_blas(False)
+            a, _, _ = oracle.analog_run(d, nthreads=3)
+            oracle.set_blas(True)
+            b, _, _ = oracle.analog_run(d, nthreads=3)
+        finally:
+            oracle.set_blas(False)
+        out[chi] = np.abs(a - b).max()
+    assert out[32] < 1e-12, out
+    assert out[16] > 1e-9, out
