@@ -123,25 +123,6 @@ __global__ void __launch_bounds__(NT, 1) expm_kernel(int chil, int D, int chir, 
   if (ltid() == 0) matvecs[b] = mv;
 }
 
-// Shared memory of a kernel that runs tc_gemm: the pipeline buffers and
-// barriers, aligned to 1024 bytes inside the dynamic allocation.
-struct CgemmSmem {
-  TcSmem t;
-  TcState st;
-};
-// One complex FP32 product per CTA on the tensor cores (tcgen05 + TMA).
-__global__ void __launch_bounds__(NT, 1) cgemm_tc_kernel(int M, int N, int K, const CUtensorMap* maps, int a_mn,
-                                                         int conj_a, int b_mn, int conj_b, float2* C, int* status) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  CgemmSmem& sm = *reinterpret_cast<CgemmSmem*>(align_smem_1024(smraw));
-  tc_setup(sm.st);
-  const TcOp A{maps + 2 * blockIdx.x, a_mn, conj_a};
-  const TcOp B{maps + 2 * blockIdx.x + 1, b_mn, conj_b};
-  const bool ok = tc_gemm<float2>(M, N, K, A, B, C + (long long)M * N * blockIdx.x, 1, M, false, sm.t, sm.st);
-  if (ltid() == 0) status[blockIdx.x] = ok ? 0 : 1;
-  tc_teardown(sm.st);
-}
-
 // FP64 FMA throughput probe: 8 independent chains per thread.
 __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x0 = ltid(), x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
@@ -972,7 +953,7 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   size_t smem = cta_smem_bytes();
   int per_sm = 0;
   if (use_tc) {  // two programs per 512-thread CTA
-    CUDA_TRY(ctx, tc_kernel_prepare(smem, &per_sm, &smem));
+    CUDA_TRY(ctx, tc_kernel_prepare(&per_sm, &smem));
     per_sm = std::min(per_sm, TMEM_PROGRAMS_PER_SM);
   } else {
     CUDA_TRY(ctx, cudaFuncSetAttribute(tjm_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1843,10 +1824,7 @@ int yaqs_batched_cgemm_tf32(yaqs_ctx* ctx, int32_t batch, int32_t M, int32_t N, 
       return set_err(ctx, YAQS_E_CUDA, "cuTensorMapEncodeTiled refused a staged operand");
   }
   CUDA_TRY(ctx, cudaMemcpy(dmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
-  const size_t smem = sizeof(CgemmSmem) + 1024;
-  CUDA_TRY(ctx, cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  cgemm_tc_kernel<<<batch, NT, smem>>>(M, N, K, dmaps, a_mn, conj_a ? 1 : 0, b_mn, conj_b ? 1 : 0, dC, dst);
-  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, tc_cgemm_launch(batch, M, N, K, dmaps, a_mn, conj_a ? 1 : 0, b_mn, conj_b ? 1 : 0, dC, dst));
   CUDA_TRY(ctx, cudaDeviceSynchronize());
   std::vector<int> st(batch);
   CUDA_TRY(ctx, cudaMemcpy(st.data(), dst, batch * sizeof(int), cudaMemcpyDeviceToHost));

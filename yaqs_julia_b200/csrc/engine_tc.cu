@@ -8,6 +8,10 @@
 // kernels of engine.cu, compiled without any tcgen05 code, keep two CTAs
 // per SM.
 #define YAQS_TC 1
+// Pipeline depth of this unit (tcgemm.cuh defaults: 2 raw, 1 plane buffer).
+// Measured on the L=30 chi=64 products: 3 or 4 raw buffers and 2 plane
+// buffers gave no faster GEMM (79 us for M=320 N=128 K=64 in every case)
+// and the larger shared memory cost the whole kernel 7 % through L1.
 #include "program.cuh"
 #include "engine_tc.h"
 
@@ -22,8 +26,9 @@ __global__ void __launch_bounds__(2 * NT, 1) tjm_step_kernel_tc(const DevParams 
   tc_teardown(sm.e.tc);
 }
 
-cudaError_t tc_kernel_prepare(size_t smem_per_program, int* programs_per_sm, size_t* smem_per_cta) {
-  const size_t smem = 2 * (smem_per_program - 1024) + 1024;  // one alignment slack per CTA
+cudaError_t tc_kernel_prepare(int* programs_per_sm, size_t* smem_per_cta) {
+  // sized here: this unit's CtaSmem holds its own (deeper) pipeline buffers
+  const size_t smem = 2 * sizeof(CtaSmem) + 1024;  // one alignment slack per CTA
   cudaError_t e = cudaFuncSetAttribute(tjm_step_kernel_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -41,3 +46,30 @@ cudaError_t tc_kernel_launch(int slots, size_t smem_per_cta, cudaStream_t stream
 }
 
 cudaError_t tc_set_prof(unsigned long long* buf) { return cudaMemcpyToSymbol(g_prof, &buf, sizeof(buf)); }
+
+// One complex FP32 product per CTA on the tensor cores (tcgen05 + TMA): the
+// yaqs_batched_cgemm_tf32 component, with the pipeline of the engine.
+struct CgemmSmem {
+  TcSmem t;
+  TcState st;
+};
+__global__ void __launch_bounds__(NT, 1) cgemm_tc_kernel(int M, int N, int K, const CUtensorMap* maps, int a_mn,
+                                                         int conj_a, int b_mn, int conj_b, float2* C, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CgemmSmem& sm = *reinterpret_cast<CgemmSmem*>(align_smem_1024(smraw));
+  tc_setup(sm.st);
+  const TcOp A{maps + 2 * blockIdx.x, a_mn, conj_a};
+  const TcOp B{maps + 2 * blockIdx.x + 1, b_mn, conj_b};
+  const bool ok = tc_gemm<float2>(M, N, K, A, B, C + (long long)M * N * blockIdx.x, 1, M, false, sm.t, sm.st);
+  if (ltid() == 0) status[blockIdx.x] = ok ? 0 : 1;
+  tc_teardown(sm.st);
+}
+
+cudaError_t tc_cgemm_launch(int batch, int M, int N, int K, const CUtensorMap* maps, int a_mn, int conj_a, int b_mn,
+                            int conj_b, float2* C, int* status) {
+  const size_t smem = sizeof(CgemmSmem) + 1024;
+  cudaError_t e = cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cgemm_tc_kernel<<<batch, NT, smem>>>(M, N, K, maps, a_mn, conj_a, b_mn, conj_b, C, status);
+  return cudaGetLastError();
+}

@@ -153,7 +153,9 @@ struct EngineSmem {
   TcState tc;
   EngineSmemU u;
 };
-static_assert(sizeof(TcSmem) <= sizeof(GemmSmem), "the tensor-core pipeline must not grow the CTA's shared memory");
+#if !YAQS_TC
+static_assert(sizeof(TcSmem) <= sizeof(GemmSmem), "the default pipeline must not grow the CTA's shared memory");
+#endif
 
 #if YAQS_TC
 // Mixed form on tcgen05 (compiled only into the tensor-core kernel,
@@ -307,7 +309,9 @@ static __device__ void dev_tridiag_expm(int m, double dt, KrySmem& ks) {
 }
 
 // h_j = <q_j, w> (j < k) into ks.h and |w|^2 in the same pass over w: the
-// first group takes seven vectors and the norm, later groups eight.
+// first group takes seven vectors and the norm, later groups eight.  Each
+// thread takes two elements per iteration so that up to 18 independent
+// loads are in flight (the pass is bound by memory latency).
 static __device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w, long long n, int k, EngineSmem& sm) {
   const int tid = ltid();
   double nw2 = 0.0;
@@ -316,21 +320,25 @@ static __device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w
     double d[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) d[e] = 0.0;
-    for (long long i = tid; i < n; i += NT) {
-      const cplx wi = w[i];
-      if (first) d[15] += cabs2(wi);
+    for (long long i0 = tid; i0 < n; i0 += 2 * NT) {
+      const long long i1 = i0 + NT;
+      const bool two = i1 < n;
+      const cplx w0 = w[i0];
+      const cplx w1 = two ? w[i1] : make_double2(0.0, 0.0);
+      cplx a0[8], a1[8];
 #pragma unroll
-      for (int e = 0; e < 7; ++e) {
-        if (j0 + e < k) {
-          const cplx p = cmulc(Q[qs * (j0 + e) + i], wi);
-          d[2 * e] += p.x;
-          d[2 * e + 1] += p.y;
-        }
+      for (int e = 0; e < 8; ++e) {
+        const bool live = e < G && j0 + e < k;
+        a0[e] = live ? Q[qs * (j0 + e) + i0] : make_double2(0.0, 0.0);
+        a1[e] = (live && two) ? Q[qs * (j0 + e) + i1] : make_double2(0.0, 0.0);
       }
-      if (!first && j0 + 7 < k) {
-        const cplx p = cmulc(Q[qs * (j0 + 7) + i], wi);
-        d[14] += p.x;
-        d[15] += p.y;
+      if (first) d[15] += cabs2(w0) + cabs2(w1);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        if (e == 7 && first) continue;
+        const cplx p = cadd(cmulc(a0[e], w0), cmulc(a1[e], w1));
+        d[2 * e] += p.x;
+        d[2 * e + 1] += p.y;
       }
     }
     block_sum_n<16>(d, sm.r);
@@ -342,21 +350,52 @@ static __device__ double lanczos_dots(const cplx* Q, long long qs, const cplx* w
   return nw2;
 }
 
-// w <- w - sum_j h_j q_j (j < k); with norm, returns |w|^2 after the update.
-static __device__ double lanczos_subtract(const cplx* Q, long long qs, cplx* w, long long n, int k, EngineSmem& sm,
-                                   bool norm) {
+// out_i = s (w_i - sum_{j<k} c_j q_j[i]) for i < n (w null: w_i = 0; out may
+// be w), c in shared memory; returns the CTA sum of |out_i|^2 when norm.
+// Basis vectors go in groups of eight, two elements per thread, so the loads
+// of a group are in flight together.  CTA-collective.
+static __device__ double basis_combine(const cplx* Q, long long qs, const cplx* w, cplx* out, long long n, int k,
+                                       const cplx* c, double s, bool norm, EngineSmem& sm) {
   double part = 0.0;
-  for (long long i = ltid(); i < n; i += NT) {
-    cplx v = w[i];
-    for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
-    w[i] = v;
-    part += cabs2(v);
+  for (long long i0 = ltid(); i0 < n; i0 += 2 * NT) {
+    const long long i1 = i0 + NT;
+    const bool two = i1 < n;
+    cplx v0 = w ? w[i0] : make_double2(0.0, 0.0);
+    cplx v1 = (w && two) ? w[i1] : make_double2(0.0, 0.0);
+    for (int j0 = 0; j0 < k; j0 += 8) {
+      cplx a0[8], a1[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const bool live = j0 + e < k;
+        a0[e] = live ? Q[qs * (j0 + e) + i0] : make_double2(0.0, 0.0);
+        a1[e] = (live && two) ? Q[qs * (j0 + e) + i1] : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        if (j0 + e < k) {
+          const cplx ce = c[j0 + e];
+          v0 = csub(v0, cmul(ce, a0[e]));
+          v1 = csub(v1, cmul(ce, a1[e]));
+        }
+      }
+    }
+    v0 = cscale(v0, s);
+    v1 = cscale(v1, s);
+    out[i0] = v0;
+    if (two) out[i1] = v1;
+    part += cabs2(v0) + cabs2(v1);
   }
   if (!norm) {
     cta_sync();
     return 0.0;
   }
   return block_sum(part, sm.r);
+}
+
+// w <- w - sum_j h_j q_j (j < k); with norm, returns |w|^2 after the update.
+static __device__ double lanczos_subtract(const cplx* Q, long long qs, cplx* w, long long n, int k, EngineSmem& sm,
+                                          bool norm) {
+  return basis_combine(Q, qs, w, w, n, k, sm.k.h, 1.0, norm, sm);
 }
 
 // In place: x <- exp(-i dt H_eff) x.  Q holds kdim+1 vectors of stride qs.
@@ -407,24 +446,17 @@ static __device__ __noinline__ int dev_expm_krylov(const HeffOp& h, cplx* x, dou
     if (tid == 0) sm.k.beta[k - 1] = b_k;
     const double inv = 1.0 / b_k;
     if (accept) {
-      for (long long i = tid; i < n; i += NT) {
-        cplx v = w[i];
-        for (int j = 0; j < k; ++j) v = csub(v, cmul(sm.k.h[j], Q[qs * j + i]));
-        w[i] = cscale(v, inv);
-      }
+      basis_combine(Q, qs, w, w, n, k, sm.k.h, inv, false, sm);
     } else {
       for (long long i = tid; i < n; i += NT) w[i] = cscale(w[i], inv);
+      cta_sync();
     }
-    cta_sync();
   }
   cta_sync();
   dev_tridiag_expm(m, dt, sm.k);
   cta_sync();
-  for (long long i = tid; i < n; i += NT) {
-    cplx v = make_double2(0.0, 0.0);
-    for (int j = 0; j < m; ++j) cfma(v, sm.k.y[j], Q[qs * j + i]);
-    x[i] = cscale(v, beta0);
-  }
+  if (tid < m) sm.k.h[tid] = make_double2(-sm.k.y[tid].x, -sm.k.y[tid].y);  // x = beta0 sum_j y_j q_j
   cta_sync();
+  basis_combine(Q, qs, nullptr, x, n, m, sm.k.h, beta0, false, sm);
   return mv;
 }

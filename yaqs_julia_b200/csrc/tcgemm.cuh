@@ -47,20 +47,30 @@
 
 // Shared memory of the pipeline (never live together with the other GEMM or
 // SVD staging; the engine keeps it in the same union).
+// Pipeline depth: TC_RAW_STAGES raw TMA buffers (TMA runs that many K steps
+// minus one ahead) and TC_PLANE_STAGES plane buffers (with two, the split of
+// step k+1 overlaps the MMAs of step k).  The defaults fit the FP64 GEMM
+// staging; the tensor-core kernel's translation unit may set deeper ones.
+#ifndef TC_RAW_STAGES
+#define TC_RAW_STAGES 2
+#endif
+#ifndef TC_PLANE_STAGES
+#define TC_PLANE_STAGES 1
+#endif
 struct __align__(1024) TcSmem {
-  float rawA[2][2048];        // 2 buffers x 8 KB: one A box (128 x 8 complex)
-  float rawB[2][1024];        // 2 buffers x 4 KB: one B box (8 x 64 complex)
-  unsigned planeA[6][1024];   // 6 planes x (128 rows x 8 k) tf32
-  unsigned planeB[6][512];    // 6 planes x (64 rows x 8 k) tf32
+  float rawA[TC_RAW_STAGES][2048];             // 8 KB each: one A box (128 x 8 complex)
+  float rawB[TC_RAW_STAGES][1024];             // 4 KB each: one B box (8 x 64 complex)
+  unsigned planeA[TC_PLANE_STAGES][6][1024];   // 6 planes x (128 rows x 8 k) tf32
+  unsigned planeB[TC_PLANE_STAGES][6][512];    // 6 planes x (64 rows x 8 k) tf32
 };
 
 // State that persists across calls (outside the union).
 struct TcState {
-  unsigned long long bar_raw[2];
-  unsigned long long bar_mma;
+  unsigned long long bar_raw[TC_RAW_STAGES];
+  unsigned long long bar_mma[TC_PLANE_STAGES];
   unsigned tmem_base;
   unsigned ph_raw;  // bit s: parity of the next phase of bar_raw[s]
-  unsigned ph_mma;  // parity of the next phase of bar_mma
+  unsigned ph_mma;  // bit s: parity of the next phase of bar_mma[s]
   int fatal;
 };
 
@@ -244,9 +254,8 @@ static __device__ __forceinline__ void tc_store_c(double2* c, float re, float im
 // permit once every program of the CTA has allocated.
 static __device__ __forceinline__ void tc_setup(TcState& st) {
   if (ltid() == 0) {
-    mbar_init(&st.bar_raw[0], 1);
-    mbar_init(&st.bar_raw[1], 1);
-    mbar_init(&st.bar_mma, 1);
+    for (int r = 0; r < TC_RAW_STAGES; ++r) mbar_init(&st.bar_raw[r], 1);
+    for (int r = 0; r < TC_PLANE_STAGES; ++r) mbar_init(&st.bar_mma[r], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     st.ph_raw = 0;
     st.ph_mma = 0;
@@ -280,14 +289,21 @@ static __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, c
   if (st.fatal) return false;
   // producers of the staged operands wrote them through the generic proxy
   fence_async_global();
+  if (tid == 0) {  // the tensor maps live in global memory: start their descriptor fetch
+    tma_prefetch_map(A.map);
+    tma_prefetch_map(B.map);
+  }
   cta_sync();
   unsigned ph_raw = st.ph_raw, ph_mma = st.ph_mma;
   bool ok = true;
   const int nM = (M + TC_BM - 1) / TC_BM, nN = (N + TC_BN - 1) / TC_BN, nK = (K + TC_BK - 1) / TC_BK;
   const unsigned BYTES = (TC_BM + TC_BN) * TC_BK * 8;
-  auto issue = [&](int kc, int stg, int m0, int n0) {
+  const int G = nM * nN * nK;  // K steps of all tiles, one stream
+  // TMA of step g into raw stage g % TC_RAW_STAGES
+  auto issue = [&](int g) {
+    const int t = g / nK, kc = g - t * nK, stg = g % TC_RAW_STAGES;
+    const int m0 = (t / nN) * TC_BM, n0 = (t % nN) * TC_BN, k0 = kc * TC_BK;
     mbar_arrive_expect_tx(&st.bar_raw[stg], BYTES);
-    const int k0 = kc * TC_BK;
     if (A.mn)
       tma_load_2d(s.rawA[stg], A.map, 2 * m0, k0, &st.bar_raw[stg]);
     else
@@ -297,43 +313,48 @@ static __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, c
     else
       tma_load_2d(s.rawB[stg], B.map, 2 * k0, n0, &st.bar_raw[stg]);
   };
-  bool pend = false;  // a commit on bar_mma not yet waited for
-  int stage = 0;
+  unsigned pend = 0;  // bit p: a commit on bar_mma[p] not yet waited for
+  auto wait_mma = [&](int p) {
+    if (pend & (1u << p)) {
+      ok &= mbar_wait(&st.bar_mma[p], (ph_mma >> p) & 1);
+      ph_mma ^= 1u << p;
+      pend &= ~(1u << p);
+    }
+  };
+  if (tid == 0)
+    for (int g = 0; g < TC_RAW_STAGES - 1 && g < G; ++g) issue(g);
   for (int t = 0; t < nM * nN; ++t) {
     const int m0 = (t / nN) * TC_BM, n0 = (t % nN) * TC_BN;
     const int nrem = min(TC_BN, N - n0);
     const int nmma = (nrem + 15) & ~15;
     const unsigned idesc = tc_idesc(nmma);
-    if (tid == 0) issue(0, stage & 1, m0, n0);
     for (int kc = 0; kc < nK; ++kc) {
-      const int sg = (stage + kc) & 1;
-      if (tid == 0 && kc + 1 < nK) issue(kc + 1, sg ^ 1, m0, n0);
+      const int g = t * nK + kc;
+      const int sg = g % TC_RAW_STAGES, pl = g % TC_PLANE_STAGES;
+      // raw stage (g - 1) % R was split at step g - 1, before its barrier
+      if (tid == 0 && g + TC_RAW_STAGES - 1 < G) issue(g + TC_RAW_STAGES - 1);
       ok &= mbar_wait(&st.bar_raw[sg], (ph_raw >> sg) & 1);
       ph_raw ^= 1u << sg;
-      if (pend) {  // the MMAs of the previous step release the planes
-        ok &= mbar_wait(&st.bar_mma, ph_mma & 1);
-        ph_mma ^= 1u;
-        pend = false;
-      }
+      wait_mma(pl);  // the MMAs that last read these planes are done
       const int k0 = kc * TC_BK;
       {  // A: 128 rows x 2 k quads, one item per thread
         const int r = tid & 127, q = tid >> 7;
         float2 v[4];
         tc_raw_quad(s.rawA[sg], A.mn, TC_BM, r, q, m0 + r < M, k0, K, A.conj != 0, v);
-        tc_split_store(&s.planeA[0][0], 1024, r, q, v);
+        tc_split_store(&s.planeA[pl][0][0], 1024, r, q, v);
       }
       if (tid < 128) {  // B: 64 rows x 2 k quads
         const int r = tid & 63, q = tid >> 6;
         float2 v[4];
         tc_raw_quad(s.rawB[sg], B.mn, TC_BN, r, q, n0 + r < N, k0, K, B.conj != 0, v);
-        tc_split_store(&s.planeB[0][0], 512, r, q, v);
+        tc_split_store(&s.planeB[pl][0][0], 512, r, q, v);
       }
       fence_async_smem();
       cta_sync();
       if (tid == 0) {
         tc_fence_after();
-        const unsigned* pa = &s.planeA[0][0];
-        const unsigned* pb = &s.planeB[0][0];
+        const unsigned* pa = &s.planeA[pl][0][0];
+        const unsigned* pb = &s.planeB[pl][0][0];
 #pragma unroll
         for (int acc = 0; acc < 3; ++acc) {
           const unsigned long long ah = tc_sdesc(pa + (2 * acc) * 1024, 128, 256);
@@ -345,17 +366,12 @@ static __device__ __noinline__ bool tc_gemm(int M, int N, int K, const TcOp A, c
           tc_mma_tf32(d, al, bh, idesc, 1u);
           tc_mma_tf32(d, ah, bh, idesc, 1u);
         }
-        tc_commit(&st.bar_mma);
+        tc_commit(&st.bar_mma[pl]);
       }
-      pend = true;
+      pend |= 1u << pl;
     }
-    stage += nK;
-    // all MMAs of the tile done
-    if (pend) {
-      ok &= mbar_wait(&st.bar_mma, ph_mma & 1);
-      ph_mma ^= 1u;
-      pend = false;
-    }
+    // all MMAs of the tile done (commits complete in issue order)
+    for (int p = 0; p < TC_PLANE_STAGES; ++p) wait_mma((t * nK + nK + p) % TC_PLANE_STAGES);
     tc_fence_after();
     // epilogue
     const int quarter = wid & 3, half = wid >> 2;
