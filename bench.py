@@ -64,7 +64,8 @@ DIG_TIMED_TRAFFIC = {(40, 512, 57): 4.458638080e9 + 15.767363584e9}
 METRIC = "TJM trajectory-steps/s (L=30 Heisenberg, chi=64, 1024 trajectories) vs plain FP64 GPU"
 # DRAM read + write bytes per trajectory-step of the trajectory kernel, from
 # one small-case ncu capture per configuration: (precision, tdvp, L, chi) -> bytes
-TRAFFIC_PER_TRAJ_STEP = {}
+TRAFFIC_PER_TRAJ_STEP = {("mixed", "dynamic", 30, 64): 276.942e9 / 148 + 189.476e9 / 148,
+                         ("fp64", "dynamic", 30, 64): 438.298e9 / 148 + 252.204e9 / 148}
 TDVP_NAMES = {"dynamic": A.YAQS_TDVP_DYNAMIC, "2site": A.YAQS_TDVP_2SITE, "1site": A.YAQS_TDVP_1SITE}
 TDVP = [A.YAQS_TDVP_DYNAMIC]  # set from --tdvp
 TDVP_DESC = {"dynamic": "1-site TDVP with 2-site growth (local dynamic TDVP)", "2site": "2-site TDVP",
@@ -475,6 +476,24 @@ def run_batch(args):
         wall = time.perf_counter() - t0
         ck = clocks.stop()
         st = srv.stats()
+    # error of every simulation against the FP64 form: its first 16
+    # trajectories again in FP64 (same seed: the same Philox streams),
+    # after the timed region
+    per_sim = []
+    if prec == "mixed" and not args.no_plain:
+        import copy
+        with api.Server(max_L=64, max_bond_dim=128, max_mpo_width=5, mixed=False, chunk=args.chunk,
+                        ctx=ctx) as srv64:
+            subs = []
+            for r in reqs:
+                psi, H, cfg, nm = r["problem"]
+                c64 = copy.copy(cfg)
+                c64.num_traj = min(16, r["nt"])
+                subs.append(srv64.submit(psi, H, c64, nm, seed=r["seed"], precision="fp64", tdvp=args.tdvp))
+            ref = [srv64.result(i) for i in subs]
+        for r, m, f in zip(reqs, res, ref):
+            n = f.trajectories.shape[0]
+            per_sim.append(float(np.abs(m.trajectories[:n] - f.trajectories).max()))
     total = sum(r["nt"] * steps for r in reqs)
     line = {"metric": "TJM trajectory-steps/s, 64 uneven analog simulations served together", "value": total / wall,
             "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0, "higher_is_better": True, "scaling": "weak",
@@ -490,6 +509,12 @@ def run_batch(args):
             "max_bond_reached": {f"chi{c}": int(max([r.max_bond.max() for q, r in zip(reqs, res) if q["chi"] == c],
                                                     default=0)) for c in (16, 32, 64, 128)},
             "jumps": int(sum(r.stats["jumps"] for r in res))}
+    if per_sim:
+        line["err_vs_fp64"] = {"z_max_abs_per_simulation": per_sim, "max": max(per_sim),
+                               "median": float(np.median(per_sim)),
+                               "simulations_above_1e-5": int(sum(e > 1e-5 for e in per_sim)),
+                               "run": "every <Z_i> at every recorded time of the first 16 trajectories of each "
+                                      "simulation against the same trajectories (same seed) in the FP64 form"}
     print(json.dumps(line), flush=True)
 
 
@@ -675,9 +700,11 @@ def run_ours(args):
                     "achieved_counts": "H_eff product flops only (8 flops per complex MAC)"}
         tt = traffic_per * nt * K if traffic_per else None
         roof.update({"kernel": "tjm_step_kernel_tc" if mixed else "tjm_step_kernel", "traffic": tt,
-                     "traffic_source": "DRAM read+write bytes per trajectory-step from a one-launch ncu capture "
-                                       "of a small case of the same configuration (profiles/), scaled by the "
-                                       "trajectory-steps of the timed launch; null when not captured",
+                     "traffic_source": "DRAM read+write bytes per trajectory-step from a one-launch ncu capture of "
+                                       "148 trajectories of the same configuration (profiles/tjm_step_kernels_L30_"
+                                       "chi64_148traj_traffic.md), scaled by the trajectory-steps of the timed launch "
+                                       "(a lower bound: the full run keeps twice the slots in L2); null when not "
+                                       "captured",
                      "traffic_gbs": tt / (main["dev_ms"] / 1e3) / 1e9 if tt else None,
                      "hbm_frac": tt / (main["dev_ms"] / 1e3) / 1e9 / peaks["hbm_gbs"] if tt else None})
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,

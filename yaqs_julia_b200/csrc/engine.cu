@@ -597,6 +597,12 @@ struct ServePool {
   long long ws_stride = 0, wsi_stride = 0;
   cplx* ws = nullptr;
   int* wsi = nullptr;
+  // servers that admit mixed runs: the tcgen05 operands of every slot sit at
+  // fixed offsets at the end of the slot (sL, sx, sT2, sR and their pitches
+  // and rows in `stage`), described by tmaps[4 slot .. 4 slot + 3]
+  int tc = 0;
+  WsLayout stage{};
+  const CUtensorMap* tmaps = nullptr;
 };
 
 }  // namespace
@@ -914,9 +920,23 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   // the mixed H_eff products run on tcgen05 in direct runs (the tensor-core
   // kernel, engine_tc.cu); server slots are shared by runs of different
   // shapes and keep the mma.sync form
-  const bool use_tc = mixed && !pool;
-  const WsLayout lay =
-      plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed, has_long_range(noise, nprocs), use_tc);
+  const bool use_tc = mixed && (!pool || pool->tc);
+  WsLayout lay =
+      plan_layout(L, caps, w.data(), true, cfg->krylov_dim, mixed, has_long_range(noise, nprocs), use_tc && !pool);
+  if (use_tc && pool) {  // the server's fixed staging region and tensor maps
+    const WsLayout& g = pool->stage;
+    if (lay.pL > g.pL || lay.rL > g.rL || lay.px > g.px || lay.rx > g.rx || lay.pT2 > g.pT2 || lay.rT2 > g.rT2 ||
+        lay.pR > g.pR || lay.rR > g.rR)
+      return set_err(ctx, YAQS_E_UNSUPPORTED, "the request's H_eff operands exceed the server's staging shape");
+    lay.sL = g.sL;
+    lay.sx = g.sx;
+    lay.sT2 = g.sT2;
+    lay.sR = g.sR;
+    lay.pL = g.pL;
+    lay.px = g.px;
+    lay.pT2 = g.pT2;
+    lay.pR = g.pR;
+  }
   const std::vector<int>& cap = caps.cap;
   const std::vector<long long>& mps_off = caps.mps_off;
   const std::vector<long long>& env_off = caps.env_off;
@@ -960,7 +980,8 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
     CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tjm_step_kernel, NT, smem));
   }
   if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
-  if (pool && (lay.total > pool->ws_stride || lay.itotal > pool->wsi_stride))
+  // a mixed request in a tensor-core server must end below the slot's staging region
+  if (pool && (lay.total > (use_tc ? pool->stage.sL : pool->ws_stride) || lay.itotal > pool->wsi_stride))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "the request's workspace exceeds the server's slot shape");
   size_t free_b = 0, total_b = 0;
   CUDA_TRY(ctx, cudaMemGetInfo(&free_b, &total_b));
@@ -1015,7 +1036,9 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   run->ncols = ncols;
   int st = setup_run(ctx, run, cap, chi0, w, mps_off, env_off, psi0, hp, ho, rng, cfg->n_times, pool);
   if (st != YAQS_OK) return st;
-  if (use_tc) {  // four tensor maps per slot over its staged operands
+  if (use_tc && pool) {
+    P.tmaps = pool->tmaps;
+  } else if (use_tc) {  // four tensor maps per slot over its staged operands
     std::vector<CUtensorMap> maps(4 * (size_t)slots);
     for (int sl = 0; sl < slots; ++sl) {
       const cplx* base = P.ws + (long long)sl * P.lay.total;

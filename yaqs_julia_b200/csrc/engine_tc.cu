@@ -13,6 +13,7 @@
 // buffers gave no faster GEMM (79 us for M=320 N=128 K=64 in every case)
 // and the larger shared memory cost the whole kernel 7 % through L1.
 #include "program.cuh"
+#include "serve.cuh"
 #include "engine_tc.h"
 
 __global__ void __launch_bounds__(2 * NT, 1) tjm_step_kernel_tc(const DevParams P, int first, int count) {
@@ -42,6 +43,39 @@ cudaError_t tc_kernel_prepare(int* programs_per_sm, size_t* smem_per_cta) {
 cudaError_t tc_kernel_launch(int slots, size_t smem_per_cta, cudaStream_t stream, const DevParams& P, int first,
                              int count) {
   tjm_step_kernel_tc<<<slots / 2, 2 * NT, smem_per_cta, stream>>>(P, first, count);
+  return cudaGetLastError();
+}
+
+// The server's kernel when it admits mixed-precision runs: the serve loop
+// (serve.cuh) in two programs per CTA; FP64 and digital units run in it too.
+__global__ void __launch_bounds__(2 * NT, 1) serve_kernel_tc(const BatchRun* runs, int nruns, int total_units,
+                                                             int* counter) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CtaSmem* both = reinterpret_cast<CtaSmem*>(align_smem_1024(smraw));
+  CtaSmem& sm = both[cta_half()];
+  __shared__ __align__(16) BatchRun br[2];
+  tc_setup(sm.e.tc);
+  __syncthreads();
+  if (threadIdx.x < 32) tmem_relinquish();
+  serve_units(runs, nruns, total_units, counter, sm, br[cta_half()]);
+  tc_teardown(sm.e.tc);
+}
+
+cudaError_t tc_serve_prepare(int* programs_per_sm, size_t* smem_per_cta) {
+  const size_t smem = 2 * sizeof(CtaSmem) + 1024;
+  cudaError_t e = cudaFuncSetAttribute(serve_kernel_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel_tc, 2 * NT, smem);
+  if (e != cudaSuccess) return e;
+  *programs_per_sm = 2 * per_sm;
+  *smem_per_cta = smem;
+  return cudaSuccess;
+}
+
+cudaError_t tc_serve_launch(int slots, size_t smem_per_cta, cudaStream_t stream, const BatchRun* runs, int nruns,
+                            int total_units, int* counter) {
+  serve_kernel_tc<<<slots / 2, 2 * NT, smem_per_cta, stream>>>(runs, nruns, total_units, counter);
   return cudaGetLastError();
 }
 

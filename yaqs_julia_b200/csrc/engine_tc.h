@@ -6,6 +6,7 @@
 #include <stddef.h>
 
 struct DevParams;
+struct BatchRun;
 
 // Sets the kernel's attributes and returns in *programs_per_sm how many
 // programs (two per CTA) fit on one SM and in *smem_per_cta the dynamic
@@ -22,3 +23,8 @@ cudaError_t tc_set_prof(unsigned long long* buf);
 // the staged A and B of problem b, status[b] = 1 when a pipeline wait gave up.
 cudaError_t tc_cgemm_launch(int batch, int M, int N, int K, const CUtensorMap* maps, int a_mn, int conj_a,
                             int b_mn, int conj_b, float2* C, int* status);
+// The server's two-program kernel (serve.cuh's loop), for servers that admit
+// mixed-precision runs: attributes and occupancy, then one launch per batch.
+cudaError_t tc_serve_prepare(int* programs_per_sm, size_t* smem_per_cta);
+cudaError_t tc_serve_launch(int slots, size_t smem_per_cta, cudaStream_t stream, const BatchRun* runs, int nruns,
+                            int total_units, int* counter);

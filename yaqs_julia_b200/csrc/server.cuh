@@ -1,13 +1,9 @@
 // server.cuh — request loop serving many simulations on one GPU
 // (yaqs_server_*).  Included at the end of engine.cu.
 //
-// Device side: serve_kernel runs one batch, i.e. a list of runs each
-// advancing positions [first, first + count) of its launch list.  Its work
-// units are (run, position, trajectory) triples, run-major and
-// position-major within a run; each CTA pulls the next unit from an atomic
-// counter, copies that run's parameters into shared memory and runs one
-// time index (or circuit layer) of one trajectory in its pool slot, with the
-// same per-trajectory ordering flags as the single-run kernels.
+// Device side (serve.cuh): serve_kernel, or its two-program tensor-core
+// form when the server admits mixed-precision runs (engine_tc.cu), runs one
+// batch of every admitted run.
 //
 // Host side: one thread per server admits queued requests (first come,
 // first served, while their footprint fits the HBM budget), builds a batch
@@ -20,62 +16,14 @@
 #include <map>
 #include <thread>
 
-struct BatchRun {
-  DevParams P;
-  DigParams D;
-  int digital;
-  int first, count;
-  int unit_begin;
-};
+#include "serve.cuh"
 
 __global__ void __launch_bounds__(NT, 2) serve_kernel(const BatchRun* runs, int nruns, int total_units,
                                                       int* counter) {
   extern __shared__ __align__(16) unsigned char smraw[];
   CtaSmem& sm = *reinterpret_cast<CtaSmem*>(align_smem_1024(smraw));
   __shared__ __align__(16) BatchRun br;
-  const int slot = cta_slot();
-  for (;;) {
-    if (ltid() == 0) {
-      const int u = atomicAdd(counter, 1);
-      int r = 0;
-      while (r + 1 < nruns && runs[r + 1].unit_begin <= u) ++r;
-      sm.bcast_i[7] = u;
-      sm.bcast_i[5] = r;
-    }
-    cta_sync();
-    const int u = sm.bcast_i[7], r = sm.bcast_i[5];
-    cta_sync();
-    if (u >= total_units) break;
-    {
-      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(runs + r);
-      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&br);
-      for (int e = ltid(); e < (int)(sizeof(BatchRun) / 8); e += NT) dst[e] = src[e];
-    }
-    cta_sync();
-    const DevParams& P = br.P;
-    const int nt = P.num_traj;
-    const int local = u - br.unit_begin, k = local / nt, t = local - k * nt, pos = br.first + k;
-    cplx* ws = P.ws + (long long)slot * P.lay.total;
-    int* wsi = P.wsi + (long long)slot * P.lay.itotal;
-    bool ready = true;
-    if (k > 0) ready = wait_done(P, t, pos - 1, sm);
-    if (ltid() == 0) sm.fail = ready ? 0 : ST_TIMEOUT;
-    cta_sync();
-    if (ready && P.status[t] == 0) {
-      Ctx c{P, sm, ws, wsi, slot, t, P.counters + (long long)slot * 8, P.flops + slot};
-      if (br.digital)
-        run_digital_step(c, br.D, P.jlist[pos]);
-      else
-        run_step(c, P.jlist[pos]);
-    }
-    cta_sync();
-    if (ltid() == 0) {
-      if (sm.fail && P.status[t] == 0) P.status[t] = sm.fail;
-      __threadfence();
-      atomicExch(P.done + t, pos);
-    }
-    cta_sync();
-  }
+  serve_units(runs, nruns, total_units, counter, sm, br);
 }
 
 namespace {
@@ -286,8 +234,12 @@ void yaqs_server::loop() {
       if (e == cudaSuccess) e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
       if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
       if (e == cudaSuccess) {
-        serve_kernel<<<pool.slots, NT, smem, stream>>>(d_batch, (int)batch.size(), units, d_counter);
-        e = cudaGetLastError();
+        if (pool.tc) {
+          e = tc_serve_launch(pool.slots, smem, stream, d_batch, (int)batch.size(), units, d_counter);
+        } else {
+          serve_kernel<<<pool.slots, NT, smem, stream>>>(d_batch, (int)batch.size(), units, d_counter);
+          e = cudaGetLastError();
+        }
       }
       if (e == cudaSuccess) e = cudaEventRecord(e1, stream);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
@@ -409,16 +361,51 @@ int yaqs_server_create(yaqs_ctx* ctx, const yaqs_server_config* cfg, yaqs_server
   plan_caps(L, nullptr, wone.data(), cfg->max_bond_dim, cd);
   const WsLayout la = plan_layout(L, ca, wmax.data(), true, cfg->krylov_dim, cfg->mixed != 0);
   const WsLayout ld = plan_layout(L, cd, wone.data(), false, 0, false);
-  srv->pool.ws_stride = std::max(la.total, ld.total);
+  long long stride = std::max(la.total, ld.total);
   srv->pool.wsi_stride = std::max(la.itotal, ld.itotal);
-  srv->smem = cta_smem_bytes();
-  CUDA_TRY(ctx, cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)srv->smem));
+  // a server that admits mixed runs serves every batch with the two-program
+  // tensor-core kernel; the tcgen05 operands of every slot sit at its end
+  srv->pool.tc = cfg->mixed != 0;
+  if (srv->pool.tc) {
+    const WsLayout lt = plan_layout(L, ca, wmax.data(), true, cfg->krylov_dim, true, false, true);
+    WsLayout g = lt;  // the staged operands are the last buffers plan_layout takes
+    g.sL = stride + (lt.sL - lt.sL);
+    g.sx = stride + (lt.sx - lt.sL);
+    g.sT2 = stride + (lt.sT2 - lt.sL);
+    g.sR = stride + (lt.sR - lt.sL);
+    srv->pool.stage = g;
+    stride += lt.total - lt.sL;
+  }
+  srv->pool.ws_stride = stride;
   int per_sm = 0;
-  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, NT, srv->smem));
+  if (srv->pool.tc) {
+    CUDA_TRY(ctx, tc_serve_prepare(&per_sm, &srv->smem));
+    per_sm = std::min(per_sm, TMEM_PROGRAMS_PER_SM);
+  } else {
+    srv->smem = cta_smem_bytes();
+    CUDA_TRY(ctx, cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)srv->smem));
+    CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, NT, srv->smem));
+  }
   if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "served kernel does not fit on an SM");
   srv->pool.slots = ctx->sms * per_sm;
   CUDA_TRY(ctx, srv->pool_mem.alloc(&srv->pool.ws, (size_t)srv->pool.slots * srv->pool.ws_stride));
   CUDA_TRY(ctx, srv->pool_mem.alloc(&srv->pool.wsi, (size_t)srv->pool.slots * srv->pool.wsi_stride));
+  if (srv->pool.tc) {  // four tensor maps per slot
+    std::vector<CUtensorMap> maps(4 * (size_t)srv->pool.slots);
+    const WsLayout& g = srv->pool.stage;
+    for (int sl = 0; sl < srv->pool.slots; ++sl) {
+      const cplx* base = srv->pool.ws + (long long)sl * stride;
+      if (!make_tc_map(&maps[4 * sl + 0], base + g.sL, g.pL, g.rL, TC_A_MN) ||
+          !make_tc_map(&maps[4 * sl + 1], base + g.sx, g.px, g.rx, TC_B_K) ||
+          !make_tc_map(&maps[4 * sl + 2], base + g.sT2, g.pT2, g.rT2, TC_A_MN) ||
+          !make_tc_map(&maps[4 * sl + 3], base + g.sR, g.pR, g.rR, TC_B_MN))
+        return set_err(ctx, YAQS_E_CUDA, "cuTensorMapEncodeTiled refused a staged H_eff operand");
+    }
+    CUtensorMap* d_maps;
+    CUDA_TRY(ctx, srv->pool_mem.alloc(&d_maps, maps.size()));
+    CUDA_TRY(ctx, cudaMemcpy(d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    srv->pool.tmaps = d_maps;
+  }
   CUDA_TRY(ctx, srv->pool_mem.alloc(&srv->d_counter, 1));
   size_t free_b = 0, total_b = 0;
   CUDA_TRY(ctx, cudaMemGetInfo(&free_b, &total_b));
