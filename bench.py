@@ -509,6 +509,8 @@ def run_batch(args):
             "max_bond_reached": {f"chi{c}": int(max([r.max_bond.max() for q, r in zip(reqs, res) if q["chi"] == c],
                                                     default=0)) for c in (16, 32, 64, 128)},
             "jumps": int(sum(r.stats["jumps"] for r in res))}
+    if prec == "mixed":
+        line["autotune"] = autotune_summary(ctx)
     if per_sim:
         line["err_vs_fp64"] = {"z_max_abs_per_simulation": per_sim, "max": max(per_sim),
                                "median": float(np.median(per_sim)),
@@ -579,6 +581,23 @@ def run_serve(args):
             "trajectory_layers_per_s": layers / wall, "device_busy_s": st["busy_s"] - base["busy_s"],
             "launches": st["launches"] - base["launches"], "clocks": ck}
     print(json.dumps(line), flush=True)
+
+
+def autotune_summary(ctx):
+    """The autotuner's measured product form per H_eff shape on this device
+    (yaqs_autotune_results): tcgen05 or mma.sync, with both timings."""
+    import ctypes as C
+    n = C.c_int32(0)
+    ctx.check(ctx._lib.yaqs_autotune_results(ctx.handle, None, 0, C.byref(n)))
+    rows = np.zeros((max(n.value, 1), 8))
+    ctx.check(ctx._lib.yaqs_autotune_results(ctx.handle, A.dptr(rows), n.value, C.byref(n)))
+    shapes = [{"chi_l": int(r[0]), "D": int(r[1]), "chi_r": int(r[2]), "w": [int(r[3]), int(r[4])],
+               "form": "mma.sync" if r[5] else "tcgen05", "us_tcgen05": round(float(r[6]), 1),
+               "us_mma_sync": round(float(r[7]), 1)} for r in rows[:n.value]]
+    return {"what": "mixed H_eff product form per shape, chosen by the engine's autotuner from timed launches "
+                    "over every slot (tcgen05 128x64 tiles vs mma.sync 3xTF32 64x64 tiles)",
+            "shapes": len(shapes), "mma_sync_chosen": sum(x["form"] == "mma.sync" for x in shapes),
+            "table": shapes}
 
 
 def measured_peaks():
@@ -725,6 +744,8 @@ def run_ours(args):
                 "stats": {"matvecs_timed": matvecs_timed, "flops_timed": flops_timed,
                           "jumps": main["res"].stats["jumps"], "svd_sweeps": main["res"].stats["svd_sweeps"],
                           "svds": main["res"].stats["svds"], "max_bond": int(main["res"].max_bond.max())}}
+        if mixed:
+            line["autotune"] = autotune_summary(ctx)
         if plain is not None:
             line["plain_fp64"] = plain
         if err is not None:

@@ -85,6 +85,15 @@ int yaqs_batched_cgemm_tf32(yaqs_ctx* ctx, int32_t batch, int32_t M, int32_t N, 
 int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n, const double* M,
                              double* U, double* S, double* SVt, void* stream);
 
+/* The autotuner's decisions on this context's device: one row of 8 doubles
+ * per measured shape (chi_l, D, chi_r, w_l, w_r, form, us per product in the
+ * tcgen05 form, us per product in the mma.sync form), form 0 = tcgen05,
+ * 1 = mma.sync.  The mixed form's H_eff products (project_site,
+ * src/Algorithms.jl:215-220) take the chosen form per shape bucket; shapes
+ * are measured once per process when a run first needs them.  Writes at
+ * most `capacity` rows and the total number into *count. */
+int yaqs_autotune_results(yaqs_ctx* ctx, double* rows, int32_t capacity, int32_t* count);
+
 /* Measured FP64 FMA throughput of the device (TFLOP/s, best of 5 runs of a
  * DFMA loop over every SM): the denominator of the FP64 form's roofline. */
 int yaqs_fp64_peak(yaqs_ctx* ctx, double* tflops);

@@ -33,6 +33,7 @@ ENTRY_POINTS = {
     "yaqs_server_wait", "yaqs_server_take", "yaqs_server_last_error", "yaqs_server_stats_get",
     "yaqs_server_destroy", "yaqs_batched_svd", "yaqs_batched_qr", "yaqs_batched_project_site",
     "yaqs_batched_expm_site", "yaqs_batched_cgemm_tf32", "yaqs_batched_svd_noalloc", "yaqs_fp64_peak",
+    "yaqs_autotune_results",
 }
 
 

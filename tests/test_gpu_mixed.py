@@ -85,3 +85,30 @@ def test_digital_rejects_mixed():
     from yaqs_julia_b200._lib import EngineError
     with pytest.raises(EngineError, match="UNSUPPORTED"):
         api.run_circuit_descriptors(d)
+
+
+def test_autotuner_measures_the_shapes_of_a_mixed_run(oracle):
+    """A direct mixed run first times both product forms on every H_eff
+    shape it will meet (yaqs_autotune_results); the run, with the chosen
+    forms, still matches the FP64 oracle within the mixed tolerance."""
+    import ctypes as C
+    from yaqs_julia_b200 import _lib
+    L = 8
+    H = api.init_general_hamiltonian(L, 1, 1, 1, 0, 0, 0.3)
+    obs = [api.Observable(f"Z{i}", api.Z, i) for i in range(1, L + 1)]
+    cfg = api.TimeEvolutionConfig(obs, 0.2, dt=0.05, num_traj=4, max_bond_dim=16)
+    nm = api.NoiseModel([{"name": "pauli_z", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    u = np.random.default_rng(9).random((4, api.max_draws(cfg)))
+    d, mixed = _run(api.MPS(L, state="Neel"), H, cfg, nm, u, A.YAQS_PREC_MIXED)
+    ref, _, _ = oracle.analog_run(d)
+    assert np.abs(mixed.trajectories - ref).max() < Z_TOL
+    ctx = _lib.default_context()
+    n = C.c_int32(0)
+    ctx.check(ctx._lib.yaqs_autotune_results(ctx.handle, None, 0, C.byref(n)))
+    rows = np.zeros((max(n.value, 1), 8))
+    ctx.check(ctx._lib.yaqs_autotune_results(ctx.handle, A.dptr(rows), n.value, C.byref(n)))
+    rows = rows[:n.value]
+    shapes = {(int(r[0]), int(r[1]), int(r[2])) for r in rows}
+    # bond caps 1 2 4 8 16 8 4 2 1: the centre bond, the sites beside it and a 2-site window over them
+    assert {(16, 1, 16), (8, 2, 16), (16, 2, 8), (8, 4, 8)} <= shapes, sorted(shapes)
+    assert set(rows[:, 5]) <= {0.0, 1.0} and (rows[:, 6] > 0).all() and (rows[:, 7] > 0).all()

@@ -72,6 +72,7 @@ def lib():
         L.yaqs_server_stats_get.argtypes = [C.c_void_p, P(A.ServerStats)]
         L.yaqs_server_destroy.argtypes = [C.c_void_p]
         L.yaqs_fp64_peak.argtypes = [C.c_void_p, P(C.c_double)]
+        L.yaqs_autotune_results.argtypes = [C.c_void_p, A.DPTR, C.c_int32, P(C.c_int32)]
         L.yaqs_batched_svd_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4 + [
             C.c_void_p]
         L.yaqs_batched_svd.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32] + [A.DPTR] * 4

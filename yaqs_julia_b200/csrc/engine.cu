@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -867,6 +869,62 @@ int yaqs_ctx_destroy(yaqs_ctx* ctx) {
 
 const char* yaqs_last_error(const yaqs_ctx* ctx) { return ctx ? ctx->err.c_str() : g_static_err.c_str(); }
 
+// Autotuner of the mixed H_eff products: per shape bucket (tune_index) the
+// tcgen05 form or the mma.sync form, whichever a launch over every slot of
+// the run applying H_eff to synthetic operands of that shape finishes first
+// (mma.sync only when it is more than 5 % faster).  Choices are measured
+// once per (device, chi_l, D, chi_r, w_l, w_r) and kept for the process, so
+// every run of a shape uses the same form and a run's results do not depend
+// on when it was tuned.  YAQS_AUTOTUNE=0 keeps tcgen05 everywhere.
+struct TuneRecord {
+  unsigned char form;
+  float us_tc, us_mma;
+};
+static std::mutex g_tune_mu;
+static std::map<std::array<int, 6>, TuneRecord> g_tune_cache;
+
+static int autotune_products(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, const std::vector<int>& w) {
+  const char* env = getenv("YAQS_AUTOTUNE");
+  if (env && env[0] == '0') return YAQS_OK;
+  DevParams& P = run->P;
+  const int L = P.L;
+  struct Shape {
+    int bl, br, l, D, r, site;
+  };
+  std::map<int, Shape> buckets;  // first occurrence of every bucket
+  for (int b = 1; b < L; ++b) buckets.emplace(tune_index(cap[b], 1, cap[b]), Shape{b, b, cap[b], 1, cap[b], b});
+  for (int i = 0; i < L; ++i)
+    buckets.emplace(tune_index(cap[i], 2, cap[i + 1]), Shape{i, i + 1, cap[i], 2, cap[i + 1], i});
+  for (int i = 0; i + 2 <= L; ++i)
+    buckets.emplace(tune_index(cap[i], 4, cap[i + 2]), Shape{i, i + 2, cap[i], 4, cap[i + 2], i});
+  unsigned char *d_tune, *d_tc, *d_mma;
+  CUDA_TRY(ctx, run->dm.alloc(&d_tune, TUNE_ENTRIES));
+  CUDA_TRY(ctx, run->dm.alloc(&d_tc, TUNE_ENTRIES));
+  CUDA_TRY(ctx, run->dm.alloc(&d_mma, TUNE_ENTRIES));
+  CUDA_TRY(ctx, cudaMemset(d_tc, 0, TUNE_ENTRIES));
+  CUDA_TRY(ctx, cudaMemset(d_mma, 1, TUNE_ENTRIES));
+  std::vector<unsigned char> table(TUNE_ENTRIES, 0);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const auto& kv : buckets) {
+    const Shape& sh = kv.second;
+    const std::array<int, 6> key{ctx->device, sh.l, sh.D, sh.r, w[sh.bl], w[sh.br]};
+    auto it = g_tune_cache.find(key);
+    if (it == g_tune_cache.end()) {
+      TuneRecord rec{0, 0.f, 0.f};
+      CUDA_TRY(ctx, tc_tune_time(P, run->slots, d_tc, sh.bl, sh.br, sh.l, sh.D, sh.r, sh.site, 4, &rec.us_tc));
+      CUDA_TRY(ctx, tc_tune_time(P, run->slots, d_mma, sh.bl, sh.br, sh.l, sh.D, sh.r, sh.site, 4, &rec.us_mma));
+      rec.us_tc *= 250.f;  // ms for 4 products -> us per product
+      rec.us_mma *= 250.f;
+      rec.form = rec.us_mma < 0.95f * rec.us_tc ? 1 : 0;
+      it = g_tune_cache.emplace(key, rec).first;
+    }
+    table[kv.first] = it->second.form;
+  }
+  CUDA_TRY(ctx, cudaMemcpy(d_tune, table.data(), TUNE_ENTRIES, cudaMemcpyHostToDevice));
+  P.tune = d_tune;
+  return YAQS_OK;
+}
+
 static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_mpo_desc* H,
                              const yaqs_noise_desc* noise, const yaqs_obs_desc* obs, int32_t n_obs,
                              const yaqs_tev_config* cfg, const yaqs_rng_desc* rng, yaqs_run** out,
@@ -1066,6 +1124,10 @@ static int analog_begin_impl(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaq
   P.wm_envR = d_views + L + (L - 1) + L;
   P.wm_bond = d_views + L + (L - 1) + L + L;
 
+  if (use_tc) {
+    st = autotune_products(ctx, run, cap, w);
+    if (st != YAQS_OK) return st;
+  }
   run->launches.push_back(0);
   for (int j = (cfg->order == 2 ? 2 : 1); j < cfg->n_times; ++j) run->launches.push_back(j);
   st = upload_positions(ctx, run);
@@ -1697,6 +1759,25 @@ int yaqs_batched_svd_noalloc(yaqs_ctx* ctx, int32_t batch, int32_t m, int32_t n,
       m, n, reinterpret_cast<const cplx*>(M), reinterpret_cast<cplx*>(U), S, reinterpret_cast<cplx*>(SVt), work,
       wstride, iwork);
   CUDA_TRY(ctx, cudaGetLastError());
+  return YAQS_OK;
+}
+
+int yaqs_autotune_results(yaqs_ctx* ctx, double* rows, int32_t capacity, int32_t* count) {
+  if (!ctx || !count || capacity < 0 || (capacity > 0 && !rows)) return set_err(ctx, YAQS_E_ARG, "bad arguments");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  int n = 0;
+  for (const auto& kv : g_tune_cache) {
+    if (kv.first[0] != ctx->device) continue;
+    if (n < capacity) {
+      double* r = rows + 8LL * n;
+      for (int k = 0; k < 5; ++k) r[k] = kv.first[k + 1];
+      r[5] = kv.second.form;
+      r[6] = kv.second.us_tc;
+      r[7] = kv.second.us_mma;
+    }
+    ++n;
+  }
+  *count = n;
   return YAQS_OK;
 }
 

@@ -79,6 +79,60 @@ cudaError_t tc_serve_launch(int slots, size_t smem_per_cta, cudaStream_t stream,
   return cudaGetLastError();
 }
 
+// The autotuner's measurement: every program of the launch stages synthetic
+// operands of one bucket's shape in its own slot (the environments of bonds
+// bl and br, sizes l x D x r) and applies H_eff `reps` times in the product
+// form the table `form` selects.  Values are deterministic and of unit size.
+__global__ void __launch_bounds__(2 * NT, 1) tune_heff_kernel_tc(const DevParams P, const unsigned char* form, int bl,
+                                                                 int br, int l, int D, int r, int site, int reps) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CtaSmem* both = reinterpret_cast<CtaSmem*>(align_smem_1024(smraw));
+  CtaSmem& sm = both[cta_half()];
+  tc_setup(sm.e.tc);
+  __syncthreads();
+  if (threadIdx.x < 32) tmem_relinquish();
+  DevParams Q = P;
+  Q.tune = form;
+  const int slot = cta_slot();
+  Ctx c{Q, sm, Q.ws + (long long)slot * Q.lay.total, Q.wsi + (long long)slot * Q.lay.itotal, slot, 0, nullptr, nullptr};
+  cplx* L = envL(c, bl);
+  cplx* R = envR(c, br);
+  cplx* x = c.ws + Q.lay.Q;
+  cplx* y = x + Q.kry_n;
+  const long long nl = (long long)l * Q.w[bl] * l, nr = (long long)r * Q.w[br] * r, nx = (long long)l * D * r;
+  for (long long e = ltid(); e < nl; e += NT) L[e] = make_double2(1.0 / (1 + e % 7), 0.5 / (1 + e % 5));
+  for (long long e = ltid(); e < nr; e += NT) R[e] = make_double2(0.5 / (1 + e % 3), 1.0 / (1 + e % 11));
+  for (long long e = ltid(); e < nx; e += NT) x[e] = make_double2(1.0 / (1 + e % 13), 0.25);
+  cta_sync();
+  const WMat& W = D == 1 ? Q.wm_bond[bl] : D == 2 ? Q.wm_heff1[site] : Q.wm_heff2[site];
+  const HeffOp h = make_heff(c, l, D, r, bl, br, W);
+  for (int k = 0; k < reps; ++k) dev_heff(h, x, y, sm.e);
+  tc_teardown(sm.e.tc);
+}
+
+cudaError_t tc_tune_time(const DevParams& P, int slots, const unsigned char* form, int bl, int br, int l, int D, int r,
+                         int site, int reps, float* ms) {
+  const size_t smem = 2 * sizeof(CtaSmem) + 1024;
+  cudaError_t e = cudaFuncSetAttribute(tune_heff_kernel_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  if ((e = cudaEventCreate(&e0)) != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return e;
+  }
+  tune_heff_kernel_tc<<<slots / 2, 2 * NT, smem>>>(P, form, bl, br, l, D, r, site, 1);  // warm-up
+  cudaEventRecord(e0);
+  tune_heff_kernel_tc<<<slots / 2, 2 * NT, smem>>>(P, form, bl, br, l, D, r, site, reps);
+  cudaEventRecord(e1);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return e;
+}
+
 cudaError_t tc_set_prof(unsigned long long* buf) { return cudaMemcpyToSymbol(g_prof, &buf, sizeof(buf)); }
 
 // One complex FP32 product per CTA on the tensor cores (tcgen05 + TMA): the

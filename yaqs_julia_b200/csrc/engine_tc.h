@@ -28,3 +28,9 @@ cudaError_t tc_cgemm_launch(int batch, int M, int N, int K, const CUtensorMap* m
 cudaError_t tc_serve_prepare(int* programs_per_sm, size_t* smem_per_cta);
 cudaError_t tc_serve_launch(int slots, size_t smem_per_cta, cudaStream_t stream, const BatchRun* runs, int nruns,
                             int total_units, int* counter);
+// The autotuner's timing of one product form on one bucket shape: a launch
+// over every slot of the run applying H_eff `reps` times to synthetic
+// operands (environments of bonds bl, br; l x D x r; the MPO map of `site`);
+// form: the per-bucket table (entries 0 = tcgen05, 1 = mma.sync).
+cudaError_t tc_tune_time(const DevParams& P, int slots, const unsigned char* form, int bl, int br, int l, int D, int r,
+                         int site, int reps, float* ms);

@@ -18,6 +18,7 @@
 #define WAPPLY_IN_CPLX 2560  // staged inputs: ni x PT values, PT = 256, 128 or 64 by what fits
 #define WAPPLY_MAXI 32
 #define WAPPLY_MAXNNZ 512
+#define WAPPLY_LB 8  // inputs a thread loads back to back
 #define KRYLOV_MAX 32
 
 // Sparse MPO matrix M[o, i] in CSR form (rows are outputs).
@@ -89,7 +90,22 @@ static __device__ __noinline__ void dev_wapply(const T* in, T* out, const WMat W
     const int q0 = live ? pair % g.n0 : 0, q1 = live ? pair / g.n0 : 0;
     const long long ib = q0 * g.is0 + q1 * g.is1, ob = q0 * g.os0 + q1 * g.os1;
     cta_sync();
-    for (int i = r0; i < W.ni; i += RS) sin[i * PT + pl] = live ? in[ib + ws.in_off[i]] : zero;
+    // batches of WAPPLY_LB loads issued before their stores: `in` may alias
+    // the staging buffer as far as the compiler knows, so a plain loop would
+    // wait out one L2 latency per input
+    for (int i0 = r0; i0 < W.ni; i0 += RS * WAPPLY_LB) {
+      T v[WAPPLY_LB];
+#pragma unroll
+      for (int k = 0; k < WAPPLY_LB; ++k) {
+        const int i = i0 + k * RS;
+        v[k] = (live && i < W.ni) ? in[ib + ws.in_off[i]] : zero;
+      }
+#pragma unroll
+      for (int k = 0; k < WAPPLY_LB; ++k) {
+        const int i = i0 + k * RS;
+        if (i < W.ni) sin[i * PT + pl] = v[k];
+      }
+    }
     cta_sync();
     if (live) {
       for (int o = r0; o < W.no; o += RS) {
@@ -167,17 +183,32 @@ static_assert(sizeof(TcSmem) <= sizeof(GemmSmem), "the default pipeline must not
 static __device__ void dev_heff_tc(const HeffOp& h, const cplx* x, cplx* y, EngineSmem& sm) {
   const int chil = h.chil, D = h.D, chir = h.chir, wl = h.wl, wr = h.wr;
   const long long n = (long long)chil * D * chir;
-  for (long long e = ltid(); e < n; e += NT) {  // Sx[nn px + k] = x[k + chil nn]
-    const cplx v = x[e];
-    const long long k = e % chil, nn = e / chil;
-    h.Sx[nn * h.px + k] = make_float2((float)v.x, (float)v.y);
+  // Sx[nn px + k] = x[k + chil nn], 8 loads in flight per thread
+  for (long long e0 = ltid(); e0 < n; e0 += 8 * NT) {
+    cplx v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = e0 + u * NT < n ? x[e0 + u * NT] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const long long e = e0 + u * NT;
+      if (e < n) h.Sx[(e / chil) * h.px + e % chil] = make_float2((float)v[u].x, (float)v[u].y);
+    }
   }
   const TcOp A1{h.maps + 0, 1, 0}, B1{h.maps + 1, 0, 0}, A2{h.maps + 2, 1, 0}, B2{h.maps + 3, 1, 0};
   tc_gemm<cflt>(chil * wl, D * chir, chil, A1, B1, h.T1f, 1, (long long)chil * wl, false, sm.u.t, sm.tc);
   if (h.W.ident) {  // bond (D = 1, wl = wr): T2 is T1 re-laid into ST2
-    for (long long e = ltid(); e < (long long)chil * wl * chir; e += NT) {
-      const long long a = e % chil, m = (e / chil) % wl, c = e / ((long long)chil * wl);
-      h.ST2[(m + (long long)wr * c) * h.pT2 + a] = h.T1f[e];
+    const long long nt1 = (long long)chil * wl * chir;
+    for (long long e0 = ltid(); e0 < nt1; e0 += 8 * NT) {
+      cflt v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = e0 + u * NT < nt1 ? h.T1f[e0 + u * NT] : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const long long e = e0 + u * NT;
+        if (e >= nt1) continue;
+        const long long a = e % chil, m = (e / chil) % wl, c = e / ((long long)chil * wl);
+        h.ST2[(m + (long long)wr * c) * h.pT2 + a] = v[u];
+      }
     }
   } else {
     WApplyGeom g;

@@ -64,6 +64,7 @@ struct DevParams {
   int mixed;  // H_eff and environment contractions in complex FP32 on the tensor cores
   int tc;     // mixed H_eff products on tcgen05 (the tensor-core kernel, engine_tc.cu)
   const CUtensorMap* tmaps;  // [slots][4]: SL, Sx, ST2, SR of each slot
+  const unsigned char* tune;  // [TUNE_ENTRIES] autotuned product form per bucket (null: tcgen05)
   int tdvp_mode;  // YAQS_TDVP_2SITE / _1SITE / _DYNAMIC
   double dt, thr;
   KrylovCfg kc;
@@ -434,7 +435,24 @@ static __device__ void update_right(Ctx& c, const DState& s, int i) { update_rig
 // ---------------------------------------------------------------------------
 // Two-site TDVP (Algorithms.jl:580-760)
 // ---------------------------------------------------------------------------
-static __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, const WMat& W, double dt) {
+// Autotuned choice of the mixed H_eff products per shape bucket
+// (tune_index): 0 = tcgen05 (128 x 64 tiles, TMA-fed), 1 = mma.sync 3xTF32
+// (64 x 64 tiles).  Buckets: ceil(log2 chi_l), ceil(log2 chi_r) in 0..7 and
+// D in {1, 2, 4}.
+#define TUNE_ENTRIES (8 * 8 * 3)
+__host__ __device__ __forceinline__ int tune_log2(int v) {
+  int e = 0;
+  while ((1 << e) < v && e < 7) ++e;
+  return e;
+}
+__host__ __device__ __forceinline__ int tune_index(int chil, int D, int chir) {
+  return (tune_log2(chil) * 8 + tune_log2(chir)) * 3 + (D == 1 ? 0 : D == 2 ? 1 : 2);
+}
+
+// The H_eff operator of a Krylov solve on (l, D, r) between environments bl
+// and br, with its operands staged for the product form chosen for the
+// bucket.  CTA-collective.
+static __device__ HeffOp make_heff(Ctx& c, int l, int D, int r, int bl, int br, const WMat& W) {
   HeffOp h;
   h.L = envL(c, bl);
   h.R = envR(c, br);
@@ -447,7 +465,8 @@ static __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int 
   h.T1 = c.ws + c.P.lay.T1;
   h.T2 = c.ws + c.P.lay.T2;
   h.mixed = c.P.mixed;
-  if (c.P.tc) {  // environments staged once per Krylov solve as the TMA operands
+  const bool tc = c.P.tc && !(c.P.tune && c.P.tune[tune_index(l, D, r)] == 1);
+  if (tc) {  // environments staged once per Krylov solve as the TMA operands
     const WsLayout& y = c.P.lay;
     h.tc = 1;
     h.maps = c.P.tmaps + 4 * c.slot;
@@ -480,6 +499,11 @@ static __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int 
     h.T1f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T1f);
     h.T2f = reinterpret_cast<cflt*>(c.ws + c.P.lay.T2f);
   }
+  return h;
+}
+
+static __device__ void evolve(Ctx& c, cplx* x, int l, int D, int r, int bl, int br, const WMat& W, double dt) {
+  const HeffOp h = make_heff(c, l, D, r, bl, br, W);
   int mv = dev_expm_krylov(h, x, dt, c.P.kc, c.ws + c.P.lay.Q, c.P.kry_n, c.sm.e);
   if (ltid() == 0) {
     c.cnt[0] += mv;
