@@ -300,6 +300,9 @@ def cpu_sample_digital(L, depth):
     return 2 * cores * depth / dt, cores, f"{2 * cores} trajectories x {depth} layers of the same circuit, {dt:.1f} s"
 
 
+START_DESC = {"sat": "saturated start", "neel": "Neel start"}
+
+
 def analog_config(args, L, chi, nt, ws):
     """The analog workload's config object (shared by both bench arms)."""
     return {"workload": f"analog TJM, L={L} Heisenberg XXX h=0.3, dephasing gamma=0.05, dt=0.05, "
@@ -611,6 +614,16 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
+def ensemble_gap_in_se(a, b):
+    """max over (site, time) of |mean(a) - mean(b)| / SE(b), SE = std/sqrt(n),
+    over the entries whose trajectories spread (SE > 1e-12); None if none do."""
+    se = b.std(axis=0, ddof=1) / np.sqrt(b.shape[0]) if b.shape[0] > 1 else np.zeros(b.shape[1:])
+    live = se > 1e-12
+    if not live.any():
+        return None
+    return float((np.abs(a.mean(0) - b.mean(0))[live] / se[live]).max())
+
+
 def timed_session(args, ctx, dist, local, problem, prec, rank, nt, n_steps):
     """One resident run: W untimed time indices, then n_steps timed ones in one
     launch (CUDA events on the launching stream, barrier + synchronize on both
@@ -682,8 +695,15 @@ def run_ours(args):
                "trajectories_above_1e-5": int((per_traj > 1e-5).sum()),
                "jumps": {"mixed": int(main["res"].stats["jumps"]), "plain": int(pl["res"].stats["jumps"])},
                "z_ensemble_mean_max_abs": float(np.abs(a[:, :L].mean(0) - b[:, :L].mean(0)).max()),
+               # the ensemble means against the plain form's standard error of
+               # the mean at every (site, time index) with a nonzero spread
+               "z_ensemble_mean_max_in_se": ensemble_gap_in_se(a[:, :L], b[:, :L]),
+               # largest per-trajectory <Z_i> difference at chosen time indices:
+               # how the separation grows along the run
+               "z_max_abs_by_time_index": {str(t): float(dz[:, :, t].max())
+                                           for t in sorted({1, 2, 5, 10, 20, 50, ncol - 1}) if t < ncol},
                "trajectories_compared": nt, "time_indices_compared": ncol,
-               "run": f"every <Z_i> and S_half at {ncol} recorded time indices (saturated start, {args.warmup} "
+               "run": f"every <Z_i> and S_half at {ncol} recorded time indices ({START_DESC[args.start]}, {args.warmup} "
                       f"warm-up and {Kp} timed indices) of the two forms on the same Philox draws"}
     # end to end: the public C-ABI call on host buffers (marshalling, uploads,
     # allocation, a complete run of K time indices from t = 0 whose first

@@ -353,3 +353,28 @@ def test_ising_circuit_bitflip_run(oracle):
                                **api._methods(c, None, None))
     ref, _, _ = oracle.digital_run(d)
     assert np.abs(res.trajectories - ref).max() <= 1e-10
+
+
+@pytest.mark.parametrize("method", ["tebd", "tdvp"])
+def test_program_sizes_agree(method, monkeypatch):
+    """Direct digital runs use the 128-thread program kernel; the 256-thread
+    kernel (YAQS_DIGITAL_THREADS=256) gives the same trajectories to rounding,
+    the same bond dimensions and the same jumps, on a noisy circuit with
+    long-range gates (TEBD SWAP chains or TDVP windows)."""
+    L = 9
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.03} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_z", "lowering")], L)
+    obs = _zs(L) + [api.Observable("S", None, 4, kind="entropy")]
+    cfg = api.TimeEvolutionConfig(obs, 1.0, dt=1.0, num_traj=40, max_bond_dim=16, truncation_threshold=1e-9)
+    c = _tdvp_circuit(L, 3, seed=11) if method == "tdvp" else _brickwork(L, 4, seed=11)
+
+    def run():
+        d = api.CircuitDescriptors(api.MPS(L), c, cfg, nm, seed=21, local_method=method, long_range_method=method)
+        return api.run_circuit_descriptors(d)
+
+    small = run()
+    monkeypatch.setenv("YAQS_DIGITAL_THREADS", "256")
+    big = run()
+    assert np.abs(small.trajectories - big.trajectories).max() <= 1e-10
+    assert np.array_equal(small.max_bond, big.max_bond)
+    assert small.stats["jumps"] == big.stats["jumps"] > 0

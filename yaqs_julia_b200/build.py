@@ -18,9 +18,10 @@ def sources():
         os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include")))]
 
 
-# translation units: engine.cu (every kernel without tcgen05 code) and
-# engine_tc.cu (the tensor-core trajectory kernel), compiled in parallel
-UNITS = ["engine.cu", "engine_tc.cu"]
+# translation units, compiled in parallel: engine.cu (every kernel without
+# tcgen05 code), engine_tc.cu (the tensor-core trajectory kernel) and
+# engine_dg.cu (the digital program in 128-thread CTAs)
+UNITS = ["engine.cu", "engine_tc.cu", "engine_dg.cu"]
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

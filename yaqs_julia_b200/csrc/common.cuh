@@ -7,7 +7,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Threads of one trajectory program: 256, or 128 in the small-program
+// digital kernel (engine_dg.cu defines NT before including this header).
+#ifndef NT
 #define NT 256
+#endif
 #define NW (NT / 32)
 
 typedef double2 cplx;

@@ -27,6 +27,7 @@
 #include "tcgemm.cuh"
 
 #include "program.cuh"
+#include "engine_dg.h"
 #include "engine_tc.h"
 
 __global__ void __launch_bounds__(NT, 2) tjm_step_kernel(const DevParams P, int first, int count) {
@@ -616,6 +617,7 @@ struct yaqs_run {
   DevMem dm;
   DevParams P;
   int digital = 0;  // 0 analog TJM program, 1 digital (circuit) program
+  int dg = 0;       // digital run on the 128-thread kernel (engine_dg.cu)
   DigParams D;
   int slots = 0;
   size_t smem = 0;
@@ -636,6 +638,7 @@ struct yaqs_run {
       unsigned long long* z = nullptr;
       cudaMemcpyToSymbol(g_prof, &z, sizeof(z));
       tc_set_prof(nullptr);
+      dg_set_prof(nullptr);
     }
     if (stream) cudaStreamSynchronize(stream);
     if (e0) cudaEventDestroy(e0);
@@ -759,6 +762,7 @@ static int setup_run(yaqs_ctx* ctx, yaqs_run* run, const std::vector<int>& cap, 
     CUDA_TRY(ctx, cudaMemset(run->d_prof, 0, (size_t)slots * PROF_N * sizeof(unsigned long long)));
     CUDA_TRY(ctx, cudaMemcpyToSymbol(g_prof, &run->d_prof, sizeof(run->d_prof)));
     CUDA_TRY(ctx, tc_set_prof(run->d_prof));  // the tensor-core kernel's translation unit
+    CUDA_TRY(ctx, dg_set_prof(run->d_prof));  // the 128-thread digital kernel's
   }
   CUDA_TRY(ctx, cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking));
   CUDA_TRY(ctx, cudaEventCreate(&run->e0));
@@ -1299,7 +1303,9 @@ int yaqs_analog_advance(yaqs_run* run, int32_t n, double* device_ms) {
     const int first = (int)run->next, cnt = std::min(n, per_launch);
     run->next += cnt;
     n -= cnt;
-    if (run->digital)
+    if (run->digital && run->dg)
+      CUDA_TRY(ctx, dg_kernel_launch(run->slots, run->smem, run->stream, run->P, run->D, first, cnt));
+    else if (run->digital)
       digital_step_kernel<<<run->slots, NT, run->smem, run->stream>>>(run->P, run->D, first, cnt);
     else
       if (run->P.tc)
@@ -1500,10 +1506,19 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   const int num_traj = cfg->num_traj;
   const int ncols = C.n_samples;
   const int n_layers = (int)C.layers.size();
-  const size_t smem = cta_smem_bytes();
-  CUDA_TRY(ctx, cudaFuncSetAttribute(digital_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // direct runs take the 128-thread program kernel (three CTAs per SM) unless
+  // YAQS_DIGITAL_THREADS=256 asks for the 256-thread one; a server's pool
+  // runs digital units in its own kernel
+  const char* dg_env = getenv("YAQS_DIGITAL_THREADS");
+  const bool use_dg = !pool && !(dg_env && atoi(dg_env) == 256);
+  size_t smem = cta_smem_bytes();
   int per_sm = 0;
-  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, digital_step_kernel, NT, smem));
+  if (use_dg) {
+    CUDA_TRY(ctx, dg_kernel_prepare(&per_sm, &smem));
+  } else {
+    CUDA_TRY(ctx, cudaFuncSetAttribute(digital_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, digital_step_kernel, NT, smem));
+  }
   if (per_sm < 1) return set_err(ctx, YAQS_E_CUDA, "kernel does not fit on an SM");
   if (pool && (lay.total > pool->ws_stride || lay.itotal > pool->wsi_stride))
     return set_err(ctx, YAQS_E_UNSUPPORTED, "the request's workspace exceeds the server's slot shape");
@@ -1524,6 +1539,7 @@ int digital_begin(yaqs_ctx* ctx, const yaqs_mps_desc* psi0, const yaqs_gate_desc
   std::unique_ptr<yaqs_run> guard(run);
   run->ctx = ctx;
   run->digital = 1;
+  run->dg = use_dg ? 1 : 0;
   DevParams& P = run->P;
   memset(&P, 0, sizeof(P));
   P.L = L;

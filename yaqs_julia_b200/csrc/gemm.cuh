@@ -7,17 +7,21 @@
 // Every tensor contraction of the TDVP path (Algorithms.jl:199-226) is
 // written as one such GEMM over the reference's column-major layouts.
 //
-// Tiling: 64x64 output tiles, 16-deep K slices staged in shared memory by
-// cp.async (double buffered, zero-filled outside the matrix), each of the
-// 256 threads owning a 4x4 register tile with rows tx+16i and columns
-// ty+16j (so stores along m are coalesced).  Conjugation is applied when a
-// slice is read from shared memory.
+// Tiling: 64 x GBN_EFF output tiles (64 x 64 for a 256-thread program, 64 x
+// 32 for a 128-thread one), 16-deep K slices staged in shared memory by
+// cp.async (double buffered, zero-filled outside the matrix), each warp
+// owning a 32 x 16 sub-tile.  Conjugation is applied when a slice is read
+// from shared memory.
 #pragma once
 #include "common.cuh"
 
 #define GBM 64
 #define GBN 64
 #define GBK 16
+// Output columns of one CTA tile: the warps form a 2 x NW/2 grid of 32 x 16
+// sub-tiles.
+#define GBN_EFF (16 * (NW / 2))
+static_assert(NW % 2 == 0 && GBN_EFF <= GBN, "the GEMM needs an even warp count of at most 8");
 
 struct GemmSmem {
   cplx As[2][GBK][GBM + 1];
@@ -77,8 +81,8 @@ static __device__ __forceinline__ void dmma884(double& d0, double& d1, double a,
 }
 
 // CTA-collective.  Ends with a cta_sync() so C is visible to all.
-// Complex products run on the FP64 tensor cores (mma.sync m8n8k4): each of
-// the 8 warps owns a 32x16 complex sub-tile of the 64x64 CTA tile as 4x2
+// Complex products run on the FP64 tensor cores (mma.sync m8n8k4): each
+// warp owns a 32x16 complex sub-tile of the 64 x GBN_EFF CTA tile as 4x2
 // blocks of 8x8, each block accumulating re and im with four real MMAs.
 // Conjugation is a template parameter (a sign flip of the imaginary
 // fragment).
@@ -87,13 +91,13 @@ static __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
   ProfScope prof_scope_(PF_GEMM);
   const int tid = ltid();
   const int lane = tid & 31, wid = tid >> 5;
-  const int wm = wid & 1, wn = wid >> 1;  // 2 x 4 warps
+  const int wm = wid & 1, wn = wid >> 1;  // 2 x NW/2 warps
   const int gq = lane >> 2, tq = lane & 3;
   const bool a_m_fast = (g.am == 1) || (g.ak != 1);
   const bool b_n_fast = (g.bn == 1) || (g.bk != 1);
   const int nk = (g.K + BK - 1) / BK;
   for (int tm = 0; tm < g.M; tm += GBM) {
-    for (int tn = 0; tn < g.N; tn += GBN) {
+    for (int tn = 0; tn < g.N; tn += GBN_EFF) {
       double cr[4][2][2], ci[4][2][2];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -104,10 +108,11 @@ static __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
         }
       auto issue = [&](int kc, int buf) {
         const int k0 = kc * BK;
+        // A: GBM x BK values, B: BK x GBN_EFF values (equal counts with 8 warps)
 #pragma unroll
         for (int e = 0; e < GBM * BK / NT; ++e) {
           const int idx = tid + NT * e;
-          int mi, ki, ni, kj;
+          int mi, ki;
           if (a_m_fast) {
             mi = idx & (GBM - 1);
             ki = idx / GBM;
@@ -115,17 +120,22 @@ static __device__ __noinline__ void cta_gemm_t(const GemmArgs g, GemmSmem& sm) {
             ki = idx & (BK - 1);
             mi = idx / BK;
           }
-          if (b_n_fast) {
-            ni = idx & (GBN - 1);
-            kj = idx / GBN;
-          } else {
-            kj = idx & (BK - 1);
-            ni = idx / BK;
-          }
-          const int mm = tm + mi, ka = k0 + ki, nn = tn + ni, kb = k0 + kj;
-          const bool va = mm < g.M && ka < g.K, vb = nn < g.N && kb < g.K;
+          const int mm = tm + mi, ka = k0 + ki;
+          const bool va = mm < g.M && ka < g.K;
           cp_async16(&sm.As[buf][ki][mi], va ? g.A + (long long)mm * g.am + (long long)ka * g.ak : g.A, va);
-          cp_async16(&sm.Bs[buf][kj][ni], vb ? g.B + (long long)kb * g.bk + (long long)nn * g.bn : g.B, vb);
+          if (e < GBN_EFF * BK / NT) {
+            int ni, kj;
+            if (b_n_fast) {
+              ni = idx & (GBN_EFF - 1);
+              kj = idx / GBN_EFF;
+            } else {
+              kj = idx & (BK - 1);
+              ni = idx / BK;
+            }
+            const int nn = tn + ni, kb = k0 + kj;
+            const bool vb = nn < g.N && kb < g.K;
+            cp_async16(&sm.Bs[buf][kj][ni], vb ? g.B + (long long)kb * g.bk + (long long)nn * g.bn : g.B, vb);
+          }
         }
         cp_async_commit();
       };
