@@ -103,6 +103,11 @@ struct RedScratch {
 };
 
 // CTA-collective sum of NV values per thread; result broadcast to every thread.
+// The warp partials are added in warp order w = 0 .. NW-1 either way.  For up
+// to four values every thread adds them itself (two barriers: the partials
+// are written, then read before anyone may write them again); for more, NV
+// threads add one value each and publish it (three barriers, fewer shared
+// loads).
 template <int NV>
 static __device__ __forceinline__ void block_sum_n(double (&x)[NV], RedScratch& rs) {
   const int lane = ltid() & 31, wid = ltid() >> 5;
@@ -113,6 +118,17 @@ static __device__ __forceinline__ void block_sum_n(double (&x)[NV], RedScratch& 
     for (int k = 0; k < NV; ++k) rs.v[wid * NV + k] = x[k];
   }
   cta_sync();
+  if (NV <= 4) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) s += rs.v[w * NV + k];
+      x[k] = s;
+    }
+    cta_sync();
+    return;
+  }
   if (ltid() < NV) {
     double s = 0.0;
     for (int w = 0; w < NW; ++w) s += rs.v[w * NV + ltid()];
@@ -135,15 +151,11 @@ static __device__ __forceinline__ double block_max(double v, RedScratch& rs) {
   v = warp_max(v);
   if (lane == 0) rs.v[wid] = v;
   cta_sync();
-  if (ltid() == 0) {
-    double s = rs.v[0];
-    for (int w = 1; w < NW; ++w) s = fmax(s, rs.v[w]);
-    rs.v[NW * 16] = s;
-  }
+  double s = rs.v[0];
+#pragma unroll
+  for (int w = 1; w < NW; ++w) s = fmax(s, rs.v[w]);
   cta_sync();
-  v = rs.v[NW * 16];
-  cta_sync();
-  return v;
+  return s;
 }
 
 // CTA-collective copy / fill helpers.

@@ -42,9 +42,10 @@ static __device__ __noinline__ void dev_qr_factor(cplx* H, int m, int n, LinalgS
     double s = 0.0;
     for (int i = j + 1 + tid; i < m; i += NT) s += cabs2(col[i]);
     const double xn2 = block_sum(s, rs);
+    // col[j] is rewritten (by thread 0) only after the barrier that follows
+    // the scaling below, so no barrier is needed between this read and it
     const cplx alpha = col[j];
     const double full = sqrt(cabs2(alpha) + xn2);
-    cta_sync();
     if (full <= null_abs || (xn2 == 0.0 && alpha.y == 0.0)) {
       for (int i = j + 1 + tid; i < m; i += NT) col[i] = make_double2(0.0, 0.0);
       if (tid == 0) ls.tau[j] = make_double2(0.0, 0.0);
