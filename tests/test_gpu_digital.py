@@ -378,3 +378,21 @@ def test_program_sizes_agree(method, monkeypatch):
     assert np.abs(small.trajectories - big.trajectories).max() <= 1e-10
     assert np.array_equal(small.max_bond, big.max_bond)
     assert small.stats["jumps"] == big.stats["jumps"] > 0
+
+
+def test_local_observables_by_transfer_matrices(oracle):
+    """After a layer, 1-site observables on a tight chain are contracted with
+    transfer matrices and the centre stays put, where the oracle moves the
+    centre across the chain as the reference does; an entropy observable
+    then moves the device's centre to its site only.  Both runs give the
+    oracle's <Z_i> on the same draws, with the same jumps and bond
+    dimensions, under Pauli and relaxation noise with long-range gates."""
+    L = 10
+    nm = api.NoiseModel([{"name": n, "sites": [i], "strength": 0.04} for i in range(1, L + 1)
+                         for n in ("pauli_x", "pauli_z", "lowering")], L)
+    c = _brickwork(L, 5, seed=17)
+    z, _ = _compare(oracle, L, c, _zs(L), nm=nm, num_traj=24, chi=16)
+    zs, _ = _compare(oracle, L, c, _zs(L) + [api.Observable("S", None, 5, kind="entropy")], nm=nm, num_traj=24,
+                     chi=16)
+    assert np.abs(z.trajectories - zs.trajectories[:, :L]).max() <= 1e-10
+    assert np.array_equal(z.max_bond, zs.max_bond) and z.stats["jumps"] == zs.stats["jumps"] > 0

@@ -1041,11 +1041,116 @@ static __device__ void stochastic_process(Ctx& c, const DState& s, double dt, in
 // ---------------------------------------------------------------------------
 // Observables
 // ---------------------------------------------------------------------------
+// Re sum_{a,p,q,b} conj(A[a,p,b]) op[p,q] T[a,q,b] for two (l, 2, r) tensors.
+// CTA-collective.
+static __device__ double env_expect(Ctx& c, const cplx* A, const cplx* T, int l, int r, const cplx* op) {
+  double sacc = 0.0;
+  for (int e = ltid(); e < l * r; e += NT) {
+    const long long a = e % l, b = e / l;
+    const cplx a0 = A[a + (long long)l * (2 * b)], a1 = A[a + (long long)l * (1 + 2 * b)];
+    const cplx t0 = T[a + (long long)l * (2 * b)], t1 = T[a + (long long)l * (1 + 2 * b)];
+    cplx u0 = make_double2(0.0, 0.0), u1 = make_double2(0.0, 0.0);
+    cfma(u0, op[0], t0);
+    cfma(u0, op[2], t1);
+    cfma(u1, op[1], t0);
+    cfma(u1, op[3], t1);
+    sacc += a0.x * u0.x + a0.y * u0.y + a1.x * u1.x + a1.y * u1.y;
+  }
+  return block_sum(sacc, c.sm.e.r);
+}
+
+// The 1-site observables of a state whose bonds are all tight.  The
+// reference (expect -> local_expect, MPS.jl:608-651) moves the orthogonality
+// centre to each observable's site and contracts the centre tensor; on a
+// tight chain those QR / LQ steps change no shape and are pure gauge moves.
+// Here the state is left as it is and each <O_i> is contracted with transfer
+// matrices, which holds in any gauge:
+//   R_L = 1,  R_b = sum_p A_b^p R_{b+1} A_b^p^dag          (right to left)
+//   E_0 = 1,  <O_i> = sum E_i[a,a'] A_i[a,q,r] O[p,q] conj(A_i[a',p,r']) R_{i+1}[r,r'],
+//   E_{i+1} = sum_p A_i^p^T E_i conj(A_i^p)                (left to right)
+// six small GEMMs a site instead of a QR step a site in each direction.  The
+// right environments go in the slot's environment arena (free between
+// sweeps) or else in the SVD scratch (B, X, Yo, Zo, adjacent); returns false,
+// having written nothing, when no observable is 1-site, the chain is not
+// tight, or neither region holds them.  CTA-collective.
+static __device__ bool local_by_envs(Ctx& c, const DState& s, int col) {
+  const DevParams& P = c.P;
+  const int L = P.L;
+  bool any1 = false;
+  for (int k = 0; k < P.nobs; ++k) any1 |= P.obs[k].kind == OBS_LOCAL1;
+  if (!any1 || !chain_tight(c, s)) return false;
+  long long need = 0;
+  for (int b = 1; b <= L; ++b) need += (long long)s.chi[b] * s.chi[b];
+  cplx* Rs;
+  if (P.lay.ER - P.lay.EL >= need)
+    Rs = c.ws + P.lay.EL;  // R_b at offset sum_{b' > b} chi_b'^2
+  else if (P.lay.Zo + (P.lay.Zo - P.lay.Yo) - P.lay.B >= need)
+    Rs = c.ws + P.lay.B;
+  else
+    return false;
+  cplx* E0 = c.ws + P.lay.tA;
+  cplx* E1 = c.ws + P.lay.tB;
+  cplx* T1 = c.ws + P.lay.tC;
+  cplx* T3 = c.ws + P.lay.th;
+  GemmSmem& gs = c.sm.e.u.gw.g;
+  cta_sync();
+  if (ltid() == 0) {
+    Rs[0] = make_double2(1.0, 0.0);  // R_L (chi_L = 1)
+    E0[0] = make_double2(1.0, 0.0);  // E_0 (chi_0 = 1)
+  }
+  cta_sync();
+  long long off = 0;  // offset of R_{b+1}
+  for (int b = L - 1; b >= 1; --b) {
+    const int l = s.chi[b], r = s.chi[b + 1];
+    const cplx* A = site_ptr(c, s, b);
+    // X[(a,p), r'] = sum_r A[a,p,r] R_{b+1}[r, r']
+    cta_gemm(gemm_args(2 * l, r, r, A, 1, 2 * l, Rs + off, 1, r, T1, 1, 2 * l), gs);
+    off += (long long)r * r;
+    // R_b[x, y] = sum_{p,r'} X[x,p,r'] conj(A[y,p,r'])
+    cta_gemm(gemm_args(l, l, 2 * r, T1, 1, l, A, l, 1, Rs + off, 1, l, false, true), gs);
+  }
+  double* vals = reinterpret_cast<double*>(c.ws + P.lay.dbl) + SVD_MAX_COLS;  // one value per observable
+  off = need;  // R_{i+1} at off - chi_{i+1}^2
+  for (int i = 0; i < L; ++i) {
+    const int l = s.chi[i], r = s.chi[i + 1];
+    const cplx* A = site_ptr(c, s, i);
+    off -= (long long)r * r;
+    bool here = false;
+    for (int k = 0; k < P.nobs; ++k) here |= P.obs[k].kind == OBS_LOCAL1 && P.obs[k].s0 == i;
+    if (here) {
+      // T1[a,q,r'] = sum_r A[a,q,r] R_{i+1}[r,r'];  T3[a',q,r'] = sum_a E_i[a,a'] T1[a,q,r']
+      cta_gemm(gemm_args(2 * l, r, r, A, 1, 2 * l, Rs + off, 1, r, T1, 1, 2 * l), gs);
+      cta_gemm(gemm_args(l, 2 * r, l, E0, l, 1, T1, 1, l, T3, 1, l), gs);
+      for (int k = 0; k < P.nobs; ++k) {
+        if (P.obs[k].kind != OBS_LOCAL1 || P.obs[k].s0 != i) continue;
+        const double v = env_expect(c, A, T3, l, r, P.obs[k].mat);
+        if (ltid() == 0) vals[k] = v;
+      }
+    }
+    if (i + 1 < L) {
+      // V[a',p,r] = sum_a E_i[a,a'] A[a,p,r];  E_{i+1}[r,r'] = sum_{a',p} V[a',p,r] conj(A[a',p,r'])
+      cta_gemm(gemm_args(l, 2 * r, l, E0, l, 1, A, 1, l, T1, 1, l), gs);
+      cta_gemm(gemm_args(r, r, 2 * l, T1, 2 * l, 1, A, 1, 2 * l, E1, 1, r, false, true), gs);
+      cplx* t = E0;
+      E0 = E1;
+      E1 = t;
+    }
+  }
+  cta_sync();
+  if (ltid() == 0)
+    for (int k = 0; k < P.nobs; ++k)
+      if (P.obs[k].kind == OBS_LOCAL1) P.traj_out[((long long)c.traj * P.nobs + k) * P.ncols + col] = vals[k];
+  cta_sync();
+  return true;
+}
+
 static __device__ void evaluate(Ctx& c, const DState& s, int col) {
   ProfScope prof_scope_(PF_EVAL);
   const int ncols = c.P.ncols;
+  const bool local_done = local_by_envs(c, s, col);
   for (int k = 0; k < c.P.nobs && !c.sm.fail; ++k) {
     const DevObs& o = c.P.obs[k];
+    if (local_done && o.kind == OBS_LOCAL1) continue;
     double val = 0.0;
     if (o.kind == OBS_LOCAL1) {
       shift_oc(c, s, o.s0);
