@@ -100,3 +100,19 @@ def test_two_digital_replicas_reproduce_one_run(oracle, tmp_path):
     parts = [np.load(tmp_path / f"dig{r}.npy") for r in range(world)]
     whole, _, st = oracle.digital_run(_circuit_problem(world * nt, 0))
     assert np.array_equal(np.concatenate(parts, axis=0), whole) and st["jumps"] > 0
+
+
+def test_bench_ensemble_gap_in_standard_errors():
+    """The mixed line's ensemble check: |mean(a) - mean(b)| / SE(b) over the
+    (site, time) entries whose trajectories spread; None when none spread."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    rng = np.random.default_rng(5)
+    b = rng.normal(size=(400, 3, 4))
+    se = b.std(axis=0, ddof=1) / np.sqrt(400)
+    a = b + 2.0 * se.max()
+    assert abs(bench.ensemble_gap_in_se(a, b) - 2.0 * se.max() / se.min()) < 1e-9
+    assert bench.ensemble_gap_in_se(b, b) == 0.0
+    flat = np.ones((50, 2, 3))
+    assert bench.ensemble_gap_in_se(flat + 1.0, flat) is None
