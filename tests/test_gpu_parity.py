@@ -152,6 +152,28 @@ def test_heisenberg_neel_dephasing_entropy_and_two_site(oracle):
     _compare(oracle, api.MPS(L, state="Neel"), H, cfg, nm, seed=3)
 
 
+def test_several_observables_per_site_and_out_of_order(oracle):
+    """X, Y and Z on every site, listed out of site order, with an entropy
+    observable between them: the device contracts the 1-site ones with
+    transfer matrices (several per site from one environment pair) and moves
+    the centre only for the entropy; every value equals the oracle's, which
+    sweeps the centre to each observable in list order."""
+    L = 7
+    H = api.init_general_hamiltonian(L, 1, 0.6, 0.8, 0.1, 0, 0.2)
+    Y = np.array([[0, -1j], [1j, 0]])
+    obs = []
+    for i in [4, 1, 7, 2, 6, 3, 5]:
+        obs += [api.Observable(f"X{i}", api.X, i), api.Observable(f"Y{i}", Y, i)]
+        if i == 2:
+            obs.append(api.Observable("S3", None, 3, kind="entropy"))
+        obs.append(api.Observable(f"Z{i}", api.Z, i))
+    cfg = api.TimeEvolutionConfig(obs, 0.6, dt=0.05, num_traj=6, max_bond_dim=12)
+    nm = api.NoiseModel([{"name": "lowering", "sites": [i], "strength": 0.1} for i in range(1, L + 1)] +
+                        [{"name": "pauli_x", "sites": [i], "strength": 0.05} for i in range(1, L + 1)], L)
+    got, _ = _compare(oracle, api.MPS(L, state="x+"), H, cfg, nm, seed=19)
+    assert got.stats["jumps"] > 0
+
+
 def test_two_site_noise_processes(oracle):
     L = 5
     H = api.init_ising(L, 1.0, 0.7)
