@@ -393,3 +393,40 @@ def test_truncate_refuses_non_finite_tensors():
     m.tensors[2][0, 0, 0] = np.nan
     with pytest.raises(ValueError, match="non-finite"):
         T.truncate(m, max_bond_dim=2)
+
+
+def _transfer_matrix_expectations(tensors, ops):
+    """<O_i> = E_i (A_i^* O_i A_i) R_{i+1} with E_0 = R_L = 1 and the one-sided
+    transfer matrices in between, for any gauge (the contraction the device
+    uses for 1-site observables on tight chains)."""
+    L = len(tensors)
+    R = [None] * (L + 1)
+    R[L] = np.ones((1, 1), complex)
+    for b in range(L - 1, -1, -1):
+        A = tensors[b]
+        R[b] = np.einsum("xpr,rs,yps->xy", A, R[b + 1], A.conj())
+    E = np.ones((1, 1), complex)
+    out = []
+    for i, A in enumerate(tensors):
+        out.append(np.einsum("ab,aqr,pq,bps,rs->", E, A, ops[i], A.conj(), R[i + 1]).real)
+        E = np.einsum("ab,apr,bps->rs", E, A, A.conj())
+    return np.array(out)
+
+
+def test_transfer_matrix_observables_equal_the_centre_sweep():
+    """On a normalised state in mixed canonical form, the 1-site expectations
+    contracted with transfer matrices (centre left in place) equal the
+    reference's evaluation, which moves the orthogonality centre to every
+    site (MPS.jl:608-676), and the thin QR / LQ steps of that sweep change
+    no bond dimension of a tight chain."""
+    L = 9
+    m = api.random_mps(L, 8, seed=21)
+    T.normalize(m)
+    T.shift_orthogonality_center(m, 4)
+    before = [t.copy() for t in m.tensors]
+    dims = [t.shape[2] for t in m.tensors]
+    ops = [api.Z if i % 3 == 0 else (api.X if i % 3 == 1 else np.array([[0, -1j], [1j, 0]])) for i in range(L)]
+    got = _transfer_matrix_expectations(before, ops)
+    ref = T.evaluate_all_local_expectations(m, ops).real
+    assert np.abs(got - ref).max() < 1e-12
+    assert [t.shape[2] for t in m.tensors] == dims
